@@ -1,0 +1,196 @@
+/*
+ * tandem_b200 C ABI: the device (sm_100a) matrix-free DG operator behind tandem's MatShell.
+ *
+ * Every entry point is plain C: pointers, sizes and an opaque handle.  Device arrays are CUDA
+ * device pointers; `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream).
+ * All device work is enqueued on `stream` and returns without synchronising unless stated.
+ * Return value: 0 on success, a negative TDG_E* code otherwise; tdg_last_error() gives the text.
+ * No exception crosses this boundary.
+ *
+ * Vector layout (tandem's BlockVector over a PETSc Vec, app/common/PetscVector.h:48-56):
+ * one block of bs = Nbf * Q values per element, basis index fastest, then component:
+ * x[e * bs + k + Nbf * p].  Multi-RHS vectors stack nrhs such vectors with leading dimension ld
+ * (ld >= E * bs): x[r * ld + e * bs + k + Nbf * p].
+ */
+#ifndef TANDEM_B200_H
+#define TANDEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes. */
+#define TDG_OK 0
+#define TDG_E_INVALID (-1)     /* invalid argument */
+#define TDG_E_CUDA (-2)        /* CUDA runtime error */
+#define TDG_E_NOT_SPD (-3)     /* a block-Jacobi diagonal block is not positive definite */
+#define TDG_E_DIVERGED (-4)    /* Krylov solve did not converge / produced NaN */
+#define TDG_E_STATE (-5)       /* call out of order (e.g. apply before set_material) */
+#define TDG_E_TIMEOUT (-6)     /* a bounded device wait ran out */
+#define TDG_E_NOMEM (-7)       /* device allocation failed */
+
+/* Local operator kind: tandem's Poisson (app/localoperator/Poisson.h:31) and
+ * Elasticity (app/localoperator/Elasticity.h:31). */
+#define TDG_POISSON 0
+#define TDG_ELASTICITY 1
+
+/* Facet boundary conditions, values of tandem's enum class BC (src/form/BC.h:6). */
+#define TDG_BC_NONE 0
+#define TDG_BC_NATURAL 1
+#define TDG_BC_FAULT 3
+#define TDG_BC_DIRICHLET 5
+
+/* Arithmetic of an apply / preconditioner / solve. */
+#define TDG_FP64 0
+#define TDG_FP32 1
+
+typedef struct tdg_op tdg_op;
+
+/*
+ * Mesh and topology as tandem's DG layer holds them:
+ *  - geo_nodes: the Curvilinear geometry nodes, geo_degree warp & blend nodes per element
+ *    (Curvilinear::vertices storage, src/geometry/Curvilinear.cpp:33-112), [E][Ngeo][dim];
+ *  - facet_up / facet_local_no / facet_bc: FacetInfo::up, ::localNo, ::bc per local facet
+ *    (src/form/FacetInfo.h:17-23, filled in src/form/DGOperatorTopo.cpp:46-85); on a boundary
+ *    facet up[1] == up[0] and localNo[1] == localNo[0].
+ * Element vertices must be numbered by sorted global vertex id (src/mesh/Simplex.h:15-36) so that
+ * the facet quadrature points of both sides coincide.
+ */
+typedef struct {
+    int32_t dim;            /* 2 or 3 */
+    int32_t degree;         /* polynomial degree N of the DG space */
+    int32_t geo_degree;     /* degree of the geometry map (tandem: Curvilinear(mesh, .., N)) */
+    int32_t reserved;
+    int64_t num_elements;
+    int64_t num_facets;
+    const double* geo_nodes;      /* [E][binom(geo_degree+dim,dim)][dim] */
+    const int64_t* facet_up;      /* [F][2] */
+    const int32_t* facet_local_no;/* [F][2] */
+    const int32_t* facet_bc;      /* [F] */
+} tdg_mesh_desc;
+
+/*
+ * Quadrature rules on the unit simplex (tandem's DGCurvilinearCommon::volRule / fctRule,
+ * src/form/DGCurvilinearCommon.cpp:13-26).  fct_points has dim-1 coordinates per point.
+ */
+typedef struct {
+    int32_t num_vol_points;
+    int32_t num_fct_points;
+    const double* vol_points;   /* [Nq][dim] */
+    const double* vol_weights;  /* [Nq] */
+    const double* fct_points;   /* [nq][dim-1] */
+    const double* fct_weights;  /* [nq] */
+} tdg_quadrature;
+
+/* --- construction (replaces DGOperator's constructor and the LocalOperator prepare_* calls,
+ *     src/form/DGOperator.h:54-105) ------------------------------------------------------ */
+
+/* Builds topology and geometry (Jacobians, normals, areas, volumes) on the host. */
+int tdg_create(const tdg_mesh_desc* mesh, const tdg_quadrature* quad, int kind, tdg_op** out);
+void tdg_destroy(tdg_op* op);
+const char* tdg_last_error(void);
+
+/* Sizes: block size bs, Nbf, components Q, Nq, nq, E, F. */
+int tdg_sizes(const tdg_op* op, int64_t out[8]);
+
+/* Physical coordinates of the volume [E][Nq][dim] and facet [F][nq][dim] quadrature points
+ * (Coords of DGCurvilinearCommon) so that the caller can evaluate its functionals there. */
+int tdg_volume_coords(const tdg_op* op, double* out);
+int tdg_facet_coords(const tdg_op* op, double* out);
+/* Facet normals (not unit, side-0 outward) [F][nq][dim] (DGCurvilinearCommon Normal). */
+int tdg_facet_normals(const tdg_op* op, double* out);
+
+/* Material at volume quadrature points, [E][Nq] each: Poisson K (c1 unused, may be NULL),
+ * Elasticity lambda and mu.  Projects onto the nodal degree-N space, evaluates the volume and
+ * facet precomputations and the interior-penalty constants (Poisson::prepare_*,
+ * app/localoperator/Poisson.cpp:133-223; Elasticity::prepare_*, Elasticity.cpp:104-292), then
+ * uploads everything to the current device. */
+int tdg_set_material(tdg_op* op, const double* c0_Q, const double* c1_Q);
+
+/* Nodal material coefficients [E][Nbf] for c = 0, 1 (after projection). */
+int tdg_material_nodal(const tdg_op* op, int c, double* out);
+/* Penalty per facet [F]. */
+int tdg_penalty(const tdg_op* op, double* out);
+
+/* --- the hot path -------------------------------------------------------------------------- */
+
+/* y = A x for nrhs stacked vectors (AbstractDGOperator::apply, src/form/AbstractDGOperator.h:34;
+ * PetscDGShell::apply, app/common/PetscDGShell.cpp:48-55).  precision selects the element
+ * arithmetic: TDG_FP64 takes double*, TDG_FP32 takes float*. */
+int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64_t ld,
+              void* stream);
+
+/* Algorithmic FLOPs and compulsory HBM bytes of one single-RHS apply (face-centric counting;
+ * tandem's own count is DGOperator::flops_apply, src/form/DGOperator.h:272-280). */
+int64_t tdg_flops_apply(const tdg_op* op);
+int64_t tdg_bytes_apply(const tdg_op* op, int precision);
+
+/* Block-Jacobi preconditioner (the element diagonal blocks of DGOperator::assemble,
+ * src/form/DGOperator.h:121-187, applied as PETSc PCPBJACOBI would).  setup assembles the
+ * diagonal blocks on the device, inverts them and stores the inverses in `precision`.
+ * Returns TDG_E_NOT_SPD when a block is not positive definite. */
+int tdg_bjacobi_setup(tdg_op* op, int precision, void* stream);
+/* z = D^-1 r; precision must match the stored inverses' precision or TDG_FP64 inverses may be
+ * applied to double vectors only. */
+int tdg_bjacobi_apply(tdg_op* op, int precision, const void* r, void* z, int nrhs, int64_t ld,
+                      void* stream);
+/* Copies the assembled (not inverted) diagonal blocks [E][bs][bs] (column-major per block) to
+ * host memory; for tests. */
+int tdg_bjacobi_blocks(tdg_op* op, double* out);
+
+/* --- right-hand side (DGOperator::rhs, src/form/DGOperator.h:189-237) ---------------------- */
+
+/* b = volume load + boundary/fault lift terms.  force_Q: [E][Q][Nq] at volume points (may be
+ * NULL); bc_q: [F][Q][nq] Dirichlet or slip data at facet points (may be NULL), given exactly as
+ * tandem's facet functional returns it for the facet (sign already oriented).  Host arrays in,
+ * host array out [E][bs]. */
+int tdg_rhs(tdg_op* op, const double* force_Q, const double* bc_q, double* b);
+
+/* --- Krylov solve on the device (PetscLinearSolver / KSPCG, app/common/PetscLinearSolver.cpp) */
+
+typedef struct {
+    int32_t precision;      /* TDG_FP64: FP64 CG; TDG_FP32: FP32 inner CG in FP64 refinement */
+    int32_t max_iterations; /* total inner iterations cap */
+    double rtol;            /* relative residual ||b - A x|| / ||b|| target (FP64 residual) */
+    double inner_rtol;      /* inner FP32 reduction per refinement step (mixed only) */
+    int32_t max_outer;      /* refinement steps cap (mixed only) */
+    int32_t use_graphs;     /* capture iteration blocks in CUDA graphs */
+} tdg_solve_opts;
+
+typedef struct {
+    int32_t iterations;     /* total Krylov iterations (inner iterations for mixed) */
+    int32_t outer;          /* refinement steps */
+    double rel_residual;    /* final FP64 relative residual */
+    double seconds;         /* device time of the solve */
+    int32_t converged;
+    int32_t reserved;
+} tdg_solve_stats;
+
+/* Solves A x = b (device double arrays, nrhs stacked with leading dimension ld) with
+ * block-Jacobi preconditioned CG.  x holds the initial guess.  tdg_bjacobi_setup must have
+ * been called with the precision the solve needs (FP64 for TDG_FP64, FP32 for TDG_FP32). */
+int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64_t ld,
+              const tdg_solve_opts* opts, tdg_solve_stats* stats, void* stream);
+
+/* --- host utilities: reference-element tables (no device work) ---------------------------- */
+
+/* Reference nodes of degree N on the unit simplex: family 0 = warp & blend
+ * (src/basis/WarpAndBlend.cpp), 1 = equidistant in VTK order (src/basis/Equidistant.cpp).
+ * out: [binom(N+dim,dim)][dim]. */
+int tdg_ref_nodes(int dim, int degree, int family, double* out);
+/* Basis of degree N at np points: family -1 = modal Dubiner (src/basis/Functions.cpp), 0/1 =
+ * nodal Lagrange basis at the warp & blend / equidistant nodes.  E: [Nbf][np] (may be NULL),
+ * grad: [Nbf][dim][np] (may be NULL). */
+int tdg_ref_basis(int dim, int degree, int family, int np, const double* points, double* E, double* grad);
+/* Conical Gauss-Jacobi product rule of at least `order` on the unit simplex
+ * (src/quadrules/TensorProductRule.cpp); returns the number of points, fills points/weights when
+ * non-NULL. */
+int tdg_conical_rule(int dim, int order, double* points, double* weights);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TANDEM_B200_H */

@@ -1,0 +1,191 @@
+"""ORACLE -- test infrastructure only (see oracle.cpp).
+
+Python bindings of the CPU restatement of tandem's DG operator and of tandem's own quadrature and
+basis sources compiled in place (``oracle/_ref``).  Imported only by tests/, the smoke check and
+bench.py's CPU baseline, as the checker; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from math import comb
+
+import numpy as np
+
+from . import build as _build
+
+_p, _i64 = C.c_void_p, C.c_int64
+_lib = None
+_ref = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        path = _build.build_oracle()
+        L = C.CDLL(str(path))
+        sig = {
+            "orc_create": (C.c_int, [_p, _p, C.c_int, C.POINTER(_p)]),
+            "orc_destroy": (None, [_p]),
+            "orc_volume_coords": (None, [_p, _p]),
+            "orc_facet_coords": (None, [_p, _p]),
+            "orc_facet_normals": (None, [_p, _p]),
+            "orc_set_material": (C.c_int, [_p, _p, _p]),
+            "orc_material_nodal": (None, [_p, C.c_int, _p]),
+            "orc_penalty": (None, [_p, _p]),
+            "orc_apply": (None, [_p, _p, _p]),
+            "orc_apply_range": (None, [_p, C.c_long, C.c_long, _p, _p]),
+            "orc_assemble_diag": (None, [_p, _p]),
+            "orc_rhs": (None, [_p, _p, _p, _p]),
+            "orc_cg": (C.c_int, [_p, _p, _p, C.c_double, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+            "orc_error_L2": (C.c_double, [_p, _p, _p]),
+            "orc_error_H1_semi": (C.c_double, [_p, _p, _p]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def ref_lib() -> C.CDLL | None:
+    """tandem's own quadrature/basis code (None where it was never built)."""
+    global _ref
+    if _ref is None:
+        path = _build.build_reference()
+        if path is None or not path.exists():
+            return None
+        L = C.CDLL(str(path))
+        L.ref_simplex_rule.restype = C.c_int
+        L.ref_simplex_rule.argtypes = [C.c_int, C.c_int, _p, _p]
+        L.ref_conical_rule.restype = C.c_int
+        L.ref_conical_rule.argtypes = [C.c_int, C.c_int, _p, _p]
+        L.ref_gauss_jacobi.restype = C.c_int
+        L.ref_gauss_jacobi.argtypes = [C.c_int, C.c_int, C.c_int, _p, _p]
+        L.ref_jacobi.restype = C.c_double
+        L.ref_jacobi.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double]
+        L.ref_dubiner.restype = C.c_double
+        L.ref_dubiner.argtypes = [C.c_int, _p, _p]
+        L.ref_grad_dubiner.restype = None
+        L.ref_grad_dubiner.argtypes = [C.c_int, _p, _p, _p]
+        _ref = L
+    return _ref
+
+
+def reference_rule(dim: int, order: int):
+    """tandem's simplexQuadratureRule<dim>(order) from the in-place build."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("reference sources were not built (oracle/_ref missing)")
+    n = L.ref_simplex_rule(dim, order, None, None)
+    x = np.zeros((n, dim))
+    w = np.zeros(n)
+    L.ref_simplex_rule(dim, order, x.ctypes.data, w.ctypes.data)
+    return x, w
+
+
+class Oracle:
+    """Element-centric CPU operator over the same mesh/quadrature/material inputs as
+    tandem_b200.operator.DGOperator."""
+
+    def __init__(self, mesh, degree: int, kind: int, quad):
+        from tandem_b200 import _ffi
+        L = lib()
+        D = mesh.dim
+        self.mesh, self.degree, self.kind, self.dim = mesh, degree, kind, D
+        c = lambda a, t: np.ascontiguousarray(a, dtype=t)  # noqa: E731
+        self._keep = dict(geo=c(mesh.geo_nodes, np.float64), up=c(mesh.facet_up, np.int64),
+                          loc=c(mesh.facet_local, np.int32), bc=c(mesh.facet_bc, np.int32),
+                          vx=c(quad.vol_x, np.float64), vw=c(quad.vol_w, np.float64),
+                          fx=c(quad.fct_x, np.float64), fw=c(quad.fct_w, np.float64))
+        k = self._keep
+        desc = _ffi.MeshDesc(D, degree, mesh.geo_degree, 0, mesh.num_elements, mesh.num_facets,
+                             k["geo"].ctypes.data, k["up"].ctypes.data, k["loc"].ctypes.data, k["bc"].ctypes.data)
+        qd = _ffi.Quadrature(len(k["vw"]), len(k["fw"]), k["vx"].ctypes.data, k["vw"].ctypes.data,
+                             k["fx"].ctypes.data, k["fw"].ctypes.data)
+        h = C.c_void_p()
+        if L.orc_create(C.byref(desc), C.byref(qd), kind, C.byref(h)) != 0:
+            raise RuntimeError("oracle construction failed")
+        self._h = h
+        self.Q = 1 if kind == 0 else D
+        self.nbf = comb(degree + D, D)
+        self.bs = self.nbf * self.Q
+        self.E, self.F = mesh.num_elements, mesh.num_facets
+        self.Nq, self.nq = len(k["vw"]), len(k["fw"])
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().orc_destroy(h)
+            self._h = None
+
+    @property
+    def ndof(self) -> int:
+        return self.E * self.bs
+
+    def volume_coords(self):
+        out = np.zeros((self.E, self.Nq, self.dim))
+        lib().orc_volume_coords(self._h, out.ctypes.data)
+        return out
+
+    def facet_coords(self):
+        out = np.zeros((self.F, self.nq, self.dim))
+        lib().orc_facet_coords(self._h, out.ctypes.data)
+        return out
+
+    def facet_normals(self):
+        out = np.zeros((self.F, self.nq, self.dim))
+        lib().orc_facet_normals(self._h, out.ctypes.data)
+        return out
+
+    def set_material(self, c0_Q, c1_Q=None):
+        a = np.ascontiguousarray(c0_Q, dtype=np.float64).reshape(self.E, self.Nq)
+        b = a if c1_Q is None else np.ascontiguousarray(c1_Q, dtype=np.float64).reshape(self.E, self.Nq)
+        self._mat = (a, b)
+        lib().orc_set_material(self._h, a.ctypes.data, b.ctypes.data)
+
+    def material_nodal(self, c: int):
+        out = np.zeros((self.E, self.nbf))
+        lib().orc_material_nodal(self._h, c, out.ctypes.data)
+        return out
+
+    def penalty(self):
+        out = np.zeros(self.F)
+        lib().orc_penalty(self._h, out.ctypes.data)
+        return out
+
+    def apply(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        lib().orc_apply(self._h, x.ctypes.data, y.ctypes.data)
+        return y
+
+    def apply_range(self, e0: int, e1: int, x: np.ndarray, y: np.ndarray) -> None:
+        lib().orc_apply_range(self._h, e0, e1, x.ctypes.data, y.ctypes.data)
+
+    def assemble_diag(self) -> np.ndarray:
+        out = np.zeros((self.E, self.bs, self.bs))
+        lib().orc_assemble_diag(self._h, out.ctypes.data)
+        return np.ascontiguousarray(out.transpose(0, 2, 1))  # [e, row, col]
+
+    def rhs(self, force_Q=None, bc_q=None) -> np.ndarray:
+        b = np.zeros(self.ndof)
+        f = None if force_Q is None else np.ascontiguousarray(force_Q, dtype=np.float64)
+        g = None if bc_q is None else np.ascontiguousarray(bc_q, dtype=np.float64)
+        lib().orc_rhs(self._h, None if f is None else f.ctypes.data, None if g is None else g.ctypes.data,
+                      b.ctypes.data)
+        return b
+
+    def cg(self, b: np.ndarray, rtol: float = 1e-10, maxit: int = 20000, x0=None):
+        x = np.zeros(self.ndof) if x0 is None else np.array(x0, dtype=np.float64)
+        it, rel = C.c_int(0), C.c_double(0.0)
+        rc = lib().orc_cg(self._h, np.ascontiguousarray(b).ctypes.data, x.ctypes.data, rtol, maxit,
+                          C.byref(it), C.byref(rel))
+        return x, dict(iterations=it.value, rel_residual=rel.value, converged=rc == 0)
+
+    def error_L2(self, x: np.ndarray, ref_Q: np.ndarray) -> float:
+        r = np.ascontiguousarray(ref_Q, dtype=np.float64)
+        return lib().orc_error_L2(self._h, np.ascontiguousarray(x).ctypes.data, r.ctypes.data)
+
+    def error_H1_semi(self, x: np.ndarray, refgrad_Q: np.ndarray) -> float:
+        r = np.ascontiguousarray(refgrad_Q, dtype=np.float64)
+        return lib().orc_error_H1_semi(self._h, np.ascontiguousarray(x).ctypes.data, r.ctypes.data)

@@ -1,0 +1,94 @@
+"""ctypes bindings of the C ABI in ``include/tandem_b200.h``.
+
+The native library is mandatory: importing this module raises if it has not been built; there is
+no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libtandem_b200.so"
+
+TDG_POISSON, TDG_ELASTICITY = 0, 1
+TDG_BC_NONE, TDG_BC_NATURAL, TDG_BC_FAULT, TDG_BC_DIRICHLET = 0, 1, 3, 5
+TDG_FP64, TDG_FP32 = 0, 1
+ERRORS = {-1: "TDG_E_INVALID", -2: "TDG_E_CUDA", -3: "TDG_E_NOT_SPD", -4: "TDG_E_DIVERGED",
+          -5: "TDG_E_STATE", -6: "TDG_E_TIMEOUT", -7: "TDG_E_NOMEM"}
+
+# Every symbol the header declares, with (restype, argtypes).
+_p = C.c_void_p
+_i64 = C.c_int64
+SYMBOLS = {
+    "tdg_create": (C.c_int, [_p, _p, C.c_int, C.POINTER(_p)]),
+    "tdg_destroy": (None, [_p]),
+    "tdg_last_error": (C.c_char_p, []),
+    "tdg_sizes": (C.c_int, [_p, _p]),
+    "tdg_volume_coords": (C.c_int, [_p, _p]),
+    "tdg_facet_coords": (C.c_int, [_p, _p]),
+    "tdg_facet_normals": (C.c_int, [_p, _p]),
+    "tdg_set_material": (C.c_int, [_p, _p, _p]),
+    "tdg_material_nodal": (C.c_int, [_p, C.c_int, _p]),
+    "tdg_penalty": (C.c_int, [_p, _p]),
+    "tdg_apply": (C.c_int, [_p, C.c_int, _p, _p, C.c_int, _i64, _p]),
+    "tdg_flops_apply": (_i64, [_p]),
+    "tdg_bytes_apply": (_i64, [_p, C.c_int]),
+    "tdg_bjacobi_setup": (C.c_int, [_p, C.c_int, _p]),
+    "tdg_bjacobi_apply": (C.c_int, [_p, C.c_int, _p, _p, C.c_int, _i64, _p]),
+    "tdg_bjacobi_blocks": (C.c_int, [_p, _p]),
+    "tdg_rhs": (C.c_int, [_p, _p, _p, _p]),
+    "tdg_solve": (C.c_int, [_p, _p, _p, C.c_int, _i64, _p, _p, _p]),
+    "tdg_ref_nodes": (C.c_int, [C.c_int, C.c_int, C.c_int, _p]),
+    "tdg_ref_basis": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _p, _p, _p]),
+    "tdg_conical_rule": (C.c_int, [C.c_int, C.c_int, _p, _p]),
+}
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("degree", C.c_int32), ("geo_degree", C.c_int32),
+                ("reserved", C.c_int32), ("num_elements", C.c_int64), ("num_facets", C.c_int64),
+                ("geo_nodes", _p), ("facet_up", _p), ("facet_local_no", _p), ("facet_bc", _p)]
+
+
+class Quadrature(C.Structure):
+    _fields_ = [("num_vol_points", C.c_int32), ("num_fct_points", C.c_int32),
+                ("vol_points", _p), ("vol_weights", _p), ("fct_points", _p), ("fct_weights", _p)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("max_iterations", C.c_int32), ("rtol", C.c_double),
+                ("inner_rtol", C.c_double), ("max_outer", C.c_int32), ("use_graphs", C.c_int32)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("outer", C.c_int32), ("rel_residual", C.c_double),
+                ("seconds", C.c_double), ("converged", C.c_int32), ("reserved", C.c_int32)]
+
+
+class TdgError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads the native library (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"tandem_b200 native library not built: {LIB_PATH} "
+                              "(run python -m tandem_b200.build)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SYMBOLS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        msg = lib().tdg_last_error().decode(errors="replace")
+        raise TdgError(f"{ERRORS.get(rc, rc)}: {msg}")

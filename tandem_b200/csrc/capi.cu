@@ -1,0 +1,772 @@
+// C ABI of tandem_b200 (include/tandem_b200.h): operator handle, device upload, apply,
+// block-Jacobi and the device Krylov drivers.
+#include "../../include/tandem_b200.h"
+#include "host/setup.hpp"
+#include "kernels/dispatch.hpp"
+#include "kernels/krylov.cuh"
+
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+namespace tdg {
+
+__global__ void k_dot_finalize(const double* __restrict__ partial, int nb, double* __restrict__ scal,
+                               int slot0, int slot1) {
+    const int rhs = blockIdx.x;
+    double s0 = 0.0, s1 = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        s0 += partial[(static_cast<int64_t>(rhs) * nb + i) * 2];
+        s1 += partial[(static_cast<int64_t>(rhs) * nb + i) * 2 + 1];
+    }
+    __shared__ double red[2][32];
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][wid] = s0;
+        red[1][wid] = s1;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x / 32;
+        s0 = lane < nw ? red[0][lane] : 0.0;
+        s1 = lane < nw ? red[1][lane] : 0.0;
+        s0 = warp_sum(s0);
+        s1 = warp_sum(s1);
+        if (lane == 0) {
+            if (slot0 >= 0) scal[rhs * kScal + slot0] = s0;
+            if (slot1 >= 0) scal[rhs * kScal + slot1] = s1;
+        }
+    }
+}
+
+__global__ void k_cg_shift(double* __restrict__ scal, int nrhs) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrhs && scal[r * kScal + kActive] != 0.0) scal[r * kScal + kRZ] = scal[r * kScal + kRZnew];
+}
+
+}  // namespace tdg
+
+using namespace tdg;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, std::string const& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define TDG_CUDA_TRY(expr)                                                                   \
+    do {                                                                                     \
+        cudaError_t err_ = (expr);                                                           \
+        if (err_ != cudaSuccess)                                                             \
+            return fail(err_ == cudaErrorMemoryAllocation ? TDG_E_NOMEM : TDG_E_CUDA,        \
+                        std::string(#expr) + ": " + cudaGetErrorString(err_));              \
+    } while (0)
+
+#define TDG_TRY(expr)                                                                        \
+    do {                                                                                     \
+        int rc_ = (expr);                                                                    \
+        if (rc_ != 0) {                                                                      \
+            if (g_last_error.empty()) g_last_error = std::string(#expr) + " failed";         \
+            return rc_;                                                                      \
+        }                                                                                    \
+    } while (0)
+
+// A set of device allocations freed together.
+struct DevArena {
+    std::vector<void*> ptrs;
+    template <typename T>
+    cudaError_t alloc(T** p, size_t n) {
+        void* v = nullptr;
+        cudaError_t e = cudaMalloc(&v, n * sizeof(T) + 16);
+        if (e == cudaSuccess) {
+            ptrs.push_back(v);
+            *p = static_cast<T*>(v);
+        }
+        return e;
+    }
+    template <typename T>
+    cudaError_t upload(T const** out, std::vector<T> const& h) {
+        T* d = nullptr;
+        cudaError_t e = alloc(&d, h.size());
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+        *out = d;
+        return e;
+    }
+    void release() {
+        for (void* p : ptrs) cudaFree(p);
+        ptrs.clear();
+    }
+    ~DevArena() { release(); }
+};
+
+template <typename T>
+std::vector<T> conv(std::vector<double> const& v) {
+    return std::vector<T>(v.begin(), v.end());
+}
+
+}  // namespace
+
+struct tdg_op {
+    HostOperator h;
+    bool uploaded64 = false, uploaded32 = false;
+    DevArena arena64, arena32, arena_common, arena_pc, arena_ws;
+    DevOp<double> op64;
+    DevOp<float> op32;
+    const double* penalty = nullptr;
+    const int4* sides = nullptr;
+    // block-Jacobi
+    double* blk = nullptr;
+    void* inv = nullptr;
+    int inv_precision = -1;
+    int* status = nullptr;
+    // solve workspace
+    size_t ws_bytes = 0;
+    void* ws = nullptr;
+};
+
+namespace {
+
+int upload_common(tdg_op* op) {
+    if (op->penalty) return 0;
+    auto& h = op->h;
+    TDG_CUDA_TRY(op->arena_common.upload(&op->penalty, h.penalty));
+    std::vector<int4> sides(h.sides.size());
+    for (size_t i = 0; i < sides.size(); ++i) {
+        auto const& s = h.sides[i];
+        sides[i] = make_int4(s.fct, s.side | (s.bc << 8), s.nb, s.nb_local);
+    }
+    TDG_CUDA_TRY(op->arena_common.upload(&op->sides, sides));
+    return 0;
+}
+
+template <typename T>
+int upload_precision(tdg_op* op, DevArena& arena, DevOp<T>& d) {
+    auto& h = op->h;
+    const int D = h.D, NBF = h.Nbf, Nq = h.Nq, nq = h.nq, NF = h.nfaces;
+    TDG_TRY(upload_common(op));
+    d.E = h.E;
+    d.F = h.F;
+    d.Nq = Nq;
+    d.nq = nq;
+    // basis tables and their transposes
+    std::vector<T> Dxi(h.Dxi_Q.begin(), h.Dxi_Q.end()), DxiT(static_cast<size_t>(NBF) * D * Nq);
+    for (int k = 0; k < NBF; ++k)
+        for (int c = 0; c < D * Nq; ++c) DxiT[static_cast<size_t>(c) * NBF + k] = Dxi[static_cast<size_t>(k) * D * Nq + c];
+    std::vector<T> Eq, ETq, Dq, DTq;
+    for (int f = 0; f < NF; ++f) {
+        for (int k = 0; k < NBF; ++k)
+            for (int q = 0; q < nq; ++q) Eq.push_back(static_cast<T>(h.E_qf[f](k, q)));
+        for (int q = 0; q < nq; ++q)
+            for (int k = 0; k < NBF; ++k) ETq.push_back(static_cast<T>(h.E_qf[f](k, q)));
+        auto const& g = h.Dxi_qf[f];
+        for (size_t i = 0; i < g.size(); ++i) Dq.push_back(static_cast<T>(g[i]));
+        std::vector<T> t(static_cast<size_t>(D) * nq * NBF);
+        for (int k = 0; k < NBF; ++k)
+            for (int c = 0; c < D * nq; ++c) t[static_cast<size_t>(c) * NBF + k] = static_cast<T>(g[static_cast<size_t>(k) * D * nq + c]);
+        DTq.insert(DTq.end(), t.begin(), t.end());
+    }
+    TDG_CUDA_TRY(arena.upload(&d.Dxi_Q, Dxi));
+    TDG_CUDA_TRY(arena.upload(&d.DxiT_Q, DxiT));
+    TDG_CUDA_TRY(arena.upload(&d.E_q, Eq));
+    TDG_CUDA_TRY(arena.upload(&d.ET_q, ETq));
+    TDG_CUDA_TRY(arena.upload(&d.Dxi_q, Dq));
+    TDG_CUDA_TRY(arena.upload(&d.DxiT_q, DTq));
+    TDG_CUDA_TRY(arena.upload(&d.w, conv<T>(h.w)));
+    TDG_CUDA_TRY(arena.upload(&d.vG, conv<T>(h.vG)));
+    TDG_CUDA_TRY(arena.upload(&d.vCoef, conv<T>(h.vCoef)));
+    TDG_CUDA_TRY(arena.upload(&d.fN, conv<T>(h.fN)));
+    TDG_CUDA_TRY(arena.upload(&d.fNunit, conv<T>(h.fNunit)));
+    TDG_CUDA_TRY(arena.upload(&d.fNl, conv<T>(h.fNl)));
+    TDG_CUDA_TRY(arena.upload(&d.fCoef, conv<T>(h.fCoef)));
+    {
+        // [F][2][DD][nq]: G0 and G1 interleaved per facet
+        const size_t per = static_cast<size_t>(D) * D * nq;
+        std::vector<T> fg(static_cast<size_t>(h.F) * 2 * per);
+        for (int64_t f = 0; f < h.F; ++f)
+            for (size_t i = 0; i < per; ++i) {
+                fg[(static_cast<size_t>(f) * 2 + 0) * per + i] = static_cast<T>(h.fG0[static_cast<size_t>(f) * per + i]);
+                fg[(static_cast<size_t>(f) * 2 + 1) * per + i] = static_cast<T>(h.fG1[static_cast<size_t>(f) * per + i]);
+            }
+        TDG_CUDA_TRY(arena.upload(&d.fG, fg));
+    }
+    d.penalty = op->penalty;
+    d.sides = op->sides;
+    TDG_CUDA_TRY(cudaDeviceSynchronize());
+    return 0;
+}
+
+int ensure_uploaded(tdg_op* op, int precision) {
+    if (!op->h.has_material) return fail(TDG_E_STATE, "tdg_set_material has not been called");
+    if (precision == TDG_FP64) {
+        if (!op->uploaded64) {
+            TDG_TRY(upload_precision<double>(op, op->arena64, op->op64));
+            op->uploaded64 = true;
+        }
+        return 0;
+    }
+    if (precision == TDG_FP32) {
+        if (!op->uploaded32) {
+            TDG_TRY(upload_precision<float>(op, op->arena32, op->op32));
+            op->uploaded32 = true;
+        }
+        return 0;
+    }
+    return fail(TDG_E_INVALID, "precision must be TDG_FP64 or TDG_FP32");
+}
+
+dim3 vec_grid(int64_t n, int nrhs) {
+    int64_t g = (n + 255) / 256;
+    int64_t cap = static_cast<int64_t>(device_sm_count()) * 8;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return dim3(static_cast<unsigned>(g), static_cast<unsigned>(nrhs));
+}
+
+int dot_blocks(int64_t n) {
+    int64_t g = (n + kDotThreads - 1) / kDotThreads;
+    int64_t cap = static_cast<int64_t>(device_sm_count()) * 4;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return static_cast<int>(g);
+}
+
+// scal[rhs][slot0] = a.b, scal[rhs][slot1] = c.d
+template <typename T>
+int dots(int64_t n, int64_t ld, int nrhs, const T* a, const T* b, const T* c, const T* d, double* partial,
+         double* scal, int slot0, int slot1, cudaStream_t s) {
+    const int nb = dot_blocks(n);
+    k_dot2<T><<<dim3(nb, nrhs), kDotThreads, 0, s>>>(n, ld, a, b, c, d, partial);
+    k_dot_finalize<<<nrhs, 256, 0, s>>>(partial, nb, scal, slot0, slot1);
+    return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "dot kernels");
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------------
+
+extern "C" {
+
+const char* tdg_last_error(void) { return g_last_error.c_str(); }
+
+int tdg_create(const tdg_mesh_desc* mesh, const tdg_quadrature* quad, int kind, tdg_op** out) {
+    g_last_error.clear();
+    if (!mesh || !quad || !out) return fail(TDG_E_INVALID, "null argument");
+    if (!mesh->geo_nodes || !mesh->facet_up || !mesh->facet_local_no || !mesh->facet_bc)
+        return fail(TDG_E_INVALID, "mesh arrays missing");
+    if (!quad->vol_points || !quad->vol_weights || !quad->fct_points || !quad->fct_weights)
+        return fail(TDG_E_INVALID, "quadrature arrays missing");
+    if (mesh->degree < kMinDegree || mesh->degree > kMaxDegree)
+        return fail(TDG_E_INVALID, "degree outside the compiled range [1, 4]");
+    try {
+        auto* op = new tdg_op();
+        op->h.build(mesh->dim, mesh->degree, mesh->geo_degree, kind, mesh->num_elements, mesh->num_facets,
+                    mesh->geo_nodes, mesh->facet_up, mesh->facet_local_no, mesh->facet_bc,
+                    quad->num_vol_points, quad->vol_points, quad->vol_weights, quad->num_fct_points,
+                    quad->fct_points, quad->fct_weights);
+        *out = op;
+        return 0;
+    } catch (std::exception const& e) {
+        return fail(TDG_E_INVALID, e.what());
+    }
+}
+
+void tdg_destroy(tdg_op* op) { delete op; }
+
+int tdg_sizes(const tdg_op* op, int64_t out[8]) {
+    if (!op || !out) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = op->h;
+    out[0] = h.bs;
+    out[1] = h.Nbf;
+    out[2] = h.Q;
+    out[3] = h.Nq;
+    out[4] = h.nq;
+    out[5] = h.E;
+    out[6] = h.F;
+    out[7] = h.D;
+    return 0;
+}
+
+int tdg_volume_coords(const tdg_op* op, double* out) {
+    if (!op || !out) return fail(TDG_E_INVALID, "null argument");
+    std::memcpy(out, op->h.vCoords.data(), op->h.vCoords.size() * sizeof(double));
+    return 0;
+}
+
+int tdg_facet_coords(const tdg_op* op, double* out) {
+    if (!op || !out) return fail(TDG_E_INVALID, "null argument");
+    std::memcpy(out, op->h.fCoords.data(), op->h.fCoords.size() * sizeof(double));
+    return 0;
+}
+
+int tdg_facet_normals(const tdg_op* op, double* out) {
+    if (!op || !out) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = op->h;
+    for (int64_t f = 0; f < h.F; ++f)
+        for (int q = 0; q < h.nq; ++q)
+            for (int i = 0; i < h.D; ++i)
+                out[(static_cast<size_t>(f) * h.nq + q) * h.D + i] = h.fN[(static_cast<size_t>(f) * h.D + i) * h.nq + q];
+    return 0;
+}
+
+int tdg_set_material(tdg_op* op, const double* c0_Q, const double* c1_Q) {
+    if (!op) return fail(TDG_E_INVALID, "null operator");
+    try {
+        op->h.set_material(c0_Q, c1_Q);
+    } catch (std::exception const& e) {
+        return fail(TDG_E_INVALID, e.what());
+    }
+    op->arena64.release();
+    op->arena32.release();
+    op->arena_common.release();
+    op->arena_pc.release();
+    op->uploaded64 = op->uploaded32 = false;
+    op->penalty = nullptr;
+    op->sides = nullptr;
+    op->blk = nullptr;
+    op->inv = nullptr;
+    op->inv_precision = -1;
+    op->status = nullptr;
+    return 0;
+}
+
+int tdg_material_nodal(const tdg_op* op, int c, double* out) {
+    if (!op || !out || c < 0 || c > 1) return fail(TDG_E_INVALID, "bad argument");
+    auto const& h = op->h;
+    if (!h.has_material) return fail(TDG_E_STATE, "no material");
+    int nm = h.mat_space.num_basis();
+    for (int64_t e = 0; e < h.E; ++e)
+        std::memcpy(out + e * nm, &h.mat_nodal[(static_cast<size_t>(e) * 2 + c) * nm], nm * sizeof(double));
+    return 0;
+}
+
+int tdg_penalty(const tdg_op* op, double* out) {
+    if (!op || !out) return fail(TDG_E_INVALID, "bad argument");
+    if (!op->h.has_material) return fail(TDG_E_STATE, "no material");
+    std::memcpy(out, op->h.penalty.data(), op->h.penalty.size() * sizeof(double));
+    return 0;
+}
+
+int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64_t ld, void* stream) {
+    if (!op || !x || !y) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = op->h;
+    if (nrhs < 1 || ld < h.E * h.bs) return fail(TDG_E_INVALID, "nrhs < 1 or ld < E * bs");
+    if (x == y) return fail(TDG_E_INVALID, "x and y must not alias");
+    TDG_TRY(ensure_uploaded(op, precision));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc;
+    if (precision == TDG_FP64)
+        rc = launch_apply<double>(h.D, h.N, h.kind, op->op64, static_cast<const double*>(x),
+                                  static_cast<double*>(y), nrhs, ld, s);
+    else
+        rc = launch_apply<float>(h.D, h.N, h.kind, op->op32, static_cast<const float*>(x),
+                                 static_cast<float*>(y), nrhs, ld, s);
+    if (rc) return fail(rc, std::string("apply launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
+int64_t tdg_flops_apply(const tdg_op* op) { return op ? op->h.flops_apply() : -1; }
+
+int64_t tdg_bytes_apply(const tdg_op* op, int precision) {
+    return op ? op->h.bytes_apply(precision == TDG_FP32 ? 4 : 8) : -1;
+}
+
+int tdg_bjacobi_setup(tdg_op* op, int precision, void* stream) {
+    if (!op) return fail(TDG_E_INVALID, "null operator");
+    if (precision != TDG_FP64 && precision != TDG_FP32) return fail(TDG_E_INVALID, "bad precision");
+    TDG_TRY(ensure_uploaded(op, TDG_FP64));
+    auto const& h = op->h;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t nblk = static_cast<size_t>(h.E) * h.bs * h.bs;
+    if (!op->blk) {
+        TDG_CUDA_TRY(op->arena_pc.alloc(&op->blk, nblk));
+        TDG_CUDA_TRY(op->arena_pc.alloc(&op->status, 1));
+        int rc = launch_bjac_assemble(h.D, h.N, h.kind, op->op64, op->blk, s);
+        if (rc) return fail(rc, "block assembly launch failed");
+    }
+    if (op->inv && op->inv_precision == precision) return 0;
+    if (op->inv) {
+        // switching precision: re-allocate (arena keeps the old buffer until release)
+        op->inv = nullptr;
+    }
+    TDG_CUDA_TRY(cudaMemsetAsync(op->status, 0, sizeof(int), s));
+    int rc;
+    if (precision == TDG_FP64) {
+        double* inv = nullptr;
+        TDG_CUDA_TRY(op->arena_pc.alloc(&inv, nblk));
+        rc = launch_bjac_invert<double>(h.bs, h.E, op->blk, inv, op->status, s);
+        op->inv = inv;
+    } else {
+        float* inv = nullptr;
+        TDG_CUDA_TRY(op->arena_pc.alloc(&inv, nblk));
+        rc = launch_bjac_invert<float>(h.bs, h.E, op->blk, inv, op->status, s);
+        op->inv = inv;
+    }
+    if (rc) return fail(rc, "block inversion launch failed");
+    op->inv_precision = precision;
+    int st = 0;
+    TDG_CUDA_TRY(cudaMemcpyAsync(&st, op->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TDG_CUDA_TRY(cudaStreamSynchronize(s));
+    if (st) {
+        op->inv = nullptr;
+        op->inv_precision = -1;
+        return fail(TDG_E_NOT_SPD, "a block-Jacobi diagonal block is not positive definite");
+    }
+    return 0;
+}
+
+int tdg_bjacobi_apply(tdg_op* op, int precision, const void* r, void* z, int nrhs, int64_t ld, void* stream) {
+    if (!op || !r || !z) return fail(TDG_E_INVALID, "null argument");
+    if (!op->inv || op->inv_precision != precision)
+        return fail(TDG_E_STATE, "tdg_bjacobi_setup not called for this precision");
+    auto const& h = op->h;
+    if (nrhs < 1 || ld < h.E * h.bs) return fail(TDG_E_INVALID, "nrhs < 1 or ld < E * bs");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc = (precision == TDG_FP64)
+                 ? launch_bjac_apply<double>(h.bs, h.E, static_cast<const double*>(op->inv),
+                                             static_cast<const double*>(r), static_cast<double*>(z), nrhs, ld, s)
+                 : launch_bjac_apply<float>(h.bs, h.E, static_cast<const float*>(op->inv),
+                                            static_cast<const float*>(r), static_cast<float*>(z), nrhs, ld, s);
+    if (rc) return fail(rc, "block-Jacobi apply launch failed");
+    return 0;
+}
+
+int tdg_bjacobi_blocks(tdg_op* op, double* out) {
+    if (!op || !out) return fail(TDG_E_INVALID, "null argument");
+    if (!op->blk) return fail(TDG_E_STATE, "tdg_bjacobi_setup not called");
+    auto const& h = op->h;
+    TDG_CUDA_TRY(cudaDeviceSynchronize());
+    TDG_CUDA_TRY(cudaMemcpy(out, op->blk, static_cast<size_t>(h.E) * h.bs * h.bs * sizeof(double),
+                            cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int tdg_rhs(tdg_op* op, const double* force_Q, const double* bc_q, double* b) {
+    if (!op || !b) return fail(TDG_E_INVALID, "null argument");
+    try {
+        op->h.rhs(force_Q, bc_q, b);
+    } catch (std::exception const& e) {
+        return fail(TDG_E_STATE, e.what());
+    }
+    return 0;
+}
+
+int tdg_ref_nodes(int dim, int degree, int family, double* out) {
+    if (!out || dim < 1 || dim > 3 || degree < 0 || degree > 15) return fail(TDG_E_INVALID, "bad argument");
+    try {
+        Points p = (family == 0) ? warp_blend_nodes(dim, degree) : equidistant_nodes(dim, degree);
+        std::memcpy(out, p.data(), p.size() * sizeof(double));
+    } catch (std::exception const& e) {
+        return fail(TDG_E_INVALID, e.what());
+    }
+    return 0;
+}
+
+int tdg_ref_basis(int dim, int degree, int family, int np, const double* points, double* E, double* grad) {
+    if (!points || dim < 1 || dim > 3 || degree < 0 || degree > 15 || np < 0)
+        return fail(TDG_E_INVALID, "bad argument");
+    try {
+        RefSpace sp = (family < 0) ? RefSpace::modal(dim, degree)
+                                   : RefSpace::nodal(dim, degree, family == 0 ? warp_blend_nodes(dim, degree)
+                                                                              : equidistant_nodes(dim, degree));
+        Points pts(points, points + static_cast<size_t>(np) * dim);
+        if (E) {
+            Dense e = sp.eval(pts);
+            std::memcpy(E, e.a.data(), e.a.size() * sizeof(double));
+        }
+        if (grad) {
+            auto g = sp.grad(pts);
+            std::memcpy(grad, g.data(), g.size() * sizeof(double));
+        }
+    } catch (std::exception const& e) {
+        return fail(TDG_E_INVALID, e.what());
+    }
+    return 0;
+}
+
+int tdg_conical_rule(int dim, int order, double* points, double* weights) {
+    if (dim < 1 || dim > 3 || order < 0) return fail(TDG_E_INVALID, "bad argument");
+    SimplexRule r = conical_product_rule(dim, order);
+    if (points) std::memcpy(points, r.x.data(), r.x.size() * sizeof(double));
+    if (weights) std::memcpy(weights, r.w.data(), r.w.size() * sizeof(double));
+    return r.size();
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Krylov drivers
+// ------------------------------------------------------------------------------------------------
+
+namespace {
+
+template <typename T>
+struct CgVectors {
+    T *r, *z, *p, *q;
+};
+
+// One preconditioned CG iteration on (A_T, M_T) with device-resident scalars.
+template <typename T>
+int cg_iteration(tdg_op* op, int prec, T* x, CgVectors<T> v, int nrhs, int64_t ld, double* partial,
+                 double* scal, cudaStream_t s) {
+    auto const& h = op->h;
+    const int64_t n = h.E * h.bs;
+    TDG_TRY(tdg_apply(op, prec, v.p, v.q, nrhs, ld, s));
+    TDG_TRY(dots<T>(n, ld, nrhs, v.p, v.q, nullptr, nullptr, partial, scal, kPQ, -1, s));
+    k_cg_xr<T><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, x, v.r, v.p, v.q, scal);
+    TDG_TRY(tdg_bjacobi_apply(op, prec, v.r, v.z, nrhs, ld, s));
+    TDG_TRY(dots<T>(n, ld, nrhs, v.r, v.z, v.r, v.r, partial, scal, kRZnew, kRR, s));
+    k_cg_p<T><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, v.p, v.z, scal);
+    k_cg_shift<<<(nrhs + 127) / 128, 128, 0, s>>>(scal, nrhs);
+    return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "CG update kernels");
+}
+
+// Runs CG iterations until every active rhs reaches sqrt(rr) <= tol_abs[rhs] or the iteration
+// budget is spent.  Returns the number of iterations done in *iters.
+template <typename T>
+int cg_loop(tdg_op* op, int prec, T* x, CgVectors<T> v, int nrhs, int64_t ld, double* partial, double* scal,
+            std::vector<double> const& tol_abs, int max_it, bool graphs, cudaStream_t s, int* iters,
+            bool* diverged) {
+    constexpr int kChunk = 8;
+    std::vector<double> hs(static_cast<size_t>(nrhs) * kScal);
+    cudaGraphExec_t exec = nullptr;
+    int done = 0;
+    *diverged = false;
+    int rc = 0;
+    for (;;) {
+        TDG_CUDA_TRY(cudaMemcpyAsync(hs.data(), scal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TDG_CUDA_TRY(cudaStreamSynchronize(s));
+        bool any = false, changed = false;
+        for (int r = 0; r < nrhs; ++r) {
+            double* sr = &hs[static_cast<size_t>(r) * kScal];
+            if (sr[kActive] == 0.0) continue;
+            double rr = sr[kRR];
+            if (!std::isfinite(rr)) {
+                *diverged = true;
+                sr[kActive] = 0.0;
+                changed = true;
+                continue;
+            }
+            if (std::sqrt(rr) <= tol_abs[r]) {
+                sr[kActive] = 0.0;
+                changed = true;
+                continue;
+            }
+            any = true;
+        }
+        if (changed)
+            TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (!any || done >= max_it) break;
+        const bool use_graph = graphs && s != nullptr && done >= kChunk;
+        if (use_graph && !exec) {
+            cudaGraph_t graph = nullptr;
+            TDG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            for (int i = 0; i < kChunk && rc == 0; ++i) rc = cg_iteration<T>(op, prec, x, v, nrhs, ld, partial, scal, s);
+            cudaError_t ce = cudaStreamEndCapture(s, &graph);
+            if (rc) return rc;
+            TDG_CUDA_TRY(ce);
+            TDG_CUDA_TRY(cudaGraphInstantiate(&exec, graph, 0));
+            cudaGraphDestroy(graph);
+        }
+        if (exec) {
+            TDG_CUDA_TRY(cudaGraphLaunch(exec, s));
+        } else {
+            for (int i = 0; i < kChunk; ++i) TDG_TRY(cg_iteration<T>(op, prec, x, v, nrhs, ld, partial, scal, s));
+        }
+        done += kChunk;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    *iters = done;
+    return 0;
+}
+
+// r = b - A x (FP64), returns per-rhs ||r|| and ||b|| on the host.
+int residual64(tdg_op* op, const double* b, const double* x, double* r, double* tmp, int nrhs, int64_t ld,
+               double* partial, double* scal, std::vector<double>& rn, std::vector<double>& bn, cudaStream_t s) {
+    auto const& h = op->h;
+    const int64_t n = h.E * h.bs;
+    TDG_TRY(tdg_apply(op, TDG_FP64, x, tmp, nrhs, ld, s));
+    k_sub<double><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, b, tmp, r);
+    TDG_TRY(dots<double>(n, ld, nrhs, r, r, b, b, partial, scal, kRR, kBB, s));
+    std::vector<double> hs(static_cast<size_t>(nrhs) * kScal);
+    TDG_CUDA_TRY(cudaMemcpyAsync(hs.data(), scal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    TDG_CUDA_TRY(cudaStreamSynchronize(s));
+    rn.resize(nrhs);
+    bn.resize(nrhs);
+    for (int i = 0; i < nrhs; ++i) {
+        rn[i] = std::sqrt(hs[static_cast<size_t>(i) * kScal + kRR]);
+        bn[i] = std::sqrt(hs[static_cast<size_t>(i) * kScal + kBB]);
+    }
+    return 0;
+}
+
+// Initialises z = M r, p = z, rz = r.z, rr = r.r, active = flags.
+template <typename T>
+int cg_start(tdg_op* op, int prec, CgVectors<T> v, int nrhs, int64_t ld, double* partial, double* scal,
+             std::vector<double> const& active, cudaStream_t s) {
+    auto const& h = op->h;
+    const int64_t n = h.E * h.bs;
+    std::vector<double> hs(static_cast<size_t>(nrhs) * kScal, 0.0);
+    for (int i = 0; i < nrhs; ++i) hs[static_cast<size_t>(i) * kScal + kActive] = active[i];
+    TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    TDG_TRY(tdg_bjacobi_apply(op, prec, v.r, v.z, nrhs, ld, s));
+    k_copy<T><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, v.z, ld, v.p);
+    TDG_TRY(dots<T>(n, ld, nrhs, v.r, v.z, v.r, v.r, partial, scal, kRZ, kRR, s));
+    // the active flags were uploaded before the dots; the dots do not touch slot kActive
+    return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "CG start");
+}
+
+}  // namespace
+
+extern "C" int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64_t ld, const tdg_solve_opts* opts,
+                         tdg_solve_stats* stats, void* stream) {
+    if (!op || !b || !x || !opts || !stats) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = op->h;
+    const int64_t n = h.E * h.bs;
+    if (nrhs < 1 || ld < n) return fail(TDG_E_INVALID, "nrhs < 1 or ld < E * bs");
+    const int prec = opts->precision;
+    if (prec != TDG_FP64 && prec != TDG_FP32) return fail(TDG_E_INVALID, "bad precision");
+    if (!op->inv || op->inv_precision != prec)
+        return fail(TDG_E_STATE, "tdg_bjacobi_setup must be called with the solve precision");
+    TDG_TRY(ensure_uploaded(op, TDG_FP64));
+    if (prec == TDG_FP32) TDG_TRY(ensure_uploaded(op, TDG_FP32));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::memset(stats, 0, sizeof(*stats));
+
+    // workspace: FP64 r, z, p, q, tmp (5 nrhs*ld) + FP32 d, r, z, p, q (5 nrhs*ld floats)
+    const size_t vec = static_cast<size_t>(nrhs) * ld;
+    const size_t partial_n = static_cast<size_t>(nrhs) * dot_blocks(n) * 2;
+    size_t need = 5 * vec * sizeof(double) + partial_n * sizeof(double) + 2 * static_cast<size_t>(nrhs) * kScal * sizeof(double) + 1024;
+    if (prec == TDG_FP32) need += 5 * vec * sizeof(float);
+    if (op->ws_bytes < need) {
+        op->arena_ws.release();
+        op->ws = nullptr;
+        unsigned char* w = nullptr;
+        TDG_CUDA_TRY(op->arena_ws.alloc(&w, need));
+        op->ws = w;
+        op->ws_bytes = need;
+    }
+    unsigned char* w = static_cast<unsigned char*>(op->ws);
+    auto take = [&](size_t bytes) {
+        unsigned char* p = w;
+        w += (bytes + 255) / 256 * 256;
+        return p;
+    };
+    double* r64 = reinterpret_cast<double*>(take(vec * sizeof(double)));
+    double* z64 = reinterpret_cast<double*>(take(vec * sizeof(double)));
+    double* p64 = reinterpret_cast<double*>(take(vec * sizeof(double)));
+    double* q64 = reinterpret_cast<double*>(take(vec * sizeof(double)));
+    double* t64 = reinterpret_cast<double*>(take(vec * sizeof(double)));
+    double* partial = reinterpret_cast<double*>(take(partial_n * sizeof(double)));
+    double* scal = reinterpret_cast<double*>(take(static_cast<size_t>(nrhs) * kScal * sizeof(double)));
+    double* scal_out = reinterpret_cast<double*>(take(static_cast<size_t>(nrhs) * kScal * sizeof(double)));
+
+    cudaEvent_t ev0, ev1;
+    TDG_CUDA_TRY(cudaEventCreate(&ev0));
+    TDG_CUDA_TRY(cudaEventCreate(&ev1));
+    TDG_CUDA_TRY(cudaEventRecord(ev0, s));
+
+    const int max_it = opts->max_iterations > 0 ? opts->max_iterations : 10000;
+    const double rtol = opts->rtol > 0 ? opts->rtol : 1e-10;
+    const bool graphs = opts->use_graphs != 0;
+    std::vector<double> rn, bn;
+    int total_it = 0, outer = 0;
+    bool diverged = false;
+    double worst = 0.0;
+
+    if (prec == TDG_FP64) {
+        // FP64 PCG with a true-residual check and restart on recurrence drift
+        for (int restart = 0; restart < 4; ++restart) {
+            TDG_TRY(residual64(op, b, x, r64, t64, nrhs, ld, partial, scal, rn, bn, s));
+            std::vector<double> tol(nrhs), act(nrhs);
+            bool any = false;
+            worst = 0.0;
+            for (int i = 0; i < nrhs; ++i) {
+                double rel = bn[i] > 0 ? rn[i] / bn[i] : 0.0;
+                worst = std::max(worst, rel);
+                tol[i] = rtol * bn[i];
+                act[i] = (rn[i] > tol[i]) ? 1.0 : 0.0;
+                any = any || act[i] != 0.0;
+            }
+            if (!any || total_it >= max_it) break;
+            TDG_TRY(cg_start<double>(op, TDG_FP64, {r64, z64, p64, q64}, nrhs, ld, partial, scal, act, s));
+            int it = 0;
+            TDG_TRY(cg_loop<double>(op, TDG_FP64, x, {r64, z64, p64, q64}, nrhs, ld, partial, scal, tol,
+                                    max_it - total_it, graphs, s, &it, &diverged));
+            total_it += it;
+            if (diverged) break;
+        }
+        if (!diverged) {
+            TDG_TRY(residual64(op, b, x, r64, t64, nrhs, ld, partial, scal, rn, bn, s));
+            worst = 0.0;
+            for (int i = 0; i < nrhs; ++i) worst = std::max(worst, bn[i] > 0 ? rn[i] / bn[i] : 0.0);
+        }
+    } else {
+        float* d32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
+        float* r32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
+        float* z32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
+        float* p32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
+        float* q32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
+        const double inner_rtol = opts->inner_rtol > 0 ? opts->inner_rtol : 1e-4;
+        const int max_outer = opts->max_outer > 0 ? opts->max_outer : 30;
+        for (outer = 0; outer < max_outer; ++outer) {
+            // FP64 residual; scal_out[kRR] = ||r||^2 is the scale of the FP32 correction
+            TDG_TRY(residual64(op, b, x, r64, t64, nrhs, ld, partial, scal_out, rn, bn, s));
+            std::vector<double> act(nrhs), tol(nrhs, inner_rtol);
+            bool any = false;
+            worst = 0.0;
+            for (int i = 0; i < nrhs; ++i) {
+                double rel = bn[i] > 0 ? rn[i] / bn[i] : 0.0;
+                worst = std::max(worst, rel);
+                act[i] = rel > rtol ? 1.0 : 0.0;
+                any = any || act[i] != 0.0;
+            }
+            if (!any || total_it >= max_it) break;
+            // inner problem A d = r / ||r|| in FP32 from d = 0
+            k_scale_convert<double, float><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, r64, ld, r32, scal_out, kRR);
+            k_fill<float><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, d32, 0.0f);
+            TDG_TRY(cg_start<float>(op, TDG_FP32, {r32, z32, p32, q32}, nrhs, ld, partial, scal, act, s));
+            int it = 0;
+            TDG_TRY(cg_loop<float>(op, TDG_FP32, d32, {r32, z32, p32, q32}, nrhs, ld, partial, scal, tol,
+                                   max_it - total_it, graphs, s, &it, &diverged));
+            total_it += it;
+            // x += ||r|| d, only for rhs that were active in this refinement step
+            {
+                std::vector<double> hs(static_cast<size_t>(nrhs) * kScal, 0.0);
+                for (int i = 0; i < nrhs; ++i) hs[static_cast<size_t>(i) * kScal + kActive] = act[i];
+                TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+                k_correct<float><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, x, ld, d32, scal_out, kRR, scal);
+            }
+            if (diverged) break;
+        }
+        stats->outer = outer;
+        if (!diverged && outer == max_outer) {
+            TDG_TRY(residual64(op, b, x, r64, t64, nrhs, ld, partial, scal_out, rn, bn, s));
+            worst = 0.0;
+            for (int i = 0; i < nrhs; ++i) worst = std::max(worst, bn[i] > 0 ? rn[i] / bn[i] : 0.0);
+        }
+    }
+
+    TDG_CUDA_TRY(cudaEventRecord(ev1, s));
+    TDG_CUDA_TRY(cudaEventSynchronize(ev1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    stats->iterations = total_it;
+    stats->rel_residual = worst;
+    stats->seconds = ms * 1e-3;
+    stats->converged = (!diverged && worst <= rtol) ? 1 : 0;
+    if (diverged) return fail(TDG_E_DIVERGED, "non-finite residual in the Krylov iteration");
+    if (!stats->converged) return fail(TDG_E_DIVERGED, "iteration limit reached before the residual target");
+    return 0;
+}

@@ -1,0 +1,85 @@
+// Host-side operator set-up: topology, curvilinear geometry at quadrature points, material
+// projection, facet coefficients and interior-penalty constants.  Produces flat arrays that the
+// device layer uploads unchanged; the device kernels only ever read these arrays.
+#pragma once
+
+#include "refelem.hpp"
+
+#include <cstdint>
+#include <vector>
+
+namespace tdg {
+
+// Per element and local face: the view of one facet from one of its elements (tandem's
+// SideInfo, src/form/FacetInfo.h:11-17).  nb == element itself on a boundary facet.
+struct Side {
+    int32_t fct;
+    int32_t side;      // 0 or 1: which FacetInfo side the element is
+    int32_t nb;        // element on the other side
+    int32_t nb_local;  // local face number of the facet in nb
+    int32_t bc;
+};
+
+struct HostOperator {
+    // sizes
+    int D = 0, N = 0, kind = 0;
+    int Nbf = 0, Q = 0, bs = 0, Nq = 0, nq = 0, nfaces = 0, geoN = 0, Ngeo = 0;
+    int64_t E = 0, F = 0;
+
+    // quadrature
+    Points vol_x, fct_x;          // unit simplex / unit facet coordinates
+    std::vector<double> W, w;     // weights
+
+    // solution space tables (modal for Poisson, nodal warp & blend for Elasticity)
+    RefSpace space, mat_space, geo_space;
+    Dense E_Q;                    // [Nbf][Nq]
+    std::vector<double> Dxi_Q;    // [Nbf][D][Nq]
+    std::vector<Dense> E_qf;      // per local face: [Nbf][nq]
+    std::vector<std::vector<double>> Dxi_qf;  // per local face: [Nbf][D][nq]
+    Dense matE_Q;                 // [Nbf][Nq] material (nodal) basis
+    std::vector<Dense> matE_qf;   // per local face [Nbf][nq]
+
+    // topology
+    std::vector<int64_t> up;      // [F][2]
+    std::vector<int32_t> loc;     // [F][2]
+    std::vector<int32_t> bc;      // [F]
+    std::vector<Side> sides;      // [E][nfaces]
+
+    // geometry (reference layout: G(e, i) = d xi_e / d x_i at each point)
+    std::vector<double> geo_nodes;   // [E][Ngeo][D]
+    std::vector<double> vG;          // [E][D*D][Nq]  index (e*D+i)
+    std::vector<double> vAbsDetJ;    // [E][Nq]
+    std::vector<double> vCoords;     // [E][Nq][D]
+    std::vector<double> volume;      // [E]
+    std::vector<double> fN;          // [F][D][nq] normal (side 0 outward, |detJ| scaled)
+    std::vector<double> fNunit;      // [F][D][nq]
+    std::vector<double> fNl;         // [F][nq]
+    std::vector<double> fG0, fG1;    // [F][D*D][nq]
+    std::vector<double> fCoords;     // [F][nq][D]
+    std::vector<double> area;        // [F]
+
+    // material (after tdg_set_material)
+    bool has_material = false;
+    std::vector<double> mat_nodal;   // [E][2][Nbf]  (Poisson: K, 0; Elasticity: lam, mu)
+    std::vector<double> vCoef;       // [E][ncoef][Nq]  Poisson: J*W*K; Elasticity: lam*W*J, mu*W*J
+    int ncoef = 0;
+    std::vector<double> fCoef;       // Poisson: [F][2][D*D][nq] K*G0, K*G1
+                                     // Elasticity: [F][4][nq] lam0, mu0, lam1, mu1
+    std::vector<double> penalty;     // [F]
+
+    void build(int D, int N, int geoN, int kind, int64_t E, int64_t F, double const* geo_nodes,
+               int64_t const* facet_up, int32_t const* facet_loc, int32_t const* facet_bc,
+               int nvol, double const* vol_x, double const* vol_w, int nfct, double const* fct_x,
+               double const* fct_w);
+    void set_material(double const* c0_Q, double const* c1_Q);
+
+    // Diagonal blocks of the assembled operator, [E][bs][bs] column-major per block
+    // (DGOperator::assemble restricted to A(e, e)).  Host reference used by tests and as the
+    // fallback-free source of truth for the device assembly kernel's layout.
+    void rhs(double const* force_Q, double const* bc_q, double* b) const;
+
+    int64_t flops_apply() const;
+    int64_t bytes_apply(int scalar_bytes) const;
+};
+
+}  // namespace tdg

@@ -1,0 +1,56 @@
+// Shared device-side definitions: operator parameter block and compile-time sizes.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tdg {
+
+constexpr int kPoisson = 0;
+constexpr int kElasticity = 1;
+
+__host__ __device__ constexpr int cbinom(int n, int k) {
+    int r = 1;
+    for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+    return r;
+}
+
+// Compile-time shape of one (dimension, degree, operator) instance.
+template <int D_, int N_, int KIND_>
+struct Shape {
+    static constexpr int D = D_;
+    static constexpr int N = N_;
+    static constexpr int KIND = KIND_;
+    static constexpr int NBF = cbinom(N_ + D_, D_);
+    static constexpr int Q = (KIND_ == kPoisson) ? 1 : D_;
+    static constexpr int BS = NBF * Q;
+    static constexpr int DD = D_ * D_;
+    static constexpr int NF = D_ + 1;
+};
+
+// Device-resident operator data in one precision T (see host/setup.hpp for the meaning of each
+// array; the device copies keep the same index order, plus transposed basis tables so that
+// threads indexed by basis function read contiguous memory).
+template <typename T>
+struct DevOp {
+    int64_t E = 0, F = 0;
+    int Nq = 0, nq = 0;
+    const T* Dxi_Q = nullptr;   // [NBF][D][Nq]
+    const T* DxiT_Q = nullptr;  // [D][Nq][NBF]
+    const T* E_q = nullptr;     // [NF][NBF][nq]
+    const T* ET_q = nullptr;    // [NF][nq][NBF]
+    const T* Dxi_q = nullptr;   // [NF][NBF][D][nq]
+    const T* DxiT_q = nullptr;  // [NF][D][nq][NBF]
+    const T* w = nullptr;       // [nq]
+    const T* vG = nullptr;      // [E][DD][Nq]
+    const T* vCoef = nullptr;   // [E][ncoef][Nq]
+    const T* fN = nullptr;      // [F][D][nq]
+    const T* fNunit = nullptr;  // [F][D][nq]
+    const T* fNl = nullptr;     // [F][nq]
+    const T* fCoef = nullptr;   // Poisson [F][2][DD][nq] (K G0, K G1); Elasticity [F][4][nq]
+    const T* fG = nullptr;      // [F][2][DD][nq] (G0, G1)
+    const double* penalty = nullptr;  // [F], kept in FP64 for every precision
+    const int4* sides = nullptr;      // [E][NF] {fct, side | bc << 8, nb, nb_local}
+};
+
+}  // namespace tdg

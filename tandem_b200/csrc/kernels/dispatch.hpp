@@ -1,0 +1,30 @@
+// Host-side launchers of the device kernels, dispatched from runtime (dim, degree, kind) to the
+// compile-time instances.  Each returns 0 or a TDG_E* code.
+#pragma once
+
+#include "common.cuh"
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tdg {
+
+// Degrees with compiled kernel instances.
+constexpr int kMinDegree = 1;
+constexpr int kMaxDegree = 4;
+
+template <typename T>
+int launch_apply(int D, int N, int kind, DevOp<T> const& op, const T* x, T* y, int nrhs,
+                 int64_t ld, cudaStream_t s);
+int launch_bjac_assemble(int D, int N, int kind, DevOp<double> const& op, double* blk,
+                         cudaStream_t s);
+template <typename T>
+int launch_bjac_invert(int bs, int64_t E, const double* blk, T* inv, int* status, cudaStream_t s);
+template <typename T>
+int launch_bjac_apply(int bs, int64_t E, const T* inv, const T* r, T* z, int nrhs, int64_t ld,
+                      cudaStream_t s);
+
+// Number of resident CTAs of a kernel on the current device times the SM count, cached.
+int device_sm_count();
+
+}  // namespace tdg

@@ -1,0 +1,188 @@
+"""Host-side mirror of tandem's DG operator interface over the C ABI.
+
+``DGOperator`` plays the role of tandem's ``AbstractDGOperator`` / ``DGOperator<LOP>``
+(src/form/AbstractDGOperator.h:18-52): ``block_size``, ``num_local_elements``, ``apply``, ``rhs``,
+the block-Jacobi part of ``assemble``, ``flops_apply``; ``solve`` plays ``PetscLinearSolver``
+(app/common/PetscLinearSolver.cpp) with CG + block Jacobi on the device.  Vectors are torch CUDA
+tensors in tandem's block layout (x[e * bs + k + Nbf * p]); every compute call goes to the native
+library, there is no host fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _ffi
+from .mesh import SimplexMesh
+
+POISSON, ELASTICITY = _ffi.TDG_POISSON, _ffi.TDG_ELASTICITY
+FP64, FP32 = _ffi.TDG_FP64, _ffi.TDG_FP32
+
+
+def _c(a: np.ndarray, dtype) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _stream(stream) -> C.c_void_p:
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(getattr(stream, "cuda_stream", stream))
+
+
+@dataclass
+class Quadrature:
+    """Volume and facet rules on the unit simplex (tandem's volRule / fctRule)."""
+    vol_x: np.ndarray
+    vol_w: np.ndarray
+    fct_x: np.ndarray
+    fct_w: np.ndarray
+
+    @staticmethod
+    def conical(dim: int, order: int) -> "Quadrature":
+        from .refelem import conical_rule
+        vx, vw = conical_rule(dim, order)
+        fx, fw = conical_rule(dim - 1, order)
+        return Quadrature(vx, vw, fx, fw)
+
+
+class DGOperator:
+    def __init__(self, mesh: SimplexMesh, degree: int, kind: int, quad: Quadrature):
+        self.mesh, self.degree, self.kind, self.quad = mesh, degree, kind, quad
+        L = _ffi.lib()
+        D = mesh.dim
+        self._keep = dict(
+            geo=_c(mesh.geo_nodes, np.float64), up=_c(mesh.facet_up, np.int64),
+            loc=_c(mesh.facet_local, np.int32), bc=_c(mesh.facet_bc, np.int32),
+            vx=_c(quad.vol_x, np.float64), vw=_c(quad.vol_w, np.float64),
+            fx=_c(quad.fct_x, np.float64), fw=_c(quad.fct_w, np.float64))
+        k = self._keep
+        desc = _ffi.MeshDesc(D, degree, mesh.geo_degree, 0, mesh.num_elements, mesh.num_facets,
+                             k["geo"].ctypes.data, k["up"].ctypes.data, k["loc"].ctypes.data,
+                             k["bc"].ctypes.data)
+        qd = _ffi.Quadrature(len(k["vw"]), len(k["fw"]), k["vx"].ctypes.data, k["vw"].ctypes.data,
+                             k["fx"].ctypes.data, k["fw"].ctypes.data)
+        h = C.c_void_p()
+        _ffi.check(L.tdg_create(C.byref(desc), C.byref(qd), kind, C.byref(h)))
+        self._h = h
+        sizes = (C.c_int64 * 8)()
+        _ffi.check(L.tdg_sizes(h, sizes))
+        self.bs, self.nbf, self.Q, self.Nq, self.nq, self.E, self.F, self.dim = [int(s) for s in sizes]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _ffi.lib().tdg_destroy(h)
+            self._h = None
+
+    # -- sizes (AbstractDGOperator) --------------------------------------------------------------
+    def block_size(self) -> int:
+        return self.bs
+
+    def num_local_elements(self) -> int:
+        return self.E
+
+    @property
+    def ndof(self) -> int:
+        return self.E * self.bs
+
+    # -- geometry for the caller's functionals -------------------------------------------------
+    def volume_coords(self) -> np.ndarray:
+        out = np.zeros((self.E, self.Nq, self.dim))
+        _ffi.check(_ffi.lib().tdg_volume_coords(self._h, out.ctypes.data))
+        return out
+
+    def facet_coords(self) -> np.ndarray:
+        out = np.zeros((self.F, self.nq, self.dim))
+        _ffi.check(_ffi.lib().tdg_facet_coords(self._h, out.ctypes.data))
+        return out
+
+    def facet_normals(self) -> np.ndarray:
+        out = np.zeros((self.F, self.nq, self.dim))
+        _ffi.check(_ffi.lib().tdg_facet_normals(self._h, out.ctypes.data))
+        return out
+
+    # -- material --------------------------------------------------------------------------------
+    def set_material(self, c0_Q: np.ndarray, c1_Q: np.ndarray | None = None) -> None:
+        a = _c(c0_Q, np.float64).reshape(self.E, self.Nq)
+        b = None if c1_Q is None else _c(c1_Q, np.float64).reshape(self.E, self.Nq)
+        self._mat = (a, b)
+        _ffi.check(_ffi.lib().tdg_set_material(self._h, a.ctypes.data, None if b is None else b.ctypes.data))
+
+    def material_nodal(self, c: int) -> np.ndarray:
+        out = np.zeros((self.E, self.nbf))
+        _ffi.check(_ffi.lib().tdg_material_nodal(self._h, c, out.ctypes.data))
+        return out
+
+    def penalty(self) -> np.ndarray:
+        out = np.zeros(self.F)
+        _ffi.check(_ffi.lib().tdg_penalty(self._h, out.ctypes.data))
+        return out
+
+    # -- hot path --------------------------------------------------------------------------------
+    def apply(self, x, y, precision: int = FP64, nrhs: int = 1, ld: int | None = None, stream=None) -> None:
+        """y = A x on the device (PetscDGShell::apply)."""
+        ld = self.ndof if ld is None else ld
+        _check_vec(x, precision, nrhs * ld)
+        _check_vec(y, precision, nrhs * ld)
+        _ffi.check(_ffi.lib().tdg_apply(self._h, precision, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                        nrhs, ld, _stream(stream)))
+
+    def flops_apply(self) -> int:
+        return int(_ffi.lib().tdg_flops_apply(self._h))
+
+    def bytes_apply(self, precision: int = FP64) -> int:
+        return int(_ffi.lib().tdg_bytes_apply(self._h, precision))
+
+    def bjacobi_setup(self, precision: int = FP64, stream=None) -> None:
+        _ffi.check(_ffi.lib().tdg_bjacobi_setup(self._h, precision, _stream(stream)))
+
+    def bjacobi_apply(self, r, z, precision: int = FP64, nrhs: int = 1, ld: int | None = None, stream=None) -> None:
+        ld = self.ndof if ld is None else ld
+        _check_vec(r, precision, nrhs * ld)
+        _check_vec(z, precision, nrhs * ld)
+        _ffi.check(_ffi.lib().tdg_bjacobi_apply(self._h, precision, C.c_void_p(r.data_ptr()),
+                                                C.c_void_p(z.data_ptr()), nrhs, ld, _stream(stream)))
+
+    def bjacobi_blocks(self) -> np.ndarray:
+        out = np.zeros((self.E, self.bs, self.bs))
+        _ffi.check(_ffi.lib().tdg_bjacobi_blocks(self._h, out.ctypes.data))
+        # stored column-major per block: out[e, col, row] -> transpose to [e, row, col]
+        return np.ascontiguousarray(out.transpose(0, 2, 1))
+
+    def rhs(self, force_Q: np.ndarray | None = None, bc_q: np.ndarray | None = None) -> np.ndarray:
+        """Right-hand side (DGOperator::rhs): force_Q [E, Q, Nq], bc_q [F, Q, nq]."""
+        b = np.zeros(self.ndof)
+        f = None if force_Q is None else _c(force_Q, np.float64).reshape(self.E, self.Q, self.Nq)
+        g = None if bc_q is None else _c(bc_q, np.float64).reshape(self.F, self.Q, self.nq)
+        _ffi.check(_ffi.lib().tdg_rhs(self._h, None if f is None else f.ctypes.data,
+                                      None if g is None else g.ctypes.data, b.ctypes.data))
+        return b
+
+    def solve(self, b, x, precision: int = FP64, rtol: float = 1e-10, max_iterations: int = 20000,
+              inner_rtol: float = 1e-4, max_outer: int = 40, use_graphs: bool = True, nrhs: int = 1,
+              ld: int | None = None, stream=None) -> dict:
+        """Block-Jacobi preconditioned CG on the device (FP64, or FP32 inner CG in FP64
+        iterative refinement).  Raises on non-convergence."""
+        ld = self.ndof if ld is None else ld
+        _check_vec(b, FP64, nrhs * ld)
+        _check_vec(x, FP64, nrhs * ld)
+        opts = _ffi.SolveOpts(precision, max_iterations, rtol, inner_rtol, max_outer, int(use_graphs))
+        st = _ffi.SolveStats()
+        rc = _ffi.lib().tdg_solve(self._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), nrhs, ld,
+                                  C.byref(opts), C.byref(st), _stream(stream))
+        stats = dict(iterations=st.iterations, outer=st.outer, rel_residual=st.rel_residual,
+                     seconds=st.seconds, converged=bool(st.converged))
+        if rc != 0:
+            raise _ffi.TdgError(f"{_ffi.ERRORS.get(rc, rc)}: {_ffi.lib().tdg_last_error().decode()} {stats}")
+        return stats
+
+
+def _check_vec(t, precision: int, n: int) -> None:
+    import torch
+    want = torch.float64 if precision == FP64 else torch.float32
+    if not (t.is_cuda and t.dtype == want and t.is_contiguous() and t.numel() >= n):
+        raise ValueError(f"expected a contiguous CUDA {want} tensor with >= {n} entries, got "
+                         f"{t.dtype} device={t.device} numel={t.numel()}")

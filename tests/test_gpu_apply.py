@@ -1,0 +1,170 @@
+"""Device apply, block Jacobi and solve against the oracle (CPU restatement of tandem).
+
+Tolerances: FP64 results agree with the oracle to 1e-12 relative (max-norm over the vector,
+summation order differs); FP32 applies to 2e-5 relative; solutions to the relative residual
+target 1e-10 of the metric."""
+import numpy as np
+import pytest
+import torch
+
+from cases import make_mesh, mms_inputs, product_and_oracle, tandem_quadrature
+from oracle import Oracle
+from tandem_b200 import _ffi
+from tandem_b200 import mesh as M
+from tandem_b200.operator import DGOperator, ELASTICITY, FP32, FP64, POISSON
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+
+CASES = [
+    # kind, dim, n, degree, curved, variable
+    (POISSON, 2, 4, 4, False, False),
+    (POISSON, 2, 3, 1, True, True),
+    (POISSON, 2, 3, 2, True, True),
+    (POISSON, 2, 3, 3, False, True),
+    (POISSON, 3, 2, 4, True, True),
+    (POISSON, 3, 2, 2, False, True),
+    (ELASTICITY, 2, 3, 4, True, True),
+    (ELASTICITY, 2, 3, 1, False, False),
+    (ELASTICITY, 3, 2, 4, True, True),
+    (ELASTICITY, 3, 2, 3, True, True),
+    (ELASTICITY, 3, 1, 1, False, True),
+]
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def dev(x, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype, device=DEV)
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "k{}d{}n{}p{}c{}v{}".format(*c))
+def test_apply_fp64_matches_oracle(case):
+    kind, dim, n, N, curved, var = case
+    _, op, orc = product_and_oracle(kind, dim, n, N, curved, var)
+    x = np.random.default_rng(7).standard_normal(op.ndof)
+    y = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+    op.apply(dev(x), y)
+    torch.cuda.synchronize()
+    assert rel(y.cpu().numpy(), orc.apply(x)) < 1e-12
+
+
+@pytest.mark.parametrize("case", CASES[::2], ids=lambda c: "k{}d{}n{}p{}c{}v{}".format(*c))
+def test_apply_fp32_close_to_oracle(case):
+    kind, dim, n, N, curved, var = case
+    _, op, orc = product_and_oracle(kind, dim, n, N, curved, var)
+    x = np.random.default_rng(8).standard_normal(op.ndof)
+    y = torch.zeros(op.ndof, dtype=torch.float32, device=DEV)
+    op.apply(dev(x, torch.float32), y, precision=FP32)
+    torch.cuda.synchronize()
+    ref = orc.apply(x.astype(np.float32).astype(np.float64))
+    assert np.linalg.norm(y.cpu().numpy() - ref) / np.linalg.norm(ref) < 2e-5
+
+
+def test_multi_rhs_apply_equals_single():
+    _, op, orc = product_and_oracle(ELASTICITY, 3, 2, 4, True, True)
+    nrhs, ld = 3, op.ndof + 37
+    X = torch.randn(nrhs, ld, dtype=torch.float64, device=DEV)
+    Y = torch.zeros(nrhs, ld, dtype=torch.float64, device=DEV)
+    op.apply(X, Y, nrhs=nrhs, ld=ld)
+    for r in range(nrhs):
+        y = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+        op.apply(X[r, :op.ndof].contiguous(), y)
+        assert torch.equal(y, Y[r, :op.ndof])
+        assert torch.all(Y[r, op.ndof:] == 0)
+
+
+@pytest.mark.parametrize("kind,dim,curved", [(POISSON, 2, False), (ELASTICITY, 2, True), (ELASTICITY, 3, True),
+                                              (POISSON, 3, True)])
+def test_block_jacobi_blocks_and_apply(kind, dim, curved):
+    _, op, orc = product_and_oracle(kind, dim, 3 if dim == 2 else 2, 4, curved, True)
+    op.bjacobi_setup(FP64)
+    blocks = op.bjacobi_blocks()
+    ref = orc.assemble_diag()
+    assert rel(blocks, ref) < 1e-12
+    r = np.random.default_rng(3).standard_normal(op.ndof)
+    z = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+    op.bjacobi_apply(dev(r), z)
+    torch.cuda.synchronize()
+    zr = np.concatenate([np.linalg.solve(ref[e], r[e * op.bs:(e + 1) * op.bs]) for e in range(op.E)])
+    assert rel(z.cpu().numpy(), zr) < 1e-10
+    op.bjacobi_setup(FP32)
+    z32 = torch.zeros(op.ndof, dtype=torch.float32, device=DEV)
+    op.bjacobi_apply(dev(r, torch.float32), z32, precision=FP32)
+    torch.cuda.synchronize()
+    assert np.linalg.norm(z32.cpu().numpy() - zr) / np.linalg.norm(zr) < 1e-4
+
+
+def test_not_spd_block_is_reported():
+    m = make_mesh(2, 2, 2)
+    op = DGOperator(m, 2, ELASTICITY, tandem_quadrature(2, 2))
+    X = op.volume_coords()
+    op.set_material(2.0 * np.ones(X.shape[:2]), -np.ones(X.shape[:2]))
+    with pytest.raises(_ffi.TdgError, match="TDG_E_NOT_SPD"):
+        op.bjacobi_setup(FP64)
+
+
+@pytest.mark.parametrize("kind,dim,n,curved", [(POISSON, 2, 8, False), (ELASTICITY, 2, 4, True),
+                                                (ELASTICITY, 3, 2, True)])
+@pytest.mark.parametrize("precision", [FP64, FP32])
+def test_solve_matches_oracle(kind, dim, n, curved, precision):
+    m, op, orc = product_and_oracle(kind, dim, n, 4, curved, True)
+    sc, c0, c1, f, g = mms_inputs(op, kind, dim, True)
+    b = op.rhs(f, g)
+    xo, st_o = orc.cg(b, rtol=1e-12)
+    op.bjacobi_setup(precision)
+    x = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+    st = op.solve(dev(b), x, precision=precision, rtol=1e-10)
+    assert st["converged"] and st["rel_residual"] <= 1e-10, st
+    xs = x.cpu().numpy()
+    # true FP64 residual through the oracle
+    assert np.linalg.norm(b - orc.apply(xs)) / np.linalg.norm(b) <= 1.5e-10
+    assert np.linalg.norm(xs - xo) / np.linalg.norm(xo) < 1e-7
+
+
+def test_config1_full_size_apply():
+    """configs[0] at full size: 64 x 64 x 2 triangles, degree 4, 122,880 DOF."""
+    m = make_mesh(2, 64, 4)
+    q = tandem_quadrature(2, 4)
+    op = DGOperator(m, 4, POISSON, q)
+    orc = Oracle(m, 4, POISSON, q)
+    K = np.ones((op.E, op.Nq))
+    op.set_material(K)
+    orc.set_material(K)
+    x = np.random.default_rng(11).standard_normal(op.ndof)
+    y = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+    op.apply(dev(x), y)
+    torch.cuda.synchronize()
+    assert rel(y.cpu().numpy(), orc.apply(x)) < 1e-12
+
+
+def test_elasticity_3d_properties_at_scale():
+    """Size-independent properties on a 12^3 x 6 curved mesh (10,368 tets, 1.1 M DOF): symmetry
+    x.Ay = y.Ax, translations annihilated up to boundary terms only, and a slice of elements
+    against the oracle."""
+    m = make_mesh(3, 12, 4, True)
+    q = tandem_quadrature(3, 4)
+    op = DGOperator(m, 4, ELASTICITY, q)
+    orc = Oracle(m, 4, ELASTICITY, q)
+    from cases import material
+    c0, c1 = material(ELASTICITY, 3, op.volume_coords(), True, ell=0.2)
+    op.set_material(c0, c1)
+    orc.set_material(c0, c1)
+    g = torch.Generator(device=DEV).manual_seed(5)
+    x = torch.randn(op.ndof, dtype=torch.float64, device=DEV, generator=g)
+    z = torch.randn(op.ndof, dtype=torch.float64, device=DEV, generator=g)
+    ax = torch.empty_like(x)
+    az = torch.empty_like(x)
+    op.apply(x, ax)
+    op.apply(z, az)
+    torch.cuda.synchronize()
+    s1, s2 = torch.dot(z, ax).item(), torch.dot(x, az).item()
+    assert abs(s1 - s2) <= 1e-12 * (torch.norm(z) * torch.norm(ax)).item()
+    xn = x.cpu().numpy()
+    yref = np.zeros(op.ndof)
+    e0, e1 = 3000, 3400
+    orc.apply_range(e0, e1, xn, yref)
+    bs = op.bs
+    assert rel(ax.cpu().numpy()[e0 * bs:e1 * bs], yref[e0 * bs:e1 * bs]) < 1e-12
