@@ -174,6 +174,30 @@ typedef struct {
 int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64_t ld,
               const tdg_solve_opts* opts, tdg_solve_stats* stats, void* stream);
 
+/* --- fault coupling, Green's functions (app/form/SeasQDDiscreteGreenOperator.cpp:493-578) ---- */
+
+typedef struct tdg_fault tdg_fault;
+
+/* Prepares the fault facets as tandem's AdapterBase::prepare does
+ * (app/localoperator/AdapterBase.cpp:44-99): oriented facet normals (flipped where they point
+ * against ref_normal), fault mass matrices of the nodal degree-N fault basis and their inverses.
+ * fault_facets lists facet numbers (BoundaryMap order).  Poisson operators only; the operator must
+ * outlive the fault object. */
+int tdg_fault_create(tdg_op* op, int64_t num_fault, const int64_t* fault_facets, const double* ref_normal,
+                     tdg_fault** out);
+void tdg_fault_destroy(tdg_fault* fault);
+/* out[0] = fault facets, out[1] = fault basis functions per facet. */
+int tdg_fault_sizes(const tdg_fault* fault, int64_t out[2]);
+/* b += right-hand side of the slip (Adapter::slip + Poisson::rhs_skeleton/boundary).  slip:
+ * device [nrhs][ld_slip] with ld_slip >= num_fault * nbf; b: device [nrhs][ld]. */
+int tdg_fault_slip_rhs(tdg_fault* fault, const double* slip, int64_t ld_slip, double* b, int nrhs, int64_t ld,
+                       void* stream);
+/* traction = fault-basis traction of (u, slip) (Poisson::traction_skeleton/boundary +
+ * Adapter<Poisson>::traction).  u: device [nrhs][ld]; slip may be NULL (zero slip); traction:
+ * device [nrhs][ld_t] with ld_t >= num_fault * nbf. */
+int tdg_fault_traction(tdg_fault* fault, const double* u, int64_t ld, const double* slip, int64_t ld_slip,
+                       double* traction, int64_t ld_t, int nrhs, void* stream);
+
 /* --- host utilities: reference-element tables (no device work) ---------------------------- */
 
 /* Reference nodes of degree N on the unit simplex: family 0 = warp & blend

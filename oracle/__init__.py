@@ -39,6 +39,8 @@ def lib() -> C.CDLL:
             "orc_cg": (C.c_int, [_p, _p, _p, C.c_double, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
             "orc_error_L2": (C.c_double, [_p, _p, _p]),
             "orc_error_H1_semi": (C.c_double, [_p, _p, _p]),
+            "orc_fault_slip_q": (None, [_p, C.c_long, _p, _p, _p, C.c_int, _p, _p]),
+            "orc_fault_traction": (None, [_p, C.c_long, _p, _p, _p, C.c_int, _p, _p, _p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -181,6 +183,33 @@ class Oracle:
         rc = lib().orc_cg(self._h, np.ascontiguousarray(b).ctypes.data, x.ctypes.data, rtol, maxit,
                           C.byref(it), C.byref(rel))
         return x, dict(iterations=it.value, rel_residual=rel.value, converged=rc == 0)
+
+    def fault_basis(self):
+        """tandem's fault space (nodal warp & blend of degree N on the facet) at the facet points."""
+        from tandem_b200.refelem import WARP_BLEND, ref_basis
+        fx = np.asarray(self._keep["fx"]).reshape(-1, self.dim - 1)
+        return np.ascontiguousarray(ref_basis(self.dim - 1, self.degree, WARP_BLEND, fx))
+
+    def fault_slip_q(self, facets, ref_normal, slip):
+        e = self.fault_basis()
+        f = np.ascontiguousarray(facets, dtype=np.int64)
+        r = np.ascontiguousarray(ref_normal, dtype=np.float64)
+        sl = np.ascontiguousarray(slip, dtype=np.float64)
+        out = np.zeros((self.F, 1, self.nq))
+        lib().orc_fault_slip_q(self._h, len(f), f.ctypes.data, r.ctypes.data, e.ctypes.data, e.shape[0],
+                               sl.ctypes.data, out.ctypes.data)
+        return out
+
+    def fault_traction(self, facets, ref_normal, u, slip):
+        e = self.fault_basis()
+        f = np.ascontiguousarray(facets, dtype=np.int64)
+        r = np.ascontiguousarray(ref_normal, dtype=np.float64)
+        sl = np.ascontiguousarray(slip, dtype=np.float64)
+        uu = np.ascontiguousarray(u, dtype=np.float64)
+        out = np.zeros((len(f), e.shape[0]))
+        lib().orc_fault_traction(self._h, len(f), f.ctypes.data, r.ctypes.data, e.ctypes.data, e.shape[0],
+                                 uu.ctypes.data, sl.ctypes.data, out.ctypes.data)
+        return out
 
     def error_L2(self, x: np.ndarray, ref_Q: np.ndarray) -> float:
         r = np.ascontiguousarray(ref_Q, dtype=np.float64)

@@ -965,3 +965,107 @@ double orc_error_H1_semi(orc_op const* op, const double* x, const double* refgra
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Fault adapter (Poisson): AdapterBase::prepare (app/localoperator/AdapterBase.cpp:44-99),
+// Adapter<Poisson>::slip / traction (app/localoperator/PoissonAdapter.cpp:22-55),
+// Poisson::traction_skeleton / traction_boundary (Poisson.cpp:678-723, kernels grad_u /
+// grad_u_bnd of app/kernels/poisson.py:146-152, evaluate_slip / evaluate_traction of
+// poisson_adapter.py:13-23).
+// ---------------------------------------------------------------------------------------------
+
+extern "C" {
+
+// slip_q on the fault facets: bc_q [F][nq] (zero elsewhere).  slip [nfault][nbf]; e_q [nbf][nq]
+// is the fault basis at the facet points (passed in; computed by the caller from tandem's nodal
+// warp & blend fault space).
+void orc_fault_slip_q(orc_op const* op, long nfault, const long* facets, const double* ref_normal, const double* e_q,
+                      int nbf, const double* slip, double* bc_q) {
+    const int D = op->D, nq = op->nq;
+    std::fill(bc_q, bc_q + static_cast<size_t>(op->F) * nq, 0.0);
+    for (long i = 0; i < nfault; ++i) {
+        const long fc = facets[i];
+        for (int q = 0; q < nq; ++q) {
+            double dot = 0.0;
+            for (int d = 0; d < D; ++d) dot += ref_normal[d] * op->Normal[(static_cast<size_t>(fc) * nq + q) * D + d];
+            double s = 0.0;
+            for (int p = 0; p < nbf; ++p) s += e_q[p * nq + q] * slip[i * nbf + p];
+            bc_q[static_cast<size_t>(fc) * nq + q] = dot < 0 ? -s : s;
+        }
+    }
+}
+
+// traction [nfault][nbf] of displacement u and slip [nfault][nbf].
+void orc_fault_traction(orc_op const* op, long nfault, const long* facets, const double* ref_normal, const double* e_q,
+                        int nbf, const double* u, const double* slip, double* traction) {
+    const int D = op->D, nq = op->nq, nbfe = op->Nbf, DD = D * D;
+    for (long i = 0; i < nfault; ++i) {
+        const long fc = facets[i];
+        FacetInfo const& fi = op->fct[fc];
+        const bool boundary = fi.up[0] == fi.up[1];
+        // AdapterBase::prepare: oriented normal, its length and the fault mass matrix
+        std::vector<double> n(static_cast<size_t>(nq) * D), nl(nq), fq(nq);
+        for (int q = 0; q < nq; ++q) {
+            double dot = 0.0, n2 = 0.0;
+            for (int d = 0; d < D; ++d) {
+                const double v = op->Normal[(static_cast<size_t>(fc) * nq + q) * D + d];
+                dot += ref_normal[d] * v;
+                n2 += v * v;
+            }
+            nl[q] = std::sqrt(n2);
+            for (int d = 0; d < D; ++d)
+                n[q * D + d] = (dot < 0 ? -1.0 : 1.0) * op->Normal[(static_cast<size_t>(fc) * nq + q) * D + d];
+            double s = 0.0;
+            for (int p = 0; p < nbf; ++p) s += e_q[p * nq + q] * slip[i * nbf + p];
+            fq[q] = (dot < 0 ? -s : s) * (boundary ? 0.5 : 1.0);  // Adapter::slip sign, bc_boundary halving
+        }
+        Dense m(nbf, nbf);
+        for (int a = 0; a < nbf; ++a)
+            for (int b = 0; b < nbf; ++b) {
+                double s = 0.0;
+                for (int q = 0; q < nq; ++q) s += op->w[q] * nl[q] * e_q[a * nq + q] * e_q[b * nq + q];
+                m(a, b) = s;
+            }
+        Dense mi = tdg::invert(m);
+        // grad_u(p, q) = 1/2 (K_Dx_q0 u0 + K_Dx_q1 u1) + c00 (E_q0 u0 - E_q1 u1 - f_q) n_unit, c00 = -penalty
+        std::vector<double> tq(nq);
+        const double c00 = -op->penalty[fc];
+        for (int q = 0; q < nq; ++q) {
+            double grad[3] = {0.0, 0.0, 0.0};
+            double ev[2] = {0.0, 0.0};
+            for (int s = 0; s < (boundary ? 1 : 2); ++s) {
+                const double* us = u + static_cast<size_t>(fi.up[s]) * op->bs;
+                auto const& Eq = op->E_q[fi.localNo[s]];
+                auto const& Dq = op->Dxi_q[fi.localNo[s]];
+                const double* KG = &(s == 0 ? op->KG0 : op->KG1)[(static_cast<size_t>(fc) * nq + q) * DD];
+                for (int l = 0; l < nbfe; ++l) {
+                    ev[s] += Eq[l + static_cast<size_t>(nbfe) * q] * us[l];
+                    for (int p = 0; p < D; ++p) {
+                        double kd = 0.0;
+                        for (int e = 0; e < D; ++e) kd += KG[e + D * p] * Dq[idx3(l, e, q, nbfe, D)];
+                        grad[p] += (boundary ? 1.0 : 0.5) * kd * us[l];
+                    }
+                }
+            }
+            const double jump = boundary ? (ev[0] - fq[q]) : (ev[0] - ev[1] - fq[q]);
+            double gn = 0.0;
+            for (int p = 0; p < D; ++p) {
+                const double g = grad[p] + c00 * jump * op->UnitNormal[(static_cast<size_t>(fc) * nq + q) * D + p];
+                gn += g * n[q * D + p];
+            }
+            tq[q] = op->w[q] * gn;
+        }
+        // evaluate_traction: traction(p) = minv(r, p) e_q_T(q, r) w(q) grad_u(k, q) n_q(k, q)
+        for (int p = 0; p < nbf; ++p) {
+            double t = 0.0;
+            for (int r = 0; r < nbf; ++r) {
+                double a = 0.0;
+                for (int q = 0; q < nq; ++q) a += e_q[r * nq + q] * tq[q];
+                t += mi(r, p) * a;
+            }
+            traction[i * nbf + p] = t;
+        }
+    }
+}
+
+}  // extern "C"

@@ -38,6 +38,11 @@ SYMBOLS = {
     "tdg_bjacobi_blocks": (C.c_int, [_p, _p]),
     "tdg_rhs": (C.c_int, [_p, _p, _p, _p]),
     "tdg_solve": (C.c_int, [_p, _p, _p, C.c_int, _i64, _p, _p, _p]),
+    "tdg_fault_create": (C.c_int, [_p, _i64, _p, _p, C.POINTER(_p)]),
+    "tdg_fault_destroy": (None, [_p]),
+    "tdg_fault_sizes": (C.c_int, [_p, _p]),
+    "tdg_fault_slip_rhs": (C.c_int, [_p, _p, _i64, _p, C.c_int, _i64, _p]),
+    "tdg_fault_traction": (C.c_int, [_p, _p, _i64, _p, _i64, _p, _i64, C.c_int, _p]),
     "tdg_ref_nodes": (C.c_int, [C.c_int, C.c_int, C.c_int, _p]),
     "tdg_ref_basis": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _p, _p, _p]),
     "tdg_conical_rule": (C.c_int, [C.c_int, C.c_int, _p, _p]),

@@ -2,12 +2,17 @@
 // block-Jacobi and the device Krylov drivers.
 #include "../../include/tandem_b200.h"
 #include "host/setup.hpp"
+#include "kernels/apply_mma.cuh"
 #include "kernels/dispatch.hpp"
 #include "kernels/krylov.cuh"
 
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <type_traits>
 #include <cstring>
 #include <exception>
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -120,6 +125,8 @@ struct tdg_op {
     DevArena arena64, arena32, arena_common, arena_pc, arena_ws;
     DevOp<double> op64;
     DevOp<float> op32;
+    MmaTiles mma;           // FP64 tensor-pipe apply: packed tables and signature tiles
+    bool use_mma = true;
     const double* penalty = nullptr;
     const int4* sides = nullptr;
     // block-Jacobi
@@ -144,6 +151,53 @@ int upload_common(tdg_op* op) {
         sides[i] = make_int4(s.fct, s.side | (s.bc << 8), s.nb, s.nb_local);
     }
     TDG_CUDA_TRY(op->arena_common.upload(&op->sides, sides));
+    return 0;
+}
+
+// Tables of the FP64 tensor-pipe apply in its shared-memory layout (apply_mma.cuh): TV[m][k] with
+// m = q * D + e the reference derivative e of basis k at volume point q; TF[f][m][k] the same at
+// the facet points of local face f followed by the basis values.  Leading dimension mma_ld(MY).
+// Tiles group elements by their neighbour-face signature (nb_local per face, 2 bits each).
+int upload_mma(tdg_op* op, DevArena& arena) {
+    auto const& h = op->h;
+    const int D = h.D, NBF = h.Nbf, Nq = h.Nq, nq = h.nq, NF = h.nfaces;
+    const int MY = (NBF + 7) / 8 * 8, LDT = mma_ld(MY);
+    const int MV = round8(D * Nq), MF = round8((D + 1) * nq);
+    std::vector<double> tab(static_cast<size_t>(MV) * LDT + static_cast<size_t>(NF) * MF * LDT, 0.0);
+    for (int q = 0; q < Nq; ++q)
+        for (int e = 0; e < D; ++e)
+            for (int k = 0; k < NBF; ++k)
+                tab[static_cast<size_t>(q * D + e) * LDT + k] = h.Dxi_Q[(static_cast<size_t>(k) * D + e) * Nq + q];
+    for (int f = 0; f < NF; ++f) {
+        double* T = &tab[static_cast<size_t>(MV) * LDT + static_cast<size_t>(f) * MF * LDT];
+        for (int q = 0; q < nq; ++q)
+            for (int k = 0; k < NBF; ++k) {
+                for (int e = 0; e < D; ++e)
+                    T[static_cast<size_t>(q * D + e) * LDT + k] = h.Dxi_qf[f][(static_cast<size_t>(k) * D + e) * nq + q];
+                T[static_cast<size_t>(D * nq + q) * LDT + k] = h.E_qf[f](k, q);
+            }
+    }
+    const int TE = mma_tile_elements(h.Q);
+    std::vector<int> sig(h.E), perm(h.E);
+    for (int64_t e = 0; e < h.E; ++e) {
+        int sg = 0;
+        for (int f = 0; f < NF; ++f) sg |= (h.sides[static_cast<size_t>(e) * NF + f].nb_local & 3) << (2 * f);
+        sig[e] = sg;
+        perm[e] = static_cast<int>(e);
+    }
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return sig[a] < sig[b]; });
+    std::vector<int4> tiles;
+    for (int64_t i = 0; i < h.E;) {
+        int64_t j = i;
+        while (j < h.E && j - i < TE && sig[perm[j]] == sig[perm[i]]) ++j;
+        tiles.push_back(make_int4(static_cast<int>(i), static_cast<int>(j - i), sig[perm[i]], 0));
+        i = j;
+    }
+    TDG_CUDA_TRY(arena.upload(&op->mma.tables, tab));
+    TDG_CUDA_TRY(arena.upload(&op->mma.perm, perm));
+    TDG_CUDA_TRY(arena.upload(&op->mma.tiles, tiles));
+    op->mma.ntiles = static_cast<int>(tiles.size());
+    op->mma.table_doubles = static_cast<int>(tab.size());
     return 0;
 }
 
@@ -199,6 +253,7 @@ int upload_precision(tdg_op* op, DevArena& arena, DevOp<T>& d) {
     }
     d.penalty = op->penalty;
     d.sides = op->sides;
+    if constexpr (std::is_same_v<T, double>) TDG_TRY(upload_mma(op, arena));
     TDG_CUDA_TRY(cudaDeviceSynchronize());
     return 0;
 }
@@ -269,6 +324,8 @@ int tdg_create(const tdg_mesh_desc* mesh, const tdg_quadrature* quad, int kind, 
         return fail(TDG_E_INVALID, "degree outside the compiled range [1, 4]");
     try {
         auto* op = new tdg_op();
+        const char* kv = std::getenv("TDG_APPLY_KERNEL");
+        op->use_mma = !(kv && std::string(kv) == "simt");
         op->h.build(mesh->dim, mesh->degree, mesh->geo_degree, kind, mesh->num_elements, mesh->num_facets,
                     mesh->geo_nodes, mesh->facet_up, mesh->facet_local_no, mesh->facet_bc,
                     quad->num_vol_points, quad->vol_points, quad->vol_weights, quad->num_fct_points,
@@ -363,11 +420,14 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
     if (x == y) return fail(TDG_E_INVALID, "x and y must not alias");
     TDG_TRY(ensure_uploaded(op, precision));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int rc;
-    if (precision == TDG_FP64)
+    int rc = TDG_E_INVALID;
+    if (precision == TDG_FP64 && op->use_mma)
+        rc = launch_apply_mma(h.D, h.N, h.kind, op->op64, op->mma, static_cast<const double*>(x),
+                              static_cast<double*>(y), nrhs, ld, s);
+    if (precision == TDG_FP64 && rc == TDG_E_INVALID)
         rc = launch_apply<double>(h.D, h.N, h.kind, op->op64, static_cast<const double*>(x),
                                   static_cast<double*>(y), nrhs, ld, s);
-    else
+    else if (precision == TDG_FP32)
         rc = launch_apply<float>(h.D, h.N, h.kind, op->op32, static_cast<const float*>(x),
                                  static_cast<float*>(y), nrhs, ld, s);
     if (rc) return fail(rc, std::string("apply launch failed: ") + cudaGetErrorString(cudaGetLastError()));
@@ -769,4 +829,119 @@ extern "C" int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64
     if (diverged) return fail(TDG_E_DIVERGED, "non-finite residual in the Krylov iteration");
     if (!stats->converged) return fail(TDG_E_DIVERGED, "iteration limit reached before the residual target");
     return 0;
+}
+
+// ------------------------------------------------------------------------------------------------
+// fault coupling (Green's functions)
+// ------------------------------------------------------------------------------------------------
+
+#include "kernels/fault.cuh"
+
+struct tdg_fault {
+    tdg_op* op = nullptr;
+    DevArena arena;
+    DevFault d;
+};
+
+extern "C" int tdg_fault_create(tdg_op* op, int64_t num_fault, const int64_t* fault_facets, const double* ref_normal,
+                                tdg_fault** out) {
+    if (!op || !fault_facets || !ref_normal || !out || num_fault < 1) return fail(TDG_E_INVALID, "bad argument");
+    auto const& h = op->h;
+    if (h.kind != 0) return fail(TDG_E_INVALID, "fault coupling is implemented for the Poisson operator");
+    if (!h.has_material) return fail(TDG_E_STATE, "tdg_set_material has not been called");
+    const int D = h.D, nq = h.nq;
+    if (nq > kFaultMaxQ) return fail(TDG_E_INVALID, "too many facet quadrature points for the fault kernels");
+    try {
+        // fault basis: nodal warp & blend of degree N on the (D-1)-simplex (RateAndStateBase::Space)
+        RefSpace fs = RefSpace::nodal(D - 1, h.N, warp_blend_nodes(D - 1, h.N));
+        const int nbf = fs.num_basis();
+        Dense eq = fs.eval(h.fct_x);  // [nbf][nq]
+        std::vector<double> e_q(eq.a.begin(), eq.a.end());
+        std::vector<int4> info(num_fault);
+        std::vector<double> sign(static_cast<size_t>(num_fault) * nq), normal(static_cast<size_t>(num_fault) * D * nq);
+        std::vector<double> minv(static_cast<size_t>(num_fault) * nbf * nbf);
+        for (int64_t i = 0; i < num_fault; ++i) {
+            const int64_t f = fault_facets[i];
+            if (f < 0 || f >= h.F) return fail(TDG_E_INVALID, "fault facet out of range");
+            info[i] = make_int4(static_cast<int>(f), static_cast<int>(h.up[2 * f]), static_cast<int>(h.up[2 * f + 1]),
+                                h.loc[2 * f] | (h.loc[2 * f + 1] << 8));
+            std::vector<double> nl(nq);
+            for (int q = 0; q < nq; ++q) {
+                double dot = 0.0, n2 = 0.0;
+                for (int d = 0; d < D; ++d) {
+                    const double v = h.fN[(static_cast<size_t>(f) * D + d) * nq + q];
+                    dot += ref_normal[d] * v;
+                    n2 += v * v;
+                }
+                if (std::fabs(dot) < 10000.0 * std::numeric_limits<double>::epsilon())
+                    return fail(TDG_E_INVALID, "fault normal and reference normal are almost perpendicular");
+                const double s = dot < 0 ? -1.0 : 1.0;
+                sign[static_cast<size_t>(i) * nq + q] = s;
+                for (int d = 0; d < D; ++d)
+                    normal[(static_cast<size_t>(i) * D + d) * nq + q] = s * h.fN[(static_cast<size_t>(f) * D + d) * nq + q];
+                nl[q] = std::sqrt(n2);
+            }
+            Dense m(nbf, nbf);
+            for (int a = 0; a < nbf; ++a)
+                for (int b = 0; b < nbf; ++b) {
+                    double s = 0.0;
+                    for (int q = 0; q < nq; ++q) s += h.w[q] * nl[q] * eq(a, q) * eq(b, q);
+                    m(a, b) = s;
+                }
+            Dense mi = invert(m);
+            std::copy(mi.a.begin(), mi.a.end(), &minv[static_cast<size_t>(i) * nbf * nbf]);
+        }
+        TDG_TRY(ensure_uploaded(op, TDG_FP64));
+        auto* fl = new tdg_fault();
+        fl->op = op;
+        fl->d.nfault = static_cast<int>(num_fault);
+        fl->d.nbf = nbf;
+        cudaError_t e = cudaSuccess;
+        if (e == cudaSuccess) e = fl->arena.upload(&fl->d.info, info);
+        if (e == cudaSuccess) e = fl->arena.upload(&fl->d.sign, sign);
+        if (e == cudaSuccess) e = fl->arena.upload(&fl->d.normal, normal);
+        if (e == cudaSuccess) e = fl->arena.upload(&fl->d.minv, minv);
+        if (e == cudaSuccess) e = fl->arena.upload(&fl->d.e_q, e_q);
+        if (e != cudaSuccess) {
+            delete fl;
+            return fail(TDG_E_CUDA, std::string("fault upload: ") + cudaGetErrorString(e));
+        }
+        *out = fl;
+        return 0;
+    } catch (std::exception const& ex) {
+        return fail(TDG_E_INVALID, ex.what());
+    }
+}
+
+extern "C" void tdg_fault_destroy(tdg_fault* fault) { delete fault; }
+
+extern "C" int tdg_fault_sizes(const tdg_fault* fault, int64_t out[2]) {
+    if (!fault || !out) return fail(TDG_E_INVALID, "null argument");
+    out[0] = fault->d.nfault;
+    out[1] = fault->d.nbf;
+    return 0;
+}
+
+extern "C" int tdg_fault_slip_rhs(tdg_fault* fault, const double* slip, int64_t ld_slip, double* b, int nrhs,
+                                  int64_t ld, void* stream) {
+    if (!fault || !slip || !b) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = fault->op->h;
+    if (ld < h.E * h.bs || ld_slip < static_cast<int64_t>(fault->d.nfault) * fault->d.nbf)
+        return fail(TDG_E_INVALID, "leading dimension too small");
+    TDG_TRY(ensure_uploaded(fault->op, TDG_FP64));
+    int rc = launch_fault(h.D, h.N, false, fault->op->op64, fault->d, nullptr, 0, slip, ld_slip, b, ld, nrhs,
+                          static_cast<cudaStream_t>(stream));
+    return rc ? fail(rc, "fault rhs launch failed") : 0;
+}
+
+extern "C" int tdg_fault_traction(tdg_fault* fault, const double* u, int64_t ld, const double* slip, int64_t ld_slip,
+                                  double* traction, int64_t ld_t, int nrhs, void* stream) {
+    if (!fault || !u || !traction) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = fault->op->h;
+    const int64_t nt = static_cast<int64_t>(fault->d.nfault) * fault->d.nbf;
+    if (ld < h.E * h.bs || ld_t < nt || (slip && ld_slip < nt)) return fail(TDG_E_INVALID, "leading dimension too small");
+    TDG_TRY(ensure_uploaded(fault->op, TDG_FP64));
+    int rc = launch_fault(h.D, h.N, true, fault->op->op64, fault->d, u, ld, slip, ld_slip, traction, ld_t, nrhs,
+                          static_cast<cudaStream_t>(stream));
+    return rc ? fail(rc, "fault traction launch failed") : 0;
 }

@@ -1,5 +1,6 @@
 // Instances and launcher of the operator apply kernel.
 #include "apply.cuh"
+#include "apply_mma.cuh"
 #include "dispatch.hpp"
 
 #include "../../../include/tandem_b200.h"
@@ -70,6 +71,63 @@ int launch_apply(int D, int N, int kind, DevOp<T> const& op, const T* x, T* y, i
     if (nrhs < 1) return TDG_E_INVALID;
     if (D == 2) return apply_deg<2, T>(N, kind, op, x, y, nrhs, ld, s);
     if (D == 3) return apply_deg<3, T>(N, kind, op, x, y, nrhs, ld, s);
+    return TDG_E_INVALID;
+}
+
+namespace {
+
+template <class S>
+int run_apply_mma(DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y, int nrhs, int64_t ld,
+                  cudaStream_t s) {
+    using L = MmaTile<S>;
+    const MmaLayout lay = mma_layout<S>(op.Nq, op.nq);
+    const size_t smem = sizeof(double) * static_cast<size_t>(lay.total);
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem + 2 * L::TE * sizeof(int) > static_cast<size_t>(optin)) return TDG_E_INVALID;
+    auto kern = apply_mma_kernel<S>;
+    static size_t configured = 0;
+    if (configured < smem) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+            cudaSuccess)
+            return TDG_E_CUDA;
+        configured = smem;
+    }
+    const int64_t nwork = static_cast<int64_t>(mt.ntiles) * nrhs;
+    int64_t grid = device_sm_count();
+    if (grid > nwork) grid = nwork;
+    if (grid < 1) grid = 1;
+    kern<<<static_cast<unsigned>(grid), L::NT, smem, s>>>(op, mt, x, y, ld, nrhs);
+    return cudaGetLastError() == cudaSuccess ? 0 : TDG_E_CUDA;
+}
+
+template <int D, int N>
+int mma_kind(int kind, DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y, int nrhs, int64_t ld,
+             cudaStream_t s) {
+    if (kind == kPoisson) return run_apply_mma<Shape<D, N, kPoisson>>(op, mt, x, y, nrhs, ld, s);
+    return run_apply_mma<Shape<D, N, kElasticity>>(op, mt, x, y, nrhs, ld, s);
+}
+
+template <int D>
+int mma_deg(int N, int kind, DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y, int nrhs,
+            int64_t ld, cudaStream_t s) {
+    switch (N) {
+        case 1: return mma_kind<D, 1>(kind, op, mt, x, y, nrhs, ld, s);
+        case 2: return mma_kind<D, 2>(kind, op, mt, x, y, nrhs, ld, s);
+        case 3: return mma_kind<D, 3>(kind, op, mt, x, y, nrhs, ld, s);
+        case 4: return mma_kind<D, 4>(kind, op, mt, x, y, nrhs, ld, s);
+        default: return TDG_E_INVALID;
+    }
+}
+
+}  // namespace
+
+int launch_apply_mma(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y,
+                     int nrhs, int64_t ld, cudaStream_t s) {
+    if (nrhs < 1 || mt.ntiles < 1) return TDG_E_INVALID;
+    if (D == 2) return mma_deg<2>(N, kind, op, mt, x, y, nrhs, ld, s);
+    if (D == 3) return mma_deg<3>(N, kind, op, mt, x, y, nrhs, ld, s);
     return TDG_E_INVALID;
 }
 

@@ -16,6 +16,11 @@ constexpr int kMaxDegree = 4;
 template <typename T>
 int launch_apply(int D, int N, int kind, DevOp<T> const& op, const T* x, T* y, int nrhs,
                  int64_t ld, cudaStream_t s);
+struct MmaTiles;
+// FP64 apply on the FP64 tensor pipe over signature-grouped element tiles (apply_mma.cuh);
+// TDG_E_INVALID when the instance's tables do not fit in shared memory.
+int launch_apply_mma(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y,
+                     int nrhs, int64_t ld, cudaStream_t s);
 int launch_bjac_assemble(int D, int N, int kind, DevOp<double> const& op, double* blk,
                          cudaStream_t s);
 template <typename T>
@@ -23,6 +28,12 @@ int launch_bjac_invert(int bs, int64_t E, const double* blk, T* inv, int* status
 template <typename T>
 int launch_bjac_apply(int bs, int64_t E, const T* inv, const T* r, T* z, int nrhs, int64_t ld,
                       cudaStream_t s);
+
+struct DevFault;
+// Poisson fault coupling: traction == false: out += rhs of slip; true: out = traction of (u, slip).
+int launch_fault(int D, int N, bool traction, DevOp<double> const& op, DevFault const& fl, const double* u,
+                 int64_t ld, const double* slip, int64_t ld_slip, double* out, int64_t ld_out, int nrhs,
+                 cudaStream_t s);
 
 // Number of resident CTAs of a kernel on the current device times the SM count, cached.
 int device_sm_count();

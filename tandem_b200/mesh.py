@@ -92,6 +92,75 @@ def cube_mesh(n: int) -> SimplexMesh:
     return SimplexMesh(3, verts, np.sort(el, axis=1))
 
 
+def _graded(h0: float, length: float, ratio: float) -> np.ndarray:
+    """Offsets 0 < d_1 < ... = length with first step h0 and geometric growth `ratio`."""
+    d, h, out = 0.0, h0, []
+    while d + h < length - 0.5 * h:
+        d += h
+        out.append(d)
+        h *= ratio
+    out.append(length)
+    return np.array(out)
+
+
+def graded_fault_mesh(num_fault_facets: int = 256, fault_length: float = 12.8, dip_deg: float = 60.0,
+                      width: float = 40.0, depth: float = 20.0, ratio: float = 1.07):
+    """2D antiplane domain (km) graded toward a planar dipping fault.
+
+    The domain is the parallelogram {x = xi - s cot(dip), y = s}, xi in [-width/2, width/2],
+    s in [-depth, 0]: its slanted sides follow the fault, which is the grid line xi = 0 from the
+    free surface (y = 0) down to the fault tip.  Along the fault the grid spacing is
+    fault_length / num_fault_facets; away from it cells grow geometrically by `ratio`.
+    Boundary conditions: free surface Natural, the other three sides Dirichlet; the interior facets
+    on xi = 0 above the tip are Fault facets (ordered by depth)."""
+    theta = np.deg2rad(dip_deg)
+    h_f = fault_length / num_fault_facets
+    tip = -fault_length * np.sin(theta)
+    ds = h_f * np.sin(theta)
+    s_fault = np.linspace(tip, 0.0, num_fault_facets + 1)
+    s_below = tip - _graded(ds, depth + tip, ratio)
+    s = np.concatenate([s_below[::-1], s_fault])
+    xi_r = _graded(h_f, 0.5 * width, ratio)
+    xi = np.concatenate([-xi_r[::-1], [0.0], xi_r])
+    nx, ns = xi.size, s.size
+    S, XI = np.meshgrid(s, xi, indexing="ij")  # vertex (j, i) -> id i + nx * j
+    X = XI - S / np.tan(theta)  # s <= 0: the fault dips toward +x
+    verts = np.stack([X.ravel(), S.ravel()], axis=1)
+    ci, cj = np.meshgrid(np.arange(nx - 1), np.arange(ns - 1), indexing="xy")
+    ci, cj = ci.ravel(), cj.ravel()
+    v00 = ci + nx * cj
+    v01, v10, v11 = v00 + 1, v00 + nx, v00 + nx + 1
+    odd = ((ci % 2) ^ (cj % 2)).astype(bool)
+    t0 = np.where(odd[:, None], np.stack([v00, v01, v11], 1), np.stack([v00, v01, v10], 1))
+    t1 = np.where(odd[:, None], np.stack([v00, v10, v11], 1), np.stack([v01, v10, v11], 1))
+    el = np.empty((2 * ci.size, 3), dtype=np.int64)
+    el[0::2], el[1::2] = t0, t1
+    m = SimplexMesh(2, verts, np.sort(el, axis=1))
+    i0 = int(np.argmin(np.abs(xi)))
+    j0 = int(np.argmin(np.abs(s - tip)))
+    m.info.update(dict(fault_column=i0, fault_tip_row=j0, nx=nx, ns=ns, dip=theta, xi=xi, s=s))
+
+    def boundary_bc(c):
+        top = np.all(np.abs(c[:, :, 1]) < 1e-9, axis=1)
+        return np.where(top, BC_NATURAL, BC_DIRICHLET)
+
+    def interior_bc(c):
+        # vertices on the fault grid line: xi == 0 and s >= tip
+        ids_xi = c[:, :, 0] + c[:, :, 1] / np.tan(theta)
+        on = np.all(np.abs(ids_xi) < 1e-9, axis=1) & np.all(c[:, :, 1] >= tip - 1e-9, axis=1)
+        return np.where(on, BC_FAULT, BC_NONE)
+
+    m.info["boundary_bc"], m.info["interior_bc"] = boundary_bc, interior_bc
+    return m
+
+
+def fault_facets(mesh: SimplexMesh) -> np.ndarray:
+    """Fault facet numbers ordered by depth (surface first)."""
+    f = np.nonzero(mesh.facet_bc == BC_FAULT)[0]
+    depth = mesh.vertices[mesh.facets[f]][:, :, 1].mean(axis=1)
+    return f[np.argsort(-depth)]
+
+
 def topology(mesh: SimplexMesh, boundary_bc: Callable[[np.ndarray], np.ndarray] | int = BC_DIRICHLET,
              interior_bc: Callable[[np.ndarray], np.ndarray] | None = None) -> SimplexMesh:
     """Facets and FacetInfo arrays.  boundary_bc maps facet vertex coordinates [F, D, D] to BC

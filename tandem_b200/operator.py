@@ -186,3 +186,69 @@ def _check_vec(t, precision: int, n: int) -> None:
     if not (t.is_cuda and t.dtype == want and t.is_contiguous() and t.numel() >= n):
         raise ValueError(f"expected a contiguous CUDA {want} tensor with >= {n} entries, got "
                          f"{t.dtype} device={t.device} numel={t.numel()}")
+
+
+class Fault:
+    """Fault coupling of a Poisson operator (tandem's Adapter<Poisson> over the fault facets):
+    slip -> right-hand side and displacement -> on-fault traction, batched over right-hand sides."""
+
+    def __init__(self, op: DGOperator, facets: np.ndarray, ref_normal):
+        self.op = op
+        self._facets = np.ascontiguousarray(facets, dtype=np.int64)
+        self._ref = np.ascontiguousarray(ref_normal, dtype=np.float64)
+        h = C.c_void_p()
+        _ffi.check(_ffi.lib().tdg_fault_create(op._h, len(self._facets), self._facets.ctypes.data,
+                                               self._ref.ctypes.data, C.byref(h)))
+        self._h = h
+        sizes = (C.c_int64 * 2)()
+        _ffi.check(_ffi.lib().tdg_fault_sizes(h, sizes))
+        self.nfault, self.nbf = int(sizes[0]), int(sizes[1])
+        self.ncoef = self.nfault * self.nbf
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _ffi.lib().tdg_fault_destroy(h)
+            self._h = None
+
+    def slip_rhs(self, slip, b, nrhs: int = 1, stream=None) -> None:
+        """b += rhs of slip; slip [nrhs, ncoef], b [nrhs, ndof] (CUDA float64)."""
+        _check_vec(slip, FP64, nrhs * self.ncoef)
+        _check_vec(b, FP64, nrhs * self.op.ndof)
+        _ffi.check(_ffi.lib().tdg_fault_slip_rhs(self._h, C.c_void_p(slip.data_ptr()), self.ncoef,
+                                                 C.c_void_p(b.data_ptr()), nrhs, self.op.ndof, _stream(stream)))
+
+    def traction(self, u, slip, out, nrhs: int = 1, stream=None) -> None:
+        """out[nrhs, ncoef] = traction of displacement u [nrhs, ndof] and slip [nrhs, ncoef]."""
+        _check_vec(u, FP64, nrhs * self.op.ndof)
+        _check_vec(out, FP64, nrhs * self.ncoef)
+        sp = None if slip is None else C.c_void_p(slip.data_ptr())
+        _ffi.check(_ffi.lib().tdg_fault_traction(self._h, C.c_void_p(u.data_ptr()), self.op.ndof, sp, self.ncoef,
+                                                 C.c_void_p(out.data_ptr()), self.ncoef, nrhs, _stream(stream)))
+
+
+def greens_function(op: DGOperator, fault: Fault, precision: int = FP64, rtol: float = 1e-10,
+                    columns=None, batch: int | None = None, **solve_kw):
+    """Discrete Green's function G[:, i] = traction(solve(rhs(slip = e_i))) for the fault basis
+    coefficients `columns` (all by default), solved as batched multi-right-hand-side launches
+    (tandem: one KSPSolve per column, app/form/SeasQDDiscreteGreenOperator.cpp:519-574).
+    Returns (G [ncoef, ncols] as a CUDA tensor, list of per-batch solve statistics)."""
+    import torch
+    cols = np.arange(fault.ncoef) if columns is None else np.asarray(columns)
+    batch = len(cols) if batch is None else batch
+    G = torch.zeros(fault.ncoef, len(cols), dtype=torch.float64, device="cuda")
+    stats = []
+    for s in range(0, len(cols), batch):
+        c = cols[s:s + batch]
+        n = len(c)
+        slip = torch.zeros(n, fault.ncoef, dtype=torch.float64, device="cuda")
+        slip[torch.arange(n, device="cuda"), torch.as_tensor(c, device="cuda")] = 1.0
+        b = torch.zeros(n, op.ndof, dtype=torch.float64, device="cuda")
+        fault.slip_rhs(slip, b, n)
+        x = torch.zeros_like(b)
+        st = op.solve(b, x, precision=precision, rtol=rtol, nrhs=n, **solve_kw)
+        stats.append(st)
+        T = torch.empty(n, fault.ncoef, dtype=torch.float64, device="cuda")
+        fault.traction(x, slip, T, n)
+        G[:, s:s + n] = T.T
+    return G, stats
