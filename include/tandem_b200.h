@@ -174,6 +174,15 @@ typedef struct {
 int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64_t ld,
               const tdg_solve_opts* opts, tdg_solve_stats* stats, void* stream);
 
+/* Solves a block-diagonal batch of independent problems held in one operator (the disjoint union
+ * of several meshes): segment s owns elements [seg_elem_offset[s], seg_elem_offset[s+1]) (host
+ * array, nseg + 1 entries, covering [0, E)) and gets its own Krylov scalars and convergence test,
+ * while every apply and preconditioner launch covers all problems at once.
+ * seg_rel_residual (host, may be NULL) receives each problem's final relative residual. */
+int tdg_solve_segmented(tdg_op* op, const double* b, double* x, int nseg, const int64_t* seg_elem_offset,
+                        const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel_residual,
+                        void* stream);
+
 /* --- fault coupling, Green's functions (app/form/SeasQDDiscreteGreenOperator.cpp:493-578) ---- */
 
 typedef struct tdg_fault tdg_fault;

@@ -18,39 +18,26 @@
 
 namespace tdg {
 
-__global__ void k_dot_finalize(const double* __restrict__ partial, int nb, double* __restrict__ scal,
-                               int slot0, int slot1) {
-    const int rhs = blockIdx.x;
+__global__ void k_dot_finalize(const double* __restrict__ partial, const int* __restrict__ seg_chunk,
+                               double* __restrict__ scal, int slot0, int slot1) {
+    const int seg = blockIdx.x;
     double s0 = 0.0, s1 = 0.0;
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-        s0 += partial[(static_cast<int64_t>(rhs) * nb + i) * 2];
-        s1 += partial[(static_cast<int64_t>(rhs) * nb + i) * 2 + 1];
+    for (int i = seg_chunk[seg] + threadIdx.x; i < seg_chunk[seg + 1]; i += blockDim.x) {
+        s0 += partial[2 * static_cast<int64_t>(i)];
+        s1 += partial[2 * static_cast<int64_t>(i) + 1];
     }
     __shared__ double red[2][32];
-    s0 = warp_sum(s0);
-    s1 = warp_sum(s1);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) {
-        red[0][wid] = s0;
-        red[1][wid] = s1;
-    }
-    __syncthreads();
-    if (wid == 0) {
-        const int nw = blockDim.x / 32;
-        s0 = lane < nw ? red[0][lane] : 0.0;
-        s1 = lane < nw ? red[1][lane] : 0.0;
-        s0 = warp_sum(s0);
-        s1 = warp_sum(s1);
-        if (lane == 0) {
-            if (slot0 >= 0) scal[rhs * kScal + slot0] = s0;
-            if (slot1 >= 0) scal[rhs * kScal + slot1] = s1;
-        }
+    s0 = block_sum(s0, red[0]);
+    s1 = block_sum(s1, red[1]);
+    if (threadIdx.x == 0) {
+        if (slot0 >= 0) scal[seg * kScal + slot0] = s0;
+        if (slot1 >= 0) scal[seg * kScal + slot1] = s1;
     }
 }
 
-__global__ void k_cg_shift(double* __restrict__ scal, int nrhs) {
+__global__ void k_cg_shift(double* __restrict__ scal, int nseg) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < nrhs && scal[r * kScal + kActive] != 0.0) scal[r * kScal + kRZ] = scal[r * kScal + kRZnew];
+    if (r < nseg && scal[r * kScal + kActive] != 0.0) scal[r * kScal + kRZ] = scal[r * kScal + kRZnew];
 }
 
 }  // namespace tdg
@@ -161,7 +148,7 @@ int upload_common(tdg_op* op) {
 int upload_mma(tdg_op* op, DevArena& arena) {
     auto const& h = op->h;
     const int D = h.D, NBF = h.Nbf, Nq = h.Nq, nq = h.nq, NF = h.nfaces;
-    const int MY = (NBF + 7) / 8 * 8, LDT = mma_ld(MY);
+    const int KP = (NBF + 3) / 4 * 4, LDT = mma_ld(KP);
     const int MV = round8(D * Nq), MF = round8((D + 1) * nq);
     std::vector<double> tab(static_cast<size_t>(MV) * LDT + static_cast<size_t>(NF) * MF * LDT, 0.0);
     for (int q = 0; q < Nq; ++q)
@@ -277,29 +264,39 @@ int ensure_uploaded(tdg_op* op, int precision) {
     return fail(TDG_E_INVALID, "precision must be TDG_FP64 or TDG_FP32");
 }
 
-dim3 vec_grid(int64_t n, int nrhs) {
-    int64_t g = (n + 255) / 256;
-    int64_t cap = static_cast<int64_t>(device_sm_count()) * 8;
-    if (g > cap) g = cap;
-    if (g < 1) g = 1;
-    return dim3(static_cast<unsigned>(g), static_cast<unsigned>(nrhs));
+// Chunk list of a segmented vector (see krylov.cuh), uploaded into solve workspace.
+struct SegPlan {
+    int nseg = 0, nchunks = 0;
+    const Chunk* chunks = nullptr;   // device [nchunks]
+    const int* seg_chunk = nullptr;  // device [nseg + 1]
+    // operator view of the stacked vectors: apply / precondition with nrhs and leading dimension
+    int op_nrhs = 1;
+    int64_t op_ld = 0;
+};
+
+void plan_chunks(std::vector<int64_t> const& seg_begin, std::vector<int64_t> const& seg_end, std::vector<Chunk>& chunks,
+                 std::vector<int>& seg_chunk) {
+    chunks.clear();
+    seg_chunk.assign(1, 0);
+    for (size_t sgi = 0; sgi < seg_begin.size(); ++sgi) {
+        for (int64_t b = seg_begin[sgi]; b < seg_end[sgi]; b += kChunk) {
+            Chunk c;
+            c.begin = b;
+            c.end = std::min(seg_end[sgi], b + kChunk);
+            c.seg = static_cast<int>(sgi);
+            c.pad = 0;
+            chunks.push_back(c);
+        }
+        seg_chunk.push_back(static_cast<int>(chunks.size()));
+    }
 }
 
-int dot_blocks(int64_t n) {
-    int64_t g = (n + kDotThreads - 1) / kDotThreads;
-    int64_t cap = static_cast<int64_t>(device_sm_count()) * 4;
-    if (g > cap) g = cap;
-    if (g < 1) g = 1;
-    return static_cast<int>(g);
-}
-
-// scal[rhs][slot0] = a.b, scal[rhs][slot1] = c.d
+// scal[seg][slot0] = a.b, scal[seg][slot1] = c.d
 template <typename T>
-int dots(int64_t n, int64_t ld, int nrhs, const T* a, const T* b, const T* c, const T* d, double* partial,
-         double* scal, int slot0, int slot1, cudaStream_t s) {
-    const int nb = dot_blocks(n);
-    k_dot2<T><<<dim3(nb, nrhs), kDotThreads, 0, s>>>(n, ld, a, b, c, d, partial);
-    k_dot_finalize<<<nrhs, 256, 0, s>>>(partial, nb, scal, slot0, slot1);
+int dots(SegPlan const& sp, const T* a, const T* b, const T* c, const T* d, double* partial, double* scal, int slot0,
+         int slot1, cudaStream_t s) {
+    k_dot2<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, a, b, c, d, partial);
+    k_dot_finalize<<<sp.nseg, 256, 0, s>>>(partial, sp.seg_chunk, scal, slot0, slot1);
     return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "dot kernels");
 }
 
@@ -576,28 +573,26 @@ struct CgVectors {
 
 // One preconditioned CG iteration on (A_T, M_T) with device-resident scalars.
 template <typename T>
-int cg_iteration(tdg_op* op, int prec, T* x, CgVectors<T> v, int nrhs, int64_t ld, double* partial,
-                 double* scal, cudaStream_t s) {
-    auto const& h = op->h;
-    const int64_t n = h.E * h.bs;
-    TDG_TRY(tdg_apply(op, prec, v.p, v.q, nrhs, ld, s));
-    TDG_TRY(dots<T>(n, ld, nrhs, v.p, v.q, nullptr, nullptr, partial, scal, kPQ, -1, s));
-    k_cg_xr<T><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, x, v.r, v.p, v.q, scal);
-    TDG_TRY(tdg_bjacobi_apply(op, prec, v.r, v.z, nrhs, ld, s));
-    TDG_TRY(dots<T>(n, ld, nrhs, v.r, v.z, v.r, v.r, partial, scal, kRZnew, kRR, s));
-    k_cg_p<T><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, v.p, v.z, scal);
-    k_cg_shift<<<(nrhs + 127) / 128, 128, 0, s>>>(scal, nrhs);
+int cg_iteration(tdg_op* op, int prec, SegPlan const& sp, T* x, CgVectors<T> v, double* partial, double* scal,
+                 cudaStream_t s) {
+    TDG_TRY(tdg_apply(op, prec, v.p, v.q, sp.op_nrhs, sp.op_ld, s));
+    TDG_TRY(dots<T>(sp, v.p, v.q, nullptr, nullptr, partial, scal, kPQ, -1, s));
+    k_cg_xr<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, v.r, v.p, v.q, scal);
+    TDG_TRY(tdg_bjacobi_apply(op, prec, v.r, v.z, sp.op_nrhs, sp.op_ld, s));
+    TDG_TRY(dots<T>(sp, v.r, v.z, v.r, v.r, partial, scal, kRZnew, kRR, s));
+    k_cg_p<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, v.p, v.z, scal);
+    k_cg_shift<<<(sp.nseg + 127) / 128, 128, 0, s>>>(scal, sp.nseg);
     return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "CG update kernels");
 }
 
-// Runs CG iterations until every active rhs reaches sqrt(rr) <= tol_abs[rhs] or the iteration
-// budget is spent.  Returns the number of iterations done in *iters.
+// Runs CG iterations until every active segment reaches sqrt(rr) <= tol_abs[seg] or the budget
+// is spent.  Convergence is checked every kCheck iterations; iteration blocks after the first are
+// replayed from a CUDA graph when graphs are enabled (stream != legacy default).
 template <typename T>
-int cg_loop(tdg_op* op, int prec, T* x, CgVectors<T> v, int nrhs, int64_t ld, double* partial, double* scal,
-            std::vector<double> const& tol_abs, int max_it, bool graphs, cudaStream_t s, int* iters,
-            bool* diverged) {
-    constexpr int kChunk = 8;
-    std::vector<double> hs(static_cast<size_t>(nrhs) * kScal);
+int cg_loop(tdg_op* op, int prec, SegPlan const& sp, T* x, CgVectors<T> v, double* partial, double* scal,
+            std::vector<double> const& tol_abs, int max_it, bool graphs, cudaStream_t s, int* iters, bool* diverged) {
+    constexpr int kCheck = 8;
+    std::vector<double> hs(static_cast<size_t>(sp.nseg) * kScal);
     cudaGraphExec_t exec = nullptr;
     int done = 0;
     *diverged = false;
@@ -606,10 +601,10 @@ int cg_loop(tdg_op* op, int prec, T* x, CgVectors<T> v, int nrhs, int64_t ld, do
         TDG_CUDA_TRY(cudaMemcpyAsync(hs.data(), scal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
         TDG_CUDA_TRY(cudaStreamSynchronize(s));
         bool any = false, changed = false;
-        for (int r = 0; r < nrhs; ++r) {
+        for (int r = 0; r < sp.nseg; ++r) {
             double* sr = &hs[static_cast<size_t>(r) * kScal];
             if (sr[kActive] == 0.0) continue;
-            double rr = sr[kRR];
+            const double rr = sr[kRR];
             if (!std::isfinite(rr)) {
                 *diverged = true;
                 sr[kActive] = 0.0;
@@ -626,13 +621,16 @@ int cg_loop(tdg_op* op, int prec, T* x, CgVectors<T> v, int nrhs, int64_t ld, do
         if (changed)
             TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         if (!any || done >= max_it) break;
-        const bool use_graph = graphs && s != nullptr && done >= kChunk;
+        const bool use_graph = graphs && s != nullptr && done >= kCheck;
         if (use_graph && !exec) {
             cudaGraph_t graph = nullptr;
             TDG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            for (int i = 0; i < kChunk && rc == 0; ++i) rc = cg_iteration<T>(op, prec, x, v, nrhs, ld, partial, scal, s);
+            for (int i = 0; i < kCheck && rc == 0; ++i) rc = cg_iteration<T>(op, prec, sp, x, v, partial, scal, s);
             cudaError_t ce = cudaStreamEndCapture(s, &graph);
-            if (rc) return rc;
+            if (rc) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
             TDG_CUDA_TRY(ce);
             TDG_CUDA_TRY(cudaGraphInstantiate(&exec, graph, 0));
             cudaGraphDestroy(graph);
@@ -640,76 +638,71 @@ int cg_loop(tdg_op* op, int prec, T* x, CgVectors<T> v, int nrhs, int64_t ld, do
         if (exec) {
             TDG_CUDA_TRY(cudaGraphLaunch(exec, s));
         } else {
-            for (int i = 0; i < kChunk; ++i) TDG_TRY(cg_iteration<T>(op, prec, x, v, nrhs, ld, partial, scal, s));
+            for (int i = 0; i < kCheck; ++i) TDG_TRY(cg_iteration<T>(op, prec, sp, x, v, partial, scal, s));
         }
-        done += kChunk;
+        done += kCheck;
     }
     if (exec) cudaGraphExecDestroy(exec);
     *iters = done;
     return 0;
 }
 
-// r = b - A x (FP64), returns per-rhs ||r|| and ||b|| on the host.
-int residual64(tdg_op* op, const double* b, const double* x, double* r, double* tmp, int nrhs, int64_t ld,
+// r = b - A x (FP64); per-segment ||r|| and ||b|| on the host.
+int residual64(tdg_op* op, SegPlan const& sp, const double* b, const double* x, double* r, double* tmp,
                double* partial, double* scal, std::vector<double>& rn, std::vector<double>& bn, cudaStream_t s) {
-    auto const& h = op->h;
-    const int64_t n = h.E * h.bs;
-    TDG_TRY(tdg_apply(op, TDG_FP64, x, tmp, nrhs, ld, s));
-    k_sub<double><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, b, tmp, r);
-    TDG_TRY(dots<double>(n, ld, nrhs, r, r, b, b, partial, scal, kRR, kBB, s));
-    std::vector<double> hs(static_cast<size_t>(nrhs) * kScal);
+    TDG_TRY(tdg_apply(op, TDG_FP64, x, tmp, sp.op_nrhs, sp.op_ld, s));
+    k_sub<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, b, tmp, r);
+    TDG_TRY(dots<double>(sp, r, r, b, b, partial, scal, kRR, kBB, s));
+    std::vector<double> hs(static_cast<size_t>(sp.nseg) * kScal);
     TDG_CUDA_TRY(cudaMemcpyAsync(hs.data(), scal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     TDG_CUDA_TRY(cudaStreamSynchronize(s));
-    rn.resize(nrhs);
-    bn.resize(nrhs);
-    for (int i = 0; i < nrhs; ++i) {
+    rn.resize(sp.nseg);
+    bn.resize(sp.nseg);
+    for (int i = 0; i < sp.nseg; ++i) {
         rn[i] = std::sqrt(hs[static_cast<size_t>(i) * kScal + kRR]);
         bn[i] = std::sqrt(hs[static_cast<size_t>(i) * kScal + kBB]);
     }
     return 0;
 }
 
-// Initialises z = M r, p = z, rz = r.z, rr = r.r, active = flags.
+// z = M r, p = z, rz = r.z, rr = r.r, active flags from `active`.
 template <typename T>
-int cg_start(tdg_op* op, int prec, CgVectors<T> v, int nrhs, int64_t ld, double* partial, double* scal,
+int cg_start(tdg_op* op, int prec, SegPlan const& sp, CgVectors<T> v, double* partial, double* scal,
              std::vector<double> const& active, cudaStream_t s) {
-    auto const& h = op->h;
-    const int64_t n = h.E * h.bs;
-    std::vector<double> hs(static_cast<size_t>(nrhs) * kScal, 0.0);
-    for (int i = 0; i < nrhs; ++i) hs[static_cast<size_t>(i) * kScal + kActive] = active[i];
+    std::vector<double> hs(static_cast<size_t>(sp.nseg) * kScal, 0.0);
+    for (int i = 0; i < sp.nseg; ++i) hs[static_cast<size_t>(i) * kScal + kActive] = active[i];
     TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-    TDG_TRY(tdg_bjacobi_apply(op, prec, v.r, v.z, nrhs, ld, s));
-    k_copy<T><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, v.z, ld, v.p);
-    TDG_TRY(dots<T>(n, ld, nrhs, v.r, v.z, v.r, v.r, partial, scal, kRZ, kRR, s));
-    // the active flags were uploaded before the dots; the dots do not touch slot kActive
+    TDG_TRY(tdg_bjacobi_apply(op, prec, v.r, v.z, sp.op_nrhs, sp.op_ld, s));
+    k_copy<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, v.z, v.p);
+    TDG_TRY(dots<T>(sp, v.r, v.z, v.r, v.r, partial, scal, kRZ, kRR, s));
     return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "CG start");
 }
 
-}  // namespace
-
-extern "C" int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64_t ld, const tdg_solve_opts* opts,
-                         tdg_solve_stats* stats, void* stream) {
-    if (!op || !b || !x || !opts || !stats) return fail(TDG_E_INVALID, "null argument");
-    auto const& h = op->h;
-    const int64_t n = h.E * h.bs;
-    if (nrhs < 1 || ld < n) return fail(TDG_E_INVALID, "nrhs < 1 or ld < E * bs");
+// Shared solve driver over a segment plan.  seg_rel (optional) receives each segment's final
+// relative residual.
+int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> const& seg_begin,
+                   std::vector<int64_t> const& seg_end, int op_nrhs, int64_t op_ld, size_t vec_entries,
+                   const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel, cudaStream_t s) {
     const int prec = opts->precision;
     if (prec != TDG_FP64 && prec != TDG_FP32) return fail(TDG_E_INVALID, "bad precision");
     if (!op->inv || op->inv_precision != prec)
         return fail(TDG_E_STATE, "tdg_bjacobi_setup must be called with the solve precision");
     TDG_TRY(ensure_uploaded(op, TDG_FP64));
     if (prec == TDG_FP32) TDG_TRY(ensure_uploaded(op, TDG_FP32));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     std::memset(stats, 0, sizeof(*stats));
 
-    // workspace: FP64 r, z, p, q, tmp (5 nrhs*ld) + FP32 d, r, z, p, q (5 nrhs*ld floats)
-    const size_t vec = static_cast<size_t>(nrhs) * ld;
-    const size_t partial_n = static_cast<size_t>(nrhs) * dot_blocks(n) * 2;
-    size_t need = 5 * vec * sizeof(double) + partial_n * sizeof(double) + 2 * static_cast<size_t>(nrhs) * kScal * sizeof(double) + 1024;
-    if (prec == TDG_FP32) need += 5 * vec * sizeof(float);
+    std::vector<Chunk> hchunks;
+    std::vector<int> hseg;
+    plan_chunks(seg_begin, seg_end, hchunks, hseg);
+    const int nseg = static_cast<int>(seg_begin.size());
+    const size_t vec = vec_entries;
+    size_t need = 5 * vec * sizeof(double) + hchunks.size() * (2 * sizeof(double) + sizeof(Chunk)) +
+                  (hseg.size()) * sizeof(int) + 2 * static_cast<size_t>(nseg) * kScal * sizeof(double) + 8 * 256;
+    if (prec == TDG_FP32) need += 5 * vec * sizeof(float) + 5 * 256;
     if (op->ws_bytes < need) {
         op->arena_ws.release();
         op->ws = nullptr;
+        op->ws_bytes = 0;
         unsigned char* w = nullptr;
         TDG_CUDA_TRY(op->arena_ws.alloc(&w, need));
         op->ws = w;
@@ -726,9 +719,20 @@ extern "C" int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64
     double* p64 = reinterpret_cast<double*>(take(vec * sizeof(double)));
     double* q64 = reinterpret_cast<double*>(take(vec * sizeof(double)));
     double* t64 = reinterpret_cast<double*>(take(vec * sizeof(double)));
-    double* partial = reinterpret_cast<double*>(take(partial_n * sizeof(double)));
-    double* scal = reinterpret_cast<double*>(take(static_cast<size_t>(nrhs) * kScal * sizeof(double)));
-    double* scal_out = reinterpret_cast<double*>(take(static_cast<size_t>(nrhs) * kScal * sizeof(double)));
+    double* partial = reinterpret_cast<double*>(take(hchunks.size() * 2 * sizeof(double)));
+    Chunk* dchunks = reinterpret_cast<Chunk*>(take(hchunks.size() * sizeof(Chunk)));
+    int* dseg = reinterpret_cast<int*>(take(hseg.size() * sizeof(int)));
+    double* scal = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * kScal * sizeof(double)));
+    double* scal_out = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * kScal * sizeof(double)));
+    TDG_CUDA_TRY(cudaMemcpyAsync(dchunks, hchunks.data(), hchunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice, s));
+    TDG_CUDA_TRY(cudaMemcpyAsync(dseg, hseg.data(), hseg.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    SegPlan sp;
+    sp.nseg = nseg;
+    sp.nchunks = static_cast<int>(hchunks.size());
+    sp.chunks = dchunks;
+    sp.seg_chunk = dseg;
+    sp.op_nrhs = op_nrhs;
+    sp.op_ld = op_ld;
 
     cudaEvent_t ev0, ev1;
     TDG_CUDA_TRY(cudaEventCreate(&ev0));
@@ -741,34 +745,26 @@ extern "C" int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64
     std::vector<double> rn, bn;
     int total_it = 0, outer = 0;
     bool diverged = false;
-    double worst = 0.0;
+    auto rel_of = [&](int i) { return bn[i] > 0 ? rn[i] / bn[i] : 0.0; };
 
     if (prec == TDG_FP64) {
         // FP64 PCG with a true-residual check and restart on recurrence drift
         for (int restart = 0; restart < 4; ++restart) {
-            TDG_TRY(residual64(op, b, x, r64, t64, nrhs, ld, partial, scal, rn, bn, s));
-            std::vector<double> tol(nrhs), act(nrhs);
+            TDG_TRY(residual64(op, sp, b, x, r64, t64, partial, scal, rn, bn, s));
+            std::vector<double> tol(nseg), act(nseg);
             bool any = false;
-            worst = 0.0;
-            for (int i = 0; i < nrhs; ++i) {
-                double rel = bn[i] > 0 ? rn[i] / bn[i] : 0.0;
-                worst = std::max(worst, rel);
+            for (int i = 0; i < nseg; ++i) {
                 tol[i] = rtol * bn[i];
                 act[i] = (rn[i] > tol[i]) ? 1.0 : 0.0;
                 any = any || act[i] != 0.0;
             }
             if (!any || total_it >= max_it) break;
-            TDG_TRY(cg_start<double>(op, TDG_FP64, {r64, z64, p64, q64}, nrhs, ld, partial, scal, act, s));
+            TDG_TRY(cg_start<double>(op, TDG_FP64, sp, {r64, z64, p64, q64}, partial, scal, act, s));
             int it = 0;
-            TDG_TRY(cg_loop<double>(op, TDG_FP64, x, {r64, z64, p64, q64}, nrhs, ld, partial, scal, tol,
-                                    max_it - total_it, graphs, s, &it, &diverged));
+            TDG_TRY(cg_loop<double>(op, TDG_FP64, sp, x, {r64, z64, p64, q64}, partial, scal, tol, max_it - total_it,
+                                    graphs, s, &it, &diverged));
             total_it += it;
             if (diverged) break;
-        }
-        if (!diverged) {
-            TDG_TRY(residual64(op, b, x, r64, t64, nrhs, ld, partial, scal, rn, bn, s));
-            worst = 0.0;
-            for (int i = 0; i < nrhs; ++i) worst = std::max(worst, bn[i] > 0 ? rn[i] / bn[i] : 0.0);
         }
     } else {
         float* d32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
@@ -779,42 +775,33 @@ extern "C" int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64
         const double inner_rtol = opts->inner_rtol > 0 ? opts->inner_rtol : 1e-4;
         const int max_outer = opts->max_outer > 0 ? opts->max_outer : 30;
         for (outer = 0; outer < max_outer; ++outer) {
-            // FP64 residual; scal_out[kRR] = ||r||^2 is the scale of the FP32 correction
-            TDG_TRY(residual64(op, b, x, r64, t64, nrhs, ld, partial, scal_out, rn, bn, s));
-            std::vector<double> act(nrhs), tol(nrhs, inner_rtol);
+            // FP64 residual; scal_out[seg][kRR] = ||r||^2 scales the FP32 correction
+            TDG_TRY(residual64(op, sp, b, x, r64, t64, partial, scal_out, rn, bn, s));
+            std::vector<double> act(nseg), tol(nseg, inner_rtol);
             bool any = false;
-            worst = 0.0;
-            for (int i = 0; i < nrhs; ++i) {
-                double rel = bn[i] > 0 ? rn[i] / bn[i] : 0.0;
-                worst = std::max(worst, rel);
-                act[i] = rel > rtol ? 1.0 : 0.0;
+            for (int i = 0; i < nseg; ++i) {
+                act[i] = rel_of(i) > rtol ? 1.0 : 0.0;
                 any = any || act[i] != 0.0;
             }
             if (!any || total_it >= max_it) break;
             // inner problem A d = r / ||r|| in FP32 from d = 0
-            k_scale_convert<double, float><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, r64, ld, r32, scal_out, kRR);
-            k_fill<float><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, d32, 0.0f);
-            TDG_TRY(cg_start<float>(op, TDG_FP32, {r32, z32, p32, q32}, nrhs, ld, partial, scal, act, s));
+            k_scale_convert<double, float><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, r64, r32, scal_out, kRR);
+            k_fill<float><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, d32, 0.0f);
+            TDG_TRY(cg_start<float>(op, TDG_FP32, sp, {r32, z32, p32, q32}, partial, scal, act, s));
             int it = 0;
-            TDG_TRY(cg_loop<float>(op, TDG_FP32, d32, {r32, z32, p32, q32}, nrhs, ld, partial, scal, tol,
-                                   max_it - total_it, graphs, s, &it, &diverged));
+            TDG_TRY(cg_loop<float>(op, TDG_FP32, sp, d32, {r32, z32, p32, q32}, partial, scal, tol, max_it - total_it,
+                                   graphs, s, &it, &diverged));
             total_it += it;
-            // x += ||r|| d, only for rhs that were active in this refinement step
-            {
-                std::vector<double> hs(static_cast<size_t>(nrhs) * kScal, 0.0);
-                for (int i = 0; i < nrhs; ++i) hs[static_cast<size_t>(i) * kScal + kActive] = act[i];
-                TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-                k_correct<float><<<vec_grid(n, nrhs), 256, 0, s>>>(n, ld, x, ld, d32, scal_out, kRR, scal);
-            }
+            // x += ||r|| d for the segments that were active in this refinement step
+            std::vector<double> hs(static_cast<size_t>(nseg) * kScal, 0.0);
+            for (int i = 0; i < nseg; ++i) hs[static_cast<size_t>(i) * kScal + kActive] = act[i];
+            TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+            k_correct<float><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, d32, scal_out, kRR, scal);
             if (diverged) break;
         }
         stats->outer = outer;
-        if (!diverged && outer == max_outer) {
-            TDG_TRY(residual64(op, b, x, r64, t64, nrhs, ld, partial, scal_out, rn, bn, s));
-            worst = 0.0;
-            for (int i = 0; i < nrhs; ++i) worst = std::max(worst, bn[i] > 0 ? rn[i] / bn[i] : 0.0);
-        }
     }
+    if (!diverged) TDG_TRY(residual64(op, sp, b, x, r64, t64, partial, scal, rn, bn, s));
 
     TDG_CUDA_TRY(cudaEventRecord(ev1, s));
     TDG_CUDA_TRY(cudaEventSynchronize(ev1));
@@ -822,13 +809,53 @@ extern "C" int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64
     cudaEventElapsedTime(&ms, ev0, ev1);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
+    double worst = 0.0;
+    if (!diverged)
+        for (int i = 0; i < nseg; ++i) {
+            worst = std::max(worst, rel_of(i));
+            if (seg_rel) seg_rel[i] = rel_of(i);
+        }
     stats->iterations = total_it;
-    stats->rel_residual = worst;
+    stats->rel_residual = diverged ? NAN : worst;
     stats->seconds = ms * 1e-3;
     stats->converged = (!diverged && worst <= rtol) ? 1 : 0;
     if (diverged) return fail(TDG_E_DIVERGED, "non-finite residual in the Krylov iteration");
     if (!stats->converged) return fail(TDG_E_DIVERGED, "iteration limit reached before the residual target");
     return 0;
+}
+
+}  // namespace
+
+extern "C" int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64_t ld, const tdg_solve_opts* opts,
+                         tdg_solve_stats* stats, void* stream) {
+    if (!op || !b || !x || !opts || !stats) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = op->h;
+    const int64_t n = h.E * h.bs;
+    if (nrhs < 1 || ld < n) return fail(TDG_E_INVALID, "nrhs < 1 or ld < E * bs");
+    std::vector<int64_t> sb(nrhs), se(nrhs);
+    for (int r = 0; r < nrhs; ++r) {
+        sb[r] = r * ld;
+        se[r] = r * ld + n;
+    }
+    return solve_segments(op, b, x, sb, se, nrhs, ld, static_cast<size_t>(nrhs) * ld, opts, stats, nullptr,
+                          static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int tdg_solve_segmented(tdg_op* op, const double* b, double* x, int nseg, const int64_t* seg_elem_offset,
+                                   const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel_residual,
+                                   void* stream) {
+    if (!op || !b || !x || !opts || !stats || !seg_elem_offset || nseg < 1) return fail(TDG_E_INVALID, "bad argument");
+    auto const& h = op->h;
+    if (seg_elem_offset[0] != 0 || seg_elem_offset[nseg] != h.E)
+        return fail(TDG_E_INVALID, "segments must cover the elements [0, E)");
+    std::vector<int64_t> sb(nseg), se(nseg);
+    for (int i = 0; i < nseg; ++i) {
+        if (seg_elem_offset[i + 1] < seg_elem_offset[i]) return fail(TDG_E_INVALID, "segment offsets must not decrease");
+        sb[i] = seg_elem_offset[i] * h.bs;
+        se[i] = seg_elem_offset[i + 1] * h.bs;
+    }
+    return solve_segments(op, b, x, sb, se, 1, h.E * h.bs, static_cast<size_t>(h.E) * h.bs, opts, stats,
+                          seg_rel_residual, static_cast<cudaStream_t>(stream));
 }
 
 // ------------------------------------------------------------------------------------------------

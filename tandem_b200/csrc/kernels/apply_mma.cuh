@@ -21,16 +21,19 @@
 // fragments; nothing is accumulated through memory, there are no atomics, and each output block
 // is written once.
 //
-// Shared-memory leading dimensions are congruent to 12 mod 16 doubles, which makes the 8x4 / 4x8
-// fragment loads of a half warp hit 16 distinct 8-byte bank pairs.
+// Shared-memory leading dimensions are congruent to 4 or 12 mod 16 doubles, which makes the
+// 8x4 / 4x8 fragment loads of a half warp hit 16 distinct 8-byte bank pairs.
 #pragma once
 
 #include "common.cuh"
 
 namespace tdg {
 
-// Padded leading dimension >= n that is congruent to 12 modulo 16 (doubles).
-__host__ __device__ constexpr int mma_ld(int n) { return (n % 16 <= 12) ? (n / 16 * 16 + 12) : (n / 16 * 16 + 28); }
+// Smallest leading dimension >= n congruent to 4 or 12 modulo 16 (doubles): the 8x4 / 4x8
+// fragment loads of a half warp then hit 16 distinct 8-byte bank pairs.
+__host__ __device__ constexpr int mma_ld(int n) {
+    return (n % 16 <= 4) ? (n - n % 16 + 4) : ((n % 16 <= 12) ? (n - n % 16 + 12) : (n - n % 16 + 20));
+}
 __host__ __device__ constexpr int mma_tile_elements(int Q) { return (24 + Q - 1) / Q; }
 
 // Layout parameters shared by the host (table packing, tiling) and the kernel.
@@ -46,7 +49,9 @@ struct MmaTile {
     static constexpr int MYT = MY / 8;                             // m-tiles of Y
     static constexpr int YT = MYT * NTN;                           // Y tiles
     static constexpr int YPW = (YT + NW - 1) / NW;                 // Y tiles per warp
-    static constexpr int LDT = mma_ld(MY);
+    // Y's A^T fragments read table columns up to MY - 1 >= KP: those extra columns fall into the
+    // next table row (finite values) and only feed Y rows >= NBF, which are never written.
+    static constexpr int LDT = mma_ld(KP);
     static constexpr int LDN = mma_ld(NP);
     static constexpr int QC = 24;                                  // volume points per chunk (QC*D % 8 == 0)
 };
@@ -91,46 +96,123 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
 }
 
 // C[M x NP] = A[M x K] B[K x NP] for rows [0, mrows): A rows from `A` (ld LDT), B from `B` (ld
-// LDN), result to `C` (ld LDN).  Warp w computes m-tiles w, w + NW, ... across all n-tiles.
+// LDN), result to `C` (ld LDN).  The (m, n) output tiles are dealt round-robin to the warps; a
+// warp advances up to four of its tiles together so that consecutive mma have independent
+// accumulators.
 template <class L>
 __device__ __forceinline__ void cta_gemm_store(const double* A, const double* B, double* C, int mrows, int ksteps,
                                                int warp, int lane) {
     const int g = lane >> 2, t = lane & 3;
-    for (int mt = warp; mt < mrows / 8; mt += L::NW) {
-        double acc[L::NTN][2];
+    const int ntiles = (mrows / 8) * L::NTN;
+    for (int t0 = warp; t0 < ntiles; t0 += 4 * L::NW) {
+        double acc[4][2];
+        const double* ap[4];
+        const double* bp[4];
+        int cnt = 0;
 #pragma unroll
-        for (int n = 0; n < L::NTN; ++n) acc[n][0] = acc[n][1] = 0.0;
-        const double* a_row = A + (mt * 8 + g) * L::LDT + t;
-        for (int ks = 0; ks < ksteps; ++ks) {
-            const double a = a_row[ks * 4];
-            const double* b_row = B + (ks * 4 + t) * L::LDN + g;
-#pragma unroll
-            for (int n = 0; n < L::NTN; ++n) dmma(acc[n], a, b_row[n * 8]);
+        for (int j = 0; j < 4; ++j) {
+            acc[j][0] = acc[j][1] = 0.0;
+            const int tile = t0 + j * L::NW;
+            const int tt = tile < ntiles ? tile : t0;
+            const int mt = tt / L::NTN, nt = tt % L::NTN;
+            ap[j] = A + (mt * 8 + g) * L::LDT + t;
+            bp[j] = B + t * L::LDN + nt * 8 + g;
+            cnt += tile < ntiles;
         }
-        double* c_row = C + (mt * 8 + g) * L::LDN + 2 * t;
+        for (int ks = 0; ks < ksteps; ++ks) {
 #pragma unroll
-        for (int n = 0; n < L::NTN; ++n) {
-            c_row[n * 8] = acc[n][0];
-            c_row[n * 8 + 1] = acc[n][1];
+            for (int j = 0; j < 4; ++j)
+                if (j < cnt) dmma(acc[j], ap[j][ks * 4], bp[j][ks * 4 * L::LDN]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (j < cnt) {
+                const int tile = t0 + j * L::NW;
+                const int mt = tile / L::NTN, nt = tile % L::NTN;
+                double* c = C + (mt * 8 + g) * L::LDN + nt * 8 + 2 * t;
+                c[0] = acc[j][0];
+                c[1] = acc[j][1];
+            }
+        }
+    }
+}
+
+// Two independent GEMMs C0 = A0 B0 and C1 = A1 B1 of the same shape, dealt to the warps as one
+// tile space (better balance than two separate passes).
+template <class L>
+__device__ __forceinline__ void cta_gemm_store2(const double* A0, const double* B0, double* C0, const double* A1,
+                                                const double* B1, double* C1, int mrows, int ksteps, int warp,
+                                                int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const int per = (mrows / 8) * L::NTN;
+    const int ntiles = 2 * per;
+    for (int t0 = warp; t0 < ntiles; t0 += 4 * L::NW) {
+        double acc[4][2];
+        const double* ap[4];
+        const double* bp[4];
+        int cnt = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            acc[j][0] = acc[j][1] = 0.0;
+            const int tile = t0 + j * L::NW;
+            const int tt = tile < ntiles ? tile : t0;
+            const int which = tt / per, loc = tt % per;
+            const int mt = loc / L::NTN, nt = loc % L::NTN;
+            ap[j] = (which ? A1 : A0) + (mt * 8 + g) * L::LDT + t;
+            bp[j] = (which ? B1 : B0) + t * L::LDN + nt * 8 + g;
+            cnt += tile < ntiles;
+        }
+        for (int ks = 0; ks < ksteps; ++ks) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (j < cnt) dmma(acc[j], ap[j][ks * 4], bp[j][ks * 4 * L::LDN]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (j < cnt) {
+                const int tile = t0 + j * L::NW;
+                const int which = tile / per, loc = tile % per;
+                const int mt = loc / L::NTN, nt = loc % L::NTN;
+                double* c = (which ? C1 : C0) + (mt * 8 + g) * L::LDN + nt * 8 + 2 * t;
+                c[0] = acc[j][0];
+                c[1] = acc[j][1];
+            }
         }
     }
 }
 
 // Y[MY x NP] += A^T B where A is [K x LDT] (rows = reduction index, columns = Y rows) and B is
-// [K x LDN].  Warp w owns Y tiles w, w + NW, ...
+// [K x LDN].  Warp w owns Y tiles w, w + NW, ...; each tile keeps two partial accumulators (even
+// and odd k-steps) and the tiles advance together, so consecutive mma never share an accumulator.
 template <class L>
-__device__ __forceinline__ void cta_gemm_acc_t(const double* A, const double* B, double (&y)[L::YPW][2], int krows,
+__device__ __forceinline__ void cta_gemm_acc_t(const double* A, const double* B, double (&y)[L::YPW][2][2], int krows,
                                                int warp, int lane) {
     const int g = lane >> 2, t = lane & 3;
+    const double* ac[L::YPW];
+    const double* bc[L::YPW];
+    bool on[L::YPW];
 #pragma unroll
     for (int j = 0; j < L::YPW; ++j) {
         const int tile = warp + j * L::NW;
-        if (tile < L::YT) {
-            const int ym = tile % L::MYT, yn = tile / L::MYT;
-            const double* a_col = A + t * L::LDT + ym * 8 + g;
-            const double* b_col = B + t * L::LDN + yn * 8 + g;
-            for (int ks = 0; ks < krows / 4; ++ks) dmma(y[j], a_col[ks * 4 * L::LDT], b_col[ks * 4 * L::LDN]);
-        }
+        on[j] = tile < L::YT;
+        const int tt = on[j] ? tile : 0;
+        const int ym = tt % L::MYT, yn = tt / L::MYT;
+        ac[j] = A + t * L::LDT + ym * 8 + g;
+        bc[j] = B + t * L::LDN + yn * 8 + g;
+    }
+    const int ks_n = krows / 4;
+    int ks = 0;
+    for (; ks + 1 < ks_n; ks += 2) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int j = 0; j < L::YPW; ++j)
+                if (on[j]) dmma(y[j][h], ac[j][(ks + h) * 4 * L::LDT], bc[j][(ks + h) * 4 * L::LDN]);
+    }
+    if (ks < ks_n) {
+#pragma unroll
+        for (int j = 0; j < L::YPW; ++j)
+            if (on[j]) dmma(y[j][0], ac[j][ks * 4 * L::LDT], bc[j][ks * 4 * L::LDN]);
     }
 }
 
@@ -179,9 +261,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 1)
         }
         __syncthreads();
 
-        double yacc[L::YPW][2];
+        double yacc[L::YPW][2][2];
 #pragma unroll
-        for (int j = 0; j < L::YPW; ++j) yacc[j][0] = yacc[j][1] = 0.0;
+        for (int j = 0; j < L::YPW; ++j) yacc[j][0][0] = yacc[j][0][1] = yacc[j][1][0] = yacc[j][1][1] = 0.0;
 
         // ---------------- volume ----------------
         for (int q0 = 0; q0 < Nq; q0 += L::QC) {
@@ -271,32 +353,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 1)
                 sUN[k * LDN + c] = v;
             }
             __syncthreads();
-            {
-                const int mtf = lay.MF / 8;
-                const int g = lane >> 2, t = lane & 3;
-                for (int job = warp; job < 2 * mtf; job += L::NW) {
-                    const int which = job / mtf, mt8 = job % mtf;
-                    const double* A = TF + (which ? lp : f) * lay.MF * LDT;
-                    const double* B = which ? sUN : sU;
-                    double* C = which ? R1 : R0;
-                    double acc[L::NTN][2];
-#pragma unroll
-                    for (int n = 0; n < L::NTN; ++n) acc[n][0] = acc[n][1] = 0.0;
-                    const double* a_row = A + (mt8 * 8 + g) * LDT + t;
-                    for (int ks = 0; ks < L::KP / 4; ++ks) {
-                        const double a = a_row[ks * 4];
-                        const double* b_row = B + (ks * 4 + t) * LDN + g;
-#pragma unroll
-                        for (int n = 0; n < L::NTN; ++n) dmma(acc[n], a, b_row[n * 8]);
-                    }
-                    double* c_row = C + (mt8 * 8 + g) * LDN + 2 * t;
-#pragma unroll
-                    for (int n = 0; n < L::NTN; ++n) {
-                        c_row[n * 8] = acc[n][0];
-                        c_row[n * 8 + 1] = acc[n][1];
-                    }
-                }
-            }
+            cta_gemm_store2<L>(TF + f * lay.MF * LDT, sU, R0, TF + lp * lay.MF * LDT, sUN, R1, lay.MF, L::KP / 4, warp,
+                               lane);
             __syncthreads();
             for (int it = tid; it < TE * nq; it += NT) {
                 const int te = it % TE, q = it / TE;
@@ -492,7 +550,7 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 1)
                         if (k < NBF && c < L::NC) {
                             const int te = c / Q, r = c % Q;
                             const int el = s_el[te];
-                            if (el >= 0) yr[static_cast<int64_t>(el) * BS + k + NBF * r] = yacc[j][h];
+                            if (el >= 0) yr[static_cast<int64_t>(el) * BS + k + NBF * r] = yacc[j][0][h] + yacc[j][1][h];
                         }
                     }
                 }

@@ -278,3 +278,24 @@ def build(mesh: SimplexMesh, degree: int, boundary_bc=BC_DIRICHLET, interior_bc=
     topology(mesh, boundary_bc, interior_bc)
     p2 = p2_nodes(mesh, curve) if curve is not None else None
     return geometry_nodes(mesh, degree, p2, transform)
+
+
+def union(meshes: list[SimplexMesh]) -> tuple[SimplexMesh, np.ndarray]:
+    """Disjoint union of meshes that already carry topology and geometry nodes: one operator over
+    the union is block diagonal with one block per mesh.  Returns the union and the element offsets
+    [0, E_0, E_0 + E_1, ...]."""
+    D = meshes[0].dim
+    eoff = np.cumsum([0] + [m.num_elements for m in meshes]).astype(np.int64)
+    voff = np.cumsum([0] + [m.vertices.shape[0] for m in meshes]).astype(np.int64)
+    u = SimplexMesh(D, np.concatenate([m.vertices for m in meshes]),
+                    np.concatenate([m.elements + voff[i] for i, m in enumerate(meshes)]))
+    u.facets = np.concatenate([m.facets + voff[i] for i, m in enumerate(meshes)])
+    u.facet_up = np.concatenate([m.facet_up + eoff[i] for i, m in enumerate(meshes)])
+    u.facet_local = np.concatenate([m.facet_local for m in meshes])
+    u.facet_bc = np.concatenate([m.facet_bc for m in meshes])
+    degs = {m.geo_degree for m in meshes}
+    if len(degs) != 1:
+        raise ValueError("meshes must share the geometry degree")
+    u.geo_degree = degs.pop()
+    u.geo_nodes = np.concatenate([m.geo_nodes for m in meshes])
+    return u, eoff

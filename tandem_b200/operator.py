@@ -180,6 +180,28 @@ class DGOperator:
         return stats
 
 
+def solve_segmented(op: DGOperator, b, x, elem_offsets, precision: int = FP64, rtol: float = 1e-10,
+                    max_iterations: int = 20000, inner_rtol: float = 1e-4, max_outer: int = 40,
+                    use_graphs: bool = True, stream=None):
+    """Independent problems held in one block-diagonal operator (a mesh union): one apply and one
+    preconditioner launch per iteration cover every problem, each problem has its own CG scalars
+    and stopping test.  Returns (aggregate stats, per-problem relative residuals)."""
+    off = np.ascontiguousarray(elem_offsets, dtype=np.int64)
+    nseg = len(off) - 1
+    _check_vec(b, FP64, op.ndof)
+    _check_vec(x, FP64, op.ndof)
+    opts = _ffi.SolveOpts(precision, max_iterations, rtol, inner_rtol, max_outer, int(use_graphs))
+    st = _ffi.SolveStats()
+    rel = np.zeros(nseg)
+    rc = _ffi.lib().tdg_solve_segmented(op._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), nseg,
+                                        off.ctypes.data, C.byref(opts), C.byref(st), rel.ctypes.data, _stream(stream))
+    stats = dict(iterations=st.iterations, outer=st.outer, rel_residual=st.rel_residual, seconds=st.seconds,
+                 converged=bool(st.converged))
+    if rc != 0:
+        raise _ffi.TdgError(f"{_ffi.ERRORS.get(rc, rc)}: {_ffi.lib().tdg_last_error().decode()} {stats}")
+    return stats, rel
+
+
 def _check_vec(t, precision: int, n: int) -> None:
     import torch
     want = torch.float64 if precision == FP64 else torch.float32

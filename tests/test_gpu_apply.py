@@ -168,3 +168,31 @@ def test_elasticity_3d_properties_at_scale():
     orc.apply_range(e0, e1, xn, yref)
     bs = op.bs
     assert rel(ax.cpu().numpy()[e0 * bs:e1 * bs], yref[e0 * bs:e1 * bs]) < 1e-12
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32])
+def test_segmented_solve_of_a_mesh_union(precision):
+    """Three independent 2D elasticity problems of different sizes in one block-diagonal operator:
+    each problem's solution equals its own solve."""
+    from tandem_b200.operator import solve_segmented
+    from cases import material
+    meshes = [make_mesh(2, n, 4, curved=True) for n in (2, 5, 3)]
+    um, eoff = M.union(meshes)
+    q = tandem_quadrature(2, 4)
+    op = DGOperator(um, 4, ELASTICITY, q)
+    orc = Oracle(um, 4, ELASTICITY, q)
+    c0, c1 = material(ELASTICITY, 2, op.volume_coords(), True)
+    op.set_material(c0, c1)
+    orc.set_material(c0, c1)
+    _, _, _, f, g = mms_inputs(op, ELASTICITY, 2, True)
+    b = op.rhs(f, g)
+    op.bjacobi_setup(precision)
+    x = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+    st, rel = solve_segmented(op, dev(b), x, eoff, precision=precision, rtol=1e-10)
+    assert st["converged"] and np.all(rel <= 1e-10), (st, rel)
+    xs = x.cpu().numpy()
+    bs = op.bs
+    r = b - orc.apply(xs)
+    for i in range(len(meshes)):
+        sl = slice(eoff[i] * bs, eoff[i + 1] * bs)
+        assert np.linalg.norm(r[sl]) / np.linalg.norm(b[sl]) <= 1.5e-10
