@@ -183,6 +183,17 @@ int tdg_solve_segmented(tdg_op* op, const double* b, double* x, int nseg, const 
                         const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel_residual,
                         void* stream);
 
+/* --- adjoint gradient (no counterpart in tandem: tandem solves forward problems only) ---------- */
+
+/* Gradient of a functional J(u) with respect to per-element constant Lame parameters of an
+ * elasticity operator whose material is piecewise constant (lambda_e, mu_e per element):
+ * grad[e][0] = dJ/dlambda_e, grad[e][1] = dJ/dmu_e = p^T db/dtheta_e - p^T dA/dtheta_e u, where u
+ * solves A u = b and p solves A p = dJ/du (A is symmetric).  u, p: device [E][bs]; bc_q: device
+ * [F][D][nq] Dirichlet / slip data used in b (NULL when b has no boundary data); grad: device
+ * [E][2].  TDG_E_INVALID when the material is not piecewise constant. */
+int tdg_adjoint_lame_gradient(tdg_op* op, const double* u, const double* p, const double* bc_q, double* grad,
+                              void* stream);
+
 /* --- fault coupling, Green's functions (app/form/SeasQDDiscreteGreenOperator.cpp:493-578) ---- */
 
 typedef struct tdg_fault tdg_fault;

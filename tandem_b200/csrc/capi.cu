@@ -972,3 +972,73 @@ extern "C" int tdg_fault_traction(tdg_fault* fault, const double* u, int64_t ld,
                           static_cast<cudaStream_t>(stream));
     return rc ? fail(rc, "fault traction launch failed") : 0;
 }
+
+// ------------------------------------------------------------------------------------------------
+// adjoint gradient with respect to per-element Lame parameters
+// ------------------------------------------------------------------------------------------------
+
+namespace {
+// Host part of the Lame gradient: checks that the material is constant per element and fills
+// dpen = [F][4] penalty derivatives (d/dlam, d/dmu of each side's contribution) followed by
+// [E][2] element (lam, mu), the layout adjoint_lame_kernel reads.
+int lame_gradient_inputs(tdg_op* op, std::vector<double>& dpen) {
+    auto const& h = op->h;
+    if (h.kind != 1) return fail(TDG_E_INVALID, "the Lame gradient needs an elasticity operator");
+    if (!h.has_material) return fail(TDG_E_STATE, "no material");
+    const int nm = h.mat_space.num_basis();
+    const int D = h.D;
+    // piecewise-constant material: every nodal coefficient of an element equals its mean
+    std::vector<double> lam(h.E), mu(h.E);
+    for (int64_t e = 0; e < h.E; ++e) {
+        const double* a = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 0) * nm];
+        const double* b = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 1) * nm];
+        double sa = 0.0, sb = 0.0;
+        for (int i = 0; i < nm; ++i) {
+            sa += a[i];
+            sb += b[i];
+        }
+        lam[e] = sa / nm;
+        mu[e] = sb / nm;
+        for (int i = 0; i < nm; ++i)
+            if (std::fabs(a[i] - lam[e]) > 1e-10 * std::fabs(lam[e]) || std::fabs(b[i] - mu[e]) > 1e-10 * std::fabs(mu[e]))
+                return fail(TDG_E_INVALID, "material is not constant per element");
+    }
+    // penalty derivatives (Elasticity::prepare_penalty with c0 = 2 mu, c1 = D lam + 2 mu):
+    // p_s = K_s c1^2 / c0, K_s = (D + 1) c_{N-1} |f| / |E_s|; interior pen = (p0 + p1) / 4
+    const double cN1 = h.N * (h.N - 1.0 + D) / static_cast<double>(D);
+    dpen.assign(static_cast<size_t>(h.F) * 4 + static_cast<size_t>(h.E) * 2, 0.0);
+    for (int64_t f = 0; f < h.F; ++f) {
+        const bool interior = h.up[2 * f] != h.up[2 * f + 1];
+        for (int s = 0; s < (interior ? 2 : 1); ++s) {
+            const int64_t e = h.up[2 * f + s];
+            const double K = (D + 1) * cN1 * h.area[f] / h.volume[e];
+            const double c0 = 2.0 * mu[e], c1 = D * lam[e] + 2.0 * mu[e];
+            const double scale = interior ? 0.25 : 1.0;
+            dpen[static_cast<size_t>(f) * 4 + 2 * s + 0] = scale * K * 2.0 * c1 * D / c0;
+            dpen[static_cast<size_t>(f) * 4 + 2 * s + 1] = scale * K * (4.0 * c1 / c0 - 2.0 * c1 * c1 / (c0 * c0));
+        }
+    }
+    for (int64_t e = 0; e < h.E; ++e) {
+        dpen[static_cast<size_t>(h.F) * 4 + 2 * e] = lam[e];
+        dpen[static_cast<size_t>(h.F) * 4 + 2 * e + 1] = mu[e];
+    }
+    return 0;
+}
+}  // namespace
+
+extern "C" int tdg_adjoint_lame_gradient(tdg_op* op, const double* u, const double* p, const double* bc_q,
+                                         double* grad, void* stream) {
+    if (!op || !u || !p || !grad) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = op->h;
+    std::vector<double> dpen;
+    TDG_TRY(lame_gradient_inputs(op, dpen));
+    TDG_TRY(ensure_uploaded(op, TDG_FP64));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double* d = nullptr;
+    TDG_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d), dpen.size() * sizeof(double), s));
+    TDG_CUDA_TRY(cudaMemcpyAsync(d, dpen.data(), dpen.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    int rc = launch_adjoint_lame(h.D, h.N, op->op64, u, p, bc_q, d, grad, s);
+    cudaFreeAsync(d, s);
+    TDG_CUDA_TRY(cudaStreamSynchronize(s));
+    return rc ? fail(rc, "adjoint gradient launch failed") : 0;
+}

@@ -35,6 +35,12 @@ int launch_fault(int D, int N, bool traction, DevOp<double> const& op, DevFault 
                  int64_t ld, const double* slip, int64_t ld_slip, double* out, int64_t ld_out, int nrhs,
                  cudaStream_t s);
 
+// Gradient of J with respect to per-element constant (lambda, mu) from state u and adjoint p
+// (adjoint.cuh).  dpen: [F][4] penalty derivatives (d/dlam, d/dmu per side) followed by [E][2]
+// element (lam, mu); bcq: [F][D][nq] Dirichlet data or null.
+int launch_adjoint_lame(int D, int N, DevOp<double> const& op, const double* u, const double* p, const double* bcq,
+                        const double* dpen, double* grad, cudaStream_t s);
+
 // Number of resident CTAs of a kernel on the current device times the SM count, cached.
 int device_sm_count();
 

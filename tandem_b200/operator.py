@@ -74,7 +74,10 @@ class DGOperator:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _ffi.lib().tdg_destroy(h)
+            try:
+                _ffi.lib().tdg_destroy(h)
+            except Exception:  # noqa: BLE001 - interpreter shutdown: the library may be gone
+                pass
             self._h = None
 
     # -- sizes (AbstractDGOperator) --------------------------------------------------------------
@@ -230,7 +233,10 @@ class Fault:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _ffi.lib().tdg_fault_destroy(h)
+            try:
+                _ffi.lib().tdg_fault_destroy(h)
+            except Exception:  # noqa: BLE001 - interpreter shutdown
+                pass
             self._h = None
 
     def slip_rhs(self, slip, b, nrhs: int = 1, stream=None) -> None:
