@@ -94,6 +94,7 @@ def _make_function():
             u = problem.forward(lam.detach().cpu().numpy(), mu.detach().cpu().numpy())
             ctx.problem = problem
             ctx.theta = (lam.detach().cpu().numpy().copy(), mu.detach().cpu().numpy().copy())
+            ctx.devices = (lam.device, mu.device)
             ctx.save_for_backward(u)
             return u
 
@@ -104,7 +105,7 @@ def _make_function():
             pb.set_parameters(*ctx.theta)
             p = pb.solve(grad_u.contiguous().to(torch.float64))
             g = pb.gradient(u, p)
-            return g[:, 0].to(grad_u.device), g[:, 1].to(grad_u.device), None
+            return g[:, 0].to(ctx.devices[0]), g[:, 1].to(ctx.devices[1]), None
 
     return LameSolve
 

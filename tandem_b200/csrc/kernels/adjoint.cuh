@@ -201,28 +201,31 @@ __global__ void __launch_bounds__(kAdjThreads)
             // operator part (subtracted): facet coefficient terms and the penalty
             gl -= wq * (-fac * (dp * jun + du * jpn) + dpl * nl * pen_jj);
             gm -= wq * (-fac * (su_ + sp_) + dpm * nl * pen_jj);
-            // right-hand side part: Dirichlet / slip data g on this facet (tandem's bc_q)
-            if (bcq) {
+            // right-hand side part: Dirichlet / slip data g on Dirichlet and fault facets
+            // (rhs_boundary / rhs_skeleton): b_s += c10 sum w sigma_s(phi) n.g + c20_s sum w |n| phi.g
+            // with c20 = +pen (side 0) / -pen (side 1); the penalty depends on both sides, so its
+            // derivative multiplies the jump of the adjoint trace.
+            if (bcq && fd) {
                 double g[D], gn = 0.0, gsym = 0.0, pg = 0.0;
                 const bool boundary = !skel;
                 const double half = (boundary && bcv == 3) ? 0.5 : 1.0;  // bc_boundary halves slip
 #pragma unroll
                 for (int i = 0; i < D; ++i) g[i] = half * bcq[(static_cast<int64_t>(fct) * D + i) * nq + q];
-                // g is given with the side-0 orientation; n0 = side-0 normal
+                // g and the normal of the lift are those of side 0
                 double n0[D];
 #pragma unroll
                 for (int i = 0; i < D; ++i) n0[i] = op.fN[(static_cast<int64_t>(fct) * D + i) * nq + q];
+                const double sg = (boundary || side == 0) ? 1.0 : -1.0;
 #pragma unroll
                 for (int i = 0; i < D; ++i) {
                     gn += g[i] * n0[i];
-                    pg += tp[i] * g[i];
+                    pg += sg * (tp[i] - tpn[i]) * g[i];  // side-0 trace minus side-1 trace
 #pragma unroll
-                    for (int s = 0; s < D; ++s) gsym += g[i] * (Jp[i][s] + Jp[s][i]) * n0[s];
+                    for (int s2 = 0; s2 < D; ++s2) gsym += g[i] * (Jp[i][s2] + Jp[s2][i]) * n0[s2];
                 }
                 const double c10 = boundary ? -1.0 : -0.5;
-                const double sg20 = (boundary || side == 0) ? 1.0 : -1.0;  // c20 = +-penalty
-                gl += wq * (c10 * dp * gn + sg20 * dpl * nl * pg);
-                gm += wq * (c10 * gsym + sg20 * dpm * nl * pg);
+                gl += wq * (c10 * dp * gn + dpl * nl * pg);
+                gm += wq * (c10 * gsym + dpm * nl * pg);
             }
         }
     }
