@@ -194,6 +194,23 @@ int tdg_solve_segmented(tdg_op* op, const double* b, double* x, int nseg, const 
 int tdg_adjoint_lame_gradient(tdg_op* op, const double* u, const double* p, const double* bc_q, double* grad,
                               void* stream);
 
+/* Allocation-free variant of tdg_adjoint_lame_gradient (no counterpart in tandem).  Same inputs,
+ * output and arithmetic; it calls no device or host allocator.  For callers that cannot allocate
+ * device memory at the time of the call: a process whose caching allocator (torch, PETSc pools)
+ * already holds the device memory, where a fresh cudaMallocAsync can fail with out-of-memory in the
+ * middle of an optimisation loop, or a caller running inside an allocator or memory-pool callback.
+ * The per-facet penalty derivatives go through a fixed device scratch, a static __device__ array
+ * of 2^20 doubles (8 MiB) per device: meshes with 4 F + 2 E > 2^20 (about 120,000 tetrahedra or
+ * 170,000 triangles) return TDG_E_INVALID with the sizes in tdg_last_error.  Every scratch entry
+ * the kernel reads is written by the call, so nothing needs clearing.  The operator's FP64 data
+ * must already be resident (one FP64 tdg_apply after tdg_set_material), else TDG_E_STATE.
+ * Calls on one device share the scratch: overlapping calls (two host threads, or two streams)
+ * race and must be serialised by the caller.  The call synchronises `stream` before returning.
+ * The first call on each device looks up the scratch address (cudaGetSymbolAddress, with that
+ * device current); make it before any stream capture begins. */
+int tdg_adjoint_lame_gradient_noalloc(tdg_op* op, const double* u, const double* p, const double* bc_q,
+                                      double* grad, void* stream);
+
 /* --- fault coupling, Green's functions (app/form/SeasQDDiscreteGreenOperator.cpp:493-578) ---- */
 
 typedef struct tdg_fault tdg_fault;

@@ -82,6 +82,19 @@ class LameProblem:
                                                         C.c_void_p(g.data_ptr()), _stream(stream)))
         return g
 
+    def gradient_noalloc(self, u, p, grad, stream=None):
+        """Allocation-free gradient into the caller's grad [E, 2] (CUDA float64): no device or host
+        allocation inside the call.  Meshes up to 4 F + 2 E <= 2^20 (fixed 8 MiB device scratch);
+        the FP64 operator data must be resident (an FP64 apply after set_material).  Calls on one
+        device must not overlap."""
+        _check_vec(u, FP64, self.op.ndof)
+        _check_vec(p, FP64, self.op.ndof)
+        _check_vec(grad, FP64, 2 * self.op.E)
+        bcq = None if self._bcq_dev is None else C.c_void_p(self._bcq_dev.data_ptr())
+        _ffi.check(_ffi.lib().tdg_adjoint_lame_gradient_noalloc(self.op._h, C.c_void_p(u.data_ptr()),
+                                                                C.c_void_p(p.data_ptr()), bcq,
+                                                                C.c_void_p(grad.data_ptr()), _stream(stream)))
+
 
 def _make_function():
     import torch

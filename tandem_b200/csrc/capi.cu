@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <type_traits>
 #include <cstring>
@@ -1040,5 +1041,83 @@ extern "C" int tdg_adjoint_lame_gradient(tdg_op* op, const double* u, const doub
     int rc = launch_adjoint_lame(h.D, h.N, op->op64, u, p, bc_q, d, grad, s);
     cudaFreeAsync(d, s);
     TDG_CUDA_TRY(cudaStreamSynchronize(s));
+    return rc ? fail(rc, "adjoint gradient launch failed") : 0;
+}
+
+// Allocation-free variant: the penalty derivatives go through the fixed device scratch of
+// adjoint.cu in chunks staged on the stack; the operator's FP64 data must already be resident.
+extern "C" int tdg_adjoint_lame_gradient_noalloc(tdg_op* op, const double* u, const double* p, const double* bc_q,
+                                                 double* grad, void* stream) {
+    if (!op || !u || !p || !grad) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = op->h;
+    if (h.kind != 1) return fail(TDG_E_INVALID, "the Lame gradient needs an elasticity operator");
+    if (!h.has_material) return fail(TDG_E_STATE, "no material");
+    const size_t need = static_cast<size_t>(h.F) * 4 + static_cast<size_t>(h.E) * 2;
+    if (need > kAdjointScratchDoubles) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg,
+                      "mesh needs %zu doubles of scratch (4 per facet + 2 per element), the fixed scratch "
+                      "holds %zu (8 MiB); use tdg_adjoint_lame_gradient",
+                      need, kAdjointScratchDoubles);
+        return fail(TDG_E_INVALID, msg);
+    }
+    if (!op->uploaded64)
+        return fail(TDG_E_STATE, "FP64 operator data not resident: call tdg_apply (FP64) once after tdg_set_material");
+    const int nm = h.mat_space.num_basis();
+    const int D = h.D;
+    auto lam_mu = [&](int64_t e, double& lam, double& mu) {
+        const double* a = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 0) * nm];
+        const double* b = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 1) * nm];
+        double sa = 0.0, sb = 0.0;
+        for (int i = 0; i < nm; ++i) {
+            sa += a[i];
+            sb += b[i];
+        }
+        lam = sa / nm;
+        mu = sb / nm;
+    };
+    for (int64_t e = 0; e < h.E; ++e) {
+        double lam, mu;
+        lam_mu(e, lam, mu);
+        const double* a = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 0) * nm];
+        const double* b = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 1) * nm];
+        for (int i = 0; i < nm; ++i)
+            if (std::fabs(a[i] - lam) > 1e-10 * std::fabs(lam) || std::fabs(b[i] - mu) > 1e-10 * std::fabs(mu))
+                return fail(TDG_E_INVALID, "material is not constant per element");
+    }
+    double* scratch = nullptr;
+    if (adjoint_scratch(&scratch)) return fail(TDG_E_CUDA, "looking up the fixed scratch failed");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the same values as lame_gradient_inputs, produced entry by entry
+    const double cN1 = h.N * (h.N - 1.0 + D) / static_cast<double>(D);
+    auto entry = [&](size_t i) -> double {
+        if (i >= static_cast<size_t>(h.F) * 4) {
+            const size_t j = i - static_cast<size_t>(h.F) * 4;
+            double lam, mu;
+            lam_mu(static_cast<int64_t>(j / 2), lam, mu);
+            return (j % 2) ? mu : lam;
+        }
+        const int64_t f = static_cast<int64_t>(i / 4);
+        const int side = static_cast<int>((i % 4) / 2);
+        const bool interior = h.up[2 * f] != h.up[2 * f + 1];
+        if (side == 1 && !interior) return 0.0;
+        const int64_t e = h.up[2 * f + side];
+        double lam, mu;
+        lam_mu(e, lam, mu);
+        const double K = (D + 1) * cN1 * h.area[f] / h.volume[e];
+        const double c0 = 2.0 * mu, c1 = D * lam + 2.0 * mu;
+        const double scale = interior ? 0.25 : 1.0;
+        return (i % 2) ? scale * K * (4.0 * c1 / c0 - 2.0 * c1 * c1 / (c0 * c0)) : scale * K * 2.0 * c1 * D / c0;
+    };
+    constexpr size_t kStage = 2048;
+    double stage[kStage];
+    for (size_t c0 = 0; c0 < need; c0 += kStage) {
+        const size_t n = std::min(kStage, need - c0);
+        for (size_t k = 0; k < n; ++k) stage[k] = entry(c0 + k);
+        TDG_CUDA_TRY(cudaMemcpyAsync(scratch + c0, stage, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        TDG_CUDA_TRY(cudaStreamSynchronize(s));  // the stage is reused
+    }
+    int rc = launch_adjoint_lame(h.D, h.N, op->op64, u, p, bc_q, scratch, grad, s);
+    TDG_CUDA_TRY(cudaStreamSynchronize(s));  // the scratch is free again when the call returns
     return rc ? fail(rc, "adjoint gradient launch failed") : 0;
 }

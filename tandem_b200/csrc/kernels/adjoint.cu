@@ -36,3 +36,35 @@ int launch_adjoint_lame(int D, int N, DevOp<double> const& op, const double* u, 
 }
 
 }  // namespace tdg
+
+// ------------------------------------------------------------------------------------------------
+// Fixed scratch of the allocation-free gradient entry point
+// ------------------------------------------------------------------------------------------------
+
+#include <mutex>
+
+namespace tdg {
+
+namespace {
+// One copy per device, part of the module image: nothing is allocated when it is used.
+static __device__ __align__(256) double g_adjoint_scratch[kAdjointScratchDoubles];
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+double* g_scratch_ptr[kMaxDevices] = {};
+}  // namespace
+
+int adjoint_scratch(double** ptr) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TDG_E_CUDA;
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        // once per device, with that device current
+        if (cudaGetSymbolAddress(&p, g_adjoint_scratch) != cudaSuccess || !p) return TDG_E_CUDA;
+        g_scratch_ptr[dev] = static_cast<double*>(p);
+    }
+    *ptr = g_scratch_ptr[dev];
+    return 0;
+}
+
+}  // namespace tdg

@@ -41,6 +41,12 @@ int launch_fault(int D, int N, bool traction, DevOp<double> const& op, DevFault 
 int launch_adjoint_lame(int D, int N, DevOp<double> const& op, const double* u, const double* p, const double* bcq,
                         const double* dpen, double* grad, cudaStream_t s);
 
+// Fixed device scratch of tdg_adjoint_lame_gradient_noalloc: 2^20 doubles (8 MiB) per device, a
+// static __device__ array.  adjoint_scratch returns its address on the current device (looked up
+// once per device); TDG_E_CUDA when the lookup fails.
+constexpr size_t kAdjointScratchDoubles = size_t(1) << 20;
+int adjoint_scratch(double** ptr);
+
 // Number of resident CTAs of a kernel on the current device times the SM count, cached.
 int device_sm_count();
 
