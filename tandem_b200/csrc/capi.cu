@@ -3,6 +3,7 @@
 #include "../../include/tandem_b200.h"
 #include "host/setup.hpp"
 #include "kernels/apply_mma.cuh"
+#include "kernels/apply_tc32.cuh"
 #include "kernels/dispatch.hpp"
 #include "kernels/krylov.cuh"
 
@@ -114,6 +115,7 @@ struct tdg_op {
     DevOp<double> op64;
     DevOp<float> op32;
     MmaTiles mma;           // FP64 tensor-pipe apply: packed tables and signature tiles
+    Tc32Tiles tc32;         // FP32 tensor-core apply (3xTF32): packed tables and signature tiles
     bool use_mma = true;
     const double* penalty = nullptr;
     const int4* sides = nullptr;
@@ -146,6 +148,8 @@ int upload_common(tdg_op* op) {
 // m = q * D + e the reference derivative e of basis k at volume point q; TF[f][m][k] the same at
 // the facet points of local face f followed by the basis values.  Leading dimension mma_ld(MY).
 // Tiles group elements by their neighbour-face signature (nb_local per face, 2 bits each).
+void signature_tiles(HostOperator const& h, int TE, std::vector<int>& perm, std::vector<int4>& tiles);
+
 int upload_mma(tdg_op* op, DevArena& arena) {
     auto const& h = op->h;
     const int D = h.D, NBF = h.Nbf, Nq = h.Nq, nq = h.nq, NF = h.nfaces;
@@ -165,8 +169,23 @@ int upload_mma(tdg_op* op, DevArena& arena) {
                 T[static_cast<size_t>(D * nq + q) * LDT + k] = h.E_qf[f](k, q);
             }
     }
-    const int TE = mma_tile_elements(h.Q);
-    std::vector<int> sig(h.E), perm(h.E);
+    std::vector<int> perm;
+    std::vector<int4> tiles;
+    signature_tiles(h, mma_tile_elements(h.Q), perm, tiles);
+    TDG_CUDA_TRY(arena.upload(&op->mma.tables, tab));
+    TDG_CUDA_TRY(arena.upload(&op->mma.perm, perm));
+    TDG_CUDA_TRY(arena.upload(&op->mma.tiles, tiles));
+    op->mma.ntiles = static_cast<int>(tiles.size());
+    op->mma.table_doubles = static_cast<int>(tab.size());
+    return 0;
+}
+
+// Elements grouped by the local face numbers their neighbours see them through (2 bits per
+// face), cut into tiles of at most TE elements with one signature each.
+void signature_tiles(HostOperator const& h, int TE, std::vector<int>& perm, std::vector<int4>& tiles) {
+    const int NF = h.nfaces;
+    std::vector<int> sig(h.E);
+    perm.resize(h.E);
     for (int64_t e = 0; e < h.E; ++e) {
         int sg = 0;
         for (int f = 0; f < NF; ++f) sg |= (h.sides[static_cast<size_t>(e) * NF + f].nb_local & 3) << (2 * f);
@@ -174,18 +193,46 @@ int upload_mma(tdg_op* op, DevArena& arena) {
         perm[e] = static_cast<int>(e);
     }
     std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return sig[a] < sig[b]; });
-    std::vector<int4> tiles;
+    tiles.clear();
     for (int64_t i = 0; i < h.E;) {
         int64_t j = i;
         while (j < h.E && j - i < TE && sig[perm[j]] == sig[perm[i]]) ++j;
         tiles.push_back(make_int4(static_cast<int>(i), static_cast<int>(j - i), sig[perm[i]], 0));
         i = j;
     }
-    TDG_CUDA_TRY(arena.upload(&op->mma.tables, tab));
-    TDG_CUDA_TRY(arena.upload(&op->mma.perm, perm));
-    TDG_CUDA_TRY(arena.upload(&op->mma.tiles, tiles));
-    op->mma.ntiles = static_cast<int>(tiles.size());
-    op->mma.table_doubles = static_cast<int>(tab.size());
+}
+
+// FP32 tensor-core apply: tables as in apply_tc32.cuh (K padded to 8, ld = K + 4, rows padded to
+// 16) and signature tiles of tc32_tile_elements elements.
+int upload_tc32(tdg_op* op, DevArena& arena) {
+    auto const& h = op->h;
+    const int D = h.D, NBF = h.Nbf, Nq = h.Nq, nq = h.nq, NF = h.nfaces;
+    const int KP = tc_round(NBF, 8), LDT = KP + 4;
+    const int MV = tc_round(D * Nq, 16), MF = tc_round((D + 1) * nq, 16);
+    std::vector<float> tab(static_cast<size_t>(MV) * LDT + static_cast<size_t>(NF) * MF * LDT, 0.0f);
+    for (int q = 0; q < Nq; ++q)
+        for (int e = 0; e < D; ++e)
+            for (int k = 0; k < NBF; ++k)
+                tab[static_cast<size_t>(q * D + e) * LDT + k] =
+                    static_cast<float>(h.Dxi_Q[(static_cast<size_t>(k) * D + e) * Nq + q]);
+    for (int f = 0; f < NF; ++f) {
+        float* T = &tab[static_cast<size_t>(MV) * LDT + static_cast<size_t>(f) * MF * LDT];
+        for (int q = 0; q < nq; ++q)
+            for (int k = 0; k < NBF; ++k) {
+                for (int e = 0; e < D; ++e)
+                    T[static_cast<size_t>(q * D + e) * LDT + k] =
+                        static_cast<float>(h.Dxi_qf[f][(static_cast<size_t>(k) * D + e) * nq + q]);
+                T[static_cast<size_t>(D * nq + q) * LDT + k] = static_cast<float>(h.E_qf[f](k, q));
+            }
+    }
+    std::vector<int> perm;
+    std::vector<int4> tiles;
+    signature_tiles(h, tc32_tile_elements(D, h.Q), perm, tiles);
+    TDG_CUDA_TRY(arena.upload(&op->tc32.tables, tab));
+    TDG_CUDA_TRY(arena.upload(&op->tc32.perm, perm));
+    TDG_CUDA_TRY(arena.upload(&op->tc32.tiles, tiles));
+    op->tc32.ntiles = static_cast<int>(tiles.size());
+    op->tc32.table_floats = static_cast<int>(tab.size());
     return 0;
 }
 
@@ -242,6 +289,7 @@ int upload_precision(tdg_op* op, DevArena& arena, DevOp<T>& d) {
     d.penalty = op->penalty;
     d.sides = op->sides;
     if constexpr (std::is_same_v<T, double>) TDG_TRY(upload_mma(op, arena));
+    if constexpr (std::is_same_v<T, float>) TDG_TRY(upload_tc32(op, arena));
     TDG_CUDA_TRY(cudaDeviceSynchronize());
     return 0;
 }
@@ -425,7 +473,10 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
     if (precision == TDG_FP64 && rc == TDG_E_INVALID)
         rc = launch_apply<double>(h.D, h.N, h.kind, op->op64, static_cast<const double*>(x),
                                   static_cast<double*>(y), nrhs, ld, s);
-    else if (precision == TDG_FP32)
+    if (precision == TDG_FP32 && op->use_mma)
+        rc = launch_apply_tc32(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const float*>(x),
+                               static_cast<float*>(y), nrhs, ld, s);
+    if (precision == TDG_FP32 && rc == TDG_E_INVALID)
         rc = launch_apply<float>(h.D, h.N, h.kind, op->op32, static_cast<const float*>(x),
                                  static_cast<float*>(y), nrhs, ld, s);
     if (rc) return fail(rc, std::string("apply launch failed: ") + cudaGetErrorString(cudaGetLastError()));

@@ -1,0 +1,70 @@
+// Instances and launcher of the FP32 tensor-core apply (apply_tc32.cuh).
+#include "apply_tc32.cuh"
+#include "dispatch.hpp"
+
+#include "../../../include/tandem_b200.h"
+
+namespace tdg {
+
+namespace {
+
+template <class S>
+int run_apply_tc32(DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y, int nrhs, int64_t ld,
+                   cudaStream_t s) {
+    using L = Tc32Tile<S>;
+    const Tc32Layout lay = tc32_layout<S>(op.Nq, op.nq);
+    const size_t smem = sizeof(float) * static_cast<size_t>(lay.total);
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem + 2 * L::TE * sizeof(int) > static_cast<size_t>(optin)) return TDG_E_INVALID;
+    auto kern = apply_tc32_kernel<S>;
+    static size_t configured = 0;
+    static int per_sm = 0;
+    if (configured < smem) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+            cudaSuccess)
+            return TDG_E_CUDA;
+        configured = smem;
+        per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L::NT, smem) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+    }
+    const int64_t nwork = static_cast<int64_t>(mt.ntiles) * nrhs;
+    int64_t grid = static_cast<int64_t>(device_sm_count()) * per_sm;
+    if (grid > nwork) grid = nwork;
+    if (grid < 1) grid = 1;
+    kern<<<static_cast<unsigned>(grid), L::NT, smem, s>>>(op, mt, x, y, ld, nrhs);
+    return cudaGetLastError() == cudaSuccess ? 0 : TDG_E_CUDA;
+}
+
+template <int D, int N>
+int tc_kind(int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y, int nrhs, int64_t ld,
+            cudaStream_t s) {
+    if (kind == kPoisson) return run_apply_tc32<Shape<D, N, kPoisson>>(op, mt, x, y, nrhs, ld, s);
+    return run_apply_tc32<Shape<D, N, kElasticity>>(op, mt, x, y, nrhs, ld, s);
+}
+
+template <int D>
+int tc_deg(int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y, int nrhs,
+           int64_t ld, cudaStream_t s) {
+    switch (N) {
+        case 1: return tc_kind<D, 1>(kind, op, mt, x, y, nrhs, ld, s);
+        case 2: return tc_kind<D, 2>(kind, op, mt, x, y, nrhs, ld, s);
+        case 3: return tc_kind<D, 3>(kind, op, mt, x, y, nrhs, ld, s);
+        case 4: return tc_kind<D, 4>(kind, op, mt, x, y, nrhs, ld, s);
+        default: return TDG_E_INVALID;
+    }
+}
+
+}  // namespace
+
+int launch_apply_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y,
+                      int nrhs, int64_t ld, cudaStream_t s) {
+    if (nrhs < 1 || mt.ntiles < 1) return TDG_E_INVALID;
+    if (D == 2) return tc_deg<2>(N, kind, op, mt, x, y, nrhs, ld, s);
+    if (D == 3) return tc_deg<3>(N, kind, op, mt, x, y, nrhs, ld, s);
+    return TDG_E_INVALID;
+}
+
+}  // namespace tdg

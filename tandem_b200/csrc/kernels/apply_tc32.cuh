@@ -1,0 +1,569 @@
+// FP32 operator apply on the tensor cores: mma.sync m16n8k8 with TF32 operands in the split
+// ("3xTF32") form a*b ~ a_hi*b_hi + a_hi*b_lo + a_lo*b_hi, where a_hi = tf32(a) and
+// a_lo = tf32(a - a_hi).  Each product then carries about 21 significant bits, close to FP32,
+// and every sum is accumulated in FP32.  This is the inner operator of the mixed-precision solve
+// (FP32 Krylov iterations inside FP64 iterative refinement); the facet penalty products are formed
+// in FP64 and rounded once.
+//
+// Same algorithm and data flow as the FP64 kernel of apply_mma.cuh (tandem's element-centric
+// apply: volume term, then per local face the own/neighbour traces, the numerical fluxes and the
+// lift-back; see apply.cuh for the reference citations), with a different work split:
+//
+//   * a tile holds TE elements; its columns are (element, component) pairs, c = te * Q + r;
+//   * forward GEMMs R = T x U (T: basis table in shared memory, U: the tile's coefficients) are
+//     cut into units (16-row m-tile, group of NPW 8-column n-tiles).  A warp keeps the U fragments
+//     of its n-tile group in registers (split into hi/lo at use), so every table fragment it loads
+//     feeds 3 * NPW mma;
+//   * back-projections Y += T^T R accumulate in registers for the whole tile.  The Y units
+//     (16-row m-tile of Y, n-tile group) are owned by fixed warps; when there are fewer units than
+//     warps, KSP warps share a unit and split the reduction index, and the partial sums meet in
+//     shared memory once per tile, where the output block is also staged for coalesced stores.
+//
+// Shared-memory strides: tables and U use ld = 4 (mod 8) floats (conflict-free A / B fragment
+// loads of the forward GEMM); R uses ld = 8 or 24 (mod 32) floats (conflict-free C stores and B
+// loads of the back-projection).  The transposed table reads of the back-projection have 2-way
+// conflicts.
+#pragma once
+
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace tdg {
+
+__host__ __device__ constexpr int tc_round(int x, int m) { return (x + m - 1) / m * m; }
+__host__ __device__ constexpr int tc_ldr(int np) {
+    return (np % 32 == 8 || np % 32 == 24) ? np : tc_ldr(np + 8);
+}
+
+// Elements per tile: 48 columns for 3D elasticity, 64 otherwise.
+__host__ __device__ constexpr int tc32_tile_elements(int D, int Q) { return ((D == 3 && Q == 3) ? 48 : 64) / Q; }
+
+template <class S>
+struct Tc32Tile {
+    static constexpr int TE = tc32_tile_elements(S::D, S::Q);
+    static constexpr int NC = TE * S::Q;
+    static constexpr int NP = tc_round(NC, 8);
+    static constexpr int NTN = NP / 8;
+    static constexpr int NPW = (NTN % 3 == 0) ? 3 : ((NTN % 2 == 0) ? 2 : 1);
+    static constexpr int NG = NTN / NPW;
+    static constexpr int KP = tc_round(S::NBF, 8);
+    static constexpr int KS = KP / 8;
+    static constexpr int LDT = KP + 4;  // = 4 mod 8
+    static constexpr int LDU = LDT;
+    static constexpr int LDR = tc_ldr(NP);
+    static constexpr int MY = tc_round(S::NBF, 16);
+    static constexpr int MYT = MY / 16;
+    static constexpr int YU = MYT * NG;
+    static constexpr int NW = (S::D == 3 && S::Q == 3 && S::NBF > 20) ? 12 : 8;
+    static constexpr int NT = 32 * NW;
+    static constexpr int KSP = (YU >= NW) ? 1 : NW / YU;
+    static constexpr int UPW = (YU + NW - 1) / NW;
+    static constexpr int MINB = (S::D == 2) ? 2 : 1;
+};
+
+struct Tc32Layout {
+    int MV, MF;                 // padded rows of TV and of each TF (multiples of 16)
+    int off_TF, off_U, off_UN, off_R0, off_R1;
+    int total;                  // floats
+};
+
+template <class S>
+__host__ __device__ inline Tc32Layout tc32_layout(int Nq, int nq) {
+    using L = Tc32Tile<S>;
+    Tc32Layout l;
+    l.MV = tc_round(S::D * Nq, 16);
+    l.MF = tc_round((S::D + 1) * nq, 16);
+    const int r0_rows = l.MV > l.MF ? l.MV : l.MF;
+    int r0 = r0_rows * L::LDR;
+    const int stage = L::KSP * L::NP * L::MY;  // Y partials / output staging
+    if (stage > r0) r0 = stage;
+    l.off_TF = l.MV * L::LDT;
+    l.off_U = l.off_TF + S::NF * l.MF * L::LDT;
+    l.off_UN = l.off_U + L::NP * L::LDU;
+    l.off_R0 = l.off_UN + L::NP * L::LDU;
+    l.off_R1 = l.off_R0 + r0;
+    l.total = l.off_R1 + l.MF * L::LDR;
+    return l;
+}
+
+struct Tc32Tiles {
+    const int4* tiles = nullptr;   // {first index into perm, count, signature, 0}
+    const int* perm = nullptr;     // element ids grouped by neighbour-face signature
+    const float* tables = nullptr; // TV then TF[0..NF-1], packed as in shared memory
+    int ntiles = 0;
+    int table_floats = 0;
+};
+
+__device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) {
+    uint32_t h;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+    h &= 0xffffe000u;
+    const float r = x - __uint_as_float(h);
+    uint32_t l;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(r));
+    hi = h;
+    lo = l & 0xffffe000u;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// a += x*y in the 3xTF32 form (small terms first).
+__device__ __forceinline__ void mma3(float (&c)[4], const uint32_t (&ah)[4], const uint32_t (&al)[4], uint32_t bh0,
+                                     uint32_t bh1, uint32_t bl0, uint32_t bl1) {
+    mma_tf32(c, al, bh0, bh1);
+    mma_tf32(c, ah, bl0, bl1);
+    mma_tf32(c, ah, bh0, bh1);
+}
+
+// Forward GEMMs: for each of `nops` (1 or 2) operand pairs (A_i: table rows [mtiles*16][LDT], B_i: U
+// [NP][LDU] column-major), R_i[m][c] = sum_k A_i[m][k] B_i[c][k], stored with ld LDR.  Units
+// (operand, m-tile, n-group) are dealt round-robin; a warp reloads its register-resident B
+// fragments only when its (operand, n-group) changes.
+template <class L>
+__device__ __forceinline__ void tc_forward(const float* A0, const float* B0, float* R0, const float* A1, const float* B1,
+                                           float* R1, int nops, int mtiles, int warp, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const int per_op = mtiles * L::NG;
+    const int units = nops * per_op;
+    int cur = -1;
+    float bv[L::NPW][L::KS][2];  // B fragments of the current (operand, n-group), split at use
+    for (int u = warp; u < units; u += L::NW) {
+        const int op = u / per_op, rem = u % per_op;
+        const int ng = rem / mtiles, mt = rem % mtiles;
+        const int key = op * L::NG + ng;
+        if (key != cur) {
+            cur = key;
+#pragma unroll
+            for (int j = 0; j < L::NPW; ++j) {
+                const float* bp = (op ? B1 : B0) + ((ng * L::NPW + j) * 8 + g) * L::LDU + t;
+#pragma unroll
+                for (int ks = 0; ks < L::KS; ++ks) {
+                    bv[j][ks][0] = bp[ks * 8];
+                    bv[j][ks][1] = bp[ks * 8 + 4];
+                }
+            }
+        }
+        float acc[L::NPW][4];
+#pragma unroll
+        for (int j = 0; j < L::NPW; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+        const float* ap = (op ? A1 : A0) + (mt * 16 + g) * L::LDT + t;
+#pragma unroll
+        for (int ks = 0; ks < L::KS; ++ks) {
+            uint32_t ah[4], al[4];
+            tf32_split(ap[ks * 8], ah[0], al[0]);
+            tf32_split(ap[ks * 8 + 8 * L::LDT], ah[1], al[1]);
+            tf32_split(ap[ks * 8 + 4], ah[2], al[2]);
+            tf32_split(ap[ks * 8 + 4 + 8 * L::LDT], ah[3], al[3]);
+#pragma unroll
+            for (int j = 0; j < L::NPW; ++j) {
+                uint32_t bh0, bl0, bh1, bl1;
+                tf32_split(bv[j][ks][0], bh0, bl0);
+                tf32_split(bv[j][ks][1], bh1, bl1);
+                mma3(acc[j], ah, al, bh0, bh1, bl0, bl1);
+            }
+        }
+        float* rp = (op ? R1 : R0) + (mt * 16 + g) * L::LDR + ng * L::NPW * 8 + 2 * t;
+#pragma unroll
+        for (int j = 0; j < L::NPW; ++j) {
+            *reinterpret_cast<float2*>(rp + j * 8) = make_float2(acc[j][0], acc[j][1]);
+            *reinterpret_cast<float2*>(rp + j * 8 + 8 * L::LDR) = make_float2(acc[j][2], acc[j][3]);
+        }
+    }
+}
+
+// Back-projection Y += A^T R over `mrows` reduction rows (a multiple of 8): A is a table
+// [mrows][LDT] (Y row index = table column), R is [mrows][LDR].  Warp w owns Y units
+// w % YU (+ NW, ...) for reduction part w / YU (k-steps kp, kp + KSP, ...).
+template <class L>
+__device__ __forceinline__ void tc_backproject(const float* A, const float* R, float (&y)[L::UPW][L::NPW][4], int mrows,
+                                               int warp, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const int kp = warp / L::YU;
+    if (kp >= L::KSP) return;
+    const int ksteps = mrows / 8;
+#pragma unroll
+    for (int uu = 0; uu < L::UPW; ++uu) {
+        const int unit = (warp % L::YU) + uu * L::NW;
+        if (L::UPW > 1 && unit >= L::YU) break;
+        const int myt = unit % L::MYT, ng = unit / L::MYT;
+        const float* ap = A + t * L::LDT + myt * 16 + g;
+        const float* rp = R + t * L::LDR + ng * L::NPW * 8 + g;
+        for (int ks = kp; ks < ksteps; ks += L::KSP) {
+            uint32_t ah[4], al[4];
+            const float* a = ap + ks * 8 * L::LDT;
+            tf32_split(a[0], ah[0], al[0]);
+            tf32_split(a[8], ah[1], al[1]);
+            tf32_split(a[4 * L::LDT], ah[2], al[2]);
+            tf32_split(a[4 * L::LDT + 8], ah[3], al[3]);
+            const float* r = rp + ks * 8 * L::LDR;
+#pragma unroll
+            for (int j = 0; j < L::NPW; ++j) {
+                uint32_t bh0, bl0, bh1, bl1;
+                tf32_split(r[j * 8], bh0, bl0);
+                tf32_split(r[j * 8 + 4 * L::LDR], bh1, bl1);
+                mma3(y[uu][j], ah, al, bh0, bh1, bl0, bl1);
+            }
+        }
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
+    apply_tc32_kernel(DevOp<float> op, Tc32Tiles mt, const float* __restrict__ x, float* __restrict__ y, int64_t ld,
+                      int nrhs) {
+    using L = Tc32Tile<S>;
+    constexpr int D = S::D, NBF = S::NBF, Q = S::Q, BS = S::BS, DD = S::DD, NF = S::NF;
+    constexpr int TE = L::TE, NT = L::NT, LDR = L::LDR, LDT = L::LDT, LDU = L::LDU;
+    const int Nq = op.Nq, nq = op.nq;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const Tc32Layout lay = tc32_layout<S>(Nq, nq);
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* sm = reinterpret_cast<float*>(smem_raw);
+    float* TV = sm;
+    float* TF = sm + lay.off_TF;
+    float* sU = sm + lay.off_U;
+    float* sUN = sm + lay.off_UN;
+    float* R0 = sm + lay.off_R0;
+    float* R1 = sm + lay.off_R1;
+    __shared__ int s_el[TE];
+    __shared__ int s_nb[TE];
+
+    for (int i = tid; i < mt.table_floats; i += NT) sm[i] = mt.tables[i];
+
+    const int64_t nwork = static_cast<int64_t>(mt.ntiles) * nrhs;
+    for (int64_t work = blockIdx.x; work < nwork; work += gridDim.x) {
+        const int tile = static_cast<int>(work % mt.ntiles);
+        const int rhs = static_cast<int>(work / mt.ntiles);
+        const float* xr = x + rhs * ld;
+        float* yr = y + rhs * ld;
+        const int4 td = mt.tiles[tile];
+        const int cnt = td.y, sig = td.z;
+        __syncthreads();
+        if (tid < TE) s_el[tid] = (tid < cnt) ? mt.perm[td.x + tid] : -1;
+        __syncthreads();
+        // U[c][k] (column-major); padding zero
+        for (int i = tid; i < L::NP * L::KP; i += NT) {
+            const int c = i / L::KP, k = i % L::KP;
+            const int te = c / Q, r = c % Q;
+            float v = 0.0f;
+            if (k < NBF && c < L::NC && s_el[te] >= 0) v = xr[static_cast<int64_t>(s_el[te]) * BS + k + NBF * r];
+            sU[c * LDU + k] = v;
+        }
+        __syncthreads();
+
+        float yacc[L::UPW][L::NPW][4];
+#pragma unroll
+        for (int a = 0; a < L::UPW; ++a)
+#pragma unroll
+            for (int j = 0; j < L::NPW; ++j) yacc[a][j][0] = yacc[a][j][1] = yacc[a][j][2] = yacc[a][j][3] = 0.0f;
+
+        // ---------------- volume ----------------
+        tc_forward<L>(TV, sU, R0, TV, sU, R0, 1, lay.MV / 16, warp, lane);
+        __syncthreads();
+        for (int it = tid; it < TE * Nq; it += NT) {
+            const int te = it % TE, q = it / TE;
+            const int el = s_el[te];
+            if (el < 0) continue;
+            float G[DD];
+            const float* vg = op.vG + static_cast<int64_t>(el) * DD * Nq + q;
+#pragma unroll
+            for (int c = 0; c < DD; ++c) G[c] = vg[c * Nq];
+            float* rr = R0 + (q * D) * LDR + te * Q;
+            if constexpr (S::KIND == kPoisson) {
+                const float jwk = op.vCoef[static_cast<int64_t>(el) * Nq + q];
+                float gx[D];
+#pragma unroll
+                for (int i = 0; i < D; ++i) {
+                    float s = 0.0f;
+#pragma unroll
+                    for (int a = 0; a < D; ++a) s += G[a * D + i] * rr[a * LDR];
+                    gx[i] = jwk * s;
+                }
+#pragma unroll
+                for (int a = 0; a < D; ++a) {
+                    float s = 0.0f;
+#pragma unroll
+                    for (int i = 0; i < D; ++i) s += G[a * D + i] * gx[i];
+                    rr[a * LDR] = s;
+                }
+            } else {
+                const float lam = op.vCoef[(static_cast<int64_t>(el) * 2 + 0) * Nq + q];
+                const float mu = op.vCoef[(static_cast<int64_t>(el) * 2 + 1) * Nq + q];
+                float Ju[D][D];
+#pragma unroll
+                for (int s = 0; s < D; ++s)
+#pragma unroll
+                    for (int r = 0; r < D; ++r) {
+                        float acc = 0.0f;
+#pragma unroll
+                        for (int a = 0; a < D; ++a) acc += G[a * D + s] * rr[a * LDR + r];
+                        Ju[s][r] = acc;
+                    }
+                float div = 0.0f;
+#pragma unroll
+                for (int r = 0; r < D; ++r) div += Ju[r][r];
+                float T[D][D];
+#pragma unroll
+                for (int uu = 0; uu < D; ++uu) {
+                    float sg[D];
+#pragma unroll
+                    for (int j = 0; j < D; ++j) sg[j] = mu * (Ju[uu][j] + Ju[j][uu]) + ((uu == j) ? lam * div : 0.0f);
+#pragma unroll
+                    for (int a = 0; a < D; ++a) {
+                        float s = 0.0f;
+#pragma unroll
+                        for (int j = 0; j < D; ++j) s += G[a * D + j] * sg[j];
+                        T[a][uu] = s;
+                    }
+                }
+#pragma unroll
+                for (int a = 0; a < D; ++a)
+#pragma unroll
+                    for (int uu = 0; uu < D; ++uu) rr[a * LDR + uu] = T[a][uu];
+            }
+        }
+        __syncthreads();
+        tc_backproject<L>(TV, R0, yacc, lay.MV, warp, lane);
+
+        // ---------------- facets ----------------
+#pragma unroll 1
+        for (int f = 0; f < NF; ++f) {
+            const int lp = (sig >> (2 * f)) & 3;
+            __syncthreads();  // previous back-projection done with R0 / sUN
+            if (tid < TE) s_nb[tid] = (s_el[tid] >= 0) ? op.sides[static_cast<int64_t>(s_el[tid]) * NF + f].z : -1;
+            __syncthreads();
+            for (int i = tid; i < L::NP * L::KP; i += NT) {
+                const int c = i / L::KP, k = i % L::KP;
+                const int te = c / Q, r = c % Q;
+                float v = 0.0f;
+                if (k < NBF && c < L::NC && s_nb[te] >= 0) v = xr[static_cast<int64_t>(s_nb[te]) * BS + k + NBF * r];
+                sUN[c * LDU + k] = v;
+            }
+            __syncthreads();
+            tc_forward<L>(TF + f * lay.MF * LDT, sU, R0, TF + lp * lay.MF * LDT, sUN, R1, 2, lay.MF / 16, warp, lane);
+            __syncthreads();
+            for (int it = tid; it < TE * nq; it += NT) {
+                const int te = it % TE, q = it / TE;
+                const int el = s_el[te];
+                if (el < 0) continue;
+                float* ga = R0 + (q * D) * LDR + te * Q;
+                float* gb = R0 + (D * nq + q) * LDR + te * Q;
+                const float* ha = R1 + (q * D) * LDR + te * Q;
+                const float* hb = R1 + (D * nq + q) * LDR + te * Q;
+                const int4 sd = op.sides[static_cast<int64_t>(el) * NF + f];
+                const int bcv = sd.y >> 8;
+                const bool skel = sd.z != el;
+                const bool fd = (bcv == 3 || bcv == 5);
+                const int mode = (bcv == 0 || (skel && fd)) ? 1 : (fd ? 2 : 0);
+                if (mode == 0) {
+#pragma unroll
+                    for (int a = 0; a < D; ++a)
+#pragma unroll
+                        for (int uu = 0; uu < Q; ++uu) ga[a * LDR + uu] = 0.0f;
+#pragma unroll
+                    for (int uu = 0; uu < Q; ++uu) gb[uu] = 0.0f;
+                    continue;
+                }
+                const int fct = sd.x;
+                const int side = sd.y & 0xff;
+                const int own = skel ? side : 0, oth = skel ? 1 - side : 0;
+                const float flip = (skel && side == 1) ? -1.0f : 1.0f;
+                float n[D], nu[D];
+#pragma unroll
+                for (int i = 0; i < D; ++i) {
+                    n[i] = flip * op.fN[(static_cast<int64_t>(fct) * D + i) * nq + q];
+                    nu[i] = flip * op.fNunit[(static_cast<int64_t>(fct) * D + i) * nq + q];
+                }
+                const double pen = op.penalty[fct];
+                const float wq = op.w[q];
+                float u0[Q], u1[Q], g0[D][Q], g1[D][Q];
+#pragma unroll
+                for (int r = 0; r < Q; ++r) {
+                    u0[r] = gb[r];
+                    u1[r] = (mode == 1) ? hb[r] : 0.0f;
+#pragma unroll
+                    for (int a = 0; a < D; ++a) {
+                        g0[a][r] = ga[a * LDR + r];
+                        g1[a][r] = (mode == 1) ? ha[a * LDR + r] : 0.0f;
+                    }
+                }
+                if constexpr (S::KIND == kPoisson) {
+                    float KG0[DD], KG1[DD];
+                    const float* kg = op.fCoef + static_cast<int64_t>(fct) * 2 * DD * nq + q;
+#pragma unroll
+                    for (int c = 0; c < DD; ++c) {
+                        KG0[c] = kg[(own * DD + c) * nq];
+                        KG1[c] = kg[(oth * DD + c) * nq];
+                    }
+                    float uh, sg[D];
+                    if (mode == 1) {
+                        uh = 0.5f * (u1[0] - u0[0]);
+                        const float pj = static_cast<float>(pen * (static_cast<double>(u0[0]) - u1[0]));
+#pragma unroll
+                        for (int p = 0; p < D; ++p) {
+                            float s = 0.0f;
+#pragma unroll
+                            for (int a = 0; a < D; ++a) s += KG0[a * D + p] * g0[a][0] + KG1[a * D + p] * g1[a][0];
+                            sg[p] = 0.5f * s - pj * nu[p];
+                        }
+                    } else {
+                        uh = -u0[0];
+                        const float pj = static_cast<float>(pen * u0[0]);
+#pragma unroll
+                        for (int p = 0; p < D; ++p) {
+                            float s = 0.0f;
+#pragma unroll
+                            for (int a = 0; a < D; ++a) s += KG0[a * D + p] * g0[a][0];
+                            sg[p] = s - pj * nu[p];
+                        }
+                    }
+                    float bsum = 0.0f;
+#pragma unroll
+                    for (int r = 0; r < D; ++r) bsum += n[r] * sg[r];
+                    gb[0] = -wq * bsum;
+#pragma unroll
+                    for (int a = 0; a < D; ++a) {
+                        float s = 0.0f;
+#pragma unroll
+                        for (int r = 0; r < D; ++r) s += n[r] * KG0[a * D + r];
+                        ga[a * LDR] = wq * uh * s;
+                    }
+                } else {
+                    float G0[DD], G1[DD];
+                    const float* gg = op.fG + static_cast<int64_t>(fct) * 2 * DD * nq + q;
+#pragma unroll
+                    for (int c = 0; c < DD; ++c) {
+                        G0[c] = gg[(own * DD + c) * nq];
+                        G1[c] = gg[(oth * DD + c) * nq];
+                    }
+                    const float* lm = op.fCoef + static_cast<int64_t>(fct) * 4 * nq + q;
+                    const float lam0 = lm[(2 * own + 0) * nq], mu0 = lm[(2 * own + 1) * nq];
+                    const float lam1 = lm[(2 * oth + 0) * nq], mu1 = lm[(2 * oth + 1) * nq];
+                    float sg[D][D];
+                    {
+                        float J0[D][D];
+#pragma unroll
+                        for (int s = 0; s < D; ++s)
+#pragma unroll
+                            for (int r = 0; r < D; ++r) {
+                                float acc0 = 0.0f;
+#pragma unroll
+                                for (int a = 0; a < D; ++a) acc0 += G0[a * D + s] * g0[a][r];
+                                J0[s][r] = acc0;
+                            }
+                        float d0 = 0.0f;
+#pragma unroll
+                        for (int r = 0; r < D; ++r) d0 += J0[r][r];
+#pragma unroll
+                        for (int i = 0; i < D; ++i)
+#pragma unroll
+                            for (int j = 0; j < D; ++j) sg[i][j] = mu0 * (J0[i][j] + J0[j][i]) + ((i == j) ? lam0 * d0 : 0.0f);
+                    }
+                    float uhm[D];
+                    if (mode == 1) {
+                        float J1[D][D];
+#pragma unroll
+                        for (int s = 0; s < D; ++s)
+#pragma unroll
+                            for (int r = 0; r < D; ++r) {
+                                float acc1 = 0.0f;
+#pragma unroll
+                                for (int a = 0; a < D; ++a) acc1 += G1[a * D + s] * g1[a][r];
+                                J1[s][r] = acc1;
+                            }
+                        float d1 = 0.0f;
+#pragma unroll
+                        for (int r = 0; r < D; ++r) d1 += J1[r][r];
+#pragma unroll
+                        for (int i = 0; i < D; ++i) {
+                            const float pj = static_cast<float>(pen * (static_cast<double>(u0[i]) - u1[i]));
+#pragma unroll
+                            for (int j = 0; j < D; ++j) {
+                                const float s1 = mu1 * (J1[i][j] + J1[j][i]) + ((i == j) ? lam1 * d1 : 0.0f);
+                                sg[i][j] = 0.5f * (sg[i][j] + s1) - pj * nu[j];
+                            }
+                            uhm[i] = 0.5f * (u1[i] - u0[i]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < D; ++i) {
+                            const float pj = static_cast<float>(pen * u0[i]);
+#pragma unroll
+                            for (int j = 0; j < D; ++j) sg[i][j] -= pj * nu[j];
+                            uhm[i] = -u0[i];
+                        }
+                    }
+                    float un = 0.0f;
+#pragma unroll
+                    for (int r = 0; r < D; ++r) un += uhm[r] * n[r];
+#pragma unroll
+                    for (int uu = 0; uu < D; ++uu) {
+                        float X[D];
+#pragma unroll
+                        for (int j = 0; j < D; ++j)
+                            X[j] = mu0 * (uhm[uu] * n[j] + uhm[j] * n[uu]) + ((uu == j) ? lam0 * un : 0.0f);
+#pragma unroll
+                        for (int a = 0; a < D; ++a) {
+                            float s = 0.0f;
+#pragma unroll
+                            for (int j = 0; j < D; ++j) s += G0[a * D + j] * X[j];
+                            ga[a * LDR + uu] = wq * s;
+                        }
+                        float bsum = 0.0f;
+#pragma unroll
+                        for (int j = 0; j < D; ++j) bsum += n[j] * sg[uu][j];
+                        gb[uu] = -wq * bsum;
+                    }
+                }
+            }
+            __syncthreads();
+            tc_backproject<L>(TF + f * lay.MF * LDT, R0, yacc, lay.MF, warp, lane);
+        }
+
+        // ---------------- reduce the k-split partials and write the tile ----------------
+        __syncthreads();
+        {
+            const int g = lane >> 2, t = lane & 3;
+            const int kp = warp / L::YU;
+            if (kp < L::KSP) {
+                float* st = R0 + kp * L::NP * L::MY;
+#pragma unroll
+                for (int uu = 0; uu < L::UPW; ++uu) {
+                    const int unit = (warp % L::YU) + uu * L::NW;
+                    if (unit >= L::YU) break;
+                    const int myt = unit % L::MYT, ng = unit / L::MYT;
+#pragma unroll
+                    for (int j = 0; j < L::NPW; ++j) {
+                        const int c = (ng * L::NPW + j) * 8 + 2 * t;
+                        const int k = myt * 16 + g;
+                        st[c * L::MY + k] = yacc[uu][j][0];
+                        st[(c + 1) * L::MY + k] = yacc[uu][j][1];
+                        st[c * L::MY + k + 8] = yacc[uu][j][2];
+                        st[(c + 1) * L::MY + k + 8] = yacc[uu][j][3];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < L::NC * NBF; i += NT) {
+            const int c = i / NBF, k = i % NBF;
+            const int te = c / Q, r = c % Q;
+            const int el = s_el[te];
+            if (el < 0) continue;
+            float v = 0.0f;
+#pragma unroll
+            for (int kp = 0; kp < L::KSP; ++kp) v += R0[kp * L::NP * L::MY + c * L::MY + k];
+            yr[static_cast<int64_t>(el) * BS + k + NBF * r] = v;
+        }
+    }
+}
+
+}  // namespace tdg

@@ -21,6 +21,12 @@ struct MmaTiles;
 // TDG_E_INVALID when the instance's tables do not fit in shared memory.
 int launch_apply_mma(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y,
                      int nrhs, int64_t ld, cudaStream_t s);
+
+// FP32 apply on the tensor cores in the 3xTF32 form (apply_tc32.cuh); TDG_E_INVALID when the
+// shape's shared-memory layout does not fit (the caller then uses the SIMT kernel).
+struct Tc32Tiles;
+int launch_apply_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y,
+                      int nrhs, int64_t ld, cudaStream_t s);
 int launch_bjac_assemble(int D, int N, int kind, DevOp<double> const& op, double* blk,
                          cudaStream_t s);
 template <typename T>
