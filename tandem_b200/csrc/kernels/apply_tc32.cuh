@@ -11,13 +11,16 @@
 //
 //   * a tile holds TE elements; its columns are (element, component) pairs, c = te * Q + r;
 //   * forward GEMMs R = T x U (T: basis table in shared memory, U: the tile's coefficients) are
-//     cut into units (16-row m-tile, group of NPW 8-column n-tiles).  A warp keeps the U fragments
-//     of its n-tile group in registers (split into hi/lo at use), so every table fragment it loads
-//     feeds 3 * NPW mma;
+//     cut into units (16-row m-tile, group of NPW 8-column n-tiles), so every table fragment a
+//     warp loads and splits feeds 3 * NPW mma;
 //   * back-projections Y += T^T R accumulate in registers for the whole tile.  The Y units
 //     (16-row m-tile of Y, n-tile group) are owned by fixed warps; when there are fewer units than
 //     warps, KSP warps share a unit and split the reduction index, and the partial sums meet in
 //     shared memory once per tile, where the output block is also staged for coalesced stores.
+//
+//   * the CTA runs NGRP independent tile pipelines ("groups" of GW warps with their own buffers and
+//     named barriers) that share the resident tables, so one group's global-memory waits overlap
+//     the other group's tensor work.
 //
 // Shared-memory strides: tables and U use ld = 4 (mod 8) floats (conflict-free A / B fragment
 // loads of the forward GEMM); R uses ld = 8 or 24 (mod 32) floats (conflict-free C stores and B
@@ -39,13 +42,17 @@ __host__ __device__ constexpr int tc_ldr(int np) {
 // Elements per tile: 48 columns for 3D elasticity, 64 otherwise.
 __host__ __device__ constexpr int tc32_tile_elements(int D, int Q) { return ((D == 3 && Q == 3) ? 48 : 64) / Q; }
 
+__host__ __device__ constexpr int tc_npw(int ntn) {
+    return (ntn % 6 == 0) ? 6 : ((ntn % 4 == 0) ? 4 : ((ntn % 3 == 0) ? 3 : ((ntn % 2 == 0) ? 2 : 1)));
+}
+
 template <class S>
 struct Tc32Tile {
     static constexpr int TE = tc32_tile_elements(S::D, S::Q);
     static constexpr int NC = TE * S::Q;
     static constexpr int NP = tc_round(NC, 8);
     static constexpr int NTN = NP / 8;
-    static constexpr int NPW = (NTN % 3 == 0) ? 3 : ((NTN % 2 == 0) ? 2 : 1);
+    static constexpr int NPW = tc_npw(NTN);                        // n-tiles per unit
     static constexpr int NG = NTN / NPW;
     static constexpr int KP = tc_round(S::NBF, 8);
     static constexpr int KS = KP / 8;
@@ -54,17 +61,23 @@ struct Tc32Tile {
     static constexpr int LDR = tc_ldr(NP);
     static constexpr int MY = tc_round(S::NBF, 16);
     static constexpr int MYT = MY / 16;
-    static constexpr int YU = MYT * NG;
-    static constexpr int NW = (S::D == 3 && S::Q == 3 && S::NBF > 20) ? 12 : 8;
+    static constexpr int YU = MYT * NG;                            // Y units per tile
+    static constexpr int NGRP = (S::D == 3) ? 2 : 1;               // tile pipelines per CTA
+    static constexpr int GW = (S::D == 3) ? 6 : 8;                 // warps per pipeline
+    static constexpr int GT = 32 * GW;
+    static constexpr int NW = GW * NGRP;
     static constexpr int NT = 32 * NW;
-    static constexpr int KSP = (YU >= NW) ? 1 : NW / YU;
-    static constexpr int UPW = (YU + NW - 1) / NW;
+    static constexpr int KSP = (YU >= GW) ? 1 : GW / YU;
+    static constexpr int UPW = (YU + GW - 1) / GW;
+    static constexpr int QCP = (S::D == 3) ? 32 : 64;              // volume points per chunk
     static constexpr int MINB = (S::D == 2) ? 2 : 1;
 };
 
 struct Tc32Layout {
     int MV, MF;                 // padded rows of TV and of each TF (multiples of 16)
-    int off_TF, off_U, off_UN, off_R0, off_R1;
+    int off_TF;                 // tables: TV at 0, TF at off_TF
+    int off_grp, grp;           // first pipeline buffer and the floats of one pipeline's buffers
+    int off_U, off_UN, off_R0, off_R1;  // offsets inside a pipeline's buffers
     int total;                  // floats
 };
 
@@ -74,16 +87,20 @@ __host__ __device__ inline Tc32Layout tc32_layout(int Nq, int nq) {
     Tc32Layout l;
     l.MV = tc_round(S::D * Nq, 16);
     l.MF = tc_round((S::D + 1) * nq, 16);
-    const int r0_rows = l.MV > l.MF ? l.MV : l.MF;
+    int vrows = tc_round(S::D * L::QCP, 16);
+    if (vrows > l.MV) vrows = l.MV;
+    const int r0_rows = vrows > l.MF ? vrows : l.MF;
     int r0 = r0_rows * L::LDR;
     const int stage = L::KSP * L::NP * L::MY;  // Y partials / output staging
     if (stage > r0) r0 = stage;
     l.off_TF = l.MV * L::LDT;
-    l.off_U = l.off_TF + S::NF * l.MF * L::LDT;
+    l.off_grp = l.off_TF + S::NF * l.MF * L::LDT;
+    l.off_U = 0;
     l.off_UN = l.off_U + L::NP * L::LDU;
     l.off_R0 = l.off_UN + L::NP * L::LDU;
     l.off_R1 = l.off_R0 + r0;
-    l.total = l.off_R1 + l.MF * L::LDR;
+    l.grp = l.off_R1 + l.MF * L::LDR;
+    l.total = l.off_grp + L::NGRP * l.grp;
     return l;
 }
 
@@ -95,15 +112,20 @@ struct Tc32Tiles {
     int table_floats = 0;
 };
 
+// x = hi + lo with hi = x rounded to TF32 (nearest, ties away from zero: add half an ulp of the
+// 10-bit mantissa to the magnitude bits, then clear the 13 low bits).  lo is passed as is: the
+// tensor core reads the upper 19 bits of a TF32 operand, so lo loses at most 2^-11 of itself,
+// i.e. 2^-22 of x.
 __device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) {
-    uint32_t h;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
-    h &= 0xffffe000u;
-    const float r = x - __uint_as_float(h);
-    uint32_t l;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(r));
+    const uint32_t h = (__float_as_uint(x) + 0x1000u) & 0xffffe000u;
     hi = h;
-    lo = l & 0xffffe000u;
+    lo = __float_as_uint(x - __uint_as_float(h));
+}
+
+// Barrier over the GT threads of pipeline `grp` (named barrier 1 + grp; 0 is __syncthreads).
+template <int GT>
+__device__ __forceinline__ void group_sync(int grp) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(GT) : "memory");
 }
 
 __device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
@@ -124,32 +146,18 @@ __device__ __forceinline__ void mma3(float (&c)[4], const uint32_t (&ah)[4], con
 
 // Forward GEMMs: for each of `nops` (1 or 2) operand pairs (A_i: table rows [mtiles*16][LDT], B_i: U
 // [NP][LDU] column-major), R_i[m][c] = sum_k A_i[m][k] B_i[c][k], stored with ld LDR.  Units
-// (operand, m-tile, n-group) are dealt round-robin; a warp reloads its register-resident B
-// fragments only when its (operand, n-group) changes.
+// (operand, m-tile, n-group) are dealt round-robin to the warps of the pipeline; each table
+// fragment a warp loads (and splits) feeds the NPW n-tiles of its unit.
 template <class L>
 __device__ __forceinline__ void tc_forward(const float* A0, const float* B0, float* R0, const float* A1, const float* B1,
                                            float* R1, int nops, int mtiles, int warp, int lane) {
     const int g = lane >> 2, t = lane & 3;
     const int per_op = mtiles * L::NG;
     const int units = nops * per_op;
-    int cur = -1;
-    float bv[L::NPW][L::KS][2];  // B fragments of the current (operand, n-group), split at use
-    for (int u = warp; u < units; u += L::NW) {
+    for (int u = warp; u < units; u += L::GW) {
         const int op = u / per_op, rem = u % per_op;
         const int ng = rem / mtiles, mt = rem % mtiles;
-        const int key = op * L::NG + ng;
-        if (key != cur) {
-            cur = key;
-#pragma unroll
-            for (int j = 0; j < L::NPW; ++j) {
-                const float* bp = (op ? B1 : B0) + ((ng * L::NPW + j) * 8 + g) * L::LDU + t;
-#pragma unroll
-                for (int ks = 0; ks < L::KS; ++ks) {
-                    bv[j][ks][0] = bp[ks * 8];
-                    bv[j][ks][1] = bp[ks * 8 + 4];
-                }
-            }
-        }
+        const float* bp = (op ? B1 : B0) + (ng * L::NPW * 8 + g) * L::LDU + t;
         float acc[L::NPW][4];
 #pragma unroll
         for (int j = 0; j < L::NPW; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
@@ -164,8 +172,8 @@ __device__ __forceinline__ void tc_forward(const float* A0, const float* B0, flo
 #pragma unroll
             for (int j = 0; j < L::NPW; ++j) {
                 uint32_t bh0, bl0, bh1, bl1;
-                tf32_split(bv[j][ks][0], bh0, bl0);
-                tf32_split(bv[j][ks][1], bh1, bl1);
+                tf32_split(bp[j * 8 * L::LDU + ks * 8], bh0, bl0);
+                tf32_split(bp[j * 8 * L::LDU + ks * 8 + 4], bh1, bl1);
                 mma3(acc[j], ah, al, bh0, bh1, bl0, bl1);
             }
         }
@@ -190,7 +198,7 @@ __device__ __forceinline__ void tc_backproject(const float* A, const float* R, f
     const int ksteps = mrows / 8;
 #pragma unroll
     for (int uu = 0; uu < L::UPW; ++uu) {
-        const int unit = (warp % L::YU) + uu * L::NW;
+        const int unit = (warp % L::YU) + uu * L::GW;
         if (L::UPW > 1 && unit >= L::YU) break;
         const int myt = unit % L::MYT, ng = unit / L::MYT;
         const float* ap = A + t * L::LDT + myt * 16 + g;
@@ -220,44 +228,50 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
                       int nrhs) {
     using L = Tc32Tile<S>;
     constexpr int D = S::D, NBF = S::NBF, Q = S::Q, BS = S::BS, DD = S::DD, NF = S::NF;
-    constexpr int TE = L::TE, NT = L::NT, LDR = L::LDR, LDT = L::LDT, LDU = L::LDU;
+    constexpr int TE = L::TE, GT = L::GT, LDR = L::LDR, LDT = L::LDT, LDU = L::LDU;
     const int Nq = op.Nq, nq = op.nq;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int grp = warp / L::GW, gw = warp % L::GW, gtid = tid - grp * GT;
     const Tc32Layout lay = tc32_layout<S>(Nq, nq);
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sm = reinterpret_cast<float*>(smem_raw);
     float* TV = sm;
     float* TF = sm + lay.off_TF;
-    float* sU = sm + lay.off_U;
-    float* sUN = sm + lay.off_UN;
-    float* R0 = sm + lay.off_R0;
-    float* R1 = sm + lay.off_R1;
-    __shared__ int s_el[TE];
-    __shared__ int s_nb[TE];
+    float* gbuf = sm + lay.off_grp + grp * lay.grp;
+    float* sU = gbuf + lay.off_U;
+    float* sUN = gbuf + lay.off_UN;
+    float* R0 = gbuf + lay.off_R0;
+    float* R1 = gbuf + lay.off_R1;
+    __shared__ int s_el_all[L::NGRP][TE];
+    __shared__ int s_nb_all[L::NGRP][TE];
+    int* s_el = s_el_all[grp];
+    int* s_nb = s_nb_all[grp];
 
-    for (int i = tid; i < mt.table_floats; i += NT) sm[i] = mt.tables[i];
+    for (int i = tid; i < mt.table_floats; i += L::NT) sm[i] = mt.tables[i];
+    __syncthreads();
 
     const int64_t nwork = static_cast<int64_t>(mt.ntiles) * nrhs;
-    for (int64_t work = blockIdx.x; work < nwork; work += gridDim.x) {
+    for (int64_t work = static_cast<int64_t>(blockIdx.x) * L::NGRP + grp; work < nwork;
+         work += static_cast<int64_t>(gridDim.x) * L::NGRP) {
         const int tile = static_cast<int>(work % mt.ntiles);
         const int rhs = static_cast<int>(work / mt.ntiles);
         const float* xr = x + rhs * ld;
         float* yr = y + rhs * ld;
         const int4 td = mt.tiles[tile];
         const int cnt = td.y, sig = td.z;
-        __syncthreads();
-        if (tid < TE) s_el[tid] = (tid < cnt) ? mt.perm[td.x + tid] : -1;
-        __syncthreads();
+        group_sync<GT>(grp);
+        if (gtid < TE) s_el[gtid] = (gtid < cnt) ? mt.perm[td.x + gtid] : -1;
+        group_sync<GT>(grp);
         // U[c][k] (column-major); padding zero
-        for (int i = tid; i < L::NP * L::KP; i += NT) {
+        for (int i = gtid; i < L::NP * L::KP; i += GT) {
             const int c = i / L::KP, k = i % L::KP;
             const int te = c / Q, r = c % Q;
             float v = 0.0f;
             if (k < NBF && c < L::NC && s_el[te] >= 0) v = xr[static_cast<int64_t>(s_el[te]) * BS + k + NBF * r];
             sU[c * LDU + k] = v;
         }
-        __syncthreads();
+        group_sync<GT>(grp);
 
         float yacc[L::UPW][L::NPW][4];
 #pragma unroll
@@ -265,92 +279,97 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
 #pragma unroll
             for (int j = 0; j < L::NPW; ++j) yacc[a][j][0] = yacc[a][j][1] = yacc[a][j][2] = yacc[a][j][3] = 0.0f;
 
-        // ---------------- volume ----------------
-        tc_forward<L>(TV, sU, R0, TV, sU, R0, 1, lay.MV / 16, warp, lane);
-        __syncthreads();
-        for (int it = tid; it < TE * Nq; it += NT) {
-            const int te = it % TE, q = it / TE;
-            const int el = s_el[te];
-            if (el < 0) continue;
-            float G[DD];
-            const float* vg = op.vG + static_cast<int64_t>(el) * DD * Nq + q;
+        // ---------------- volume, in chunks of QCP points ----------------
+        for (int q0 = 0; q0 < Nq; q0 += L::QCP) {
+            const int nqc = (Nq - q0 < L::QCP) ? (Nq - q0) : L::QCP;
+            const int rows = tc_round(nqc * D, 16);
+            if (q0 > 0) group_sync<GT>(grp);  // previous chunk's back-projection done with R0
+            tc_forward<L>(TV + q0 * D * LDT, sU, R0, TV, sU, R0, 1, rows / 16, gw, lane);
+            group_sync<GT>(grp);
+            for (int it = gtid; it < TE * nqc; it += GT) {
+                const int te = it % TE, qq = it / TE, q = q0 + qq;
+                const int el = s_el[te];
+                if (el < 0) continue;
+                float G[DD];
+                const float* vg = op.vG + static_cast<int64_t>(el) * DD * Nq + q;
 #pragma unroll
-            for (int c = 0; c < DD; ++c) G[c] = vg[c * Nq];
-            float* rr = R0 + (q * D) * LDR + te * Q;
-            if constexpr (S::KIND == kPoisson) {
-                const float jwk = op.vCoef[static_cast<int64_t>(el) * Nq + q];
-                float gx[D];
+                for (int c = 0; c < DD; ++c) G[c] = vg[c * Nq];
+                float* rr = R0 + (qq * D) * LDR + te * Q;
+                if constexpr (S::KIND == kPoisson) {
+                    const float jwk = op.vCoef[static_cast<int64_t>(el) * Nq + q];
+                    float gx[D];
 #pragma unroll
-                for (int i = 0; i < D; ++i) {
-                    float s = 0.0f;
+                    for (int i = 0; i < D; ++i) {
+                        float s = 0.0f;
 #pragma unroll
-                    for (int a = 0; a < D; ++a) s += G[a * D + i] * rr[a * LDR];
-                    gx[i] = jwk * s;
-                }
-#pragma unroll
-                for (int a = 0; a < D; ++a) {
-                    float s = 0.0f;
-#pragma unroll
-                    for (int i = 0; i < D; ++i) s += G[a * D + i] * gx[i];
-                    rr[a * LDR] = s;
-                }
-            } else {
-                const float lam = op.vCoef[(static_cast<int64_t>(el) * 2 + 0) * Nq + q];
-                const float mu = op.vCoef[(static_cast<int64_t>(el) * 2 + 1) * Nq + q];
-                float Ju[D][D];
-#pragma unroll
-                for (int s = 0; s < D; ++s)
-#pragma unroll
-                    for (int r = 0; r < D; ++r) {
-                        float acc = 0.0f;
-#pragma unroll
-                        for (int a = 0; a < D; ++a) acc += G[a * D + s] * rr[a * LDR + r];
-                        Ju[s][r] = acc;
+                        for (int a = 0; a < D; ++a) s += G[a * D + i] * rr[a * LDR];
+                        gx[i] = jwk * s;
                     }
-                float div = 0.0f;
-#pragma unroll
-                for (int r = 0; r < D; ++r) div += Ju[r][r];
-                float T[D][D];
-#pragma unroll
-                for (int uu = 0; uu < D; ++uu) {
-                    float sg[D];
-#pragma unroll
-                    for (int j = 0; j < D; ++j) sg[j] = mu * (Ju[uu][j] + Ju[j][uu]) + ((uu == j) ? lam * div : 0.0f);
 #pragma unroll
                     for (int a = 0; a < D; ++a) {
                         float s = 0.0f;
 #pragma unroll
-                        for (int j = 0; j < D; ++j) s += G[a * D + j] * sg[j];
-                        T[a][uu] = s;
+                        for (int i = 0; i < D; ++i) s += G[a * D + i] * gx[i];
+                        rr[a * LDR] = s;
                     }
+                } else {
+                    const float lam = op.vCoef[(static_cast<int64_t>(el) * 2 + 0) * Nq + q];
+                    const float mu = op.vCoef[(static_cast<int64_t>(el) * 2 + 1) * Nq + q];
+                    float Ju[D][D];
+#pragma unroll
+                    for (int s = 0; s < D; ++s)
+#pragma unroll
+                        for (int r = 0; r < D; ++r) {
+                            float acc = 0.0f;
+#pragma unroll
+                            for (int a = 0; a < D; ++a) acc += G[a * D + s] * rr[a * LDR + r];
+                            Ju[s][r] = acc;
+                        }
+                    float div = 0.0f;
+#pragma unroll
+                    for (int r = 0; r < D; ++r) div += Ju[r][r];
+                    float T[D][D];
+#pragma unroll
+                    for (int uu = 0; uu < D; ++uu) {
+                        float sg[D];
+#pragma unroll
+                        for (int j = 0; j < D; ++j) sg[j] = mu * (Ju[uu][j] + Ju[j][uu]) + ((uu == j) ? lam * div : 0.0f);
+#pragma unroll
+                        for (int a = 0; a < D; ++a) {
+                            float s = 0.0f;
+#pragma unroll
+                            for (int j = 0; j < D; ++j) s += G[a * D + j] * sg[j];
+                            T[a][uu] = s;
+                        }
+                    }
+#pragma unroll
+                    for (int a = 0; a < D; ++a)
+#pragma unroll
+                        for (int uu = 0; uu < D; ++uu) rr[a * LDR + uu] = T[a][uu];
                 }
-#pragma unroll
-                for (int a = 0; a < D; ++a)
-#pragma unroll
-                    for (int uu = 0; uu < D; ++uu) rr[a * LDR + uu] = T[a][uu];
             }
+            group_sync<GT>(grp);
+            tc_backproject<L>(TV + q0 * D * LDT, R0, yacc, rows, gw, lane);
         }
-        __syncthreads();
-        tc_backproject<L>(TV, R0, yacc, lay.MV, warp, lane);
 
         // ---------------- facets ----------------
 #pragma unroll 1
         for (int f = 0; f < NF; ++f) {
             const int lp = (sig >> (2 * f)) & 3;
-            __syncthreads();  // previous back-projection done with R0 / sUN
-            if (tid < TE) s_nb[tid] = (s_el[tid] >= 0) ? op.sides[static_cast<int64_t>(s_el[tid]) * NF + f].z : -1;
-            __syncthreads();
-            for (int i = tid; i < L::NP * L::KP; i += NT) {
+            group_sync<GT>(grp);  // previous back-projection done with R0 / sUN
+            if (gtid < TE) s_nb[gtid] = (s_el[gtid] >= 0) ? op.sides[static_cast<int64_t>(s_el[gtid]) * NF + f].z : -1;
+            group_sync<GT>(grp);
+            for (int i = gtid; i < L::NP * L::KP; i += GT) {
                 const int c = i / L::KP, k = i % L::KP;
                 const int te = c / Q, r = c % Q;
                 float v = 0.0f;
                 if (k < NBF && c < L::NC && s_nb[te] >= 0) v = xr[static_cast<int64_t>(s_nb[te]) * BS + k + NBF * r];
                 sUN[c * LDU + k] = v;
             }
-            __syncthreads();
-            tc_forward<L>(TF + f * lay.MF * LDT, sU, R0, TF + lp * lay.MF * LDT, sUN, R1, 2, lay.MF / 16, warp, lane);
-            __syncthreads();
-            for (int it = tid; it < TE * nq; it += NT) {
+            group_sync<GT>(grp);
+            tc_forward<L>(TF + f * lay.MF * LDT, sU, R0, TF + lp * lay.MF * LDT, sUN, R1, 2, lay.MF / 16, gw, lane);
+            group_sync<GT>(grp);
+            for (int it = gtid; it < TE * nq; it += GT) {
                 const int te = it % TE, q = it / TE;
                 const int el = s_el[te];
                 if (el < 0) continue;
@@ -524,20 +543,20 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
                     }
                 }
             }
-            __syncthreads();
-            tc_backproject<L>(TF + f * lay.MF * LDT, R0, yacc, lay.MF, warp, lane);
+            group_sync<GT>(grp);
+            tc_backproject<L>(TF + f * lay.MF * LDT, R0, yacc, lay.MF, gw, lane);
         }
 
         // ---------------- reduce the k-split partials and write the tile ----------------
-        __syncthreads();
+        group_sync<GT>(grp);
         {
             const int g = lane >> 2, t = lane & 3;
-            const int kp = warp / L::YU;
+            const int kp = gw / L::YU;
             if (kp < L::KSP) {
                 float* st = R0 + kp * L::NP * L::MY;
 #pragma unroll
                 for (int uu = 0; uu < L::UPW; ++uu) {
-                    const int unit = (warp % L::YU) + uu * L::NW;
+                    const int unit = (gw % L::YU) + uu * L::GW;
                     if (unit >= L::YU) break;
                     const int myt = unit % L::MYT, ng = unit / L::MYT;
 #pragma unroll
@@ -552,8 +571,8 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
                 }
             }
         }
-        __syncthreads();
-        for (int i = tid; i < L::NC * NBF; i += NT) {
+        group_sync<GT>(grp);
+        for (int i = gtid; i < L::NC * NBF; i += GT) {
             const int c = i / NBF, k = i % NBF;
             const int te = c / Q, r = c % Q;
             const int el = s_el[te];
