@@ -132,13 +132,30 @@ int64_t tdg_bytes_apply(const tdg_op* op, int precision);
  * diagonal blocks on the device, inverts them and stores the inverses in `precision`.
  * Returns TDG_E_NOT_SPD when a block is not positive definite. */
 int tdg_bjacobi_setup(tdg_op* op, int precision, void* stream);
-/* z = D^-1 r; precision must match the stored inverses' precision or TDG_FP64 inverses may be
- * applied to double vectors only. */
+/* z = D^-1 r; precision is the vectors' precision: TDG_FP32 vectors need FP32 inverses, TDG_FP64
+ * vectors take FP64 or FP32 inverses (the latter as the fallback preconditioner of the mixed
+ * solve). */
 int tdg_bjacobi_apply(tdg_op* op, int precision, const void* r, void* z, int nrhs, int64_t ld,
                       void* stream);
 /* Copies the assembled (not inverted) diagonal blocks [E][bs][bs] (column-major per block) to
  * host memory; for tests. */
 int tdg_bjacobi_blocks(tdg_op* op, double* out);
+
+/* --- autotuning (no counterpart in tandem) ---------------------------------------------------- */
+
+typedef struct {
+    int family;       /* 0 = tensor-core kernel, 1 = SIMT kernel */
+    int ctas_per_sm;  /* persistent CTAs per SM requested (0 = default) */
+    double ms;        /* measured time of one apply */
+} tdg_tune_entry;
+
+/* Times the apply of this operator (its own mesh, `nrhs` right-hand sides, `precision`) for each
+ * candidate launch configuration -- the tensor-core kernel at 1 to 4 persistent CTAs per SM
+ * (clipped to the occupancy limit of the shape's tile) and the SIMT kernel -- with CUDA events on
+ * `stream`, and keeps the fastest for later tdg_apply / tdg_solve calls of that precision.
+ * entries (optional, up to max_entries) receives every measurement; n_entries their count. */
+int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_entry* entries, int max_entries,
+                 int* n_entries);
 
 /* --- right-hand side (DGOperator::rhs, src/form/DGOperator.h:189-237) ---------------------- */
 
@@ -151,25 +168,30 @@ int tdg_rhs(tdg_op* op, const double* force_Q, const double* bc_q, double* b);
 /* --- Krylov solve on the device (PetscLinearSolver / KSPCG, app/common/PetscLinearSolver.cpp) */
 
 typedef struct {
-    int32_t precision;      /* TDG_FP64: FP64 CG; TDG_FP32: FP32 inner CG in FP64 refinement */
-    int32_t max_iterations; /* total inner iterations cap */
+    int32_t precision;      /* TDG_FP64: FP64 CG; TDG_FP32: FP32 CG recurrence with FP64 reliable
+                               updates (solution and true residual kept in FP64); problems whose
+                               FP32 recurrence stalls above the target continue in FP64 */
+    int32_t max_iterations; /* total Krylov iterations cap */
     double rtol;            /* relative residual ||b - A x|| / ||b|| target (FP64 residual) */
-    double inner_rtol;      /* inner FP32 reduction per refinement step (mixed only) */
-    int32_t max_outer;      /* refinement steps cap (mixed only) */
+    double inner_rtol;      /* reliable-update threshold: the FP64 residual replaces the recurrence
+                               residual whenever the latter has dropped by this factor
+                               (0 = default: 0.1 for TDG_FP32, 0.01 for TDG_FP64) */
+    int32_t max_outer;      /* cap on reliable updates (0 = none) */
     int32_t use_graphs;     /* capture iteration blocks in CUDA graphs */
 } tdg_solve_opts;
 
 typedef struct {
-    int32_t iterations;     /* total Krylov iterations (inner iterations for mixed) */
-    int32_t outer;          /* refinement steps */
+    int32_t iterations;     /* total Krylov iterations */
+    int32_t outer;          /* reliable updates (FP64 residual replacements) */
     double rel_residual;    /* final FP64 relative residual */
     double seconds;         /* device time of the solve */
     int32_t converged;
-    int32_t reserved;
+    int32_t fp64_iterations; /* mixed: iterations of the FP64 continuation (0 if none) */
 } tdg_solve_stats;
 
 /* Solves A x = b (device double arrays, nrhs stacked with leading dimension ld) with
- * block-Jacobi preconditioned CG.  x holds the initial guess.  tdg_bjacobi_setup must have
+ * block-Jacobi preconditioned CG (reliable updates: the recurrence residual is periodically
+ * replaced by the FP64 residual b - A x, keeping the search direction).  x holds the initial guess.  tdg_bjacobi_setup must have
  * been called with the precision the solve needs (FP64 for TDG_FP64, FP32 for TDG_FP32). */
 int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64_t ld,
               const tdg_solve_opts* opts, tdg_solve_stats* stats, void* stream);

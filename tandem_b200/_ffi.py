@@ -41,6 +41,7 @@ SYMBOLS = {
     "tdg_solve_segmented": (C.c_int, [_p, _p, _p, C.c_int, _p, _p, _p, _p, _p]),
     "tdg_adjoint_lame_gradient": (C.c_int, [_p, _p, _p, _p, _p, _p]),
     "tdg_adjoint_lame_gradient_noalloc": (C.c_int, [_p, _p, _p, _p, _p, _p]),
+    "tdg_autotune": (C.c_int, [_p, C.c_int, C.c_int, _p, _p, C.c_int, _p]),
     "tdg_fault_create": (C.c_int, [_p, _i64, _p, _p, C.POINTER(_p)]),
     "tdg_fault_destroy": (None, [_p]),
     "tdg_fault_sizes": (C.c_int, [_p, _p]),
@@ -63,6 +64,10 @@ class Quadrature(C.Structure):
                 ("vol_points", _p), ("vol_weights", _p), ("fct_points", _p), ("fct_weights", _p)]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("family", C.c_int), ("ctas_per_sm", C.c_int), ("ms", C.c_double)]
+
+
 class SolveOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("max_iterations", C.c_int32), ("rtol", C.c_double),
                 ("inner_rtol", C.c_double), ("max_outer", C.c_int32), ("use_graphs", C.c_int32)]
@@ -70,7 +75,7 @@ class SolveOpts(C.Structure):
 
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("outer", C.c_int32), ("rel_residual", C.c_double),
-                ("seconds", C.c_double), ("converged", C.c_int32), ("reserved", C.c_int32)]
+                ("seconds", C.c_double), ("converged", C.c_int32), ("fp64_iterations", C.c_int32)]
 
 
 class TdgError(RuntimeError):

@@ -117,6 +117,10 @@ struct tdg_op {
     MmaTiles mma;           // FP64 tensor-pipe apply: packed tables and signature tiles
     Tc32Tiles tc32;         // FP32 tensor-core apply (3xTF32): packed tables and signature tiles
     bool use_mma = true;
+    // per precision (0 = FP64, 1 = FP32): kernel family (0 tensor cores, 1 SIMT) and persistent CTAs
+    // per SM (0 = default); set by tdg_autotune
+    int family[2] = {0, 0};
+    int ctas[2] = {0, 0};
     const double* penalty = nullptr;
     const int4* sides = nullptr;
     // block-Jacobi
@@ -467,19 +471,88 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
     TDG_TRY(ensure_uploaded(op, precision));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int rc = TDG_E_INVALID;
-    if (precision == TDG_FP64 && op->use_mma)
+    const int pi = precision == TDG_FP32 ? 1 : 0;
+    const bool tensor = op->use_mma && op->family[pi] == 0;
+    if (precision == TDG_FP64 && tensor)
         rc = launch_apply_mma(h.D, h.N, h.kind, op->op64, op->mma, static_cast<const double*>(x),
-                              static_cast<double*>(y), nrhs, ld, s);
+                              static_cast<double*>(y), nrhs, ld, s, op->ctas[0]);
     if (precision == TDG_FP64 && rc == TDG_E_INVALID)
         rc = launch_apply<double>(h.D, h.N, h.kind, op->op64, static_cast<const double*>(x),
                                   static_cast<double*>(y), nrhs, ld, s);
-    if (precision == TDG_FP32 && op->use_mma)
+    if (precision == TDG_FP32 && tensor)
         rc = launch_apply_tc32(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const float*>(x),
-                               static_cast<float*>(y), nrhs, ld, s);
+                               static_cast<float*>(y), nrhs, ld, s, op->ctas[1]);
     if (precision == TDG_FP32 && rc == TDG_E_INVALID)
         rc = launch_apply<float>(h.D, h.N, h.kind, op->op32, static_cast<const float*>(x),
                                  static_cast<float*>(y), nrhs, ld, s);
     if (rc) return fail(rc, std::string("apply launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
+int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_entry* entries, int max_entries,
+                 int* n_entries) {
+    if (!op || nrhs < 1 || (precision != TDG_FP64 && precision != TDG_FP32))
+        return fail(TDG_E_INVALID, "bad argument");
+    TDG_TRY(ensure_uploaded(op, precision));
+    auto const& h = op->h;
+    const int pi = precision == TDG_FP32 ? 1 : 0;
+    const size_t esz = precision == TDG_FP32 ? sizeof(float) : sizeof(double);
+    const int64_t ld = h.E * h.bs;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    void *x = nullptr, *y = nullptr;
+    if (cudaMalloc(&x, esz * ld * nrhs) != cudaSuccess) return fail(TDG_E_NOMEM, "autotune buffers");
+    if (cudaMalloc(&y, esz * ld * nrhs) != cudaSuccess) {
+        cudaFree(x);
+        return fail(TDG_E_NOMEM, "autotune buffers");
+    }
+    cudaMemsetAsync(x, 0x3f, esz * ld * nrhs, s);
+    // candidates: tensor-core kernel at 1..4 persistent CTAs per SM (clipped to the occupancy
+    // limit), then the SIMT kernel
+    struct Cand {
+        int family, ctas;
+    };
+    std::vector<Cand> cands;
+    if (op->use_mma)
+        for (int c = 1; c <= 4; ++c) cands.push_back({0, c});
+    cands.push_back({1, 0});
+    const int fam0 = op->family[pi], ct0 = op->ctas[pi];
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 1e300;
+    int bi = -1, n = 0, rc = 0;
+    for (size_t i = 0; i < cands.size() && rc == 0; ++i) {
+        op->family[pi] = cands[i].family;
+        op->ctas[pi] = cands[i].ctas;
+        for (int w = 0; w < 2 && rc == 0; ++w) rc = tdg_apply(op, precision, x, y, nrhs, ld, stream);
+        if (rc) break;
+        constexpr int reps = 5;
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps && rc == 0; ++r) rc = tdg_apply(op, precision, x, y, nrhs, ld, stream);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double per = ms / reps;
+        if (entries && n < max_entries) entries[n] = tdg_tune_entry{cands[i].family, cands[i].ctas, per};
+        ++n;
+        if (per < best) {
+            best = per;
+            bi = static_cast<int>(i);
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(x);
+    cudaFree(y);
+    if (rc || bi < 0) {
+        op->family[pi] = fam0;
+        op->ctas[pi] = ct0;
+        return rc ? rc : fail(TDG_E_CUDA, "autotune found no candidate");
+    }
+    op->family[pi] = cands[bi].family;
+    op->ctas[pi] = cands[bi].ctas;
+    if (n_entries) *n_entries = n;
     return 0;
 }
 
@@ -535,16 +608,22 @@ int tdg_bjacobi_setup(tdg_op* op, int precision, void* stream) {
 
 int tdg_bjacobi_apply(tdg_op* op, int precision, const void* r, void* z, int nrhs, int64_t ld, void* stream) {
     if (!op || !r || !z) return fail(TDG_E_INVALID, "null argument");
-    if (!op->inv || op->inv_precision != precision)
+    // FP64 vectors take FP64 or FP32 inverses; FP32 vectors take FP32 inverses
+    if (!op->inv || (precision == TDG_FP32 && op->inv_precision != TDG_FP32))
         return fail(TDG_E_STATE, "tdg_bjacobi_setup not called for this precision");
     auto const& h = op->h;
     if (nrhs < 1 || ld < h.E * h.bs) return fail(TDG_E_INVALID, "nrhs < 1 or ld < E * bs");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int rc = (precision == TDG_FP64)
-                 ? launch_bjac_apply<double>(h.bs, h.E, static_cast<const double*>(op->inv),
-                                             static_cast<const double*>(r), static_cast<double*>(z), nrhs, ld, s)
-                 : launch_bjac_apply<float>(h.bs, h.E, static_cast<const float*>(op->inv),
-                                            static_cast<const float*>(r), static_cast<float*>(z), nrhs, ld, s);
+    int rc;
+    if (precision == TDG_FP32)
+        rc = launch_bjac_apply<float, float>(h.bs, h.E, static_cast<const float*>(op->inv),
+                                             static_cast<const float*>(r), static_cast<float*>(z), nrhs, ld, s);
+    else if (op->inv_precision == TDG_FP32)
+        rc = launch_bjac_apply<float, double>(h.bs, h.E, static_cast<const float*>(op->inv),
+                                              static_cast<const double*>(r), static_cast<double*>(z), nrhs, ld, s);
+    else
+        rc = launch_bjac_apply<double, double>(h.bs, h.E, static_cast<const double*>(op->inv),
+                                               static_cast<const double*>(r), static_cast<double*>(z), nrhs, ld, s);
     if (rc) return fail(rc, "block-Jacobi apply launch failed");
     return 0;
 }
@@ -730,6 +809,180 @@ int cg_start(tdg_op* op, int prec, SegPlan const& sp, CgVectors<T> v, double* pa
     return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "CG start");
 }
 
+// Rebuilds the search direction after a residual replacement.  The block ended with
+// p = z_old + beta p_prev, beta = rz_old / rz_prev; with the replaced residual the recurrence
+// gives p = z_new + (rz_new / rz_prev) p_prev = z_new + (rz_new / rz_old) (p - z_old), and z
+// takes z_new.  Segments flagged in scal[seg][kTmp] restart from p = z_new.  rz_new is in slot
+// kRZnew, rz_old in kRZ (k_cg_shift then moves rz_new to kRZ).
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads)
+    k_replace_dir(const Chunk* __restrict__ chunks, T* __restrict__ p, T* __restrict__ z, const T* __restrict__ znew,
+                  const double* __restrict__ scal) {
+    const Chunk ch = chunks[blockIdx.x];
+    const double* sc = scal + ch.seg * kScal;
+    if (sc[kActive] == 0.0) return;
+    const double rz = sc[kRZ];
+    const T c = static_cast<T>((sc[kTmp] != 0.0 || rz == 0.0) ? 0.0 : sc[kRZnew] / rz);
+    for (int64_t i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+        const T zn = znew[i];
+        p[i] = zn + c * (p[i] - z[i]);
+        z[i] = zn;
+    }
+}
+
+// x += (double) xh; xh = 0 (flush of the low-precision correction).
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads)
+    k_flush(const Chunk* __restrict__ chunks, double* __restrict__ x, T* __restrict__ xh) {
+    const Chunk ch = chunks[blockIdx.x];
+    for (int64_t i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+        x[i] += static_cast<double>(xh[i]);
+        xh[i] = T(0);
+    }
+}
+
+// Preconditioned CG with reliable updates (residual replacement; Clark et al., "Solving lattice
+// QCD systems of equations using mixed precision solvers on GPUs", 2010; van der Vorst & Ye,
+// "Residual replacement strategies for Krylov subspace iterative methods", 2000).  The recurrence
+// runs in T (operator, preconditioner and vectors in T, dot products accumulated in FP64) and
+// accumulates its correction in xh.  Whenever a segment's recurrence residual has dropped by
+// `delta` since the last update, or claims convergence, the correction is flushed into the FP64
+// solution x, the true residual r64 = b - A x is recomputed in FP64 and replaces the recurrence
+// residual; the search direction is rebuilt from the replaced residual with the CG recurrence
+// (k_replace_dir), so the Krylov information is kept -- unless the true residual exceeds the
+// recurrence residual by more than 2x (accumulated drift), in which case that segment restarts
+// from p = z.  A segment whose true residual gains less than 1% over max(2000, iterations / 2)
+// iterations has reached the attainable accuracy of the recurrence and stops unconverged.  Convergence is decided on the FP64 residual only.  For T = double xh
+// aliases x and rh aliases r64.
+template <typename T>
+int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, double* x, T* xh, double* r64, T* rh,
+                 CgVectors<T> v, double* t64, double* partial, double* scal, double rtol, double delta, int max_it,
+                 int max_updates, bool graphs, cudaStream_t s, std::vector<double>& rn, std::vector<double>& bn,
+                 int* iters, int* updates, bool* diverged) {
+    constexpr bool kLow = !std::is_same_v<T, double>;
+    constexpr int kCheck = 8;
+    const int nseg = sp.nseg;
+    if (max_updates <= 0) max_updates = 1 << 20;
+    std::vector<double> tol(nseg), act(nseg), rmax(nseg), best(nseg);
+    std::vector<int> stall(nseg, 0);
+    std::vector<double> hs(static_cast<size_t>(nseg) * kScal);
+    *iters = 0;
+    *updates = 0;
+    *diverged = false;
+    // true residual, activity, recurrence start
+    TDG_TRY(residual64(op, sp, b, x, r64, t64, partial, scal, rn, bn, s));
+    bool any = false;
+    for (int i = 0; i < nseg; ++i) {
+        tol[i] = rtol * bn[i];
+        act[i] = rn[i] > tol[i] ? 1.0 : 0.0;
+        rmax[i] = rn[i];
+        best[i] = rn[i];
+        any = any || act[i] != 0.0;
+    }
+    if (!any) return 0;
+    if constexpr (kLow) {
+        k_scale_convert<double, T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, r64, rh, scal, -1);
+        k_fill<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, xh, T(0));
+    }
+    TDG_TRY(cg_start<T>(op, prec, sp, v, partial, scal, act, s));
+    cudaGraphExec_t exec = nullptr;
+    int rc = 0;
+    for (;;) {
+        // one block of iterations
+        const bool use_graph = graphs && s != nullptr && *iters >= kCheck;
+        if (use_graph && !exec) {
+            cudaGraph_t graph = nullptr;
+            rc = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess ? 0 : TDG_E_CUDA;
+            for (int i = 0; i < kCheck && rc == 0; ++i) rc = cg_iteration<T>(op, prec, sp, xh, v, partial, scal, s);
+            cudaError_t ce = cudaStreamEndCapture(s, &graph);
+            if (rc == 0 && ce == cudaSuccess) rc = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess ? 0 : TDG_E_CUDA;
+            else if (rc == 0) rc = TDG_E_CUDA;
+            if (graph) cudaGraphDestroy(graph);
+            if (rc) break;
+        }
+        if (exec) {
+            if (cudaGraphLaunch(exec, s) != cudaSuccess) {
+                rc = fail(TDG_E_CUDA, "graph launch");
+                break;
+            }
+        } else {
+            for (int i = 0; i < kCheck && rc == 0; ++i) rc = cg_iteration<T>(op, prec, sp, xh, v, partial, scal, s);
+            if (rc) break;
+        }
+        *iters += kCheck;
+        // decide on reliable updates from the recurrence residuals
+        if (cudaMemcpyAsync(hs.data(), scal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = fail(TDG_E_CUDA, "reading the Krylov scalars");
+            break;
+        }
+        bool update = *iters >= max_it;
+        for (int i = 0; i < nseg; ++i) {
+            if (hs[static_cast<size_t>(i) * kScal + kActive] == 0.0) continue;
+            const double rr = std::sqrt(hs[static_cast<size_t>(i) * kScal + kRR]);
+            if (!std::isfinite(rr) || rr <= delta * rmax[i] || rr <= tol[i]) update = true;
+        }
+        if (!update) continue;
+        // reliable update: flush, FP64 residual, replace the recurrence residual
+        ++*updates;
+        if constexpr (kLow) k_flush<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, xh);
+        if ((rc = residual64(op, sp, b, x, r64, t64, partial, scal, rn, bn, s))) break;
+        any = false;
+        bool restart_any = false;
+        for (int i = 0; i < nseg; ++i) {
+            double* sr = &hs[static_cast<size_t>(i) * kScal];
+            sr[kTmp] = 0.0;
+            if (sr[kActive] == 0.0) continue;
+            if (!std::isfinite(rn[i])) {
+                *diverged = true;
+                sr[kActive] = 0.0;
+                continue;
+            }
+            if (rn[i] <= tol[i]) {
+                sr[kActive] = 0.0;
+                continue;
+            }
+            // stagnation: no 1% gain of the true residual over the last max(2000, iters / 2)
+            // iterations -- the attainable accuracy of this recurrence is reached
+            if (rn[i] < 0.99 * best[i]) {
+                best[i] = rn[i];
+                stall[i] = *iters;
+            } else if (*iters - stall[i] > std::max(2000, *iters / 2)) {
+                sr[kActive] = 0.0;
+                continue;
+            }
+            // the recurrence residual fell below the true one: its search direction no longer
+            // matches the replaced residual, restart it
+            const double rrec = std::sqrt(sr[kRR]);
+            if (!(rn[i] <= 2.0 * rrec)) {
+                sr[kTmp] = 1.0;
+                restart_any = true;
+            }
+            rmax[i] = rn[i];
+            any = true;
+        }
+        if (!any || *diverged || *iters >= max_it || *updates >= max_updates) break;
+        // restore the scalars (alpha / beta state, activity, restart flags) that residual64
+        // overwrote, then recompute z = M rh, rz and rr from the replaced residual; the search
+        // direction p stays unless the segment restarts
+        if (cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) {
+            rc = fail(TDG_E_CUDA, "writing the Krylov scalars");
+            break;
+        }
+        if constexpr (kLow) k_scale_convert<double, T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, r64, rh, scal, -1);
+        // z_new = M r_new into q (free between iterations), rz_new, rr; then p and z
+        if ((rc = tdg_bjacobi_apply(op, prec, rh, v.q, sp.op_nrhs, sp.op_ld, s))) break;
+        if ((rc = dots<T>(sp, rh, v.q, rh, rh, partial, scal, kRZnew, kRR, s))) break;
+        k_replace_dir<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, v.p, v.z, v.q, scal);
+        k_cg_shift<<<(nseg + 127) / 128, 128, 0, s>>>(scal, nseg);
+        (void)restart_any;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (rc) return rc;
+    if constexpr (kLow) k_flush<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, xh);
+    return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "solve kernels");
+}
+
 // Shared solve driver over a segment plan.  seg_rel (optional) receives each segment's final
 // relative residual.
 int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> const& seg_begin,
@@ -795,64 +1048,40 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     const double rtol = opts->rtol > 0 ? opts->rtol : 1e-10;
     const bool graphs = opts->use_graphs != 0;
     std::vector<double> rn, bn;
-    int total_it = 0, outer = 0;
+    int total_it = 0, updates = 0;
     bool diverged = false;
     auto rel_of = [&](int i) { return bn[i] > 0 ? rn[i] / bn[i] : 0.0; };
-
     if (prec == TDG_FP64) {
-        // FP64 PCG with a true-residual check and restart on recurrence drift
-        for (int restart = 0; restart < 4; ++restart) {
-            TDG_TRY(residual64(op, sp, b, x, r64, t64, partial, scal, rn, bn, s));
-            std::vector<double> tol(nseg), act(nseg);
-            bool any = false;
-            for (int i = 0; i < nseg; ++i) {
-                tol[i] = rtol * bn[i];
-                act[i] = (rn[i] > tol[i]) ? 1.0 : 0.0;
-                any = any || act[i] != 0.0;
-            }
-            if (!any || total_it >= max_it) break;
-            TDG_TRY(cg_start<double>(op, TDG_FP64, sp, {r64, z64, p64, q64}, partial, scal, act, s));
-            int it = 0;
-            TDG_TRY(cg_loop<double>(op, TDG_FP64, sp, x, {r64, z64, p64, q64}, partial, scal, tol, max_it - total_it,
-                                    graphs, s, &it, &diverged));
-            total_it += it;
-            if (diverged) break;
-        }
+        // the recurrence residual is r64 itself and x accumulates directly
+        const double delta = opts->inner_rtol > 0 ? opts->inner_rtol : 1e-2;
+        TDG_TRY((pcg_reliable<double>(op, TDG_FP64, sp, b, x, x, r64, r64, {r64, z64, p64, q64}, t64, partial, scal,
+                                      rtol, delta, max_it, opts->max_outer, graphs, s, rn, bn, &total_it, &updates,
+                                      &diverged)));
     } else {
-        float* d32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
+        float* xh = reinterpret_cast<float*>(take(vec * sizeof(float)));
         float* r32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
         float* z32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
         float* p32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
         float* q32 = reinterpret_cast<float*>(take(vec * sizeof(float)));
-        const double inner_rtol = opts->inner_rtol > 0 ? opts->inner_rtol : 1e-4;
-        const int max_outer = opts->max_outer > 0 ? opts->max_outer : 30;
-        for (outer = 0; outer < max_outer; ++outer) {
-            // FP64 residual; scal_out[seg][kRR] = ||r||^2 scales the FP32 correction
-            TDG_TRY(residual64(op, sp, b, x, r64, t64, partial, scal_out, rn, bn, s));
-            std::vector<double> act(nseg), tol(nseg, inner_rtol);
-            bool any = false;
-            for (int i = 0; i < nseg; ++i) {
-                act[i] = rel_of(i) > rtol ? 1.0 : 0.0;
-                any = any || act[i] != 0.0;
-            }
-            if (!any || total_it >= max_it) break;
-            // inner problem A d = r / ||r|| in FP32 from d = 0
-            k_scale_convert<double, float><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, r64, r32, scal_out, kRR);
-            k_fill<float><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, d32, 0.0f);
-            TDG_TRY(cg_start<float>(op, TDG_FP32, sp, {r32, z32, p32, q32}, partial, scal, act, s));
-            int it = 0;
-            TDG_TRY(cg_loop<float>(op, TDG_FP32, sp, d32, {r32, z32, p32, q32}, partial, scal, tol, max_it - total_it,
-                                   graphs, s, &it, &diverged));
-            total_it += it;
-            // x += ||r|| d for the segments that were active in this refinement step
-            std::vector<double> hs(static_cast<size_t>(nseg) * kScal, 0.0);
-            for (int i = 0; i < nseg; ++i) hs[static_cast<size_t>(i) * kScal + kActive] = act[i];
-            TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-            k_correct<float><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, d32, scal_out, kRR, scal);
-            if (diverged) break;
+        const double delta = opts->inner_rtol > 0 ? opts->inner_rtol : 0.1;
+        TDG_TRY((pcg_reliable<float>(op, TDG_FP32, sp, b, x, xh, r64, r32, {r32, z32, p32, q32}, t64, partial, scal,
+                                     rtol, delta, max_it, opts->max_outer, graphs, s, rn, bn, &total_it, &updates,
+                                     &diverged)));
+        // problems still above the target (the FP32 recurrence stalled) continue in FP64 with the
+        // FP32 inverses as preconditioner
+        bool rest = false;
+        for (int i = 0; i < nseg && !diverged; ++i) rest = rest || rel_of(i) > rtol;
+        if (rest && !diverged && total_it < max_it) {
+            int it2 = 0, up2 = 0;
+            TDG_TRY((pcg_reliable<double>(op, TDG_FP64, sp, b, x, x, r64, r64, {r64, z64, p64, q64}, t64, partial,
+                                          scal, rtol, 1e-2, max_it - total_it, opts->max_outer, graphs, s, rn, bn,
+                                          &it2, &up2, &diverged)));
+            total_it += it2;
+            updates += up2;
+            stats->fp64_iterations = it2;
         }
-        stats->outer = outer;
     }
+    stats->outer = updates;
     if (!diverged) TDG_TRY(residual64(op, sp, b, x, r64, t64, partial, scal, rn, bn, s));
 
     TDG_CUDA_TRY(cudaEventRecord(ev1, s));

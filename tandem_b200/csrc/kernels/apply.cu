@@ -78,7 +78,7 @@ namespace {
 
 template <class S>
 int run_apply_mma(DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y, int nrhs, int64_t ld,
-                  cudaStream_t s) {
+                  cudaStream_t s, int ctas) {
     using L = MmaTile<S>;
     const MmaLayout lay = mma_layout<S>(op.Nq, op.nq);
     const size_t smem = sizeof(double) * static_cast<size_t>(lay.total);
@@ -88,14 +88,18 @@ int run_apply_mma(DevOp<double> const& op, MmaTiles const& mt, const double* x, 
     if (smem + 2 * L::TE * sizeof(int) > static_cast<size_t>(optin)) return TDG_E_INVALID;
     auto kern = apply_mma_kernel<S>;
     static size_t configured = 0;
+    static int per_sm = 1;
     if (configured < smem) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
             cudaSuccess)
             return TDG_E_CUDA;
         configured = smem;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L::NT, smem) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
     }
     const int64_t nwork = static_cast<int64_t>(mt.ntiles) * nrhs;
-    int64_t grid = device_sm_count();
+    const int want = (ctas > 0 && ctas < per_sm) ? ctas : (ctas > 0 ? per_sm : 1);
+    int64_t grid = static_cast<int64_t>(device_sm_count()) * want;
     if (grid > nwork) grid = nwork;
     if (grid < 1) grid = 1;
     kern<<<static_cast<unsigned>(grid), L::NT, smem, s>>>(op, mt, x, y, ld, nrhs);
@@ -104,19 +108,19 @@ int run_apply_mma(DevOp<double> const& op, MmaTiles const& mt, const double* x, 
 
 template <int D, int N>
 int mma_kind(int kind, DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y, int nrhs, int64_t ld,
-             cudaStream_t s) {
-    if (kind == kPoisson) return run_apply_mma<Shape<D, N, kPoisson>>(op, mt, x, y, nrhs, ld, s);
-    return run_apply_mma<Shape<D, N, kElasticity>>(op, mt, x, y, nrhs, ld, s);
+             cudaStream_t s, int ctas) {
+    if (kind == kPoisson) return run_apply_mma<Shape<D, N, kPoisson>>(op, mt, x, y, nrhs, ld, s, ctas);
+    return run_apply_mma<Shape<D, N, kElasticity>>(op, mt, x, y, nrhs, ld, s, ctas);
 }
 
 template <int D>
 int mma_deg(int N, int kind, DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y, int nrhs,
-            int64_t ld, cudaStream_t s) {
+            int64_t ld, cudaStream_t s, int ctas) {
     switch (N) {
-        case 1: return mma_kind<D, 1>(kind, op, mt, x, y, nrhs, ld, s);
-        case 2: return mma_kind<D, 2>(kind, op, mt, x, y, nrhs, ld, s);
-        case 3: return mma_kind<D, 3>(kind, op, mt, x, y, nrhs, ld, s);
-        case 4: return mma_kind<D, 4>(kind, op, mt, x, y, nrhs, ld, s);
+        case 1: return mma_kind<D, 1>(kind, op, mt, x, y, nrhs, ld, s, ctas);
+        case 2: return mma_kind<D, 2>(kind, op, mt, x, y, nrhs, ld, s, ctas);
+        case 3: return mma_kind<D, 3>(kind, op, mt, x, y, nrhs, ld, s, ctas);
+        case 4: return mma_kind<D, 4>(kind, op, mt, x, y, nrhs, ld, s, ctas);
         default: return TDG_E_INVALID;
     }
 }
@@ -124,10 +128,10 @@ int mma_deg(int N, int kind, DevOp<double> const& op, MmaTiles const& mt, const 
 }  // namespace
 
 int launch_apply_mma(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y,
-                     int nrhs, int64_t ld, cudaStream_t s) {
+                     int nrhs, int64_t ld, cudaStream_t s, int ctas) {
     if (nrhs < 1 || mt.ntiles < 1) return TDG_E_INVALID;
-    if (D == 2) return mma_deg<2>(N, kind, op, mt, x, y, nrhs, ld, s);
-    if (D == 3) return mma_deg<3>(N, kind, op, mt, x, y, nrhs, ld, s);
+    if (D == 2) return mma_deg<2>(N, kind, op, mt, x, y, nrhs, ld, s, ctas);
+    if (D == 3) return mma_deg<3>(N, kind, op, mt, x, y, nrhs, ld, s, ctas);
     return TDG_E_INVALID;
 }
 

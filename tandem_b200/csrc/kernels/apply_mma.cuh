@@ -217,7 +217,7 @@ __device__ __forceinline__ void cta_gemm_acc_t(const double* A, const double* B,
 }
 
 template <class S>
-__global__ void __launch_bounds__(MmaTile<S>::NT, 1)
+__global__ void __launch_bounds__(MmaTile<S>::NT, (S::D == 2) ? 2 : 1)
     apply_mma_kernel(DevOp<double> op, MmaTiles mt, const double* __restrict__ x, double* __restrict__ y, int64_t ld,
                      int nrhs) {
     using L = MmaTile<S>;

@@ -10,7 +10,7 @@ namespace {
 
 template <class S>
 int run_apply_tc32(DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y, int nrhs, int64_t ld,
-                   cudaStream_t s) {
+                   cudaStream_t s, int ctas) {
     using L = Tc32Tile<S>;
     const Tc32Layout lay = tc32_layout<S>(op.Nq, op.nq);
     const size_t smem = sizeof(float) * static_cast<size_t>(lay.total);
@@ -31,7 +31,8 @@ int run_apply_tc32(DevOp<float> const& op, Tc32Tiles const& mt, const float* x, 
             per_sm = 1;
     }
     const int64_t nwork = static_cast<int64_t>(mt.ntiles) * nrhs;
-    int64_t grid = static_cast<int64_t>(device_sm_count()) * per_sm;
+    const int want = (ctas > 0 && ctas < per_sm) ? ctas : per_sm;
+    int64_t grid = static_cast<int64_t>(device_sm_count()) * want;
     if (grid > nwork) grid = nwork;
     if (grid < 1) grid = 1;
     kern<<<static_cast<unsigned>(grid), L::NT, smem, s>>>(op, mt, x, y, ld, nrhs);
@@ -40,19 +41,19 @@ int run_apply_tc32(DevOp<float> const& op, Tc32Tiles const& mt, const float* x, 
 
 template <int D, int N>
 int tc_kind(int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y, int nrhs, int64_t ld,
-            cudaStream_t s) {
-    if (kind == kPoisson) return run_apply_tc32<Shape<D, N, kPoisson>>(op, mt, x, y, nrhs, ld, s);
-    return run_apply_tc32<Shape<D, N, kElasticity>>(op, mt, x, y, nrhs, ld, s);
+            cudaStream_t s, int ctas) {
+    if (kind == kPoisson) return run_apply_tc32<Shape<D, N, kPoisson>>(op, mt, x, y, nrhs, ld, s, ctas);
+    return run_apply_tc32<Shape<D, N, kElasticity>>(op, mt, x, y, nrhs, ld, s, ctas);
 }
 
 template <int D>
 int tc_deg(int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y, int nrhs,
-           int64_t ld, cudaStream_t s) {
+           int64_t ld, cudaStream_t s, int ctas) {
     switch (N) {
-        case 1: return tc_kind<D, 1>(kind, op, mt, x, y, nrhs, ld, s);
-        case 2: return tc_kind<D, 2>(kind, op, mt, x, y, nrhs, ld, s);
-        case 3: return tc_kind<D, 3>(kind, op, mt, x, y, nrhs, ld, s);
-        case 4: return tc_kind<D, 4>(kind, op, mt, x, y, nrhs, ld, s);
+        case 1: return tc_kind<D, 1>(kind, op, mt, x, y, nrhs, ld, s, ctas);
+        case 2: return tc_kind<D, 2>(kind, op, mt, x, y, nrhs, ld, s, ctas);
+        case 3: return tc_kind<D, 3>(kind, op, mt, x, y, nrhs, ld, s, ctas);
+        case 4: return tc_kind<D, 4>(kind, op, mt, x, y, nrhs, ld, s, ctas);
         default: return TDG_E_INVALID;
     }
 }
@@ -60,10 +61,10 @@ int tc_deg(int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const f
 }  // namespace
 
 int launch_apply_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y,
-                      int nrhs, int64_t ld, cudaStream_t s) {
+                      int nrhs, int64_t ld, cudaStream_t s, int ctas) {
     if (nrhs < 1 || mt.ntiles < 1) return TDG_E_INVALID;
-    if (D == 2) return tc_deg<2>(N, kind, op, mt, x, y, nrhs, ld, s);
-    if (D == 3) return tc_deg<3>(N, kind, op, mt, x, y, nrhs, ld, s);
+    if (D == 2) return tc_deg<2>(N, kind, op, mt, x, y, nrhs, ld, s, ctas);
+    if (D == 3) return tc_deg<3>(N, kind, op, mt, x, y, nrhs, ld, s, ctas);
     return TDG_E_INVALID;
 }
 

@@ -49,15 +49,15 @@ int run_invert(int64_t E, const double* blk, T* inv, int* status, cudaStream_t s
     return cudaGetLastError() == cudaSuccess ? 0 : TDG_E_CUDA;
 }
 
-template <int BS, typename T>
-int run_bapply(int64_t E, const T* inv, const T* r, T* z, int nrhs, int64_t ld, cudaStream_t s) {
+template <int BS, typename TM, typename TV>
+int run_bapply(int64_t E, const TM* inv, const TV* r, TV* z, int nrhs, int64_t ld, cudaStream_t s) {
     constexpr int TE = (256 / BS) > 0 ? (256 / BS) : 1;
     const int64_t ntiles = (E + TE - 1) / TE;
     int64_t grid = static_cast<int64_t>(device_sm_count()) * 8;
     if (grid > ntiles) grid = ntiles;
     if (grid < 1) grid = 1;
     dim3 g(static_cast<unsigned>(grid), static_cast<unsigned>(nrhs));
-    bjac_apply_kernel<BS, T><<<g, 256, 0, s>>>(E, inv, r, z, ld);
+    bjac_apply_kernel<BS, TM, TV><<<g, 256, 0, s>>>(E, inv, r, z, ld);
     return cudaGetLastError() == cudaSuccess ? 0 : TDG_E_CUDA;
 }
 
@@ -84,12 +84,12 @@ int launch_bjac_invert(int bs, int64_t E, const double* blk, T* inv, int* status
     }
 }
 
-template <typename T>
-int launch_bjac_apply(int bs, int64_t E, const T* inv, const T* r, T* z, int nrhs, int64_t ld,
+template <typename TM, typename TV>
+int launch_bjac_apply(int bs, int64_t E, const TM* inv, const TV* r, TV* z, int nrhs, int64_t ld,
                       cudaStream_t s) {
     switch (bs) {
 #define TDG_CASE(B) \
-    case B: return run_bapply<B, T>(E, inv, r, z, nrhs, ld, s);
+    case B: return run_bapply<B, TM, TV>(E, inv, r, z, nrhs, ld, s);
         TDG_FOR_EACH_BS(TDG_CASE)
 #undef TDG_CASE
         default: return TDG_E_INVALID;
@@ -98,9 +98,11 @@ int launch_bjac_apply(int bs, int64_t E, const T* inv, const T* r, T* z, int nrh
 
 template int launch_bjac_invert<double>(int, int64_t, const double*, double*, int*, cudaStream_t);
 template int launch_bjac_invert<float>(int, int64_t, const double*, float*, int*, cudaStream_t);
-template int launch_bjac_apply<double>(int, int64_t, const double*, const double*, double*, int, int64_t,
-                                       cudaStream_t);
-template int launch_bjac_apply<float>(int, int64_t, const float*, const float*, float*, int, int64_t,
-                                      cudaStream_t);
+template int launch_bjac_apply<double, double>(int, int64_t, const double*, const double*, double*, int, int64_t,
+                                               cudaStream_t);
+template int launch_bjac_apply<float, float>(int, int64_t, const float*, const float*, float*, int, int64_t,
+                                             cudaStream_t);
+template int launch_bjac_apply<float, double>(int, int64_t, const float*, const double*, double*, int, int64_t,
+                                              cudaStream_t);
 
 }  // namespace tdg

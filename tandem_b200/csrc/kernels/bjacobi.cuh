@@ -186,12 +186,12 @@ __global__ void __launch_bounds__(256)
 }
 
 // z = Dinv r for nrhs vectors: one thread per (element, row).
-template <int BS, typename T>
-__global__ void __launch_bounds__(256) bjac_apply_kernel(int64_t E, const T* __restrict__ inv,
-                                                         const T* __restrict__ r, T* __restrict__ z,
+template <int BS, typename TM, typename TV>
+__global__ void __launch_bounds__(256) bjac_apply_kernel(int64_t E, const TM* __restrict__ inv,
+                                                         const TV* __restrict__ r, TV* __restrict__ z,
                                                          int64_t ld) {
     constexpr int TE = (256 / BS) > 0 ? (256 / BS) : 1;
-    __shared__ T sr[TE * BS];
+    __shared__ TV sr[TE * BS];
     const int rhs = blockIdx.y;
     r += rhs * ld;
     z += rhs * ld;
@@ -200,16 +200,16 @@ __global__ void __launch_bounds__(256) bjac_apply_kernel(int64_t E, const T* __r
         const int64_t e0 = tile * TE;
         __syncthreads();
         for (int i = threadIdx.x; i < TE * BS; i += blockDim.x)
-            sr[i] = (e0 + i / BS < E) ? r[e0 * BS + i] : T(0);
+            sr[i] = (e0 + i / BS < E) ? r[e0 * BS + i] : TV(0);
         __syncthreads();
         const int te = threadIdx.x / BS, row = threadIdx.x % BS;
         const int64_t e = e0 + te;
         if (te < TE && e < E) {
-            const T* m = inv + e * BS * BS + row;
-            const T* rv = sr + te * BS;
-            T s = T(0);
+            const TM* m = inv + e * BS * BS + row;
+            const TV* rv = sr + te * BS;
+            TV s = TV(0);
 #pragma unroll 8
-            for (int c = 0; c < BS; ++c) s += m[c * BS] * rv[c];
+            for (int c = 0; c < BS; ++c) s += static_cast<TV>(m[c * BS]) * rv[c];
             z[e * BS + row] = s;
         }
     }

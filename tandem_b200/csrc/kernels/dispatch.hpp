@@ -19,20 +19,24 @@ int launch_apply(int D, int N, int kind, DevOp<T> const& op, const T* x, T* y, i
 struct MmaTiles;
 // FP64 apply on the FP64 tensor pipe over signature-grouped element tiles (apply_mma.cuh);
 // TDG_E_INVALID when the instance's tables do not fit in shared memory.
+// ctas: persistent CTAs per SM requested (clipped to the occupancy limit); 0 = the default
+// (1 for the FP64 tensor kernel, the occupancy limit for the FP32 one).
 int launch_apply_mma(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y,
-                     int nrhs, int64_t ld, cudaStream_t s);
+                     int nrhs, int64_t ld, cudaStream_t s, int ctas = 0);
 
 // FP32 apply on the tensor cores in the 3xTF32 form (apply_tc32.cuh); TDG_E_INVALID when the
 // shape's shared-memory layout does not fit (the caller then uses the SIMT kernel).
 struct Tc32Tiles;
 int launch_apply_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y,
-                      int nrhs, int64_t ld, cudaStream_t s);
+                      int nrhs, int64_t ld, cudaStream_t s, int ctas = 0);
 int launch_bjac_assemble(int D, int N, int kind, DevOp<double> const& op, double* blk,
                          cudaStream_t s);
 template <typename T>
 int launch_bjac_invert(int bs, int64_t E, const double* blk, T* inv, int* status, cudaStream_t s);
-template <typename T>
-int launch_bjac_apply(int bs, int64_t E, const T* inv, const T* r, T* z, int nrhs, int64_t ld,
+// z = D^-1 r with inverses stored as TM and vectors TV (TM = float, TV = double: FP32 inverses
+// applied to FP64 vectors).
+template <typename TM, typename TV>
+int launch_bjac_apply(int bs, int64_t E, const TM* inv, const TV* r, TV* z, int nrhs, int64_t ld,
                       cudaStream_t s);
 
 struct DevFault;

@@ -133,6 +133,15 @@ class DGOperator:
         _ffi.check(_ffi.lib().tdg_apply(self._h, precision, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
                                         nrhs, ld, _stream(stream)))
 
+    def autotune(self, precision: int = FP64, nrhs: int = 1, stream=None) -> list[dict]:
+        """Times the candidate apply launch configurations on this operator and keeps the fastest
+        for later applies and solves in `precision` (tdg_autotune).  Returns every measurement."""
+        entries = (_ffi.TuneEntry * 16)()
+        n = C.c_int(0)
+        _ffi.check(_ffi.lib().tdg_autotune(self._h, precision, nrhs, _stream(stream), entries, 16, C.byref(n)))
+        return [dict(family=("tensor" if e.family == 0 else "simt"), ctas_per_sm=e.ctas_per_sm, ms=e.ms)
+                for e in entries[:n.value]]
+
     def flops_apply(self) -> int:
         return int(_ffi.lib().tdg_flops_apply(self._h))
 
@@ -165,10 +174,11 @@ class DGOperator:
         return b
 
     def solve(self, b, x, precision: int = FP64, rtol: float = 1e-10, max_iterations: int = 20000,
-              inner_rtol: float = 1e-4, max_outer: int = 40, use_graphs: bool = True, nrhs: int = 1,
+              inner_rtol: float = 0.0, max_outer: int = 0, use_graphs: bool = True, nrhs: int = 1,
               ld: int | None = None, stream=None) -> dict:
-        """Block-Jacobi preconditioned CG on the device (FP64, or FP32 inner CG in FP64
-        iterative refinement).  Raises on non-convergence."""
+        """Block-Jacobi preconditioned CG on the device: FP64, or FP32 (operator, preconditioner
+        and recurrence in FP32, solution and true residual in FP64 via reliable updates).
+        inner_rtol: reliable-update threshold (0 = default); raises on non-convergence."""
         ld = self.ndof if ld is None else ld
         _check_vec(b, FP64, nrhs * ld)
         _check_vec(x, FP64, nrhs * ld)
@@ -177,14 +187,14 @@ class DGOperator:
         rc = _ffi.lib().tdg_solve(self._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), nrhs, ld,
                                   C.byref(opts), C.byref(st), _stream(stream))
         stats = dict(iterations=st.iterations, outer=st.outer, rel_residual=st.rel_residual,
-                     seconds=st.seconds, converged=bool(st.converged))
+                     seconds=st.seconds, converged=bool(st.converged), fp64_iterations=st.fp64_iterations)
         if rc != 0:
             raise _ffi.TdgError(f"{_ffi.ERRORS.get(rc, rc)}: {_ffi.lib().tdg_last_error().decode()} {stats}")
         return stats
 
 
 def solve_segmented(op: DGOperator, b, x, elem_offsets, precision: int = FP64, rtol: float = 1e-10,
-                    max_iterations: int = 20000, inner_rtol: float = 1e-4, max_outer: int = 40,
+                    max_iterations: int = 20000, inner_rtol: float = 0.0, max_outer: int = 0,
                     use_graphs: bool = True, stream=None):
     """Independent problems held in one block-diagonal operator (a mesh union): one apply and one
     preconditioner launch per iteration cover every problem, each problem has its own CG scalars
@@ -199,7 +209,7 @@ def solve_segmented(op: DGOperator, b, x, elem_offsets, precision: int = FP64, r
     rc = _ffi.lib().tdg_solve_segmented(op._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), nseg,
                                         off.ctypes.data, C.byref(opts), C.byref(st), rel.ctypes.data, _stream(stream))
     stats = dict(iterations=st.iterations, outer=st.outer, rel_residual=st.rel_residual, seconds=st.seconds,
-                 converged=bool(st.converged))
+                 converged=bool(st.converged), fp64_iterations=st.fp64_iterations)
     if rc != 0:
         raise _ffi.TdgError(f"{_ffi.ERRORS.get(rc, rc)}: {_ffi.lib().tdg_last_error().decode()} {stats}")
     return stats, rel

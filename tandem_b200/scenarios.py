@@ -3,9 +3,9 @@ quadrature-point coordinates the operator exposes -- the role tandem's Lua scena
 (app/common/Scenario.h:37-78).
 
 * ``PoissonSinSin``: -div(K grad u) = f with K = 1, u = sin(pi x) sin(pi y) (2D), f = 2 pi^2 u.
-* ``RandomField``: smooth log-normal field exp(sigma Z - sigma^2 / 2), Z a unit-variance Gaussian
-  random field with Gaussian covariance of length ell realised by M random Fourier features from a
-  seed (closed form, so gradients are exact).
+* ``RandomField``: smooth log-normal field mean exp(sigma Z - sigma^2 / 2) (or the Gaussian field
+  mean + sigma Z), Z a unit-variance Gaussian random field with Gaussian covariance of length ell
+  realised by M random Fourier features from a seed (closed form, so gradients are exact).
 * ``ElasticityCosine``: isotropic elasticity with variable lambda, mu and the cosine manufactured
   solution of tandem's examples/elasticity/3d/cosine.lua, u = (cos pi x cos pi y, 0,
   cos pi x cos pi z) (2D: (cos pi x cos pi y, 0)); f = -div sigma(u) with
@@ -43,12 +43,12 @@ class PoissonSinSin:
 
 class RandomField:
     def __init__(self, dim: int, seed: int, ell: float = 0.2, sigma: float = 0.3, features: int = 256,
-                 mean: float = 1.0):
+                 mean: float = 1.0, lognormal: bool = True):
         rng = np.random.Generator(np.random.PCG64(seed))
         self.omega = rng.normal(0.0, 1.0 / ell, size=(features, dim))
         self.phase = rng.uniform(0.0, 2.0 * PI, size=features)
         self.amp = np.sqrt(2.0 / features)
-        self.sigma, self.mean = sigma, mean
+        self.sigma, self.mean, self.lognormal = sigma, mean, lognormal
 
     CHUNK = 1 << 18  # points per block (bounds the [points, features] temporaries)
 
@@ -68,11 +68,16 @@ class RandomField:
             z[s:s + self.CHUNK] = self.amp * torch.cos(arg).sum(dim=1)
             if grad:
                 dz[s:s + self.CHUNK] = -self.amp * (torch.sin(arg) @ om)
-        v = self.mean * torch.exp(self.sigma * z - 0.5 * self.sigma ** 2)
+        if self.lognormal:
+            v = self.mean * torch.exp(self.sigma * z - 0.5 * self.sigma ** 2)
+            scale = self.sigma * v
+        else:  # Gaussian field mean + sigma Z
+            v = self.mean + self.sigma * z
+            scale = torch.full_like(z, self.sigma)
         val = v.cpu().numpy().reshape(shape[:-1])
         if not grad:
             return val, None
-        g = ((self.sigma * v)[:, None] * dz).cpu().numpy().reshape(shape)
+        g = (scale[:, None] * dz).cpu().numpy().reshape(shape)
         return val, g
 
     def __call__(self, x):

@@ -6,6 +6,10 @@
   manufactured solution with Dirichlet data.
 * ``poisson_square``: 2D Poisson, degree N, tandem GenMesh<2> n x n x 2 triangles, K = 1,
   u = sin(pi x) sin(pi y), all-Dirichlet.
+* ``uneven_batch``: `count` independent 2D elasticity problems, degree N, on unit squares with
+  P2-curved boundaries whose element counts are log-uniform in [lo, hi] (seeded), each with its
+  own log-normal random lambda / mu (as above) and a random-Fourier-feature body force,
+  homogeneous Dirichlet data; held as one block-diagonal operator over the mesh union.
 """
 from __future__ import annotations
 
@@ -56,3 +60,44 @@ def poisson_square(n: int, degree: int, quad: Quadrature) -> Workload:
     g = PoissonSinSin.solution(Xf)[:, None, :]
     name = f"2D Poisson SIPG p{degree}, unit square {n}x{n}x2 triangles ({m.num_elements:,}), K=1, sin sin MMS"
     return Workload(name, m, quad, POISSON, degree, c0, None, np.ascontiguousarray(f), np.ascontiguousarray(g), op)
+
+
+@dataclass
+class Batch:
+    name: str
+    mesh: M.SimplexMesh
+    quad: Quadrature
+    degree: int
+    elem_offsets: np.ndarray
+    sizes: np.ndarray
+    force: np.ndarray
+    bc: np.ndarray
+    op: DGOperator
+
+
+def uneven_batch(count: int, degree: int, quad: Quadrature, seed: int = 7, lo: int = 1000, hi: int = 40000,
+                 ell: float = 0.2) -> Batch:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    target = np.exp(rng.uniform(np.log(lo), np.log(hi), size=count))
+    cells = np.maximum(2, np.rint(np.sqrt(target / 2.0))).astype(int)  # n x n x 2 triangles
+    meshes = [M.build(M.square_mesh(int(n)), degree, curve=M.box_boundary_surface(0.02)) for n in cells]
+    um, eoff = M.union(meshes)
+    op = DGOperator(um, degree, ELASTICITY, quad)
+    X = op.volume_coords()
+    lam = np.empty(X.shape[:2])
+    mu = np.empty(X.shape[:2])
+    force = np.empty((op.E, 2, op.Nq))
+    for i in range(count):
+        sl = slice(eoff[i], eoff[i + 1])
+        s = seed * 1000 + 10 * i
+        lam[sl] = RandomField(2, s + 1, ell=ell)(X[sl])
+        mu[sl] = RandomField(2, s + 2, ell=ell)(X[sl])
+        force[sl, 0] = RandomField(2, s + 3, ell=ell, mean=0.0, sigma=1.0, lognormal=False)(X[sl])
+        force[sl, 1] = RandomField(2, s + 4, ell=ell, mean=0.0, sigma=1.0, lognormal=False)(X[sl])
+    op.set_material(lam, mu)
+    bc = np.zeros((op.F, 2, op.nq))
+    sizes = np.diff(eoff)
+    name = (f"{count} independent 2D elasticity problems p{degree}, curved P2 unit squares, "
+            f"{int(sizes.min()):,}-{int(sizes.max()):,} triangles each ({op.E:,} total), log-normal lambda/mu, "
+            f"RFF body force, zero Dirichlet")
+    return Batch(name, um, quad, degree, eoff, sizes, np.ascontiguousarray(force), bc, op)
