@@ -42,9 +42,11 @@ extern "C" {
 #define TDG_BC_FAULT 3
 #define TDG_BC_DIRICHLET 5
 
-/* Arithmetic of an apply / preconditioner / solve. */
+/* Arithmetic of an apply / preconditioner / solve.  TDG_MIXED: FP32 operator arithmetic (and FP32
+ * block inverses) on FP64 vectors; as a solve precision, an FP64 CG recurrence around them. */
 #define TDG_FP64 0
 #define TDG_FP32 1
+#define TDG_MIXED 2
 
 typedef struct tdg_op tdg_op;
 
@@ -118,7 +120,8 @@ int tdg_penalty(const tdg_op* op, double* out);
 
 /* y = A x for nrhs stacked vectors (AbstractDGOperator::apply, src/form/AbstractDGOperator.h:34;
  * PetscDGShell::apply, app/common/PetscDGShell.cpp:48-55).  precision selects the element
- * arithmetic: TDG_FP64 takes double*, TDG_FP32 takes float*. */
+ * arithmetic: TDG_FP64 takes double*, TDG_FP32 takes float*, TDG_MIXED takes double* and computes
+ * in FP32 on the tensor cores (x rounded to FP32 on load, y widened on store). */
 int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64_t ld,
               void* stream);
 
@@ -133,8 +136,7 @@ int64_t tdg_bytes_apply(const tdg_op* op, int precision);
  * Returns TDG_E_NOT_SPD when a block is not positive definite. */
 int tdg_bjacobi_setup(tdg_op* op, int precision, void* stream);
 /* z = D^-1 r; precision is the vectors' precision: TDG_FP32 vectors need FP32 inverses, TDG_FP64
- * vectors take FP64 or FP32 inverses (the latter as the fallback preconditioner of the mixed
- * solve). */
+ * and TDG_MIXED (FP64 vectors) take FP64 or FP32 inverses. */
 int tdg_bjacobi_apply(tdg_op* op, int precision, const void* r, void* z, int nrhs, int64_t ld,
                       void* stream);
 /* Copies the assembled (not inverted) diagonal blocks [E][bs][bs] (column-major per block) to
@@ -168,14 +170,17 @@ int tdg_rhs(tdg_op* op, const double* force_Q, const double* bc_q, double* b);
 /* --- Krylov solve on the device (PetscLinearSolver / KSPCG, app/common/PetscLinearSolver.cpp) */
 
 typedef struct {
-    int32_t precision;      /* TDG_FP64: FP64 CG; TDG_FP32: FP32 CG recurrence with FP64 reliable
-                               updates (solution and true residual kept in FP64); problems whose
-                               FP32 recurrence stalls above the target continue in FP64 */
+    int32_t precision;      /* TDG_FP64: FP64 CG.  TDG_MIXED: FP64 CG recurrence around the FP32
+                               operator, with the block inverses of the last tdg_bjacobi_setup
+                               (FP32 or FP64).  TDG_FP32: FP32 CG
+                               recurrence and vectors.  Both reduced-precision modes keep the
+                               solution and the true residual in FP64 (reliable updates); problems
+                               whose TDG_FP32 recurrence stalls above the target continue in FP64 */
     int32_t max_iterations; /* total Krylov iterations cap */
     double rtol;            /* relative residual ||b - A x|| / ||b|| target (FP64 residual) */
     double inner_rtol;      /* reliable-update threshold: the FP64 residual replaces the recurrence
                                residual whenever the latter has dropped by this factor
-                               (0 = default: 0.1 for TDG_FP32, 0.01 for TDG_FP64) */
+                               (0 = default: 0.1) */
     int32_t max_outer;      /* cap on reliable updates (0 = none) */
     int32_t use_graphs;     /* capture iteration blocks in CUDA graphs */
 } tdg_solve_opts;

@@ -307,7 +307,7 @@ int ensure_uploaded(tdg_op* op, int precision) {
         }
         return 0;
     }
-    if (precision == TDG_FP32) {
+    if (precision == TDG_FP32 || precision == TDG_MIXED) {
         if (!op->uploaded32) {
             TDG_TRY(upload_precision<float>(op, op->arena32, op->op32));
             op->uploaded32 = true;
@@ -471,7 +471,7 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
     TDG_TRY(ensure_uploaded(op, precision));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int rc = TDG_E_INVALID;
-    const int pi = precision == TDG_FP32 ? 1 : 0;
+    const int pi = precision == TDG_FP64 ? 0 : 1;
     const bool tensor = op->use_mma && op->family[pi] == 0;
     if (precision == TDG_FP64 && tensor)
         rc = launch_apply_mma(h.D, h.N, h.kind, op->op64, op->mma, static_cast<const double*>(x),
@@ -480,8 +480,15 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
         rc = launch_apply<double>(h.D, h.N, h.kind, op->op64, static_cast<const double*>(x),
                                   static_cast<double*>(y), nrhs, ld, s);
     if (precision == TDG_FP32 && tensor)
-        rc = launch_apply_tc32(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const float*>(x),
-                               static_cast<float*>(y), nrhs, ld, s, op->ctas[1]);
+        rc = launch_apply_tc32<float>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const float*>(x),
+                                      static_cast<float*>(y), nrhs, ld, s, op->ctas[1]);
+    if (precision == TDG_MIXED) {
+        if (!op->use_mma) return fail(TDG_E_INVALID, "TDG_MIXED needs the tensor-core kernels");
+        rc = launch_apply_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const double*>(x),
+                                       static_cast<double*>(y), nrhs, ld, s, op->ctas[1]);
+        if (rc) return fail(rc, std::string("mixed apply launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+        return 0;
+    }
     if (precision == TDG_FP32 && rc == TDG_E_INVALID)
         rc = launch_apply<float>(h.D, h.N, h.kind, op->op32, static_cast<const float*>(x),
                                  static_cast<float*>(y), nrhs, ld, s);
@@ -564,6 +571,7 @@ int64_t tdg_bytes_apply(const tdg_op* op, int precision) {
 
 int tdg_bjacobi_setup(tdg_op* op, int precision, void* stream) {
     if (!op) return fail(TDG_E_INVALID, "null operator");
+    if (precision == TDG_MIXED) precision = TDG_FP32;  // FP32 inverses (the lighter mixed preconditioner)
     if (precision != TDG_FP64 && precision != TDG_FP32) return fail(TDG_E_INVALID, "bad precision");
     TDG_TRY(ensure_uploaded(op, TDG_FP64));
     auto const& h = op->h;
@@ -608,7 +616,7 @@ int tdg_bjacobi_setup(tdg_op* op, int precision, void* stream) {
 
 int tdg_bjacobi_apply(tdg_op* op, int precision, const void* r, void* z, int nrhs, int64_t ld, void* stream) {
     if (!op || !r || !z) return fail(TDG_E_INVALID, "null argument");
-    // FP64 vectors take FP64 or FP32 inverses; FP32 vectors take FP32 inverses
+    // FP64 and mixed (FP64 vectors) take FP64 or FP32 inverses; FP32 vectors take FP32 inverses
     if (!op->inv || (precision == TDG_FP32 && op->inv_precision != TDG_FP32))
         return fail(TDG_E_STATE, "tdg_bjacobi_setup not called for this precision");
     auto const& h = op->h;
@@ -851,8 +859,9 @@ __global__ void __launch_bounds__(kVecThreads)
 // residual; the search direction is rebuilt from the replaced residual with the CG recurrence
 // (k_replace_dir), so the Krylov information is kept -- unless the true residual exceeds the
 // recurrence residual by more than 2x (accumulated drift), in which case that segment restarts
-// from p = z.  A segment whose true residual gains less than 1% over max(2000, iterations / 2)
-// iterations has reached the attainable accuracy of the recurrence and stops unconverged.  Convergence is decided on the FP64 residual only.  For T = double xh
+// from p = z.  A segment within three decades of its target whose true residual gains less than
+// 1% over max(2000, iterations / 2) iterations has reached the attainable accuracy of the
+// recurrence and stops unconverged.  Convergence is decided on the FP64 residual only.  For T = double xh
 // aliases x and rh aliases r64.
 template <typename T>
 int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, double* x, T* xh, double* r64, T* rh,
@@ -942,12 +951,13 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
                 sr[kActive] = 0.0;
                 continue;
             }
-            // stagnation: no 1% gain of the true residual over the last max(2000, iters / 2)
-            // iterations -- the attainable accuracy of this recurrence is reached
+            // stagnation near the target (CG residual norms are not monotone, so only within
+            // three decades of it): no 1% gain of the true residual over the last
+            // max(2000, iters / 2) iterations -- the attainable accuracy of this recurrence
             if (rn[i] < 0.99 * best[i]) {
                 best[i] = rn[i];
                 stall[i] = *iters;
-            } else if (*iters - stall[i] > std::max(2000, *iters / 2)) {
+            } else if (rn[i] <= 1e3 * tol[i] && *iters - stall[i] > std::max(2000, *iters / 2)) {
                 sr[kActive] = 0.0;
                 continue;
             }
@@ -989,11 +999,12 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
                    std::vector<int64_t> const& seg_end, int op_nrhs, int64_t op_ld, size_t vec_entries,
                    const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel, cudaStream_t s) {
     const int prec = opts->precision;
-    if (prec != TDG_FP64 && prec != TDG_FP32) return fail(TDG_E_INVALID, "bad precision");
-    if (!op->inv || op->inv_precision != prec)
+    if (prec != TDG_FP64 && prec != TDG_FP32 && prec != TDG_MIXED) return fail(TDG_E_INVALID, "bad precision");
+    // FP64 needs FP64 inverses, FP32 needs FP32 inverses, MIXED takes either
+    if (!op->inv || (prec != TDG_MIXED && op->inv_precision != prec))
         return fail(TDG_E_STATE, "tdg_bjacobi_setup must be called with the solve precision");
     TDG_TRY(ensure_uploaded(op, TDG_FP64));
-    if (prec == TDG_FP32) TDG_TRY(ensure_uploaded(op, TDG_FP32));
+    if (prec != TDG_FP64) TDG_TRY(ensure_uploaded(op, TDG_FP32));
     std::memset(stats, 0, sizeof(*stats));
 
     std::vector<Chunk> hchunks;
@@ -1051,10 +1062,12 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     int total_it = 0, updates = 0;
     bool diverged = false;
     auto rel_of = [&](int i) { return bn[i] > 0 ? rn[i] / bn[i] : 0.0; };
-    if (prec == TDG_FP64) {
-        // the recurrence residual is r64 itself and x accumulates directly
-        const double delta = opts->inner_rtol > 0 ? opts->inner_rtol : 1e-2;
-        TDG_TRY((pcg_reliable<double>(op, TDG_FP64, sp, b, x, x, r64, r64, {r64, z64, p64, q64}, t64, partial, scal,
+    if (prec == TDG_FP64 || prec == TDG_MIXED) {
+        // FP64 recurrence: the recurrence residual is r64 itself and x accumulates directly; the
+        // mixed mode applies the operator in FP32 arithmetic and the FP32 inverses, so its
+        // recurrence residual drifts from the true one and is replaced more often
+        const double delta = opts->inner_rtol > 0 ? opts->inner_rtol : 0.1;
+        TDG_TRY((pcg_reliable<double>(op, prec, sp, b, x, x, r64, r64, {r64, z64, p64, q64}, t64, partial, scal,
                                       rtol, delta, max_it, opts->max_outer, graphs, s, rn, bn, &total_it, &updates,
                                       &diverged)));
     } else {

@@ -8,8 +8,8 @@ namespace tdg {
 
 namespace {
 
-template <class S>
-int run_apply_tc32(DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y, int nrhs, int64_t ld,
+template <class S, typename TX>
+int run_apply_tc32(DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y, int nrhs, int64_t ld,
                    cudaStream_t s, int ctas) {
     using L = Tc32Tile<S>;
     const Tc32Layout lay = tc32_layout<S>(op.Nq, op.nq);
@@ -18,7 +18,7 @@ int run_apply_tc32(DevOp<float> const& op, Tc32Tiles const& mt, const float* x, 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (smem + 2 * L::TE * sizeof(int) > static_cast<size_t>(optin)) return TDG_E_INVALID;
-    auto kern = apply_tc32_kernel<S>;
+    auto kern = apply_tc32_kernel<S, TX>;
     static size_t configured = 0;
     static int per_sm = 0;
     if (configured < smem) {
@@ -39,33 +39,39 @@ int run_apply_tc32(DevOp<float> const& op, Tc32Tiles const& mt, const float* x, 
     return cudaGetLastError() == cudaSuccess ? 0 : TDG_E_CUDA;
 }
 
-template <int D, int N>
-int tc_kind(int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y, int nrhs, int64_t ld,
+template <int D, int N, typename TX>
+int tc_kind(int kind, DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y, int nrhs, int64_t ld,
             cudaStream_t s, int ctas) {
-    if (kind == kPoisson) return run_apply_tc32<Shape<D, N, kPoisson>>(op, mt, x, y, nrhs, ld, s, ctas);
-    return run_apply_tc32<Shape<D, N, kElasticity>>(op, mt, x, y, nrhs, ld, s, ctas);
+    if (kind == kPoisson) return run_apply_tc32<Shape<D, N, kPoisson>, TX>(op, mt, x, y, nrhs, ld, s, ctas);
+    return run_apply_tc32<Shape<D, N, kElasticity>, TX>(op, mt, x, y, nrhs, ld, s, ctas);
 }
 
-template <int D>
-int tc_deg(int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y, int nrhs,
+template <int D, typename TX>
+int tc_deg(int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y, int nrhs,
            int64_t ld, cudaStream_t s, int ctas) {
     switch (N) {
-        case 1: return tc_kind<D, 1>(kind, op, mt, x, y, nrhs, ld, s, ctas);
-        case 2: return tc_kind<D, 2>(kind, op, mt, x, y, nrhs, ld, s, ctas);
-        case 3: return tc_kind<D, 3>(kind, op, mt, x, y, nrhs, ld, s, ctas);
-        case 4: return tc_kind<D, 4>(kind, op, mt, x, y, nrhs, ld, s, ctas);
+        case 1: return tc_kind<D, 1, TX>(kind, op, mt, x, y, nrhs, ld, s, ctas);
+        case 2: return tc_kind<D, 2, TX>(kind, op, mt, x, y, nrhs, ld, s, ctas);
+        case 3: return tc_kind<D, 3, TX>(kind, op, mt, x, y, nrhs, ld, s, ctas);
+        case 4: return tc_kind<D, 4, TX>(kind, op, mt, x, y, nrhs, ld, s, ctas);
         default: return TDG_E_INVALID;
     }
 }
 
 }  // namespace
 
-int launch_apply_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y,
+template <typename TX>
+int launch_apply_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y,
                       int nrhs, int64_t ld, cudaStream_t s, int ctas) {
     if (nrhs < 1 || mt.ntiles < 1) return TDG_E_INVALID;
-    if (D == 2) return tc_deg<2>(N, kind, op, mt, x, y, nrhs, ld, s, ctas);
-    if (D == 3) return tc_deg<3>(N, kind, op, mt, x, y, nrhs, ld, s, ctas);
+    if (D == 2) return tc_deg<2, TX>(N, kind, op, mt, x, y, nrhs, ld, s, ctas);
+    if (D == 3) return tc_deg<3, TX>(N, kind, op, mt, x, y, nrhs, ld, s, ctas);
     return TDG_E_INVALID;
 }
+
+template int launch_apply_tc32<float>(int, int, int, DevOp<float> const&, Tc32Tiles const&, const float*, float*, int,
+                                      int64_t, cudaStream_t, int);
+template int launch_apply_tc32<double>(int, int, int, DevOp<float> const&, Tc32Tiles const&, const double*, double*,
+                                       int, int64_t, cudaStream_t, int);
 
 }  // namespace tdg

@@ -222,9 +222,11 @@ __device__ __forceinline__ void tc_backproject(const float* A, const float* R, f
     }
 }
 
-template <class S>
+// TX: the vectors' type -- float, or double for the mixed solve (FP32 operator arithmetic on FP64
+// vectors: x is rounded to FP32 when it is gathered, y widened when it is stored).
+template <class S, typename TX>
 __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
-    apply_tc32_kernel(DevOp<float> op, Tc32Tiles mt, const float* __restrict__ x, float* __restrict__ y, int64_t ld,
+    apply_tc32_kernel(DevOp<float> op, Tc32Tiles mt, const TX* __restrict__ x, TX* __restrict__ y, int64_t ld,
                       int nrhs) {
     using L = Tc32Tile<S>;
     constexpr int D = S::D, NBF = S::NBF, Q = S::Q, BS = S::BS, DD = S::DD, NF = S::NF;
@@ -256,8 +258,8 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
          work += static_cast<int64_t>(gridDim.x) * L::NGRP) {
         const int tile = static_cast<int>(work % mt.ntiles);
         const int rhs = static_cast<int>(work / mt.ntiles);
-        const float* xr = x + rhs * ld;
-        float* yr = y + rhs * ld;
+        const TX* xr = x + rhs * ld;
+        TX* yr = y + rhs * ld;
         const int4 td = mt.tiles[tile];
         const int cnt = td.y, sig = td.z;
         group_sync<GT>(grp);
@@ -268,7 +270,8 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
             const int c = i / L::KP, k = i % L::KP;
             const int te = c / Q, r = c % Q;
             float v = 0.0f;
-            if (k < NBF && c < L::NC && s_el[te] >= 0) v = xr[static_cast<int64_t>(s_el[te]) * BS + k + NBF * r];
+            if (k < NBF && c < L::NC && s_el[te] >= 0)
+                v = static_cast<float>(xr[static_cast<int64_t>(s_el[te]) * BS + k + NBF * r]);
             sU[c * LDU + k] = v;
         }
         group_sync<GT>(grp);
@@ -363,7 +366,8 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
                 const int c = i / L::KP, k = i % L::KP;
                 const int te = c / Q, r = c % Q;
                 float v = 0.0f;
-                if (k < NBF && c < L::NC && s_nb[te] >= 0) v = xr[static_cast<int64_t>(s_nb[te]) * BS + k + NBF * r];
+                if (k < NBF && c < L::NC && s_nb[te] >= 0)
+                    v = static_cast<float>(xr[static_cast<int64_t>(s_nb[te]) * BS + k + NBF * r]);
                 sUN[c * LDU + k] = v;
             }
             group_sync<GT>(grp);
@@ -580,7 +584,7 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
             float v = 0.0f;
 #pragma unroll
             for (int kp = 0; kp < L::KSP; ++kp) v += R0[kp * L::NP * L::MY + c * L::MY + k];
-            yr[static_cast<int64_t>(el) * BS + k + NBF * r] = v;
+            yr[static_cast<int64_t>(el) * BS + k + NBF * r] = static_cast<TX>(v);
         }
     }
 }

@@ -27,7 +27,9 @@ int launch_apply_mma(int D, int N, int kind, DevOp<double> const& op, MmaTiles c
 // FP32 apply on the tensor cores in the 3xTF32 form (apply_tc32.cuh); TDG_E_INVALID when the
 // shape's shared-memory layout does not fit (the caller then uses the SIMT kernel).
 struct Tc32Tiles;
-int launch_apply_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const float* x, float* y,
+// TX = float (FP32 vectors) or double (FP64 vectors, FP32 operator arithmetic).
+template <typename TX>
+int launch_apply_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y,
                       int nrhs, int64_t ld, cudaStream_t s, int ctas = 0);
 int launch_bjac_assemble(int D, int N, int kind, DevOp<double> const& op, double* blk,
                          cudaStream_t s);

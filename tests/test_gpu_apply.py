@@ -196,3 +196,38 @@ def test_segmented_solve_of_a_mesh_union(precision):
     for i in range(len(meshes)):
         sl = slice(eoff[i] * bs, eoff[i + 1] * bs)
         assert np.linalg.norm(r[sl]) / np.linalg.norm(b[sl]) <= 1.5e-10
+
+
+@pytest.mark.parametrize("case", CASES[::3], ids=lambda c: "k{}d{}n{}p{}c{}v{}".format(*c))
+def test_apply_mixed_fp64_vectors(case):
+    """TDG_MIXED: FP32 tensor-core arithmetic on FP64 vectors agrees with the oracle to FP32
+    accuracy (2e-5 relative, as the FP32 apply) and with the FP32-vector apply of the same rounded
+    input to 1e-6 (same kernel, only the vector type differs)."""
+    from tandem_b200.operator import MIXED
+    kind, dim, n, N, curved, var = case
+    _, op, orc = product_and_oracle(kind, dim, n, N, curved, var)
+    x = np.random.default_rng(9).standard_normal(op.ndof)
+    xr = x.astype(np.float32).astype(np.float64)
+    y = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+    op.apply(dev(xr), y, precision=MIXED)
+    y32 = torch.zeros(op.ndof, dtype=torch.float32, device=DEV)
+    op.apply(dev(xr, torch.float32), y32, precision=FP32)
+    torch.cuda.synchronize()
+    ref = orc.apply(xr)
+    got = y.cpu().numpy()
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-5
+    assert np.linalg.norm(got - y32.double().cpu().numpy()) / np.linalg.norm(ref) < 1e-6
+
+
+@pytest.mark.parametrize("kind,dim,n,curved", [(POISSON, 2, 8, False), (ELASTICITY, 3, 2, True)])
+def test_mixed_solve_reaches_fp64_target(kind, dim, n, curved):
+    from tandem_b200.operator import MIXED
+    m, op, orc = product_and_oracle(kind, dim, n, 4, curved, True)
+    sc, c0, c1, f, g = mms_inputs(op, kind, dim, True)
+    b = op.rhs(f, g)
+    op.bjacobi_setup(MIXED)
+    x = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+    st = op.solve(dev(b), x, precision=MIXED, rtol=1e-10)
+    assert st["converged"] and st["rel_residual"] <= 1e-10, st
+    xs = x.cpu().numpy()
+    assert np.linalg.norm(b - orc.apply(xs)) / np.linalg.norm(b) <= 1.5e-10
