@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from . import _ffi
-from .operator import FP64, DGOperator, _check_vec, _stream
+from .operator import FP32, FP64, DGOperator, _check_vec, _stream
 
 
 class LameProblem:

@@ -175,7 +175,7 @@ int upload_mma(tdg_op* op, DevArena& arena) {
     }
     std::vector<int> perm;
     std::vector<int4> tiles;
-    signature_tiles(h, mma_tile_elements(h.Q), perm, tiles);
+    signature_tiles(h, mma_tile_elements(h.D, h.N, h.Q), perm, tiles);
     TDG_CUDA_TRY(arena.upload(&op->mma.tables, tab));
     TDG_CUDA_TRY(arena.upload(&op->mma.perm, perm));
     TDG_CUDA_TRY(arena.upload(&op->mma.tiles, tiles));

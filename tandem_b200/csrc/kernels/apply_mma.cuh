@@ -19,7 +19,9 @@
 // number; elements are grouped into tiles with one neighbour-face signature, so every GEMM of a
 // tile uses a single table (host side: build_tiles in capi.cu).  Y lives in mma accumulator
 // fragments; nothing is accumulated through memory, there are no atomics, and each output block
-// is written once.
+// is written once.  Where the tables leave room (mma_pipelines), a CTA runs two independent tile
+// pipelines with their own buffers and named barriers over the shared tables, so one pipeline's
+// global-memory waits overlap the other's tensor work.
 //
 // Shared-memory leading dimensions are congruent to 4 or 12 mod 16 doubles, which makes the
 // 8x4 / 4x8 fragment loads of a half warp hit 16 distinct 8-byte bank pairs.
@@ -34,13 +36,20 @@ namespace tdg {
 __host__ __device__ constexpr int mma_ld(int n) {
     return (n % 16 <= 4) ? (n - n % 16 + 4) : ((n % 16 <= 12) ? (n - n % 16 + 12) : (n - n % 16 + 20));
 }
-__host__ __device__ constexpr int mma_tile_elements(int Q) { return (24 + Q - 1) / Q; }
+// Elements per tile: 24 columns; 12 for 3D elasticity of degree 4, whose tables leave room for
+// two tile pipelines only with the narrower tile.
+__host__ __device__ constexpr int mma_tile_elements(int D, int N, int Q) {
+    return (D == 3 && Q == 3 && N == 4) ? 4 : (24 + Q - 1) / Q;
+}
+__host__ __device__ constexpr int mma_pipelines(int D, int N, int Q) { return (D == 3 && Q == 3 && N == 4) ? 2 : 1; }
 
 // Layout parameters shared by the host (table packing, tiling) and the kernel.
 template <class S>
 struct MmaTile {
     static constexpr int NT = 256, NW = 8;
-    static constexpr int TE = mma_tile_elements(S::Q);             // elements per tile
+    static constexpr int NGRP = mma_pipelines(S::D, S::N, S::Q);   // tile pipelines per CTA
+    static constexpr int GW = NW / NGRP, GT = 32 * GW;             // warps / threads per pipeline
+    static constexpr int TE = mma_tile_elements(S::D, S::N, S::Q); // elements per tile
     static constexpr int NC = TE * S::Q;                           // used columns
     static constexpr int NP = (NC + 7) / 8 * 8;                    // padded columns
     static constexpr int NTN = NP / 8;                             // n-tiles
@@ -48,7 +57,7 @@ struct MmaTile {
     static constexpr int MY = (S::NBF + 7) / 8 * 8;                // padded Nbf (M of Y)
     static constexpr int MYT = MY / 8;                             // m-tiles of Y
     static constexpr int YT = MYT * NTN;                           // Y tiles
-    static constexpr int YPW = (YT + NW - 1) / NW;                 // Y tiles per warp
+    static constexpr int YPW = (YT + GW - 1) / GW;                 // Y tiles per warp
     // Y's A^T fragments read table columns up to MY - 1 >= KP: those extra columns fall into the
     // next table row (finite values) and only feed Y rows >= NBF, which are never written.
     static constexpr int LDT = mma_ld(KP);
@@ -60,7 +69,9 @@ __host__ __device__ inline int round8(int x) { return (x + 7) / 8 * 8; }
 
 struct MmaLayout {
     int MV, MF;           // padded rows of TV and of each TF
-    int off_TF, off_U, off_UN, off_R0, off_R1;  // offsets (doubles) in shared memory
+    int off_TF;           // tables: TV at 0, TF at off_TF (doubles)
+    int off_grp, grp;     // first pipeline buffer, doubles per pipeline
+    int off_U, off_UN, off_R0, off_R1;  // offsets inside a pipeline's buffers
     int total;            // doubles
 };
 
@@ -73,11 +84,13 @@ __host__ __device__ inline MmaLayout mma_layout(int Nq, int nq) {
     int rv = L::QC * S::D;
     int mr = l.MF > rv ? l.MF : rv;
     l.off_TF = l.MV * L::LDT;
-    l.off_U = l.off_TF + S::NF * l.MF * L::LDT;
+    l.off_grp = l.off_TF + S::NF * l.MF * L::LDT;
+    l.off_U = 0;
     l.off_UN = l.off_U + L::KP * L::LDN;
     l.off_R0 = l.off_UN + L::KP * L::LDN;
     l.off_R1 = l.off_R0 + mr * L::LDN;
-    l.total = l.off_R1 + l.MF * L::LDN;
+    l.grp = l.off_R1 + l.MF * L::LDN;
+    l.total = l.off_grp + L::NGRP * l.grp;
     return l;
 }
 
@@ -104,7 +117,7 @@ __device__ __forceinline__ void cta_gemm_store(const double* A, const double* B,
                                                int warp, int lane) {
     const int g = lane >> 2, t = lane & 3;
     const int ntiles = (mrows / 8) * L::NTN;
-    for (int t0 = warp; t0 < ntiles; t0 += 4 * L::NW) {
+    for (int t0 = warp; t0 < ntiles; t0 += 4 * L::GW) {
         double acc[4][2];
         const double* ap[4];
         const double* bp[4];
@@ -112,7 +125,7 @@ __device__ __forceinline__ void cta_gemm_store(const double* A, const double* B,
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             acc[j][0] = acc[j][1] = 0.0;
-            const int tile = t0 + j * L::NW;
+            const int tile = t0 + j * L::GW;
             const int tt = tile < ntiles ? tile : t0;
             const int mt = tt / L::NTN, nt = tt % L::NTN;
             ap[j] = A + (mt * 8 + g) * L::LDT + t;
@@ -127,7 +140,7 @@ __device__ __forceinline__ void cta_gemm_store(const double* A, const double* B,
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             if (j < cnt) {
-                const int tile = t0 + j * L::NW;
+                const int tile = t0 + j * L::GW;
                 const int mt = tile / L::NTN, nt = tile % L::NTN;
                 double* c = C + (mt * 8 + g) * L::LDN + nt * 8 + 2 * t;
                 c[0] = acc[j][0];
@@ -146,7 +159,7 @@ __device__ __forceinline__ void cta_gemm_store2(const double* A0, const double* 
     const int g = lane >> 2, t = lane & 3;
     const int per = (mrows / 8) * L::NTN;
     const int ntiles = 2 * per;
-    for (int t0 = warp; t0 < ntiles; t0 += 4 * L::NW) {
+    for (int t0 = warp; t0 < ntiles; t0 += 4 * L::GW) {
         double acc[4][2];
         const double* ap[4];
         const double* bp[4];
@@ -154,7 +167,7 @@ __device__ __forceinline__ void cta_gemm_store2(const double* A0, const double* 
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             acc[j][0] = acc[j][1] = 0.0;
-            const int tile = t0 + j * L::NW;
+            const int tile = t0 + j * L::GW;
             const int tt = tile < ntiles ? tile : t0;
             const int which = tt / per, loc = tt % per;
             const int mt = loc / L::NTN, nt = loc % L::NTN;
@@ -170,7 +183,7 @@ __device__ __forceinline__ void cta_gemm_store2(const double* A0, const double* 
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             if (j < cnt) {
-                const int tile = t0 + j * L::NW;
+                const int tile = t0 + j * L::GW;
                 const int which = tile / per, loc = tile % per;
                 const int mt = loc / L::NTN, nt = loc % L::NTN;
                 double* c = (which ? C1 : C0) + (mt * 8 + g) * L::LDN + nt * 8 + 2 * t;
@@ -182,7 +195,7 @@ __device__ __forceinline__ void cta_gemm_store2(const double* A0, const double* 
 }
 
 // Y[MY x NP] += A^T B where A is [K x LDT] (rows = reduction index, columns = Y rows) and B is
-// [K x LDN].  Warp w owns Y tiles w, w + NW, ...; each tile keeps two partial accumulators (even
+// [K x LDN].  Warp w of the pipeline owns Y tiles w, w + GW, ...; each tile keeps two partial accumulators (even
 // and odd k-steps) and the tiles advance together, so consecutive mma never share an accumulator.
 template <class L>
 __device__ __forceinline__ void cta_gemm_acc_t(const double* A, const double* B, double (&y)[L::YPW][2][2], int krows,
@@ -193,7 +206,7 @@ __device__ __forceinline__ void cta_gemm_acc_t(const double* A, const double* B,
     bool on[L::YPW];
 #pragma unroll
     for (int j = 0; j < L::YPW; ++j) {
-        const int tile = warp + j * L::NW;
+        const int tile = warp + j * L::GW;
         on[j] = tile < L::YT;
         const int tt = on[j] ? tile : 0;
         const int ym = tt % L::MYT, yn = tt / L::MYT;
@@ -216,50 +229,62 @@ __device__ __forceinline__ void cta_gemm_acc_t(const double* A, const double* B,
     }
 }
 
+// Barrier over the GT threads of tile pipeline `grp` (named barrier 1 + grp; 0 is __syncthreads).
+template <int GT>
+__device__ __forceinline__ void mma_group_sync(int grp) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(GT) : "memory");
+}
+
 template <class S>
 __global__ void __launch_bounds__(MmaTile<S>::NT, (S::D == 2) ? 2 : 1)
     apply_mma_kernel(DevOp<double> op, MmaTiles mt, const double* __restrict__ x, double* __restrict__ y, int64_t ld,
                      int nrhs) {
     using L = MmaTile<S>;
     constexpr int D = S::D, NBF = S::NBF, Q = S::Q, BS = S::BS, DD = S::DD, NF = S::NF;
-    constexpr int TE = L::TE, NT = L::NT, LDN = L::LDN, LDT = L::LDT;
+    constexpr int TE = L::TE, GT = L::GT, LDN = L::LDN, LDT = L::LDT;
     const int Nq = op.Nq, nq = op.nq;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int grp = warp / L::GW, gw = warp % L::GW, gtid = tid - grp * GT;
     const MmaLayout lay = mma_layout<S>(Nq, nq);
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sm = reinterpret_cast<double*>(smem_raw);
     double* TV = sm;
     double* TF = sm + lay.off_TF;
-    double* sU = sm + lay.off_U;
-    double* sUN = sm + lay.off_UN;
-    double* R0 = sm + lay.off_R0;
-    double* R1 = sm + lay.off_R1;
-    __shared__ int s_el[TE];
-    __shared__ int s_nb[TE];
+    double* gbuf = sm + lay.off_grp + grp * lay.grp;
+    double* sU = gbuf + lay.off_U;
+    double* sUN = gbuf + lay.off_UN;
+    double* R0 = gbuf + lay.off_R0;
+    double* R1 = gbuf + lay.off_R1;
+    __shared__ int s_el_all[L::NGRP][TE];
+    __shared__ int s_nb_all[L::NGRP][TE];
+    int* s_el = s_el_all[grp];
+    int* s_nb = s_nb_all[grp];
 
-    for (int i = tid; i < mt.table_doubles; i += NT) sm[i] = mt.tables[i];
+    for (int i = tid; i < mt.table_doubles; i += L::NT) sm[i] = mt.tables[i];
+    __syncthreads();
 
     const int64_t nwork = static_cast<int64_t>(mt.ntiles) * nrhs;
-    for (int64_t work = blockIdx.x; work < nwork; work += gridDim.x) {
+    for (int64_t work = static_cast<int64_t>(blockIdx.x) * L::NGRP + grp; work < nwork;
+         work += static_cast<int64_t>(gridDim.x) * L::NGRP) {
         const int tile = static_cast<int>(work % mt.ntiles);
         const int rhs = static_cast<int>(work / mt.ntiles);
         const double* xr = x + rhs * ld;
         double* yr = y + rhs * ld;
         const int4 td = mt.tiles[tile];
         const int cnt = td.y, sig = td.z;
-        __syncthreads();
-        if (tid < TE) s_el[tid] = (tid < cnt) ? mt.perm[td.x + tid] : -1;
-        __syncthreads();
+        mma_group_sync<GT>(grp);
+        if (gtid < TE) s_el[gtid] = (gtid < cnt) ? mt.perm[td.x + gtid] : -1;
+        mma_group_sync<GT>(grp);
         // U[k][te * Q + r]; padding rows / columns zero
-        for (int i = tid; i < L::KP * L::NP; i += NT) {
+        for (int i = gtid; i < L::KP * L::NP; i += GT) {
             const int k = i / L::NP, c = i % L::NP;
             const int te = c / Q, r = c % Q;
             double v = 0.0;
             if (k < NBF && c < L::NC && s_el[te] >= 0) v = xr[static_cast<int64_t>(s_el[te]) * BS + k + NBF * r];
             sU[k * LDN + c] = v;
         }
-        __syncthreads();
+        mma_group_sync<GT>(grp);
 
         double yacc[L::YPW][2][2];
 #pragma unroll
@@ -269,9 +294,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, (S::D == 2) ? 2 : 1)
         for (int q0 = 0; q0 < Nq; q0 += L::QC) {
             const int nqc = (Nq - q0 < L::QC) ? (Nq - q0) : L::QC;
             const int rows = round8(nqc * D);
-            cta_gemm_store<L>(TV + q0 * D * LDT, sU, R0, rows, L::KP / 4, warp, lane);
-            __syncthreads();
-            for (int it = tid; it < TE * nqc; it += NT) {
+            cta_gemm_store<L>(TV + q0 * D * LDT, sU, R0, rows, L::KP / 4, gw, lane);
+            mma_group_sync<GT>(grp);
+            for (int it = gtid; it < TE * nqc; it += GT) {
                 const int te = it % TE, qq = it / TE;
                 const int el = s_el[te];
                 if (el < 0) continue;
@@ -334,29 +359,29 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, (S::D == 2) ? 2 : 1)
                         for (int uu = 0; uu < D; ++uu) rr[a * LDN + uu] = T[a][uu];
                 }
             }
-            __syncthreads();
-            cta_gemm_acc_t<L>(TV + q0 * D * LDT, R0, yacc, rows, warp, lane);
-            __syncthreads();
+            mma_group_sync<GT>(grp);
+            cta_gemm_acc_t<L>(TV + q0 * D * LDT, R0, yacc, rows, gw, lane);
+            mma_group_sync<GT>(grp);
         }
 
         // ---------------- facets ----------------
 #pragma unroll 1
         for (int f = 0; f < NF; ++f) {
             const int lp = (sig >> (2 * f)) & 3;
-            if (tid < TE) s_nb[tid] = (s_el[tid] >= 0) ? op.sides[static_cast<int64_t>(s_el[tid]) * NF + f].z : -1;
-            __syncthreads();
-            for (int i = tid; i < L::KP * L::NP; i += NT) {
+            if (gtid < TE) s_nb[gtid] = (s_el[gtid] >= 0) ? op.sides[static_cast<int64_t>(s_el[gtid]) * NF + f].z : -1;
+            mma_group_sync<GT>(grp);
+            for (int i = gtid; i < L::KP * L::NP; i += GT) {
                 const int k = i / L::NP, c = i % L::NP;
                 const int te = c / Q, r = c % Q;
                 double v = 0.0;
                 if (k < NBF && c < L::NC && s_nb[te] >= 0) v = xr[static_cast<int64_t>(s_nb[te]) * BS + k + NBF * r];
                 sUN[k * LDN + c] = v;
             }
-            __syncthreads();
-            cta_gemm_store2<L>(TF + f * lay.MF * LDT, sU, R0, TF + lp * lay.MF * LDT, sUN, R1, lay.MF, L::KP / 4, warp,
+            mma_group_sync<GT>(grp);
+            cta_gemm_store2<L>(TF + f * lay.MF * LDT, sU, R0, TF + lp * lay.MF * LDT, sUN, R1, lay.MF, L::KP / 4, gw,
                                lane);
-            __syncthreads();
-            for (int it = tid; it < TE * nq; it += NT) {
+            mma_group_sync<GT>(grp);
+            for (int it = gtid; it < TE * nq; it += GT) {
                 const int te = it % TE, q = it / TE;
                 const int el = s_el[te];
                 if (el < 0) continue;
@@ -530,9 +555,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, (S::D == 2) ? 2 : 1)
                     }
                 }
             }
-            __syncthreads();
-            cta_gemm_acc_t<L>(TF + f * lay.MF * LDT, R0, yacc, lay.MF, warp, lane);
-            __syncthreads();
+            mma_group_sync<GT>(grp);
+            cta_gemm_acc_t<L>(TF + f * lay.MF * LDT, R0, yacc, lay.MF, gw, lane);
+            mma_group_sync<GT>(grp);
         }
 
         // ---------------- write the output tile ----------------
@@ -540,7 +565,7 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, (S::D == 2) ? 2 : 1)
             const int g = lane >> 2, t = lane & 3;
 #pragma unroll
             for (int j = 0; j < L::YPW; ++j) {
-                const int tl = warp + j * L::NW;
+                const int tl = gw + j * L::GW;
                 if (tl < L::YT) {
                     const int ym = tl % L::MYT, yn = tl / L::MYT;
                     const int k = ym * 8 + g;

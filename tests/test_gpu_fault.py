@@ -86,3 +86,43 @@ def test_greens_function_mixed_precision():
     assert all(s["converged"] for s in stats)
     err = (torch.norm(G32 - G64) / torch.norm(G64)).item()
     assert err < 1e-8, err
+
+
+def test_greens_operator_resume_and_traction_update(tmp_path):
+    """G computed in two sessions through a checkpoint (the second one with the fault facets in
+    reverse order) equals G computed in one; update_traction(s, t) = G s + t t_boundary equals the
+    traction of the solve with slip s and the boundary data scaled by t."""
+    from tandem_b200.greens import DiscreteGreensOperator
+    m, op, orc, facets = fault_case(nf=4)
+    op.bjacobi_setup(FP64)
+    fl = Fault(op, facets, REF_NORMAL)
+    full = DiscreteGreensOperator(op, fl)
+    full.compute(rtol=1e-12, batch=8)
+    ck = str(tmp_path / "gf.npz")
+    part = DiscreteGreensOperator(op, fl)
+    part.compute(rtol=1e-12, batch=8, checkpoint=ck, max_batches=1)
+    assert 0 < part.current < part.n
+    rev = Fault(op, facets[::-1].copy(), REF_NORMAL)
+    resumed = DiscreteGreensOperator(op, rev)
+    assert resumed.load(ck) == part.current
+    resumed.compute(rtol=1e-12, batch=8)
+    nbf = fl.nbf
+    perm = np.arange(fl.nfault)[::-1]
+    idx = torch.as_tensor((perm[:, None] * nbf + np.arange(nbf)[None, :]).ravel(), device="cuda")
+    Gr = resumed.G[idx][:, idx]
+    assert torch.max(torch.abs(Gr - full.G)).item() <= 1e-10 * torch.max(torch.abs(full.G)).item()
+
+    # traction update vs a direct solve
+    Xf = op.facet_coords()
+    g = np.ascontiguousarray((0.1 * np.cos(Xf[..., 0]) + 0.05 * Xf[..., 1])[:, None, :])
+    full.compute_boundary_traction(None, g, rtol=1e-12)
+    s = torch.as_tensor(np.random.default_rng(5).standard_normal(fl.ncoef), device="cuda")
+    t = 0.7
+    b = torch.as_tensor(t * op.rhs(None, g), device="cuda")
+    fl.slip_rhs(s, b)
+    x = torch.zeros_like(b)
+    op.solve(b, x, rtol=1e-12)
+    direct = torch.empty(fl.ncoef, dtype=torch.float64, device="cuda")
+    fl.traction(x, s, direct)
+    upd = full.update_traction(s, t)
+    assert torch.max(torch.abs(upd - direct)).item() <= 1e-8 * torch.max(torch.abs(direct)).item()
