@@ -24,6 +24,12 @@ struct MmaTiles;
 int launch_apply_mma(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, const double* x, double* y,
                      int nrhs, int64_t ld, cudaStream_t s, int ctas = 0);
 
+// Face-centric FP64 apply (apply_face.cuh): volume kernel (y = volume term) then facet kernel
+// (y += facet terms, each facet once for both sides).
+struct FaceTiles;
+int launch_apply_face(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft,
+                      const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas = 0);
+
 // FP32 apply on the tensor cores in the 3xTF32 form (apply_tc32.cuh); TDG_E_INVALID when the
 // shape's shared-memory layout does not fit (the caller then uses the SIMT kernel).
 struct Tc32Tiles;

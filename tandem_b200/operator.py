@@ -19,6 +19,7 @@ from .mesh import SimplexMesh
 
 POISSON, ELASTICITY = _ffi.TDG_POISSON, _ffi.TDG_ELASTICITY
 FP64, FP32, MIXED = _ffi.TDG_FP64, _ffi.TDG_FP32, _ffi.TDG_MIXED
+FAMILIES = ("tensor", "simt", "face")
 
 
 def _c(a: np.ndarray, dtype) -> np.ndarray:
@@ -139,8 +140,12 @@ class DGOperator:
         entries = (_ffi.TuneEntry * 16)()
         n = C.c_int(0)
         _ffi.check(_ffi.lib().tdg_autotune(self._h, precision, nrhs, _stream(stream), entries, 16, C.byref(n)))
-        return [dict(family=("tensor" if e.family == 0 else "simt"), ctas_per_sm=e.ctas_per_sm, ms=e.ms)
-                for e in entries[:n.value]]
+        return [dict(family=FAMILIES[e.family], ctas_per_sm=e.ctas_per_sm, ms=e.ms) for e in entries[:n.value]]
+
+    def set_apply_config(self, precision: int, family: str, ctas_per_sm: int = 0) -> None:
+        """Selects the apply kernel explicitly: family "tensor" (element-centric tensor cores),
+        "face" (face-centric, FP64) or "simt"; ctas_per_sm 0 = the default occupancy."""
+        _ffi.check(_ffi.lib().tdg_set_apply_config(self._h, precision, FAMILIES.index(family), ctas_per_sm))
 
     def flops_apply(self) -> int:
         return int(_ffi.lib().tdg_flops_apply(self._h))
