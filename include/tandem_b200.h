@@ -147,13 +147,13 @@ int tdg_bjacobi_blocks(tdg_op* op, double* out);
 
 typedef struct {
     int family;       /* 0 = element-centric tensor-core kernel, 1 = SIMT kernel, 2 = face-centric
-                         tensor-core kernels (FP64: volume kernel + one pass over the facets) */
+                         tensor-core kernels (volume kernel + one pass over the facets) */
     int ctas_per_sm;  /* persistent CTAs per SM requested (0 = default) */
     double ms;        /* measured time of one apply */
 } tdg_tune_entry;
 
 /* Times the apply of this operator (its own mesh, `nrhs` right-hand sides, `precision`) for each
- * candidate launch configuration -- the tensor-core kernels (element-centric, and for FP64 the
+ * candidate launch configuration -- the tensor-core kernels (element-centric, and the
  * face-centric pair) at 1 to 4 persistent CTAs per SM (clipped to the occupancy limit of the
  * shape's tile) and the SIMT kernel -- with CUDA events on
  * `stream`, and keeps the fastest for later tdg_apply / tdg_solve calls of that precision.
@@ -161,7 +161,7 @@ typedef struct {
 int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_entry* entries, int max_entries,
                  int* n_entries);
 /* Sets the apply configuration of `precision` (TDG_FP64 / TDG_FP32; TDG_MIXED follows TDG_FP32)
- * explicitly: kernel family as in tdg_tune_entry (2 is FP64 only) and persistent CTAs per SM. */
+ * explicitly: kernel family as in tdg_tune_entry and persistent CTAs per SM. */
 int tdg_set_apply_config(tdg_op* op, int precision, int family, int ctas_per_sm);
 
 /* --- right-hand side (DGOperator::rhs, src/form/DGOperator.h:189-237) ---------------------- */

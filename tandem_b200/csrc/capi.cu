@@ -5,6 +5,7 @@
 #include "kernels/apply_mma.cuh"
 #include "kernels/apply_tc32.cuh"
 #include "kernels/apply_face.cuh"
+#include "kernels/apply_face_tc32.cuh"
 #include "kernels/dispatch.hpp"
 #include "kernels/krylov.cuh"
 
@@ -118,6 +119,7 @@ struct tdg_op {
     MmaTiles mma;           // FP64 tensor-pipe apply: packed tables and signature tiles
     Tc32Tiles tc32;         // FP32 tensor-core apply (3xTF32): packed tables and signature tiles
     FaceTiles face;         // face-centric FP64 apply: facet tiles grouped by (l0, l1, mode)
+    FaceTiles face32;       // face-centric FP32 apply: the same grouping with the FP32 tile size
     bool use_mma = true;
     // per precision (0 = FP64, 1 = FP32): kernel family (0 tensor cores, 1 SIMT) and persistent CTAs
     // per SM (0 = default); set by tdg_autotune
@@ -156,6 +158,44 @@ int upload_common(tdg_op* op) {
 // Tiles group elements by their neighbour-face signature (nb_local per face, 2 bits each).
 void signature_tiles(HostOperator const& h, int TE, std::vector<int>& perm, std::vector<int4>& tiles);
 
+// Face-centric apply: every facet with a flux once, grouped by (l0, l1, mode) -- mode 1 interior
+// (both sides), 2 boundary Dirichlet / fault (side 0), 3 boundary with code None (side 0, the
+// element as its own neighbour, as the element-centric apply treats it) -- and cut into tiles of
+// at most TE facets with one key.  finfo[f] = {up0, up1, l0 | l1 << 8, mode}.
+void facet_tiles(HostOperator const& h, int TE, std::vector<int4>& finfo, std::vector<int>& fids,
+                 std::vector<int4>& ftiles) {
+    finfo.assign(static_cast<size_t>(h.F), make_int4(0, 0, 0, 0));
+    std::vector<int> fkey(static_cast<size_t>(h.F), 0);
+    fids.clear();
+    for (int64_t f = 0; f < h.F; ++f) {
+        int64_t up0 = h.up[2 * f], up1 = h.up[2 * f + 1];
+        int l0 = h.loc[2 * f], l1 = h.loc[2 * f + 1];
+        const int bc = h.bc[f];
+        const bool interior = up0 != up1;
+        int mode;
+        if (interior) {
+            mode = (bc == 0 || bc == 3 || bc == 5) ? 1 : 0;
+        } else {
+            mode = (bc == 3 || bc == 5) ? 2 : (bc == 0 ? 3 : 0);
+            up1 = up0;
+            l1 = l0;
+        }
+        finfo[f] = make_int4(static_cast<int>(up0), static_cast<int>(up1), l0 | (l1 << 8), mode);
+        if (mode) {
+            fkey[f] = l0 | (l1 << 2) | (mode << 4);
+            fids.push_back(static_cast<int>(f));
+        }
+    }
+    std::stable_sort(fids.begin(), fids.end(), [&](int a, int b) { return fkey[a] < fkey[b]; });
+    ftiles.clear();
+    for (size_t i = 0; i < fids.size();) {
+        size_t j = i;
+        while (j < fids.size() && static_cast<int>(j - i) < TE && fkey[fids[j]] == fkey[fids[i]]) ++j;
+        ftiles.push_back(make_int4(static_cast<int>(i), static_cast<int>(j - i), fkey[fids[i]], 0));
+        i = j;
+    }
+}
+
 int upload_mma(tdg_op* op, DevArena& arena) {
     auto const& h = op->h;
     const int D = h.D, NBF = h.Nbf, Nq = h.Nq, nq = h.nq, NF = h.nfaces;
@@ -184,39 +224,9 @@ int upload_mma(tdg_op* op, DevArena& arena) {
     op->mma.ntiles = static_cast<int>(tiles.size());
     op->mma.table_doubles = static_cast<int>(tab.size());
 
-    // face-centric apply: every facet with a flux once, grouped by (l0, l1, mode) -- mode 1
-    // interior (both sides), 2 boundary Dirichlet / fault (side 0), 3 boundary with code None
-    // (side 0, the element as its own neighbour, as the element-centric apply treats it)
-    const int TE = mma_tile_elements(D, h.N, h.Q);
-    std::vector<int4> finfo(static_cast<size_t>(h.F));
-    std::vector<int> fids, fkey(static_cast<size_t>(h.F), 0);
-    for (int64_t f = 0; f < h.F; ++f) {
-        int64_t up0 = h.up[2 * f], up1 = h.up[2 * f + 1];
-        int l0 = h.loc[2 * f], l1 = h.loc[2 * f + 1];
-        const int bc = h.bc[f];
-        const bool interior = up0 != up1;
-        int mode;
-        if (interior) {
-            mode = (bc == 0 || bc == 3 || bc == 5) ? 1 : 0;
-        } else {
-            mode = (bc == 3 || bc == 5) ? 2 : (bc == 0 ? 3 : 0);
-            up1 = up0;
-            l1 = l0;
-        }
-        finfo[f] = make_int4(static_cast<int>(up0), static_cast<int>(up1), l0 | (l1 << 8), mode);
-        if (mode) {
-            fkey[f] = l0 | (l1 << 2) | (mode << 4);
-            fids.push_back(static_cast<int>(f));
-        }
-    }
-    std::stable_sort(fids.begin(), fids.end(), [&](int a, int b) { return fkey[a] < fkey[b]; });
-    std::vector<int4> ftiles;
-    for (size_t i = 0; i < fids.size();) {
-        size_t j = i;
-        while (j < fids.size() && static_cast<int>(j - i) < TE && fkey[fids[j]] == fkey[fids[i]]) ++j;
-        ftiles.push_back(make_int4(static_cast<int>(i), static_cast<int>(j - i), fkey[fids[i]], 0));
-        i = j;
-    }
+    std::vector<int4> finfo, ftiles;
+    std::vector<int> fids;
+    facet_tiles(h, mma_tile_elements(D, h.N, h.Q), finfo, fids, ftiles);
     if (!fids.empty()) {
         TDG_CUDA_TRY(arena.upload(&op->face.fperm, fids));
         TDG_CUDA_TRY(arena.upload(&op->face.ftiles, ftiles));
@@ -280,6 +290,17 @@ int upload_tc32(tdg_op* op, DevArena& arena) {
     TDG_CUDA_TRY(arena.upload(&op->tc32.tiles, tiles));
     op->tc32.ntiles = static_cast<int>(tiles.size());
     op->tc32.table_floats = static_cast<int>(tab.size());
+    {
+        std::vector<int4> finfo, ftiles;
+        std::vector<int> fids;
+        facet_tiles(h, tc32_tile_elements(D, h.Q), finfo, fids, ftiles);
+        if (!fids.empty()) {
+            TDG_CUDA_TRY(arena.upload(&op->face32.fperm, fids));
+            TDG_CUDA_TRY(arena.upload(&op->face32.ftiles, ftiles));
+        }
+        TDG_CUDA_TRY(arena.upload(&op->face32.finfo, finfo));
+        op->face32.nftiles = static_cast<int>(ftiles.size());
+    }
     return 0;
 }
 
@@ -525,13 +546,23 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
     if (precision == TDG_FP64 && rc == TDG_E_INVALID)
         rc = launch_apply<double>(h.D, h.N, h.kind, op->op64, static_cast<const double*>(x),
                                   static_cast<double*>(y), nrhs, ld, s);
-    if (precision == TDG_FP32 && tensor)
+    const bool face32 = op->use_mma && op->family[1] == 2;
+    if (precision == TDG_FP32 && face32)
+        rc = launch_apply_face_tc32<float>(h.D, h.N, h.kind, op->op32, op->tc32, op->face32,
+                                           static_cast<const float*>(x), static_cast<float*>(y), nrhs, ld, s,
+                                           op->ctas[1]);
+    else if (precision == TDG_FP32 && tensor)
         rc = launch_apply_tc32<float>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const float*>(x),
                                       static_cast<float*>(y), nrhs, ld, s, op->ctas[1]);
     if (precision == TDG_MIXED) {
         if (!op->use_mma) return fail(TDG_E_INVALID, "TDG_MIXED needs the tensor-core kernels");
-        rc = launch_apply_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const double*>(x),
-                                       static_cast<double*>(y), nrhs, ld, s, op->ctas[1]);
+        if (face32)
+            rc = launch_apply_face_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, op->face32,
+                                                static_cast<const double*>(x), static_cast<double*>(y), nrhs, ld, s,
+                                                op->ctas[1]);
+        else
+            rc = launch_apply_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const double*>(x),
+                                           static_cast<double*>(y), nrhs, ld, s, op->ctas[1]);
         if (rc) return fail(rc, std::string("mixed apply launch failed: ") + cudaGetErrorString(cudaGetLastError()));
         return 0;
     }
@@ -545,7 +576,6 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
 int tdg_set_apply_config(tdg_op* op, int precision, int family, int ctas_per_sm) {
     if (!op || (precision != TDG_FP64 && precision != TDG_FP32) || family < 0 || family > 2 || ctas_per_sm < 0)
         return fail(TDG_E_INVALID, "bad argument");
-    if (family == 2 && precision != TDG_FP64) return fail(TDG_E_INVALID, "the face-centric kernel is FP64 only");
     const int pi = precision == TDG_FP64 ? 0 : 1;
     op->family[pi] = family;
     op->ctas[pi] = ctas_per_sm;
@@ -577,7 +607,7 @@ int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_ent
     std::vector<Cand> cands;
     if (op->use_mma)
         for (int c = 1; c <= 4; ++c) cands.push_back({0, c});
-    if (op->use_mma && precision == TDG_FP64)
+    if (op->use_mma)
         for (int c = 1; c <= 4; ++c) cands.push_back({2, c});
     cands.push_back({1, 0});
     const int fam0 = op->family[pi], ct0 = op->ctas[pi];

@@ -40,120 +40,121 @@ struct FaceTiles {
 // normal (scaled / unit); u0, g0: own trace and reference gradients; u1, g1: the other side's
 // (zero for mode 2); G0 / G1: own / other J^-1; c0 / c1: own / other coefficients (Poisson K G
 // [DD]; elasticity lam, mu).
-template <class S>
-__device__ __forceinline__ void facet_lift(int mode, const double* n, const double* nu, double pen, double wq,
-                                           const double (&u0)[S::Q], const double (&g0)[S::D][S::Q],
-                                           const double (&u1)[S::Q], const double (&g1)[S::D][S::Q], const double* G0,
-                                           const double* G1, const double* c0, const double* c1,
-                                           double (&ga)[S::D][S::Q], double (&gb)[S::Q]) {
-    constexpr int D = S::D, DD = S::DD;
+// T: the arithmetic (double, or float for the FP32 kernels); the penalty times the jump is formed
+// in FP64 and rounded once.
+template <class S, typename T>
+__device__ __forceinline__ void facet_lift(int mode, const T* n, const T* nu, double pen, T wq, const T (&u0)[S::Q],
+                                           const T (&g0)[S::D][S::Q], const T (&u1)[S::Q],
+                                           const T (&g1)[S::D][S::Q], const T* G0, const T* G1, const T* c0,
+                                           const T* c1, T (&ga)[S::D][S::Q], T (&gb)[S::Q]) {
+    constexpr int D = S::D;
+    const T half = T(0.5);
     if constexpr (S::KIND == kPoisson) {
-        double uh, sg[D];
+        T uh, sg[D];
         if (mode != 2) {
-            uh = 0.5 * (u1[0] - u0[0]);
-            const double pj = pen * (u0[0] - u1[0]);
+            uh = half * (u1[0] - u0[0]);
+            const T pj = static_cast<T>(pen * (static_cast<double>(u0[0]) - static_cast<double>(u1[0])));
 #pragma unroll
             for (int p = 0; p < D; ++p) {
-                double s = 0.0;
+                T s = T(0);
 #pragma unroll
                 for (int a = 0; a < D; ++a) s += c0[a * D + p] * g0[a][0] + c1[a * D + p] * g1[a][0];
-                sg[p] = 0.5 * s - pj * nu[p];
+                sg[p] = half * s - pj * nu[p];
             }
         } else {
             uh = -u0[0];
-            const double pj = pen * u0[0];
+            const T pj = static_cast<T>(pen * static_cast<double>(u0[0]));
 #pragma unroll
             for (int p = 0; p < D; ++p) {
-                double s = 0.0;
+                T s = T(0);
 #pragma unroll
                 for (int a = 0; a < D; ++a) s += c0[a * D + p] * g0[a][0];
                 sg[p] = s - pj * nu[p];
             }
         }
-        double bsum = 0.0;
+        T bsum = T(0);
 #pragma unroll
         for (int r = 0; r < D; ++r) bsum += n[r] * sg[r];
         gb[0] = -wq * bsum;
 #pragma unroll
         for (int a = 0; a < D; ++a) {
-            double s = 0.0;
+            T s = T(0);
 #pragma unroll
             for (int r = 0; r < D; ++r) s += n[r] * c0[a * D + r];
             ga[a][0] = wq * uh * s;
         }
     } else {
-        (void)DD;
-        const double lam0 = c0[0], mu0 = c0[1], lam1 = c1[0], mu1 = c1[1];
-        double sg[D][D];
+        const T lam0 = c0[0], mu0 = c0[1], lam1 = c1[0], mu1 = c1[1];
+        T sg[D][D];
         {
-            double J0[D][D];
+            T J0[D][D];
 #pragma unroll
             for (int s = 0; s < D; ++s)
 #pragma unroll
                 for (int r = 0; r < D; ++r) {
-                    double acc0 = 0.0;
+                    T acc0 = T(0);
 #pragma unroll
                     for (int a = 0; a < D; ++a) acc0 += G0[a * D + s] * g0[a][r];
                     J0[s][r] = acc0;
                 }
-            double d0 = 0.0;
+            T d0 = T(0);
 #pragma unroll
             for (int r = 0; r < D; ++r) d0 += J0[r][r];
 #pragma unroll
             for (int i = 0; i < D; ++i)
 #pragma unroll
-                for (int j = 0; j < D; ++j) sg[i][j] = mu0 * (J0[i][j] + J0[j][i]) + ((i == j) ? lam0 * d0 : 0.0);
+                for (int j = 0; j < D; ++j) sg[i][j] = mu0 * (J0[i][j] + J0[j][i]) + ((i == j) ? lam0 * d0 : T(0));
         }
-        double uhm[D];
+        T uhm[D];
         if (mode != 2) {
-            double J1[D][D];
+            T J1[D][D];
 #pragma unroll
             for (int s = 0; s < D; ++s)
 #pragma unroll
                 for (int r = 0; r < D; ++r) {
-                    double acc1 = 0.0;
+                    T acc1 = T(0);
 #pragma unroll
                     for (int a = 0; a < D; ++a) acc1 += G1[a * D + s] * g1[a][r];
                     J1[s][r] = acc1;
                 }
-            double d1 = 0.0;
+            T d1 = T(0);
 #pragma unroll
             for (int r = 0; r < D; ++r) d1 += J1[r][r];
 #pragma unroll
             for (int i = 0; i < D; ++i) {
-                const double pj = pen * (u0[i] - u1[i]);
+                const T pj = static_cast<T>(pen * (static_cast<double>(u0[i]) - static_cast<double>(u1[i])));
 #pragma unroll
                 for (int j = 0; j < D; ++j) {
-                    const double s1 = mu1 * (J1[i][j] + J1[j][i]) + ((i == j) ? lam1 * d1 : 0.0);
-                    sg[i][j] = 0.5 * (sg[i][j] + s1) - pj * nu[j];
+                    const T s1 = mu1 * (J1[i][j] + J1[j][i]) + ((i == j) ? lam1 * d1 : T(0));
+                    sg[i][j] = half * (sg[i][j] + s1) - pj * nu[j];
                 }
-                uhm[i] = 0.5 * (u1[i] - u0[i]);
+                uhm[i] = half * (u1[i] - u0[i]);
             }
         } else {
 #pragma unroll
             for (int i = 0; i < D; ++i) {
-                const double pj = pen * u0[i];
+                const T pj = static_cast<T>(pen * static_cast<double>(u0[i]));
 #pragma unroll
                 for (int j = 0; j < D; ++j) sg[i][j] -= pj * nu[j];
                 uhm[i] = -u0[i];
             }
         }
-        double un = 0.0;
+        T un = T(0);
 #pragma unroll
         for (int r = 0; r < D; ++r) un += uhm[r] * n[r];
 #pragma unroll
         for (int uu = 0; uu < D; ++uu) {
-            double X[D];
+            T X[D];
 #pragma unroll
-            for (int j = 0; j < D; ++j) X[j] = mu0 * (uhm[uu] * n[j] + uhm[j] * n[uu]) + ((uu == j) ? lam0 * un : 0.0);
+            for (int j = 0; j < D; ++j) X[j] = mu0 * (uhm[uu] * n[j] + uhm[j] * n[uu]) + ((uu == j) ? lam0 * un : T(0));
 #pragma unroll
             for (int a = 0; a < D; ++a) {
-                double s = 0.0;
+                T s = T(0);
 #pragma unroll
                 for (int j = 0; j < D; ++j) s += G0[a * D + j] * X[j];
                 ga[a][uu] = wq * s;
             }
-            double bsum = 0.0;
+            T bsum = T(0);
 #pragma unroll
             for (int j = 0; j < D; ++j) bsum += n[j] * sg[uu][j];
             gb[uu] = -wq * bsum;
@@ -471,9 +472,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
                 // in registers, so the lift inputs can overwrite the traces right away
                 double ga[D][Q], gb[Q];
                 if (mode == 3)
-                    facet_lift<S>(1, n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs0, cs0, cs0, ga, gb);
+                    facet_lift<S, double>(1, n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs0, cs0, cs0, ga, gb);
                 else
-                    facet_lift<S>(mode, n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs1, cs0, cs1, ga, gb);
+                    facet_lift<S, double>(mode, n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs1, cs0, cs1, ga, gb);
 #pragma unroll
                 for (int r = 0; r < Q; ++r) {
                     gb0p[r] = gb[r];
@@ -483,7 +484,7 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
             }
             if (two) {
                 double ha[D][Q], hb[Q];
-                facet_lift<S>(1, mn, mnu, pen, wq, u1, g1, u0, g0, Gs1, Gs0, cs1, cs0, ha, hb);
+                facet_lift<S, double>(1, mn, mnu, pen, wq, u1, g1, u0, g0, Gs1, Gs0, cs1, cs0, ha, hb);
 #pragma unroll
                 for (int r = 0; r < Q; ++r) {
                     gb1p[r] = hb[r];

@@ -30,6 +30,12 @@ struct FaceTiles;
 int launch_apply_face(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft,
                       const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas = 0);
 
+// Face-centric FP32 apply (apply_face_tc32.cuh), TX = float or double vectors.
+struct Tc32Tiles;
+template <typename TX>
+int launch_apply_face_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, FaceTiles const& ft,
+                           const TX* x, TX* y, int nrhs, int64_t ld, cudaStream_t s, int ctas = 0);
+
 // FP32 apply on the tensor cores in the 3xTF32 form (apply_tc32.cuh); TDG_E_INVALID when the
 // shape's shared-memory layout does not fit (the caller then uses the SIMT kernel).
 struct Tc32Tiles;

@@ -261,3 +261,23 @@ def test_face_centric_multi_rhs_and_solve():
         scale = torch.max(torch.abs(y)).item()
         assert torch.max(torch.abs(y - Y[r, :op.ndof])).item() <= 1e-14 * scale
         assert torch.all(Y[r, op.ndof:] == 7.0)
+
+
+@pytest.mark.parametrize("case", CASES[::2], ids=lambda c: "k{}d{}n{}p{}c{}v{}".format(*c))
+def test_apply_face_centric_fp32_and_mixed(case):
+    """Face-centric FP32 kernels (3xTF32) on FP32 and on FP64 vectors (mixed) against the oracle to
+    FP32 accuracy (2e-5, as the element-centric FP32 apply)."""
+    from tandem_b200.operator import MIXED
+    kind, dim, n, N, curved, var = case
+    _, op, orc = product_and_oracle(kind, dim, n, N, curved, var)
+    op.set_apply_config(FP32, "face")
+    x = np.random.default_rng(12).standard_normal(op.ndof)
+    xr = x.astype(np.float32).astype(np.float64)
+    ref = orc.apply(xr)
+    y32 = torch.zeros(op.ndof, dtype=torch.float32, device=DEV)
+    op.apply(dev(xr, torch.float32), y32, precision=FP32)
+    ym = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+    op.apply(dev(xr), ym, precision=MIXED)
+    torch.cuda.synchronize()
+    for got in (y32.double().cpu().numpy(), ym.cpu().numpy()):
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-5
