@@ -215,6 +215,22 @@ int tdg_solve_segmented(tdg_op* op, const double* b, double* x, int nseg, const 
                         const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel_residual,
                         void* stream);
 
+/* --- explicit wave operator (Elasticity::wave_rhs, app/localoperator/Elasticity.cpp:865-880) -- */
+
+/* Density rho at the volume points [E][Nq] (Elasticity's optional rho functional,
+ * Elasticity.cpp:28-35; 1/rho is projected onto the nodal material space like lam and mu).
+ * Default rho = 1.  Elasticity only. */
+int tdg_set_density(tdg_op* op, const double* rho_Q);
+/* y = -(1/rho)-weighted inverse mass applied to x (tandem's apply_inverse_mass kernel,
+ * app/kernels/elasticity.py:236-237: the reference inverse mass with -rhoInv W / |J| at the volume
+ * points); device FP64 arrays, nrhs stacked with leading dimension ld; y may alias x. */
+int tdg_apply_inverse_mass(tdg_op* op, const double* x, double* y, int nrhs, int64_t ld, void* stream);
+/* y = wave_rhs(x) = inverse mass applied to (A x - b): the acceleration of rho u'' = b - A u.  b is
+ * the boundary / slip data part of the right-hand side at the current time (tdg_rhs with only
+ * bc_q, uploaded; tandem adds the same data inside the fluxes), or NULL for none.  y must not
+ * alias x or b. */
+int tdg_wave_rhs(tdg_op* op, const double* x, const double* b, double* y, int nrhs, int64_t ld, void* stream);
+
 /* --- adjoint gradient (no counterpart in tandem: tandem solves forward problems only) ---------- */
 
 /* Gradient of a functional J(u) with respect to per-element constant Lame parameters of an

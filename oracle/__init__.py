@@ -36,6 +36,8 @@ def lib() -> C.CDLL:
             "orc_apply_range": (None, [_p, C.c_long, C.c_long, _p, _p]),
             "orc_assemble_diag": (None, [_p, _p]),
             "orc_rhs": (None, [_p, _p, _p, _p]),
+            "orc_set_density": (C.c_int, [_p, _p]),
+            "orc_apply_inverse_mass": (None, [_p, _p, _p]),
             "orc_cg": (C.c_int, [_p, _p, _p, C.c_double, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
             "orc_error_L2": (C.c_double, [_p, _p, _p]),
             "orc_error_H1_semi": (C.c_double, [_p, _p, _p]),
@@ -168,6 +170,18 @@ class Oracle:
         out = np.zeros((self.E, self.bs, self.bs))
         lib().orc_assemble_diag(self._h, out.ctypes.data)
         return np.ascontiguousarray(out.transpose(0, 2, 1))  # [e, row, col]
+
+    def set_density(self, rho_Q):
+        """Elasticity density at the volume points [E, Nq] (default 1)."""
+        r = np.ascontiguousarray(rho_Q, dtype=np.float64).reshape(self.E, self.Nq)
+        lib().orc_set_density(self._h, r.ctypes.data)
+
+    def apply_inverse_mass(self, x: np.ndarray) -> np.ndarray:
+        """-1/rho weighted inverse mass of Elasticity::wave_rhs applied to x."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.ndof)
+        lib().orc_apply_inverse_mass(self._h, x.ctypes.data, y.ctypes.data)
+        return y
 
     def rhs(self, force_Q=None, bc_q=None) -> np.ndarray:
         b = np.zeros(self.ndof)

@@ -18,6 +18,10 @@
 //   solver     preconditioned CG (PETSc KSPCG as configured by app/common/PetscLinearSolver.cpp:22-28)
 //              with the element block-Jacobi preconditioner (PCPBJACOBI over the assembled P)
 //   errors     Error<D>::L2 / H1_semi (src/form/Error.cpp) with the operator's volume rule
+//   wave       the inverse mass of Elasticity::wave_rhs (app/localoperator/Elasticity.cpp:865-880,
+//              app/kernels/elasticity.py:236-237) with negative_rhoInv_W_Jinv_Q of
+//              precomputeVolume (elasticity.py:44-48) and 1/rho projected like lam and mu
+//              (project_material_rhs, elasticity.py:38-42)
 // The reference-element tables (Dubiner / warp & blend bases, nodes) come from the product's
 // tdg::RefSpace, which the tests pin against tandem's own known-answer tests.
 #include "../include/tandem_b200.h"
@@ -79,6 +83,7 @@ struct orc_op {
     std::vector<double> KG0, KG1;              // Poisson K_G_q side 0/1 (e, i, q)
     std::vector<double> lam0, mu0, lam1, mu1;  // Elasticity facet material (q)
     std::vector<double> penalty;
+    std::vector<double> rhoInv;                // Elasticity: nodal 1/rho [E][Nbf] (empty: rho = 1)
     bool ready = false;
     // block-Jacobi inverses
     std::vector<double> pc;
@@ -853,6 +858,75 @@ void orc_rhs(orc_op const* op, const double* force_Q, const double* bc_q, double
 
 // Block-Jacobi preconditioned CG (FP64) on the unpreconditioned residual: stops when the true
 // relative residual ||b - A x|| / ||b|| <= rtol.  Returns 0 on convergence.
+// 1/rho at the volume points, projected onto the nodal material space (project_material_lhs /
+// project_material_rhs with rhoInv_Q = 1 / rho_Q, Elasticity.cpp:104-175)
+int orc_set_density(orc_op* op, const double* rho_Q) {
+    const int Nq = op->Nq, nbf = op->Nbf;
+    op->rhoInv.assign(static_cast<size_t>(op->E) * nbf, 0.0);
+#pragma omp parallel for schedule(static)
+    for (long el = 0; el < op->E; ++el) {
+        const double* J = &op->AbsDetJ[static_cast<size_t>(el) * Nq];
+        Dense M(nbf, nbf);
+        for (int k = 0; k < nbf; ++k)
+            for (int l = 0; l < nbf; ++l) {
+                double s = 0.0;
+                for (int q = 0; q < Nq; ++q)
+                    s += op->matE_Q[q + static_cast<size_t>(Nq) * k] * op->W[q] * J[q] * op->matE_Q[q + static_cast<size_t>(Nq) * l];
+                M(k, l) = s;
+            }
+        std::vector<double> b(nbf);
+        for (int k = 0; k < nbf; ++k) {
+            double s = 0.0;
+            for (int q = 0; q < Nq; ++q)
+                s += (1.0 / rho_Q[static_cast<size_t>(el) * Nq + q]) * op->matE_Q[q + static_cast<size_t>(Nq) * k] * op->W[q] * J[q];
+            b[k] = s;
+        }
+        tdg::solve_in_place(M, b.data());
+        std::copy(b.begin(), b.end(), &op->rhoInv[static_cast<size_t>(el) * nbf]);
+    }
+    return 0;
+}
+
+// Unew(k, p) = MinvRef(k, r) Jinv_Q(q) E_Q(r, q) E_Q(s, q) MinvRef(s, l) U(l, p) with
+// Jinv_Q(q) = -rhoInv(q) W(q) / |J|(q) (apply_inverse_mass of Elasticity::wave_rhs)
+void orc_apply_inverse_mass(orc_op const* op, const double* x, double* y) {
+    const int Nq = op->Nq, nbf = op->Nbf, Q = op->Q;
+    Dense Minv = tdg::invert(op->space.mass_matrix());
+#pragma omp parallel for schedule(static)
+    for (long el = 0; el < op->E; ++el) {
+        const double* U = x + static_cast<size_t>(el) * op->bs;
+        double* Y = y + static_cast<size_t>(el) * op->bs;
+        std::vector<double> a(static_cast<size_t>(nbf) * Q, 0.0), b(static_cast<size_t>(nbf) * Q, 0.0);
+        for (int p = 0; p < Q; ++p)
+            for (int s = 0; s < nbf; ++s) {
+                double t = 0.0;
+                for (int l = 0; l < nbf; ++l) t += Minv(s, l) * U[l + nbf * p];
+                a[s + nbf * p] = t;
+            }
+        for (int q = 0; q < Nq; ++q) {
+            double ri = 1.0;
+            if (!op->rhoInv.empty()) {
+                ri = 0.0;
+                for (int t = 0; t < nbf; ++t)
+                    ri += op->matE_Q[q + static_cast<size_t>(Nq) * t] * op->rhoInv[static_cast<size_t>(el) * nbf + t];
+            }
+            const double jq = -ri * op->W[q] / op->AbsDetJ[static_cast<size_t>(el) * Nq + q];
+            for (int p = 0; p < Q; ++p) {
+                double v = 0.0;
+                for (int s = 0; s < nbf; ++s) v += op->E_Q[s + static_cast<size_t>(nbf) * q] * a[s + nbf * p];
+                v *= jq;
+                for (int r = 0; r < nbf; ++r) b[r + nbf * p] += op->E_Q[r + static_cast<size_t>(nbf) * q] * v;
+            }
+        }
+        for (int p = 0; p < Q; ++p)
+            for (int k = 0; k < nbf; ++k) {
+                double t = 0.0;
+                for (int r = 0; r < nbf; ++r) t += Minv(k, r) * b[r + nbf * p];
+                Y[k + nbf * p] = t;
+            }
+    }
+}
+
 int orc_cg(orc_op* op, const double* b, double* x, double rtol, int maxit, int* iters, double* relres) {
     const long n = op->E * op->bs;
     const int bs = op->bs;

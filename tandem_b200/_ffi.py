@@ -44,6 +44,9 @@ SYMBOLS = {
     "tdg_adjoint_lame_gradient_noalloc": (C.c_int, [_p, _p, _p, _p, _p, _p]),
     "tdg_autotune": (C.c_int, [_p, C.c_int, C.c_int, _p, _p, C.c_int, _p]),
     "tdg_set_apply_config": (C.c_int, [_p, C.c_int, C.c_int, C.c_int]),
+    "tdg_set_density": (C.c_int, [_p, _p]),
+    "tdg_apply_inverse_mass": (C.c_int, [_p, _p, _p, C.c_int, _i64, _p]),
+    "tdg_wave_rhs": (C.c_int, [_p, _p, _p, _p, C.c_int, _i64, _p]),
     "tdg_fault_create": (C.c_int, [_p, _i64, _p, _p, C.POINTER(_p)]),
     "tdg_fault_destroy": (None, [_p]),
     "tdg_fault_sizes": (C.c_int, [_p, _p]),

@@ -6,6 +6,7 @@
 #include "kernels/apply_tc32.cuh"
 #include "kernels/apply_face.cuh"
 #include "kernels/apply_face_tc32.cuh"
+#include "kernels/wave.cuh"
 #include "kernels/dispatch.hpp"
 #include "kernels/krylov.cuh"
 
@@ -120,6 +121,10 @@ struct tdg_op {
     Tc32Tiles tc32;         // FP32 tensor-core apply (3xTF32): packed tables and signature tiles
     FaceTiles face;         // face-centric FP64 apply: facet tiles grouped by (l0, l1, mode)
     FaceTiles face32;       // face-centric FP32 apply: the same grouping with the FP32 tile size
+    // explicit wave operator: basis at the volume points, reference inverse mass, -rhoInv W / |J|
+    DevArena arena_wave;
+    WaveData wave;
+    bool wave_uploaded = false;
     bool use_mma = true;
     // per precision (0 = FP64, 1 = FP32): kernel family (0 tensor cores, 1 SIMT) and persistent CTAs
     // per SM (0 = default); set by tdg_autotune
@@ -1501,4 +1506,60 @@ extern "C" int tdg_adjoint_lame_gradient_noalloc(tdg_op* op, const double* u, co
     int rc = launch_adjoint_lame(h.D, h.N, op->op64, u, p, bc_q, scratch, grad, s);
     TDG_CUDA_TRY(cudaStreamSynchronize(s));  // the scratch is free again when the call returns
     return rc ? fail(rc, "adjoint gradient launch failed") : 0;
+}
+
+// ------------------------------------------------------------------------------------------------
+// explicit wave operator of elasticity (Elasticity::wave_rhs)
+// ------------------------------------------------------------------------------------------------
+
+namespace {
+int ensure_wave(tdg_op* op) {
+    if (op->wave_uploaded) return 0;
+    auto const& h = op->h;
+    op->arena_wave.release();
+    const double *eq = nullptr, *mi = nullptr, *nr = nullptr;
+    TDG_CUDA_TRY(op->arena_wave.upload(&eq, h.E_Q.a));
+    TDG_CUDA_TRY(op->arena_wave.upload(&mi, h.Minv_ref.a));
+    TDG_CUDA_TRY(op->arena_wave.upload(&nr, h.nrwj));
+    op->wave.EQ = eq;
+    op->wave.Minv = mi;
+    op->wave.nrwj = nr;
+    op->wave_uploaded = true;
+    return 0;
+}
+}  // namespace
+
+extern "C" int tdg_set_density(tdg_op* op, const double* rho_Q) {
+    if (!op || !rho_Q) return fail(TDG_E_INVALID, "null argument");
+    if (op->h.kind != 1) return fail(TDG_E_INVALID, "the density belongs to the elasticity operator");
+    try {
+        op->h.set_density(rho_Q);
+    } catch (std::exception const& e) {
+        return fail(TDG_E_INVALID, e.what());
+    }
+    op->wave_uploaded = false;
+    return 0;
+}
+
+extern "C" int tdg_apply_inverse_mass(tdg_op* op, const double* x, double* y, int nrhs, int64_t ld, void* stream) {
+    if (!op || !x || !y) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = op->h;
+    if (h.kind != 1) return fail(TDG_E_INVALID, "the wave operator is defined for elasticity");
+    if (nrhs < 1 || ld < h.E * h.bs) return fail(TDG_E_INVALID, "nrhs < 1 or ld < E * bs");
+    TDG_TRY(ensure_wave(op));
+    int rc = launch_inverse_mass(h.D, h.N, op->wave, h.E, h.Nq, x, nullptr, y, nrhs, ld,
+                                 static_cast<cudaStream_t>(stream));
+    return rc ? fail(rc, "inverse mass launch failed") : 0;
+}
+
+extern "C" int tdg_wave_rhs(tdg_op* op, const double* x, const double* b, double* y, int nrhs, int64_t ld,
+                            void* stream) {
+    if (!op || !x || !y) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = op->h;
+    if (h.kind != 1) return fail(TDG_E_INVALID, "the wave operator is defined for elasticity");
+    if (x == y || (b && b == y)) return fail(TDG_E_INVALID, "y must not alias x or b");
+    TDG_TRY(tdg_apply(op, TDG_FP64, x, y, nrhs, ld, stream));
+    TDG_TRY(ensure_wave(op));
+    int rc = launch_inverse_mass(h.D, h.N, op->wave, h.E, h.Nq, y, b, y, nrhs, ld, static_cast<cudaStream_t>(stream));
+    return rc ? fail(rc, "inverse mass launch failed") : 0;
 }

@@ -230,6 +230,46 @@ void HostOperator::build(int D_, int N_, int geoN_, int kind_, int64_t E_, int64
         area[f] = a;
     }
     has_material = false;
+    default_density();
+}
+
+void HostOperator::default_density() {
+    Minv_ref = invert(space.mass_matrix());
+    nrwj.assign(static_cast<std::size_t>(E) * Nq, 0.0);
+    for (int64_t el = 0; el < E; ++el)
+        for (int q = 0; q < Nq; ++q)
+            nrwj[static_cast<std::size_t>(el) * Nq + q] = -W[q] / vAbsDetJ[static_cast<std::size_t>(el) * Nq + q];
+}
+
+// 1/rho at the volume points projected onto the nodal material space like lam and mu
+// (project_material_rhs, app/kernels/elasticity.py:38-42), then evaluated at the points.
+void HostOperator::set_density(double const* rho_Q) {
+    if (!rho_Q) throw std::invalid_argument("density missing");
+    if (Minv_ref.rows == 0) default_density();
+    int nm = mat_space.num_basis();
+#pragma omp parallel for schedule(static)
+    for (int64_t el = 0; el < E; ++el) {
+        Dense M(nm, nm);
+        double const* J = &vAbsDetJ[static_cast<std::size_t>(el) * Nq];
+        for (int k = 0; k < nm; ++k)
+            for (int l = 0; l < nm; ++l) {
+                double s = 0.0;
+                for (int q = 0; q < Nq; ++q) s += matE_Q(k, q) * W[q] * J[q] * matE_Q(l, q);
+                M(k, l) = s;
+            }
+        std::vector<double> b(nm);
+        for (int k = 0; k < nm; ++k) {
+            double s = 0.0;
+            for (int q = 0; q < Nq; ++q) s += (1.0 / rho_Q[static_cast<std::size_t>(el) * Nq + q]) * matE_Q(k, q) * W[q] * J[q];
+            b[k] = s;
+        }
+        solve_in_place(M, b.data());
+        for (int q = 0; q < Nq; ++q) {
+            double ri = 0.0;
+            for (int t = 0; t < nm; ++t) ri += matE_Q(t, q) * b[t];
+            nrwj[static_cast<std::size_t>(el) * Nq + q] = -ri * W[q] / J[q];
+        }
+    }
 }
 
 void HostOperator::set_material(double const* c0_Q, double const* c1_Q) {

@@ -73,6 +73,14 @@ struct HostOperator {
                double const* fct_w);
     void set_material(double const* c0_Q, double const* c1_Q);
 
+    // Explicit wave operator (Elasticity::wave_rhs, app/localoperator/Elasticity.cpp:865-880):
+    // Minv_ref = inverse of the reference mass matrix, nrwj[E][Nq] = -rhoInv(x_q) W_q / |J|_q
+    // (negative_rhoInv_W_Jinv_Q, app/kernels/elasticity.py:44-48), rho = 1 until set_density.
+    Dense Minv_ref;
+    std::vector<double> nrwj;
+    void set_density(double const* rho_Q);
+    void default_density();
+
     // Diagonal blocks of the assembled operator, [E][bs][bs] column-major per block
     // (DGOperator::assemble restricted to A(e, e)).  Host reference used by tests and as the
     // fallback-free source of truth for the device assembly kernel's layout.

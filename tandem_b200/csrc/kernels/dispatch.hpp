@@ -71,6 +71,12 @@ int launch_adjoint_lame(int D, int N, DevOp<double> const& op, const double* u, 
 constexpr size_t kAdjointScratchDoubles = size_t(1) << 20;
 int adjoint_scratch(double** ptr);
 
+// y = Minv_rho (x - b) (elasticity inverse mass of the wave operator, wave.cuh); b may be null,
+// y may alias x.
+struct WaveData;
+int launch_inverse_mass(int D, int N, WaveData const& wd, int64_t E, int Nq, const double* x, const double* b,
+                        double* y, int nrhs, int64_t ld, cudaStream_t s);
+
 // Number of resident CTAs of a kernel on the current device times the SM count, cached.
 int device_sm_count();
 

@@ -134,6 +134,34 @@ class DGOperator:
         _ffi.check(_ffi.lib().tdg_apply(self._h, precision, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
                                         nrhs, ld, _stream(stream)))
 
+    # -- explicit wave operator (Elasticity::wave_rhs) ------------------------------------------
+    def set_density(self, rho_Q: np.ndarray) -> None:
+        """Density at the volume points [E, Nq] (elasticity; default 1)."""
+        r = _c(rho_Q, np.float64).reshape(self.E, self.Nq)
+        self._rho = r
+        _ffi.check(_ffi.lib().tdg_set_density(self._h, r.ctypes.data))
+
+    def apply_inverse_mass(self, x, y, nrhs: int = 1, ld: int | None = None, stream=None) -> None:
+        """y = -(1/rho)-weighted inverse mass of x (tandem's apply_inverse_mass)."""
+        ld = self.ndof if ld is None else ld
+        _check_vec(x, FP64, nrhs * ld)
+        _check_vec(y, FP64, nrhs * ld)
+        _ffi.check(_ffi.lib().tdg_apply_inverse_mass(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                                     nrhs, ld, _stream(stream)))
+
+    def wave_rhs(self, x, y, b=None, nrhs: int = 1, ld: int | None = None, stream=None) -> None:
+        """y = inverse mass of (A x - b), the acceleration of rho u'' = b - A u; b: boundary-data
+        right-hand side (device FP64) or None."""
+        ld = self.ndof if ld is None else ld
+        _check_vec(x, FP64, nrhs * ld)
+        _check_vec(y, FP64, nrhs * ld)
+        bp = None
+        if b is not None:
+            _check_vec(b, FP64, nrhs * ld)
+            bp = C.c_void_p(b.data_ptr())
+        _ffi.check(_ffi.lib().tdg_wave_rhs(self._h, C.c_void_p(x.data_ptr()), bp, C.c_void_p(y.data_ptr()), nrhs,
+                                           ld, _stream(stream)))
+
     def autotune(self, precision: int = FP64, nrhs: int = 1, stream=None) -> list[dict]:
         """Times the candidate apply launch configurations on this operator and keeps the fastest
         for later applies and solves in `precision` (tdg_autotune).  Returns every measurement."""

@@ -104,3 +104,24 @@ def test_fault_facets_rhs():
     orc.set_material(np.ones((op.E, op.Nq)))
     g = np.ones((op.F, 1, op.nq))
     np.testing.assert_allclose(op.rhs(None, g), orc.rhs(None, g), atol=1e-12)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_oracle_inverse_mass_inverts_the_mass_on_affine_elements(dim):
+    """The -(1/rho)-weighted inverse mass of Elasticity::wave_rhs is the exact element inverse mass
+    on affine elements: applied to the load of a nodal field it returns minus the field / rho."""
+    from cases import make_mesh, tandem_quadrature
+    from tandem_b200 import refelem
+    from tandem_b200.operator import ELASTICITY
+    N = 3
+    m = make_mesh(dim, 2, N, False)
+    q = tandem_quadrature(dim, N)
+    o = Oracle(m, N, ELASTICITY, q)
+    X = o.volume_coords()
+    o.set_material(2.0 + X[..., 0], np.ones(X.shape[:2]))
+    o.set_density(np.full(X.shape[:2], 2.0))
+    EQ = refelem.ref_basis(dim, N, refelem.WARP_BLEND, q.vol_x)
+    u = np.random.default_rng(dim).standard_normal(o.ndof)
+    fQ = np.einsum("epk,kq->epq", u.reshape(o.E, dim, -1), EQ)
+    y = o.apply_inverse_mass(o.rhs(fQ, None))
+    assert np.abs(y + 0.5 * u).max() <= 1e-12 * np.abs(u).max()
