@@ -40,9 +40,10 @@ __global__ void k_dot_finalize(const double* __restrict__ partial, const int* __
     }
 }
 
-__global__ void k_cg_shift(double* __restrict__ scal, int nseg) {
+__global__ void k_cg_shift(double* __restrict__ scal, int nseg, int only_replaced) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < nseg && scal[r * kScal + kActive] != 0.0) scal[r * kScal + kRZ] = scal[r * kScal + kRZnew];
+    if (r < nseg && scal[r * kScal + kActive] != 0.0 && (!only_replaced || scal[r * kScal + kRepl] != 0.0))
+        scal[r * kScal + kRZ] = scal[r * kScal + kRZnew];
 }
 
 }  // namespace tdg
@@ -914,14 +915,15 @@ int cg_start(tdg_op* op, int prec, SegPlan const& sp, CgVectors<T> v, double* pa
 // p = z_old + beta p_prev, beta = rz_old / rz_prev; with the replaced residual the recurrence
 // gives p = z_new + (rz_new / rz_prev) p_prev = z_new + (rz_new / rz_old) (p - z_old), and z
 // takes z_new.  Segments flagged in scal[seg][kTmp] restart from p = z_new.  rz_new is in slot
-// kRZnew, rz_old in kRZ (k_cg_shift then moves rz_new to kRZ).
+// kRZnew, rz_old in kRZ (k_cg_shift then moves rz_new to kRZ).  Only the segments flagged kRepl
+// (whose residual was replaced) change.
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads)
     k_replace_dir(const Chunk* __restrict__ chunks, T* __restrict__ p, T* __restrict__ z, const T* __restrict__ znew,
                   const double* __restrict__ scal) {
     const Chunk ch = chunks[blockIdx.x];
     const double* sc = scal + ch.seg * kScal;
-    if (sc[kActive] == 0.0) return;
+    if (sc[kActive] == 0.0 || sc[kRepl] == 0.0) return;
     const double rz = sc[kRZ];
     const T c = static_cast<T>((sc[kTmp] != 0.0 || rz == 0.0) ? 0.0 : sc[kRZnew] / rz);
     for (int64_t i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
@@ -948,14 +950,19 @@ __global__ void __launch_bounds__(kVecThreads)
 // runs in T (operator, preconditioner and vectors in T, dot products accumulated in FP64) and
 // accumulates its correction in xh.  Whenever a segment's recurrence residual has dropped by
 // `delta` since the last update, or claims convergence, the correction is flushed into the FP64
-// solution x, the true residual r64 = b - A x is recomputed in FP64 and replaces the recurrence
-// residual; the search direction is rebuilt from the replaced residual with the CG recurrence
+// solution x and the true residual b - A x is recomputed in FP64 for every segment.  It replaces
+// the recurrence residual of the segments that asked for the update (the others keep their
+// recurrence untouched, so one problem of a batch does not disturb the Krylov space of another);
+// the search direction is rebuilt from the replaced residual with the CG recurrence
 // (k_replace_dir), so the Krylov information is kept -- unless the true residual exceeds the
 // recurrence residual by more than 2x (accumulated drift), in which case that segment restarts
-// from p = z.  A segment within three decades of its target whose true residual gains less than
-// 1% over max(2000, iterations / 2) iterations has reached the attainable accuracy of the
-// recurrence and stops unconverged.  Convergence is decided on the FP64 residual only.  For T = double xh
-// aliases x and rh aliases r64.
+// from p = z.  Every segment whose true residual meets its target stops.  A segment within three
+// decades of its target whose true residual gains less than 1% over max(2000, iterations / 2)
+// iterations has reached the attainable accuracy of the recurrence and stops unconverged; so
+// does, for a low-precision recurrence, a segment whose true residual realised less than half of
+// the claimed decades at two consecutive replacements that followed a `delta` reduction.
+// Convergence is decided on the FP64 residual only.  For T = double xh aliases x and rh aliases
+// r64 (the true residual is then formed in q, free between iterations).
 template <typename T>
 int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, double* x, T* xh, double* r64, T* rh,
                  CgVectors<T> v, double* t64, double* partial, double* scal, double rtol, double delta, int max_it,
@@ -966,7 +973,7 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
     const int nseg = sp.nseg;
     if (max_updates <= 0) max_updates = 1 << 20;
     std::vector<double> tol(nseg), act(nseg), rmax(nseg), best(nseg);
-    std::vector<int> stall(nseg, 0);
+    std::vector<int> stall(nseg, 0), poor(nseg, 0);
     std::vector<double> hs(static_cast<size_t>(nseg) * kScal);
     *iters = 0;
     *updates = 0;
@@ -1018,19 +1025,31 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
             rc = fail(TDG_E_CUDA, "reading the Krylov scalars");
             break;
         }
-        bool update = *iters >= max_it;
+        const bool last = *iters >= max_it;
+        bool update = last;
         for (int i = 0; i < nseg; ++i) {
-            if (hs[static_cast<size_t>(i) * kScal + kActive] == 0.0) continue;
-            const double rr = std::sqrt(hs[static_cast<size_t>(i) * kScal + kRR]);
-            if (!std::isfinite(rr) || rr <= delta * rmax[i] || rr <= tol[i]) update = true;
+            double* sr = &hs[static_cast<size_t>(i) * kScal];
+            sr[kRepl] = 0.0;
+            if (sr[kActive] == 0.0) continue;
+            const double rr = std::sqrt(sr[kRR]);
+            if (last || !std::isfinite(rr) || rr <= delta * rmax[i] || rr <= tol[i]) {
+                sr[kRepl] = 1.0;
+                update = true;
+            }
         }
         if (!update) continue;
-        // reliable update: flush, FP64 residual, replace the recurrence residual
+        // reliable update: flush, FP64 residual of every segment into rt, replace the recurrence
+        // residual of the flagged segments
         ++*updates;
-        if constexpr (kLow) k_flush<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, xh);
-        if ((rc = residual64(op, sp, b, x, r64, t64, partial, scal, rn, bn, s))) break;
+        double* rt;
+        if constexpr (kLow) {
+            k_flush<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, xh);
+            rt = r64;
+        } else {
+            rt = v.q;
+        }
+        if ((rc = residual64(op, sp, b, x, rt, t64, partial, scal, rn, bn, s))) break;
         any = false;
-        bool restart_any = false;
         for (int i = 0; i < nseg; ++i) {
             double* sr = &hs[static_cast<size_t>(i) * kScal];
             sr[kTmp] = 0.0;
@@ -1054,31 +1073,45 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
                 sr[kActive] = 0.0;
                 continue;
             }
-            // the recurrence residual fell below the true one: its search direction no longer
-            // matches the replaced residual, restart it
-            const double rrec = std::sqrt(sr[kRR]);
-            if (!(rn[i] <= 2.0 * rrec)) {
-                sr[kTmp] = 1.0;
-                restart_any = true;
+            if (sr[kRepl] != 0.0) {
+                const double rrec = std::sqrt(sr[kRR]);
+                if constexpr (kLow) {
+                    // twice in a row the recurrence claimed a `delta` reduction while the true
+                    // residual realised less than half of its decades: near its attainable
+                    // accuracy a low-precision iteration (about half the cost of an FP64 one)
+                    // gains less than an FP64 iteration would, so the segment stops here (the
+                    // caller continues it in FP64)
+                    if (rrec <= delta * rmax[i] && rn[i] > std::sqrt(rrec * rmax[i])) {
+                        if (++poor[i] >= 2) {
+                            sr[kActive] = 0.0;
+                            continue;
+                        }
+                    } else {
+                        poor[i] = 0;
+                    }
+                }
+                // the recurrence residual fell below the true one: its search direction no longer
+                // matches the replaced residual, restart it
+                if (!(rn[i] <= 2.0 * rrec)) sr[kTmp] = 1.0;
+                rmax[i] = rn[i];
             }
-            rmax[i] = rn[i];
             any = true;
         }
-        if (!any || *diverged || *iters >= max_it || *updates >= max_updates) break;
-        // restore the scalars (alpha / beta state, activity, restart flags) that residual64
-        // overwrote, then recompute z = M rh, rz and rr from the replaced residual; the search
-        // direction p stays unless the segment restarts
+        if (!any || *diverged || last || *updates >= max_updates) break;
+        // restore the scalars (alpha / beta state, activity, replace and restart flags) that
+        // residual64 overwrote; on the flagged segments replace the residual, recompute
+        // z = M rh, rz and rr, and rebuild p (unless the segment restarts)
         if (cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) {
             rc = fail(TDG_E_CUDA, "writing the Krylov scalars");
             break;
         }
-        if constexpr (kLow) k_scale_convert<double, T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, r64, rh, scal, -1);
-        // z_new = M r_new into q (free between iterations), rz_new, rr; then p and z
+        k_replace_residual<double, T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, rt, rh, scal);
+        // z_new = M r into q (free between iterations; for T = double its true residual is
+        // consumed above), rz_new, rr; the unflagged segments get z_new = z and are left as is
         if ((rc = tdg_bjacobi_apply(op, prec, rh, v.q, sp.op_nrhs, sp.op_ld, s))) break;
         if ((rc = dots<T>(sp, rh, v.q, rh, rh, partial, scal, kRZnew, kRR, s))) break;
         k_replace_dir<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, v.p, v.z, v.q, scal);
-        k_cg_shift<<<(nseg + 127) / 128, 128, 0, s>>>(scal, nseg);
-        (void)restart_any;
+        k_cg_shift<<<(nseg + 127) / 128, 128, 0, s>>>(scal, nseg, 1);
     }
     if (exec) cudaGraphExecDestroy(exec);
     if (rc) return rc;

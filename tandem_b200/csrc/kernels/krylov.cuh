@@ -16,7 +16,8 @@
 namespace tdg {
 
 constexpr int kScal = 8;
-enum ScalSlot { kRZ = 0, kPQ = 1, kRZnew = 2, kRR = 3, kActive = 4, kBB = 5, kTmp = 6 };
+// kRepl flags the segments whose recurrence residual a reliable update replaces.
+enum ScalSlot { kRZ = 0, kPQ = 1, kRZnew = 2, kRR = 3, kActive = 4, kBB = 5, kTmp = 6, kRepl = 7 };
 constexpr int kVecThreads = 256;
 constexpr int64_t kChunk = 32 * 1024;
 
@@ -97,8 +98,19 @@ __global__ void __launch_bounds__(kVecThreads)
     for (int64_t i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) p[i] = z[i] + beta * p[i];
 }
 
-// rz = rz_new for every active segment.
-__global__ void k_cg_shift(double* __restrict__ scal, int nseg);
+// rz = rz_new for every active segment (only_replaced: for the active segments flagged kRepl).
+__global__ void k_cg_shift(double* __restrict__ scal, int nseg, int only_replaced = 0);
+
+// out = in on the active segments flagged kRepl (with type conversion); other segments untouched.
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(kVecThreads)
+    k_replace_residual(const Chunk* __restrict__ chunks, const Tin* __restrict__ in, Tout* __restrict__ out,
+                       const double* __restrict__ scal) {
+    const Chunk ch = chunks[blockIdx.x];
+    const double* s = scal + ch.seg * kScal;
+    if (s[kActive] == 0.0 || s[kRepl] == 0.0) return;
+    for (int64_t i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) out[i] = static_cast<Tout>(in[i]);
+}
 
 // out = in / sqrt(scal[seg][slot]) (type conversion; slot < 0: plain conversion).
 template <typename Tin, typename Tout>
