@@ -215,6 +215,61 @@ int tdg_solve_segmented(tdg_op* op, const double* b, double* x, int nseg, const 
                         const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel_residual,
                         void* stream);
 
+/* --- p-multigrid preconditioner (PetscLinearSolver::setup_mg, app/common/PetscLinearSolver.cpp:53-114,
+ *     MGConfig, app/common/MGConfig.cpp:11-41, options examples/options/mg_cheby.cfg) ------------ */
+
+#define TDG_PC_BJACOBI 0
+#define TDG_PC_MG 1
+
+#define TDG_MG_TWOLEVEL 0
+#define TDG_MG_LOGARITHMIC 1
+#define TDG_MG_FULL 2
+
+typedef struct {
+    int32_t strategy;        /* TDG_MG_TWOLEVEL / LOGARITHMIC / FULL (MGStrategy; default logarithmic) */
+    int32_t coarse_degree;   /* degree of the coarsest level (MGConfig coarse_level; default 1) */
+    int32_t smooth_its;      /* Chebyshev steps per smoothing (-mg_levels_ksp_max_it; default 10) */
+    double esteig_lo;        /* smoothing interval [esteig_lo, esteig_hi] x lambda_max(D^-1 A)   */
+    double esteig_hi;        /* (-mg_levels_ksp_chebyshev_esteig 0,lo,0,hi; default 0.01, 1.1)    */
+    int32_t esteig_steps;    /* Lanczos steps of the lambda_max estimate (default 10) */
+    double coarse_rtol;      /* coarsest-level CG relative tolerance (-mg_coarse_ksp_rtol; 0.1) */
+    int32_t coarse_max_it;   /* coarsest-level CG iteration cap (default 1000) */
+    int32_t smooth_precision; /* TDG_FP64, or TDG_MIXED: FP32 arithmetic for the finest level's
+                                 smoother applies (the level operators stay FP64) */
+} tdg_mg_opts;
+
+/* Builds the p-multigrid hierarchy: level degrees from the strategy; the element interpolation
+ * between consecutive degrees (modal injection for Poisson, nodal interpolation for elasticity,
+ * ModalInterpolation.h:40-44, NodalInterpolation.cpp:8-36); Galerkin coarse operators
+ * A_l = I^T A_{l+1} I (the first by probing the matrix-free operator with a distance-2 element
+ * colouring, the others by block triple products) stored element block-sparse on the device;
+ * point-Jacobi diagonals; the lambda_max estimates of the Chebyshev smoothers; block-Jacobi
+ * inverses of the coarsest level.  opts may be NULL (defaults).  Does not select the
+ * preconditioner (tdg_set_preconditioner). */
+int tdg_mg_setup(tdg_op* op, const tdg_mg_opts* opts, void* stream);
+/* z = M r, one V-cycle per right-hand side (PCMG's apply): Chebyshev pre-smoothing from zero,
+ * restriction of the residual, the coarser levels, prolongation, Chebyshev post-smoothing; CG with
+ * block Jacobi on the coarsest level.  FP64 device vectors. */
+int tdg_mg_apply(tdg_op* op, const double* r, double* z, int nrhs, int64_t ld, void* stream);
+/* Preconditioner of tdg_solve / tdg_solve_segmented (and the Green's-function and adjoint solves
+ * built on them): TDG_PC_BJACOBI (default) or TDG_PC_MG (needs tdg_mg_setup; TDG_FP64 and
+ * TDG_MIXED solves; the Krylov method becomes flexible CG, since the coarse CG makes the
+ * preconditioner vary slightly between iterations). */
+int tdg_set_preconditioner(tdg_op* op, int pc);
+/* Hierarchy description: number of levels; per level (coarsest first, up to max_levels) the
+ * degree, block size and lambda_max estimate (the finest level's too; level 0 has none: 0).
+ * Any output may be NULL.  coarse_its: coarsest-level CG iterations since setup (may be NULL). */
+int tdg_mg_info(tdg_op* op, int* nlevels, int max_levels, int* degrees, int* block_sizes, double* lambda_max,
+                int64_t* coarse_its);
+/* Copies level `level` (< nlevels - 1) of the hierarchy to host memory: blocks [E][NB][bs][bs]
+ * (column-major per block, NB = 1 + faces per element) and its neighbour table nbr [E][NB]
+ * (slot 0 the element, slot 1 + f the element behind face f, -1 none); for tests. */
+int tdg_mg_level_matrix(tdg_op* op, int level, double* blocks, int32_t* nbr);
+/* Host utilities (no device): the level degrees of a strategy (returns their count; degrees may
+ * be NULL) and the reference interpolation matrix [Nbf(n_to)][Nbf(n_from)] of one component. */
+int tdg_mg_level_degrees(int strategy, int coarse_degree, int degree, int* degrees);
+int tdg_mg_interpolation(int dim, int kind, int n_to, int n_from, double* out);
+
 /* --- explicit wave operator (Elasticity::wave_rhs, app/localoperator/Elasticity.cpp:865-880) -- */
 
 /* Density rho at the volume points [E][Nq] (Elasticity's optional rho functional,

@@ -43,6 +43,8 @@ def lib() -> C.CDLL:
             "orc_error_H1_semi": (C.c_double, [_p, _p, _p]),
             "orc_fault_slip_q": (None, [_p, C.c_long, _p, _p, _p, C.c_int, _p, _p]),
             "orc_fault_traction": (None, [_p, C.c_long, _p, _p, _p, C.c_int, _p, _p, _p]),
+            "orc_mg_interpolation": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _p]),
+            "orc_mg_levels": (C.c_int, [C.c_int, C.c_int, C.c_int, _p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -232,3 +234,74 @@ class Oracle:
     def error_H1_semi(self, x: np.ndarray, refgrad_Q: np.ndarray) -> float:
         r = np.ascontiguousarray(refgrad_Q, dtype=np.float64)
         return lib().orc_error_H1_semi(self._h, np.ascontiguousarray(x).ctypes.data, r.ctypes.data)
+
+
+# ---- p-multigrid restated (tandem's PCMG configuration) ---------------------------------------------
+
+def mg_interpolation(dim: int, kind: int, n_to: int, n_from: int) -> np.ndarray:
+    """One component's interpolation block [Nbf(n_to), Nbf(n_from)] as tandem assembles it
+    (NodalInterpolation.cpp:8-36 / ModalInterpolation.h:31-45)."""
+    from math import comb
+    out = np.zeros((comb(n_to + dim, dim), comb(n_from + dim, dim)))
+    if lib().orc_mg_interpolation(dim, kind, n_to, n_from, out.ctypes.data) != 0:
+        raise ValueError("bad interpolation degrees")
+    return out
+
+
+def mg_levels(strategy: int, coarse: int, degree: int) -> list[int]:
+    """MGConfig::levels (app/common/MGConfig.cpp:11-41), coarsest first."""
+    out = (C.c_int * 32)()
+    n = lib().orc_mg_levels(strategy, coarse, degree, out)
+    if n < 0:
+        raise ValueError("bad strategy")
+    return list(out[:n])
+
+
+def element_interpolation(E: int, Q: int, I: np.ndarray) -> np.ndarray:
+    """Dense block-diagonal interpolation of E elements (tandem's InterpolationOperator::assemble,
+    src/form/InterpolationOperator.h:28-49): I(k + p N1, l + p N2) per element and component."""
+    return np.kron(np.eye(E), np.kron(np.eye(Q), I))
+
+
+class DenseMultigrid:
+    """The V-cycle of PETSc's PCMG as tandem configures it (app/common/PetscLinearSolver.cpp:53-114,
+    examples/options/mg_cheby.cfg) on dense matrices: Galerkin coarse operators A_l = P^T A_{l+1} P,
+    Chebyshev smoothing with point Jacobi on [lo, hi] x lambda_max (Saad, Iterative Methods, Alg.
+    12.1), the same number of steps before and after the coarse correction, and an exact solve on
+    the coarsest level.  lambda_max per smoothed level is given (the product's estimates), so the
+    restatement and the device V-cycle apply the same polynomials."""
+
+    def __init__(self, A: np.ndarray, P: list[np.ndarray], lmax: list[float], smooth_its: int = 10,
+                 esteig: tuple[float, float] = (0.01, 1.1)):
+        self.P = P  # P[l]: level l -> level l + 1
+        self.A = [None] * len(P) + [A]
+        for l in range(len(P) - 1, -1, -1):
+            self.A[l] = P[l].T @ self.A[l + 1] @ P[l]
+        self.lmax, self.its, self.esteig = lmax, smooth_its, esteig
+
+    def smooth(self, l: int, b: np.ndarray, x: np.ndarray | None) -> np.ndarray:
+        A = self.A[l]
+        dinv = 1.0 / np.diag(A)
+        emax, emin = self.esteig[1] * self.lmax[l], self.esteig[0] * self.lmax[l]
+        theta, delta = 0.5 * (emax + emin), 0.5 * (emax - emin)
+        sigma = theta / delta
+        rho = 1.0 / sigma
+        r = b.copy() if x is None else b - A @ x
+        d = dinv * r / theta
+        x = d.copy() if x is None else x + d
+        for _ in range(1, self.its):
+            r = r - A @ d
+            rho1 = 1.0 / (2.0 * sigma - rho)
+            d = rho1 * rho * d + 2.0 * rho1 / delta * dinv * r
+            x = x + d
+            rho = rho1
+        return x
+
+    def vcycle(self, b: np.ndarray, l: int | None = None) -> np.ndarray:
+        l = len(self.A) - 1 if l is None else l
+        if l == 0:
+            return np.linalg.solve(self.A[0], b)
+        x = self.smooth(l, b, None)
+        r = b - self.A[l] @ x
+        x = x + self.P[l - 1] @ self.vcycle(self.P[l - 1].T @ r, l - 1)
+        return self.smooth(l, b, x)

@@ -1143,3 +1143,53 @@ void orc_fault_traction(orc_op const* op, long nfault, const long* facets, const
 }
 
 }  // extern "C"
+
+// ---- p-multigrid set-up restated (test side) ------------------------------------------------------
+extern "C" {
+
+// NodalInterpolation::assemble (app/localoperator/NodalInterpolation.cpp:8-36): one component's
+// block is V_to.leftCols(N2) * VInv_from, V the Dubiner Vandermonde at the warp & blend nodes;
+// ModalInterpolation::assemble (app/localoperator/ModalInterpolation.h:31-45): injection of the
+// first N2 modal coefficients.  out: [N1][N2].
+int orc_mg_interpolation(int D, int kind, int n_to, int n_from, double* out) {
+    if (n_to <= n_from || n_from < 0) return -1;
+    const int N1 = static_cast<int>(tdg::binom(n_to + D, D)), N2 = static_cast<int>(tdg::binom(n_from + D, D));
+    std::fill(out, out + static_cast<size_t>(N1) * N2, 0.0);
+    if (kind == kPoisson) {
+        for (int l = 0; l < N2; ++l) out[static_cast<size_t>(l) * N2 + l] = 1.0;
+        return 0;
+    }
+    Dense Vto = tdg::vandermonde(D, n_to, tdg::warp_blend_nodes(D, n_to));
+    Dense VinvFrom = tdg::invert(tdg::vandermonde(D, n_from, tdg::warp_blend_nodes(D, n_from)));
+    for (int k = 0; k < N1; ++k)
+        for (int l = 0; l < N2; ++l) {
+            double s = 0.0;
+            for (int j = 0; j < N2; ++j) s += Vto(k, j) * VinvFrom(j, l);
+            out[static_cast<size_t>(k) * N2 + l] = s;
+        }
+    return 0;
+}
+
+// MGConfig::levels (app/common/MGConfig.cpp:11-41); returns the number of levels.
+int orc_mg_levels(int strategy, int coarse, int N, int* out) {
+    if (N <= coarse) coarse = N > 0 ? N - 1 : 0;
+    std::vector<int> lv;
+    switch (strategy) {
+        case 0: lv = {coarse, N}; break;
+        case 1: {
+            std::vector<int> down{N};
+            while (down.back() > coarse) down.push_back(down.back() / 2);
+            if (down.back() != coarse) down.back() = coarse;
+            lv.assign(down.rbegin(), down.rend());
+            break;
+        }
+        case 2:
+            for (int d = coarse; d <= N; ++d) lv.push_back(d);
+            break;
+        default: return -1;
+    }
+    std::copy(lv.begin(), lv.end(), out);
+    return static_cast<int>(lv.size());
+}
+
+}  // extern "C"

@@ -47,6 +47,13 @@ SYMBOLS = {
     "tdg_set_density": (C.c_int, [_p, _p]),
     "tdg_apply_inverse_mass": (C.c_int, [_p, _p, _p, C.c_int, _i64, _p]),
     "tdg_wave_rhs": (C.c_int, [_p, _p, _p, _p, C.c_int, _i64, _p]),
+    "tdg_mg_setup": (C.c_int, [_p, _p, _p]),
+    "tdg_mg_apply": (C.c_int, [_p, _p, _p, C.c_int, _i64, _p]),
+    "tdg_set_preconditioner": (C.c_int, [_p, C.c_int]),
+    "tdg_mg_info": (C.c_int, [_p, _p, C.c_int, _p, _p, _p, _p]),
+    "tdg_mg_level_matrix": (C.c_int, [_p, C.c_int, _p, _p]),
+    "tdg_mg_level_degrees": (C.c_int, [C.c_int, C.c_int, C.c_int, _p]),
+    "tdg_mg_interpolation": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _p]),
     "tdg_fault_create": (C.c_int, [_p, _i64, _p, _p, C.POINTER(_p)]),
     "tdg_fault_destroy": (None, [_p]),
     "tdg_fault_sizes": (C.c_int, [_p, _p]),
@@ -76,6 +83,16 @@ class TuneEntry(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("max_iterations", C.c_int32), ("rtol", C.c_double),
                 ("inner_rtol", C.c_double), ("max_outer", C.c_int32), ("use_graphs", C.c_int32)]
+
+
+TDG_PC_BJACOBI, TDG_PC_MG = 0, 1
+TDG_MG_TWOLEVEL, TDG_MG_LOGARITHMIC, TDG_MG_FULL = 0, 1, 2
+
+
+class MgOpts(C.Structure):
+    _fields_ = [("strategy", C.c_int32), ("coarse_degree", C.c_int32), ("smooth_its", C.c_int32),
+                ("esteig_lo", C.c_double), ("esteig_hi", C.c_double), ("esteig_steps", C.c_int32),
+                ("coarse_rtol", C.c_double), ("coarse_max_it", C.c_int32), ("smooth_precision", C.c_int32)]
 
 
 class SolveStats(C.Structure):

@@ -9,6 +9,7 @@
 #include "kernels/wave.cuh"
 #include "kernels/dispatch.hpp"
 #include "kernels/krylov.cuh"
+#include "kernels/mg.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -112,6 +113,45 @@ std::vector<T> conv(std::vector<double> const& v) {
 
 }  // namespace
 
+namespace {
+
+// One level of the p-multigrid hierarchy.  Coarse levels hold their Galerkin operator as element
+// block-sparse blocks A [E][NB][bs][bs]; the finest level is the matrix-free operator.  ip is the
+// interpolation from this level to the next finer one.  x, b are the level's solution and
+// right-hand side (the caller's z and r on the finest level), r, d, y, w work vectors.
+struct MgLevel {
+    int degree = 0, bs = 0;
+    int64_t n = 0;
+    double* A = nullptr;
+    double* dinv = nullptr;
+    MgInterp ip{};
+    double *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *y = nullptr, *w = nullptr;
+    double lmax = 0.0;
+};
+
+struct MgHierarchy {
+    bool ready = false;
+    tdg_mg_opts opts{};
+    int fine_prec = TDG_FP64;
+    int NB = 0, ncolours = 0;
+    std::vector<MgLevel> lv;  // coarsest first; lv.back() is the matrix-free operator
+    DevArena arena;
+    int32_t* nbr = nullptr;
+    int32_t* colour = nullptr;
+    // coarsest-level CG: block-Jacobi inverses, vectors, single-segment plan and scalars
+    double* cinv = nullptr;
+    double *cr = nullptr, *cz = nullptr, *cp = nullptr, *cq = nullptr;
+    double* partial = nullptr;
+    double* scal = nullptr;
+    Chunk* chunks = nullptr;
+    int* seg_chunk = nullptr;
+    int nchunks = 0;
+    int* status = nullptr;
+    int64_t coarse_its = 0;
+};
+
+}  // namespace
+
 struct tdg_op {
     HostOperator h;
     bool uploaded64 = false, uploaded32 = false;
@@ -141,6 +181,9 @@ struct tdg_op {
     // solve workspace
     size_t ws_bytes = 0;
     void* ws = nullptr;
+    // p-multigrid hierarchy and the preconditioner the solves use
+    MgHierarchy mg;
+    int pc = TDG_PC_BJACOBI;
 };
 
 namespace {
@@ -423,6 +466,382 @@ int dots(SegPlan const& sp, const T* a, const T* b, const T* c, const T* d, doub
     return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "dot kernels");
 }
 
+// ---- block-Jacobi diagonal blocks ---------------------------------------------------------------
+
+// Assembles the element diagonal blocks once (block Jacobi, and the point-Jacobi diagonal of the
+// finest multigrid level).
+int ensure_blocks(tdg_op* op, cudaStream_t s) {
+    if (op->blk) return 0;
+    TDG_TRY(ensure_uploaded(op, TDG_FP64));
+    auto const& h = op->h;
+    TDG_CUDA_TRY(op->arena_pc.alloc(&op->blk, static_cast<size_t>(h.E) * h.bs * h.bs));
+    TDG_CUDA_TRY(op->arena_pc.alloc(&op->status, 1));
+    int rc = launch_bjac_assemble(h.D, h.N, h.kind, op->op64, op->blk, s);
+    if (rc) {
+        op->blk = nullptr;
+        return fail(rc, "block assembly launch failed");
+    }
+    return 0;
+}
+
+// ---- p-multigrid (PCMG with Chebyshev / point-Jacobi smoothing) ---------------------------------
+
+int mgk(int rc, const char* what) { return rc ? fail(rc, std::string("multigrid: ") + what) : 0; }
+
+// y = A_l x, or y = b - A_l x when b != nullptr.
+int mg_level_apply(tdg_op* op, int l, const double* x, double* y, const double* b, cudaStream_t s) {
+    auto& mg = op->mg;
+    auto const& L = mg.lv[static_cast<size_t>(l)];
+    if (l + 1 == static_cast<int>(mg.lv.size())) {
+        TDG_TRY(tdg_apply(op, mg.fine_prec, x, y, 1, L.n, s));
+        if (b) TDG_TRY(mgk(launch_vec_sub(L.n, b, y, y, s), "residual"));
+        return 0;
+    }
+    return mgk(launch_mg_bsr_apply(op->h.E, mg.NB, L.bs, mg.nbr, L.A, x, b, y, s), "level apply");
+}
+
+// Chebyshev smoothing of A_l x = b on [esteig_lo, esteig_hi] x lambda_max(D^-1 A_l), smooth_its
+// steps (Saad, Alg. 12.1, with the point-Jacobi preconditioner), from x = 0 or from the given x.
+int mg_smooth(tdg_op* op, int l, const double* b, double* x, bool x_zero, cudaStream_t s) {
+    auto& mg = op->mg;
+    auto& L = mg.lv[static_cast<size_t>(l)];
+    const double emax = mg.opts.esteig_hi * L.lmax, emin = mg.opts.esteig_lo * L.lmax;
+    const double theta = 0.5 * (emax + emin), delta = 0.5 * (emax - emin), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    if (x_zero)
+        TDG_TRY(mgk(launch_vec_axpby(L.n, 1.0, b, 0.0, L.r, s), "copy"));
+    else
+        TDG_TRY(mg_level_apply(op, l, x, L.r, b, s));
+    TDG_TRY(mgk(launch_cheb_first(L.n, L.dinv, L.r, L.d, x, 1.0 / theta, x_zero ? 1 : 0, s), "Chebyshev"));
+    for (int k = 1; k < mg.opts.smooth_its; ++k) {
+        TDG_TRY(mg_level_apply(op, l, L.d, L.y, nullptr, s));
+        const double rho1 = 1.0 / (2.0 * sigma - rho);
+        TDG_TRY(mgk(launch_cheb_step(L.n, L.dinv, L.y, L.r, L.d, x, rho1 * rho, 2.0 * rho1 / delta, s), "Chebyshev"));
+        rho = rho1;
+    }
+    return 0;
+}
+
+int mg_read_scalars(tdg_op* op, double* hs, cudaStream_t s) {
+    TDG_CUDA_TRY(cudaMemcpyAsync(hs, op->mg.scal, kScal * sizeof(double), cudaMemcpyDeviceToHost, s));
+    TDG_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+// Coarsest level: CG with the block-Jacobi inverses from x = 0 until ||r|| <= coarse_rtol ||b||
+// (checked every 4 iterations) or coarse_max_it iterations.
+int mg_coarse_solve(tdg_op* op, const double* b, double* x, cudaStream_t s) {
+    auto& mg = op->mg;
+    auto const& L = mg.lv[0];
+    SegPlan sp;
+    sp.nseg = 1;
+    sp.nchunks = mg.nchunks;
+    sp.chunks = mg.chunks;
+    sp.seg_chunk = mg.seg_chunk;
+    sp.op_nrhs = 1;
+    sp.op_ld = L.n;
+    double hs[kScal] = {};
+    hs[kActive] = 1.0;
+    TDG_CUDA_TRY(cudaMemsetAsync(x, 0, L.n * sizeof(double), s));
+    TDG_CUDA_TRY(cudaMemcpyAsync(mg.cr, b, L.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    TDG_CUDA_TRY(cudaMemcpyAsync(mg.scal, hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+    TDG_TRY(mgk(launch_bjac_apply<double, double>(L.bs, op->h.E, mg.cinv, mg.cr, mg.cz, 1, L.n, s), "coarse PC"));
+    k_copy<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, mg.cz, mg.cp);
+    TDG_TRY(dots<double>(sp, mg.cr, mg.cz, mg.cr, mg.cr, mg.partial, mg.scal, kRZ, kRR, s));
+    TDG_TRY(mg_read_scalars(op, hs, s));
+    const double tol2 = mg.opts.coarse_rtol * mg.opts.coarse_rtol * hs[kRR];
+    if (!(hs[kRR] > 0.0)) return 0;
+    int it = 0;
+    while (it < mg.opts.coarse_max_it) {
+        for (int k = 0; k < 4; ++k) {
+            TDG_TRY(mgk(launch_mg_bsr_apply(op->h.E, mg.NB, L.bs, mg.nbr, L.A, mg.cp, nullptr, mg.cq, s), "coarse A"));
+            TDG_TRY(dots<double>(sp, mg.cp, mg.cq, nullptr, nullptr, mg.partial, mg.scal, kPQ, -1, s));
+            k_cg_xr<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, mg.cr, mg.cp, mg.cq, mg.scal);
+            TDG_TRY(mgk(launch_bjac_apply<double, double>(L.bs, op->h.E, mg.cinv, mg.cr, mg.cz, 1, L.n, s), "coarse PC"));
+            TDG_TRY(dots<double>(sp, mg.cr, mg.cz, mg.cr, mg.cr, mg.partial, mg.scal, kRZnew, kRR, s));
+            k_cg_p<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, mg.cp, mg.cz, mg.scal);
+            k_cg_shift<<<1, 128, 0, s>>>(mg.scal, 1);
+        }
+        it += 4;
+        TDG_TRY(mg_read_scalars(op, hs, s));
+        if (!std::isfinite(hs[kRR])) return fail(TDG_E_DIVERGED, "multigrid: coarse CG diverged");
+        if (hs[kRR] <= tol2) break;
+    }
+    mg.coarse_its += it;
+    return 0;
+}
+
+// One V-cycle on level l: x = M_l b.
+int mg_vcycle(tdg_op* op, int l, const double* b, double* x, cudaStream_t s) {
+    if (l == 0) return mg_coarse_solve(op, b, x, s);
+    auto& mg = op->mg;
+    auto& L = mg.lv[static_cast<size_t>(l)];
+    auto& C = mg.lv[static_cast<size_t>(l - 1)];
+    const int64_t E = op->h.E;
+    TDG_TRY(mg_smooth(op, l, b, x, true, s));
+    TDG_TRY(mg_level_apply(op, l, x, L.r, b, s));
+    TDG_TRY(mgk(launch_mg_restrict(E, C.ip, L.r, C.b, s), "restriction"));
+    TDG_TRY(mg_vcycle(op, l - 1, C.b, C.x, s));
+    TDG_TRY(mgk(launch_mg_prolong_add(E, C.ip, C.x, x, s), "prolongation"));
+    return mg_smooth(op, l, b, x, false, s);
+}
+
+// Largest eigenvalue of the symmetric tridiagonal matrix (a diagonal, c off-diagonal) by Sturm
+// bisection.
+double tridiag_lmax(std::vector<double> const& a, std::vector<double> const& c) {
+    const size_t m = a.size();
+    double lo = std::numeric_limits<double>::max(), hi = -lo;
+    for (size_t i = 0; i < m; ++i) {
+        const double r = (i > 0 ? std::fabs(c[i - 1]) : 0.0) + (i + 1 < m ? std::fabs(c[i]) : 0.0);
+        lo = std::min(lo, a[i] - r);
+        hi = std::max(hi, a[i] + r);
+    }
+    auto count_below = [&](double x) {  // eigenvalues < x
+        int cnt = 0;
+        double d = 1.0;
+        for (size_t i = 0; i < m; ++i) {
+            d = a[i] - x - (i > 0 ? c[i - 1] * c[i - 1] / d : 0.0);
+            if (d == 0.0) d = -1e-300;
+            if (d < 0.0) ++cnt;
+        }
+        return cnt;
+    };
+    for (int it = 0; it < 200 && hi - lo > 1e-14 * std::max(1.0, std::fabs(hi)); ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (count_below(mid) >= static_cast<int>(m)) hi = mid;
+        else lo = mid;
+    }
+    return hi;
+}
+
+// lambda_max(D^-1 A_l) from esteig_steps Jacobi-preconditioned CG (Lanczos) steps on a seeded
+// random right-hand side: the Lanczos tridiagonal T has diagonal 1/alpha_k + beta_{k-1}/alpha_{k-1}
+// and off-diagonal sqrt(beta_k)/alpha_k.
+int mg_estimate_lmax(tdg_op* op, int l, cudaStream_t s) {
+    auto& mg = op->mg;
+    auto& L = mg.lv[static_cast<size_t>(l)];
+    const int64_t n = L.n;
+    double* r = L.r;
+    double* p = L.d;
+    double* q = L.y;
+    double* z = L.w;
+    double* dsc = mg.partial + kDotBlocks;
+    auto dot = [&](const double* a, const double* b, double* out) -> int {
+        TDG_TRY(mgk(launch_vec_dot(n, a, b, mg.partial, dsc, s), "dot"));
+        TDG_CUDA_TRY(cudaMemcpyAsync(out, dsc, sizeof(double), cudaMemcpyDeviceToHost, s));
+        TDG_CUDA_TRY(cudaStreamSynchronize(s));
+        return 0;
+    };
+    TDG_TRY(mgk(launch_vec_random(n, 0x7a6d3c1b5e9f2d41ull + static_cast<uint64_t>(l), r, s), "random"));
+    TDG_TRY(mgk(launch_vec_mul(n, L.dinv, r, z, s), "jacobi"));
+    TDG_TRY(mgk(launch_vec_axpby(n, 1.0, z, 0.0, p, s), "copy"));
+    double rz = 0.0;
+    TDG_TRY(dot(r, z, &rz));
+    std::vector<double> alpha, beta;
+    for (int k = 0; k < mg.opts.esteig_steps && rz > 0.0; ++k) {
+        TDG_TRY(mg_level_apply(op, l, p, q, nullptr, s));
+        double pq = 0.0;
+        TDG_TRY(dot(p, q, &pq));
+        if (!(pq > 0.0)) break;
+        const double a = rz / pq;
+        TDG_TRY(mgk(launch_vec_axpby(n, -a, q, 1.0, r, s), "axpy"));
+        TDG_TRY(mgk(launch_vec_mul(n, L.dinv, r, z, s), "jacobi"));
+        double rz1 = 0.0;
+        TDG_TRY(dot(r, z, &rz1));
+        const double bta = rz1 / rz;
+        alpha.push_back(a);
+        beta.push_back(bta);
+        TDG_TRY(mgk(launch_vec_axpby(n, 1.0, z, bta, p, s), "xpay"));
+        rz = rz1;
+    }
+    if (alpha.empty()) return fail(TDG_E_NOT_SPD, "multigrid: the level operator is not positive definite");
+    const size_t m = alpha.size();
+    std::vector<double> a(m), c(m > 1 ? m - 1 : 0);
+    for (size_t k = 0; k < m; ++k) {
+        a[k] = 1.0 / alpha[k] + (k > 0 ? beta[k - 1] / alpha[k - 1] : 0.0);
+        if (k + 1 < m) c[k] = std::sqrt(beta[k]) / alpha[k];
+    }
+    L.lmax = tridiag_lmax(a, c);
+    if (!(L.lmax > 0.0) || !std::isfinite(L.lmax)) return fail(TDG_E_NOT_SPD, "multigrid: bad eigenvalue estimate");
+    return 0;
+}
+
+// The first coarse level's Galerkin operator I^T A I by probing the matrix-free operator: for each
+// colour and each coarse basis column j, one multi-RHS apply of the interpolated unit columns on
+// all elements of that colour.
+int mg_probe(tdg_op* op, cudaStream_t s) {
+    auto& mg = op->mg;
+    const size_t nl = mg.lv.size();
+    auto& C = mg.lv[nl - 2];
+    const int64_t nf = mg.lv[nl - 1].n, E = op->h.E;
+    const int nj = std::min(C.bs, 16);
+    double *V = nullptr, *Y = nullptr;
+    TDG_CUDA_TRY(cudaMalloc(&V, sizeof(double) * nj * nf));
+    cudaError_t ce = cudaMalloc(&Y, sizeof(double) * nj * nf);
+    if (ce != cudaSuccess) {
+        cudaFree(V);
+        return fail(TDG_E_NOMEM, "multigrid: probe vectors");
+    }
+    int rc = 0;
+    for (int c = 0; c < mg.ncolours && rc == 0; ++c)
+        for (int j0 = 0; j0 < C.bs && rc == 0; j0 += nj) {
+            const int nb = std::min(nj, C.bs - j0);
+            if (cudaMemsetAsync(V, 0, sizeof(double) * nb * nf, s) != cudaSuccess) rc = fail(TDG_E_CUDA, "memset");
+            if (!rc) rc = mgk(launch_mg_probe_fill(E, mg.colour, c, C.ip, j0, nb, V, nf, s), "probe fill");
+            if (!rc) rc = tdg_apply(op, TDG_FP64, V, Y, nb, nf, s);
+            if (!rc)
+                rc = mgk(launch_mg_probe_extract(E, mg.NB, mg.nbr, mg.colour, c, C.ip, j0, nb, Y, nf, C.A, s),
+                         "probe extract");
+        }
+    cudaStreamSynchronize(s);
+    cudaFree(V);
+    cudaFree(Y);
+    return rc;
+}
+
+int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
+    auto& h = op->h;
+    auto& mg = op->mg;
+    if (o.smooth_its <= 0) o.smooth_its = 10;
+    if (!(o.esteig_lo > 0.0)) o.esteig_lo = 0.01;
+    if (!(o.esteig_hi > 0.0)) o.esteig_hi = 1.1;
+    if (o.esteig_steps <= 0) o.esteig_steps = 10;
+    if (!(o.coarse_rtol > 0.0)) o.coarse_rtol = 0.1;
+    if (o.coarse_max_it <= 0) o.coarse_max_it = 1000;
+    if (o.coarse_degree < 0) o.coarse_degree = 1;
+    if (o.smooth_precision != TDG_MIXED) o.smooth_precision = TDG_FP64;
+    if (o.strategy < 0 || o.strategy > 2) return fail(TDG_E_INVALID, "multigrid: unknown strategy");
+    if (!(o.esteig_lo < o.esteig_hi)) return fail(TDG_E_INVALID, "multigrid: esteig_lo must be below esteig_hi");
+    if (!h.has_material) return fail(TDG_E_STATE, "multigrid: tdg_set_material first");
+    std::vector<int> deg;
+    try {
+        deg = mg_level_degrees(o.strategy, o.coarse_degree, h.N);
+    } catch (std::exception const& e) {
+        return fail(TDG_E_INVALID, e.what());
+    }
+    if (deg.size() < 2) return fail(TDG_E_INVALID, "multigrid: needs at least two levels");
+    // a fresh hierarchy
+    mg.arena.release();
+    mg.lv.clear();
+    mg.ready = false;
+    mg.coarse_its = 0;
+    mg.opts = o;
+    mg.fine_prec = o.smooth_precision;
+    TDG_TRY(ensure_uploaded(op, TDG_FP64));
+    if (mg.fine_prec == TDG_MIXED) TDG_TRY(ensure_uploaded(op, TDG_FP32));
+    TDG_TRY(ensure_blocks(op, s));
+    const int64_t E = h.E;
+    mg.NB = 1 + h.nfaces;
+    std::vector<int32_t> nbr = element_neighbours(h);
+    std::vector<int32_t> col = distance2_colouring(nbr, E, mg.NB, &mg.ncolours);
+    const int32_t* dn = nullptr;
+    const int32_t* dc = nullptr;
+    TDG_CUDA_TRY(mg.arena.upload(&dn, nbr));
+    TDG_CUDA_TRY(mg.arena.upload(&dc, col));
+    mg.nbr = const_cast<int32_t*>(dn);
+    mg.colour = const_cast<int32_t*>(dc);
+    const int nl = static_cast<int>(deg.size());
+    mg.lv.resize(static_cast<size_t>(nl));
+    for (int l = 0; l < nl; ++l) {
+        auto& L = mg.lv[static_cast<size_t>(l)];
+        L.degree = deg[static_cast<size_t>(l)];
+        L.bs = num_basis(h.D, L.degree) * h.Q;
+        L.n = E * L.bs;
+        const size_t n = static_cast<size_t>(L.n);
+        if (l + 1 < nl) {
+            TDG_CUDA_TRY(mg.arena.alloc(&L.A, static_cast<size_t>(E) * mg.NB * L.bs * L.bs));
+            TDG_CUDA_TRY(cudaMemsetAsync(L.A, 0, sizeof(double) * E * mg.NB * L.bs * L.bs, s));
+            TDG_CUDA_TRY(mg.arena.alloc(&L.x, n));
+            TDG_CUDA_TRY(mg.arena.alloc(&L.b, n));
+            Dense I = interpolation_matrix(h.D, h.kind, deg[static_cast<size_t>(l + 1)], L.degree);
+            const double* dI = nullptr;
+            TDG_CUDA_TRY(mg.arena.upload(&dI, I.a));
+            L.ip = MgInterp{dI, I.rows, I.cols, h.Q};
+        }
+        TDG_CUDA_TRY(mg.arena.alloc(&L.dinv, n));
+        TDG_CUDA_TRY(mg.arena.alloc(&L.r, n));
+        TDG_CUDA_TRY(mg.arena.alloc(&L.d, n));
+        TDG_CUDA_TRY(mg.arena.alloc(&L.y, n));
+        TDG_CUDA_TRY(mg.arena.alloc(&L.w, n));
+    }
+    // dot partials: the level dots (kDotBlocks + a result slot) and the coarsest CG's chunk pairs
+    const size_t nchunk_max = static_cast<size_t>(mg.lv[0].n / kChunk) + 2;
+    TDG_CUDA_TRY(mg.arena.alloc(&mg.partial, std::max<size_t>(kDotBlocks + 8, 2 * nchunk_max)));
+    TDG_CUDA_TRY(mg.arena.alloc(&mg.status, 1));
+    TDG_CUDA_TRY(cudaMemsetAsync(mg.status, 0, sizeof(int), s));
+    // Galerkin operators: probing below the finest level, triple products further down
+    TDG_TRY(mg_probe(op, s));
+    for (int l = nl - 3; l >= 0; --l)
+        TDG_TRY(mgk(launch_mg_triple(E, mg.NB, mg.nbr, mg.lv[static_cast<size_t>(l)].ip,
+                                     mg.lv[static_cast<size_t>(l + 1)].A, mg.lv[static_cast<size_t>(l)].A, s),
+                    "Galerkin triple product"));
+    // point-Jacobi diagonals
+    for (int l = 0; l < nl; ++l) {
+        auto& L = mg.lv[static_cast<size_t>(l)];
+        if (l + 1 == nl)
+            TDG_TRY(mgk(launch_mg_diag_inv(E, L.bs, static_cast<int64_t>(L.bs) * L.bs, op->blk, L.dinv, mg.status, s),
+                        "diagonal"));
+        else
+            TDG_TRY(mgk(launch_mg_diag_inv(E, L.bs, static_cast<int64_t>(mg.NB) * L.bs * L.bs, L.A, L.dinv, mg.status, s),
+                        "diagonal"));
+    }
+    // coarsest level: block-Jacobi inverses, CG vectors and plan
+    auto& L0 = mg.lv[0];
+    {
+        double* blk0 = nullptr;
+        TDG_CUDA_TRY(cudaMalloc(&blk0, sizeof(double) * E * L0.bs * L0.bs));
+        int rc = mgk(launch_mg_self_blocks(E, mg.NB, L0.bs, L0.A, blk0, s), "coarse blocks");
+        if (!rc) {
+            cudaError_t ce = mg.arena.alloc(&mg.cinv, static_cast<size_t>(E) * L0.bs * L0.bs);
+            rc = ce == cudaSuccess ? 0 : fail(TDG_E_NOMEM, "multigrid: coarse inverses");
+        }
+        if (!rc) rc = mgk(launch_bjac_invert<double>(L0.bs, E, blk0, mg.cinv, mg.status, s), "coarse inversion");
+        cudaStreamSynchronize(s);
+        cudaFree(blk0);
+        if (rc) return rc;
+    }
+    int st = 0;
+    TDG_CUDA_TRY(cudaMemcpyAsync(&st, mg.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TDG_CUDA_TRY(cudaStreamSynchronize(s));
+    if (st) return fail(TDG_E_NOT_SPD, "multigrid: a level diagonal or coarse block is not positive definite");
+    for (double** v : {&mg.cr, &mg.cz, &mg.cp, &mg.cq}) TDG_CUDA_TRY(mg.arena.alloc(v, static_cast<size_t>(L0.n)));
+    {
+        std::vector<Chunk> hc;
+        std::vector<int> hsc;
+        plan_chunks({0}, {L0.n}, hc, hsc);
+        const Chunk* dch = nullptr;
+        const int* dsc = nullptr;
+        TDG_CUDA_TRY(mg.arena.upload(&dch, hc));
+        TDG_CUDA_TRY(mg.arena.upload(&dsc, hsc));
+        mg.chunks = const_cast<Chunk*>(dch);
+        mg.seg_chunk = const_cast<int*>(dsc);
+        mg.nchunks = static_cast<int>(hc.size());
+        TDG_CUDA_TRY(mg.arena.alloc(&mg.scal, static_cast<size_t>(kScal)));
+    }
+    // Chebyshev bounds of the smoothed levels
+    for (int l = 1; l < nl; ++l) TDG_TRY(mg_estimate_lmax(op, l, s));
+    mg.ready = true;
+    return 0;
+}
+
+int mg_apply(tdg_op* op, const double* r, double* z, int nrhs, int64_t ld, cudaStream_t s) {
+    auto& mg = op->mg;
+    if (!mg.ready) return fail(TDG_E_STATE, "tdg_mg_setup not called");
+    if (nrhs < 1 || ld < mg.lv.back().n) return fail(TDG_E_INVALID, "nrhs < 1 or ld < E * bs");
+    const int top = static_cast<int>(mg.lv.size()) - 1;
+    for (int k = 0; k < nrhs; ++k) TDG_TRY(mg_vcycle(op, top, r + k * ld, z + k * ld, s));
+    return 0;
+}
+
+// z = M r with the preconditioner the solves use (multigrid for FP64 vectors when selected).
+template <typename T>
+int precondition(tdg_op* op, int prec, const T* r, T* z, int nrhs, int64_t ld, cudaStream_t s) {
+    if constexpr (std::is_same_v<T, double>) {
+        if (op->pc == TDG_PC_MG) return mg_apply(op, r, z, nrhs, ld, s);
+    }
+    return tdg_bjacobi_apply(op, prec, r, z, nrhs, ld, s);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------------------
@@ -667,16 +1086,10 @@ int tdg_bjacobi_setup(tdg_op* op, int precision, void* stream) {
     if (!op) return fail(TDG_E_INVALID, "null operator");
     if (precision == TDG_MIXED) precision = TDG_FP32;  // FP32 inverses (the lighter mixed preconditioner)
     if (precision != TDG_FP64 && precision != TDG_FP32) return fail(TDG_E_INVALID, "bad precision");
-    TDG_TRY(ensure_uploaded(op, TDG_FP64));
     auto const& h = op->h;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t nblk = static_cast<size_t>(h.E) * h.bs * h.bs;
-    if (!op->blk) {
-        TDG_CUDA_TRY(op->arena_pc.alloc(&op->blk, nblk));
-        TDG_CUDA_TRY(op->arena_pc.alloc(&op->status, 1));
-        int rc = launch_bjac_assemble(h.D, h.N, h.kind, op->op64, op->blk, s);
-        if (rc) return fail(rc, "block assembly launch failed");
-    }
+    TDG_TRY(ensure_blocks(op, s));
     if (op->inv && op->inv_precision == precision) return 0;
     if (op->inv) {
         // switching precision: re-allocate (arena keeps the old buffer until release)
@@ -804,80 +1217,21 @@ struct CgVectors {
     T *r, *z, *p, *q;
 };
 
-// One preconditioned CG iteration on (A_T, M_T) with device-resident scalars.
+// One preconditioned CG iteration on (A_T, M_T) with device-resident scalars; with the multigrid
+// preconditioner the flexible CG step (beta from z_new . q).
 template <typename T>
 int cg_iteration(tdg_op* op, int prec, SegPlan const& sp, T* x, CgVectors<T> v, double* partial, double* scal,
                  cudaStream_t s) {
+    const bool flexible = op->pc == TDG_PC_MG;
     TDG_TRY(tdg_apply(op, prec, v.p, v.q, sp.op_nrhs, sp.op_ld, s));
     TDG_TRY(dots<T>(sp, v.p, v.q, nullptr, nullptr, partial, scal, kPQ, -1, s));
     k_cg_xr<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, v.r, v.p, v.q, scal);
-    TDG_TRY(tdg_bjacobi_apply(op, prec, v.r, v.z, sp.op_nrhs, sp.op_ld, s));
+    TDG_TRY(precondition<T>(op, prec, v.r, v.z, sp.op_nrhs, sp.op_ld, s));
     TDG_TRY(dots<T>(sp, v.r, v.z, v.r, v.r, partial, scal, kRZnew, kRR, s));
-    k_cg_p<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, v.p, v.z, scal);
+    if (flexible) TDG_TRY(dots<T>(sp, v.z, v.q, nullptr, nullptr, partial, scal, kZQ, -1, s));
+    k_cg_p<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, v.p, v.z, scal, flexible ? 1 : 0);
     k_cg_shift<<<(sp.nseg + 127) / 128, 128, 0, s>>>(scal, sp.nseg);
     return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "CG update kernels");
-}
-
-// Runs CG iterations until every active segment reaches sqrt(rr) <= tol_abs[seg] or the budget
-// is spent.  Convergence is checked every kCheck iterations; iteration blocks after the first are
-// replayed from a CUDA graph when graphs are enabled (stream != legacy default).
-template <typename T>
-int cg_loop(tdg_op* op, int prec, SegPlan const& sp, T* x, CgVectors<T> v, double* partial, double* scal,
-            std::vector<double> const& tol_abs, int max_it, bool graphs, cudaStream_t s, int* iters, bool* diverged) {
-    constexpr int kCheck = 8;
-    std::vector<double> hs(static_cast<size_t>(sp.nseg) * kScal);
-    cudaGraphExec_t exec = nullptr;
-    int done = 0;
-    *diverged = false;
-    int rc = 0;
-    for (;;) {
-        TDG_CUDA_TRY(cudaMemcpyAsync(hs.data(), scal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-        TDG_CUDA_TRY(cudaStreamSynchronize(s));
-        bool any = false, changed = false;
-        for (int r = 0; r < sp.nseg; ++r) {
-            double* sr = &hs[static_cast<size_t>(r) * kScal];
-            if (sr[kActive] == 0.0) continue;
-            const double rr = sr[kRR];
-            if (!std::isfinite(rr)) {
-                *diverged = true;
-                sr[kActive] = 0.0;
-                changed = true;
-                continue;
-            }
-            if (std::sqrt(rr) <= tol_abs[r]) {
-                sr[kActive] = 0.0;
-                changed = true;
-                continue;
-            }
-            any = true;
-        }
-        if (changed)
-            TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        if (!any || done >= max_it) break;
-        const bool use_graph = graphs && s != nullptr && done >= kCheck;
-        if (use_graph && !exec) {
-            cudaGraph_t graph = nullptr;
-            TDG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            for (int i = 0; i < kCheck && rc == 0; ++i) rc = cg_iteration<T>(op, prec, sp, x, v, partial, scal, s);
-            cudaError_t ce = cudaStreamEndCapture(s, &graph);
-            if (rc) {
-                if (graph) cudaGraphDestroy(graph);
-                return rc;
-            }
-            TDG_CUDA_TRY(ce);
-            TDG_CUDA_TRY(cudaGraphInstantiate(&exec, graph, 0));
-            cudaGraphDestroy(graph);
-        }
-        if (exec) {
-            TDG_CUDA_TRY(cudaGraphLaunch(exec, s));
-        } else {
-            for (int i = 0; i < kCheck; ++i) TDG_TRY(cg_iteration<T>(op, prec, sp, x, v, partial, scal, s));
-        }
-        done += kCheck;
-    }
-    if (exec) cudaGraphExecDestroy(exec);
-    *iters = done;
-    return 0;
 }
 
 // r = b - A x (FP64); per-segment ||r|| and ||b|| on the host.
@@ -905,7 +1259,7 @@ int cg_start(tdg_op* op, int prec, SegPlan const& sp, CgVectors<T> v, double* pa
     std::vector<double> hs(static_cast<size_t>(sp.nseg) * kScal, 0.0);
     for (int i = 0; i < sp.nseg; ++i) hs[static_cast<size_t>(i) * kScal + kActive] = active[i];
     TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-    TDG_TRY(tdg_bjacobi_apply(op, prec, v.r, v.z, sp.op_nrhs, sp.op_ld, s));
+    TDG_TRY(precondition<T>(op, prec, v.r, v.z, sp.op_nrhs, sp.op_ld, s));
     k_copy<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, v.z, v.p);
     TDG_TRY(dots<T>(sp, v.r, v.z, v.r, v.r, partial, scal, kRZ, kRR, s));
     return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "CG start");
@@ -969,7 +1323,11 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
                  int max_updates, bool graphs, cudaStream_t s, std::vector<double>& rn, std::vector<double>& bn,
                  int* iters, int* updates, bool* diverged) {
     constexpr bool kLow = !std::is_same_v<T, double>;
-    constexpr int kCheck = 8;
+    // the multigrid preconditioner synchronises with the host (coarse CG), so its iterations are
+    // neither captured in graphs nor batched between checks
+    const bool mg = op->pc == TDG_PC_MG;
+    const int kCheck = mg ? 1 : 8;
+    graphs = graphs && !mg;
     const int nseg = sp.nseg;
     if (max_updates <= 0) max_updates = 1 << 20;
     std::vector<double> tol(nseg), act(nseg), rmax(nseg), best(nseg);
@@ -1091,8 +1449,9 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
                     }
                 }
                 // the recurrence residual fell below the true one: its search direction no longer
-                // matches the replaced residual, restart it
-                if (!(rn[i] <= 2.0 * rrec)) sr[kTmp] = 1.0;
+                // matches the replaced residual, restart it (always with the flexible step, whose
+                // direction recurrence the rebuild does not follow)
+                if (mg || !(rn[i] <= 2.0 * rrec)) sr[kTmp] = 1.0;
                 rmax[i] = rn[i];
             }
             any = true;
@@ -1108,7 +1467,7 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
         k_replace_residual<double, T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, rt, rh, scal);
         // z_new = M r into q (free between iterations; for T = double its true residual is
         // consumed above), rz_new, rr; the unflagged segments get z_new = z and are left as is
-        if ((rc = tdg_bjacobi_apply(op, prec, rh, v.q, sp.op_nrhs, sp.op_ld, s))) break;
+        if ((rc = precondition<T>(op, prec, rh, v.q, sp.op_nrhs, sp.op_ld, s))) break;
         if ((rc = dots<T>(sp, rh, v.q, rh, rh, partial, scal, kRZnew, kRR, s))) break;
         k_replace_dir<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, v.p, v.z, v.q, scal);
         k_cg_shift<<<(nseg + 127) / 128, 128, 0, s>>>(scal, nseg, 1);
@@ -1126,9 +1485,13 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
                    const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel, cudaStream_t s) {
     const int prec = opts->precision;
     if (prec != TDG_FP64 && prec != TDG_FP32 && prec != TDG_MIXED) return fail(TDG_E_INVALID, "bad precision");
-    // FP64 needs FP64 inverses, FP32 needs FP32 inverses, MIXED takes either
-    if (!op->inv || (prec != TDG_MIXED && op->inv_precision != prec))
+    if (op->pc == TDG_PC_MG) {
+        if (!op->mg.ready) return fail(TDG_E_STATE, "tdg_mg_setup must be called before a multigrid solve");
+        if (prec == TDG_FP32) return fail(TDG_E_INVALID, "the multigrid preconditioner needs TDG_FP64 or TDG_MIXED");
+    } else if (!op->inv || (prec != TDG_MIXED && op->inv_precision != prec)) {
+        // FP64 needs FP64 inverses, FP32 needs FP32 inverses, MIXED takes either
         return fail(TDG_E_STATE, "tdg_bjacobi_setup must be called with the solve precision");
+    }
     TDG_TRY(ensure_uploaded(op, TDG_FP64));
     if (prec != TDG_FP64) TDG_TRY(ensure_uploaded(op, TDG_FP32));
     std::memset(stats, 0, sizeof(*stats));
@@ -1191,8 +1554,12 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     if (prec == TDG_FP64 || prec == TDG_MIXED) {
         // FP64 recurrence: the recurrence residual is r64 itself and x accumulates directly; the
         // mixed mode applies the operator in FP32 arithmetic and the FP32 inverses, so its
-        // recurrence residual drifts from the true one and is replaced more often
-        const double delta = opts->inner_rtol > 0 ? opts->inner_rtol : 0.1;
+        // recurrence residual drifts from the true one and is replaced more often.  Multigrid
+        // needs few iterations per decade and restarts at every replacement, so it replaces
+        // rarely (FP64: drift-free up to the convergence test)
+        const double delta = opts->inner_rtol > 0 ? opts->inner_rtol
+                             : op->pc == TDG_PC_MG ? (prec == TDG_FP64 ? 1e-4 : 1e-2)
+                                                    : 0.1;
         TDG_TRY((pcg_reliable<double>(op, prec, sp, b, x, x, r64, r64, {r64, z64, p64, q64}, t64, partial, scal,
                                       rtol, delta, max_it, opts->max_outer, graphs, s, rn, bn, &total_it, &updates,
                                       &diverged)));
@@ -1276,6 +1643,90 @@ extern "C" int tdg_solve_segmented(tdg_op* op, const double* b, double* x, int n
     }
     return solve_segments(op, b, x, sb, se, 1, h.E * h.bs, static_cast<size_t>(h.E) * h.bs, opts, stats,
                           seg_rel_residual, static_cast<cudaStream_t>(stream));
+}
+
+// ---- p-multigrid ---------------------------------------------------------------------------------
+
+extern "C" int tdg_mg_setup(tdg_op* op, const tdg_mg_opts* opts, void* stream) {
+    if (!op) return fail(TDG_E_INVALID, "null operator");
+    tdg_mg_opts o{};
+    if (opts) {
+        o = *opts;
+    } else {
+        o.strategy = TDG_MG_LOGARITHMIC;
+        o.coarse_degree = 1;
+    }
+    try {
+        return mg_setup(op, o, static_cast<cudaStream_t>(stream));
+    } catch (std::exception const& e) {
+        op->mg.ready = false;
+        return fail(TDG_E_INVALID, std::string("multigrid set-up: ") + e.what());
+    }
+}
+
+extern "C" int tdg_mg_apply(tdg_op* op, const double* r, double* z, int nrhs, int64_t ld, void* stream) {
+    if (!op || !r || !z) return fail(TDG_E_INVALID, "null argument");
+    return mg_apply(op, r, z, nrhs, ld, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int tdg_set_preconditioner(tdg_op* op, int pc) {
+    if (!op) return fail(TDG_E_INVALID, "null operator");
+    if (pc != TDG_PC_BJACOBI && pc != TDG_PC_MG) return fail(TDG_E_INVALID, "unknown preconditioner");
+    op->pc = pc;
+    return 0;
+}
+
+extern "C" int tdg_mg_info(tdg_op* op, int* nlevels, int max_levels, int* degrees, int* block_sizes,
+                           double* lambda_max, int64_t* coarse_its) {
+    if (!op) return fail(TDG_E_INVALID, "null operator");
+    auto const& mg = op->mg;
+    if (!mg.ready) return fail(TDG_E_STATE, "tdg_mg_setup not called");
+    const int nl = static_cast<int>(mg.lv.size());
+    if (nlevels) *nlevels = nl;
+    for (int l = 0; l < std::min(nl, max_levels); ++l) {
+        if (degrees) degrees[l] = mg.lv[static_cast<size_t>(l)].degree;
+        if (block_sizes) block_sizes[l] = mg.lv[static_cast<size_t>(l)].bs;
+        if (lambda_max) lambda_max[l] = mg.lv[static_cast<size_t>(l)].lmax;
+    }
+    if (coarse_its) *coarse_its = mg.coarse_its;
+    return 0;
+}
+
+extern "C" int tdg_mg_level_matrix(tdg_op* op, int level, double* blocks, int32_t* nbr) {
+    if (!op) return fail(TDG_E_INVALID, "null operator");
+    auto const& mg = op->mg;
+    if (!mg.ready) return fail(TDG_E_STATE, "tdg_mg_setup not called");
+    if (level < 0 || level + 1 >= static_cast<int>(mg.lv.size()))
+        return fail(TDG_E_INVALID, "level must be a coarse (block-sparse) level");
+    auto const& L = mg.lv[static_cast<size_t>(level)];
+    const size_t E = static_cast<size_t>(op->h.E);
+    TDG_CUDA_TRY(cudaDeviceSynchronize());
+    if (blocks)
+        TDG_CUDA_TRY(cudaMemcpy(blocks, L.A, sizeof(double) * E * mg.NB * L.bs * L.bs, cudaMemcpyDeviceToHost));
+    if (nbr) TDG_CUDA_TRY(cudaMemcpy(nbr, mg.nbr, sizeof(int32_t) * E * mg.NB, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+extern "C" int tdg_mg_level_degrees(int strategy, int coarse_degree, int degree, int* degrees) {
+    try {
+        std::vector<int> d = mg_level_degrees(strategy, coarse_degree, degree);
+        if (degrees) std::copy(d.begin(), d.end(), degrees);
+        return static_cast<int>(d.size());
+    } catch (std::exception const& e) {
+        return fail(TDG_E_INVALID, e.what());
+    }
+}
+
+extern "C" int tdg_mg_interpolation(int dim, int kind, int n_to, int n_from, double* out) {
+    if (!out || dim < 2 || dim > 3 || (kind != TDG_POISSON && kind != TDG_ELASTICITY))
+        return fail(TDG_E_INVALID, "bad argument");
+    try {
+        Dense I = interpolation_matrix(dim, kind, n_to, n_from);
+        std::copy(I.a.begin(), I.a.end(), out);
+        return 0;
+    } catch (std::exception const& e) {
+        return fail(TDG_E_INVALID, e.what());
+    }
 }
 
 // ------------------------------------------------------------------------------------------------

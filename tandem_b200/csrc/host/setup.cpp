@@ -506,4 +506,79 @@ int64_t HostOperator::bytes_apply(int s) const {
     return E * per_el * s + F * (per_f * s + 20);
 }
 
+// ---- p-multigrid set-up ----------------------------------------------------------------------
+
+Dense interpolation_matrix(int D, int kind, int n_to, int n_from) {
+    if (n_to <= n_from || n_from < 0) throw std::invalid_argument("interpolation needs n_to > n_from >= 0");
+    const int N1 = num_basis(D, n_to), N2 = num_basis(D, n_from);
+    Dense I(N1, N2);
+    if (kind == kPoisson) {
+        // graded Dubiner ordering: the first N2 modal functions span the degree-n_from space
+        for (int l = 0; l < N2; ++l) I(l, l) = 1.0;
+        return I;
+    }
+    RefSpace coarse = RefSpace::nodal(D, n_from, warp_blend_nodes(D, n_from));
+    Dense Ec = coarse.eval(warp_blend_nodes(D, n_to));  // [N2][N1]: coarse basis l at fine node k
+    for (int k = 0; k < N1; ++k)
+        for (int l = 0; l < N2; ++l) I(k, l) = Ec(l, k);
+    return I;
+}
+
+std::vector<int> mg_level_degrees(int strategy, int coarse, int N) {
+    if (N <= coarse) coarse = N > 0 ? N - 1 : 0;
+    std::vector<int> lv;
+    if (strategy == 0) {
+        lv = {coarse, N};
+    } else if (strategy == 1) {
+        lv.push_back(N);
+        while (lv.back() > coarse) lv.push_back(lv.back() / 2);
+        if (lv.back() != coarse) lv.back() = coarse;
+        std::reverse(lv.begin(), lv.end());
+    } else if (strategy == 2) {
+        for (int d = coarse; d <= N; ++d) lv.push_back(d);
+    } else {
+        throw std::invalid_argument("unknown multigrid strategy");
+    }
+    return lv;
+}
+
+std::vector<int32_t> element_neighbours(HostOperator const& h) {
+    const int NB = 1 + h.nfaces;
+    std::vector<int32_t> nbr(static_cast<size_t>(h.E) * NB, -1);
+    for (int64_t e = 0; e < h.E; ++e) {
+        nbr[static_cast<size_t>(e) * NB] = static_cast<int32_t>(e);
+        for (int f = 0; f < h.nfaces; ++f) {
+            const Side& s = h.sides[static_cast<size_t>(e) * h.nfaces + f];
+            if (s.nb != e) nbr[static_cast<size_t>(e) * NB + 1 + f] = s.nb;
+        }
+    }
+    return nbr;
+}
+
+std::vector<int32_t> distance2_colouring(std::vector<int32_t> const& nbr, int64_t E, int NB, int* ncolors) {
+    std::vector<int32_t> col(static_cast<size_t>(E), -1);
+    std::vector<int64_t> stamp;  // stamp[c] == e: colour c is taken near element e
+    int nc = 0;
+    for (int64_t e = 0; e < E; ++e) {
+        auto mark = [&](int32_t t) {
+            if (t >= 0 && col[t] >= 0) stamp[col[t]] = e;
+        };
+        for (int a = 0; a < NB; ++a) {
+            const int32_t n = nbr[static_cast<size_t>(e) * NB + a];
+            if (n < 0) continue;
+            mark(n);
+            for (int b = 1; b < NB; ++b) mark(nbr[static_cast<size_t>(n) * NB + b]);
+        }
+        int c = 0;
+        while (c < nc && stamp[c] == e) ++c;
+        if (c == nc) {
+            stamp.push_back(-1);
+            ++nc;
+        }
+        col[e] = c;
+    }
+    *ncolors = nc;
+    return col;
+}
+
 }  // namespace tdg

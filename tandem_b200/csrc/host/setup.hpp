@@ -90,4 +90,27 @@ struct HostOperator {
     int64_t bytes_apply(int scalar_bytes) const;
 };
 
+// ---- p-multigrid set-up (tandem's PCMG path, app/common/PetscLinearSolver.cpp:53-114) ----------
+
+// Reference interpolation from degree n_from to degree n_to > n_from, [Nbf(n_to)][Nbf(n_from)]
+// per component (the element interpolation is block diagonal over components).  Modal spaces
+// (Poisson): injection of the first Nbf(n_from) Dubiner coefficients (ModalInterpolation.h:40-44).
+// Nodal spaces (Elasticity): the coarse Lagrange basis at the fine warp & blend nodes, which is
+// V_to[:, :N2] V_from^-1 (NodalInterpolation.cpp:8-36).  Both embed the coarse space exactly.
+Dense interpolation_matrix(int D, int kind, int n_to, int n_from);
+
+// Polynomial degrees of the levels, coarsest first (MGConfig::levels, app/common/MGConfig.cpp:11-41):
+// strategy 0 two-level {coarse, N}; 1 logarithmic (N, N/2, ... down to coarse); 2 full
+// (coarse, coarse+1, ..., N).  A coarse degree >= N becomes N - 1.
+std::vector<int> mg_level_degrees(int strategy, int coarse, int N);
+
+// Element neighbours across interior facets: nbr[e][0] = e, nbr[e][1 + f] = the element behind
+// local face f, or -1 on a boundary facet (whose coupling is part of the element's own block).
+std::vector<int32_t> element_neighbours(HostOperator const& h);
+
+// Greedy distance-2 colouring of the element graph: two elements that share a facet or a
+// neighbour get different colours, so every element's closed neighbourhood holds each colour at
+// most once.  Returns the colour per element and sets ncolors.
+std::vector<int32_t> distance2_colouring(std::vector<int32_t> const& nbr, int64_t E, int NB, int* ncolors);
+
 }  // namespace tdg

@@ -63,7 +63,7 @@ int run_bapply(int64_t E, const TM* inv, const TV* r, TV* z, int nrhs, int64_t l
 
 // Block sizes bs = binom(N + D, D) * Q for D in {2, 3}, N in [1, 4], Q in {1, D}.
 #define TDG_FOR_EACH_BS(X) \
-    X(3) X(4) X(6) X(10) X(12) X(15) X(20) X(30) X(35) X(60) X(105)
+    X(1) X(2) X(3) X(4) X(6) X(10) X(12) X(15) X(20) X(30) X(35) X(60) X(105)
 
 }  // namespace
 

@@ -15,9 +15,10 @@
 
 namespace tdg {
 
-constexpr int kScal = 8;
-// kRepl flags the segments whose recurrence residual a reliable update replaces.
-enum ScalSlot { kRZ = 0, kPQ = 1, kRZnew = 2, kRR = 3, kActive = 4, kBB = 5, kTmp = 6, kRepl = 7 };
+constexpr int kScal = 10;
+// kRepl flags the segments whose recurrence residual a reliable update replaces; kZQ holds
+// z_new . q for the flexible CG step.
+enum ScalSlot { kRZ = 0, kPQ = 1, kRZnew = 2, kRR = 3, kActive = 4, kBB = 5, kTmp = 6, kRepl = 7, kZQ = 8 };
 constexpr int kVecThreads = 256;
 constexpr int64_t kChunk = 32 * 1024;
 
@@ -85,16 +86,18 @@ __global__ void __launch_bounds__(kVecThreads)
     }
 }
 
-// p = z + beta p with beta = rz_new / rz of the segment (inactive: no-op).
+// p = z + beta p with beta = rz_new / rz of the segment (inactive: no-op).  flexible: beta =
+// -(z_new . q) / (p . q), the flexible CG step for a preconditioner that varies between
+// iterations (Notay, "Flexible conjugate gradients", SIAM J. Sci. Comput. 22, 2000).
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads)
     k_cg_p(const Chunk* __restrict__ chunks, T* __restrict__ p, const T* __restrict__ z,
-           const double* __restrict__ scal) {
+           const double* __restrict__ scal, int flexible = 0) {
     const Chunk ch = chunks[blockIdx.x];
     const double* s = scal + ch.seg * kScal;
     if (s[kActive] == 0.0) return;
-    const double rz = s[kRZ];
-    const T beta = static_cast<T>(rz != 0.0 ? s[kRZnew] / rz : 0.0);
+    const double rz = s[kRZ], pq = s[kPQ];
+    const T beta = static_cast<T>(flexible ? (pq != 0.0 ? -s[kZQ] / pq : 0.0) : (rz != 0.0 ? s[kRZnew] / rz : 0.0));
     for (int64_t i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) p[i] = z[i] + beta * p[i];
 }
 

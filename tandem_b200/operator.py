@@ -20,6 +20,8 @@ from .mesh import SimplexMesh
 POISSON, ELASTICITY = _ffi.TDG_POISSON, _ffi.TDG_ELASTICITY
 FP64, FP32, MIXED = _ffi.TDG_FP64, _ffi.TDG_FP32, _ffi.TDG_MIXED
 FAMILIES = ("tensor", "simt", "face")
+MG_STRATEGIES = ("twolevel", "logarithmic", "full")  # MGStrategy (app/common/MGConfig.h:8)
+PRECONDITIONERS = ("bjacobi", "mg")
 
 
 def _c(a: np.ndarray, dtype) -> np.ndarray:
@@ -197,6 +199,51 @@ class DGOperator:
         # stored column-major per block: out[e, col, row] -> transpose to [e, row, col]
         return np.ascontiguousarray(out.transpose(0, 2, 1))
 
+    # -- p-multigrid preconditioner (PetscLinearSolver::setup_mg + mg_cheby.cfg) -------------------
+    def mg_setup(self, strategy: str = "logarithmic", coarse_degree: int = 1, smooth_its: int = 10,
+                 esteig: tuple[float, float] = (0.01, 1.1), esteig_steps: int = 10, coarse_rtol: float = 0.1,
+                 coarse_max_it: int = 1000, smooth_precision: int = FP64, stream=None) -> None:
+        """Builds the p-multigrid hierarchy (tdg_mg_setup): levels by MGConfig strategy, Galerkin
+        coarse operators, Chebyshev smoothers on esteig x lambda_max(D^-1 A) with point Jacobi, CG
+        with block Jacobi on the coarsest level.  smooth_precision MIXED runs the finest level's
+        smoother applies in FP32 arithmetic."""
+        o = _ffi.MgOpts(MG_STRATEGIES.index(strategy), coarse_degree, smooth_its, esteig[0], esteig[1],
+                        esteig_steps, coarse_rtol, coarse_max_it, smooth_precision)
+        _ffi.check(_ffi.lib().tdg_mg_setup(self._h, C.byref(o), _stream(stream)))
+
+    def mg_apply(self, r, z, nrhs: int = 1, ld: int | None = None, stream=None) -> None:
+        """z = M r, one multigrid V-cycle per right-hand side (FP64 device vectors)."""
+        ld = self.ndof if ld is None else ld
+        _check_vec(r, FP64, nrhs * ld)
+        _check_vec(z, FP64, nrhs * ld)
+        _ffi.check(_ffi.lib().tdg_mg_apply(self._h, C.c_void_p(r.data_ptr()), C.c_void_p(z.data_ptr()), nrhs, ld,
+                                           _stream(stream)))
+
+    def set_preconditioner(self, pc: str) -> None:
+        """Preconditioner of the solves: "bjacobi" (default) or "mg" (flexible CG around the V-cycle)."""
+        _ffi.check(_ffi.lib().tdg_set_preconditioner(self._h, PRECONDITIONERS.index(pc)))
+
+    def mg_info(self) -> dict:
+        n = C.c_int(0)
+        deg, bs = (C.c_int * 8)(), (C.c_int * 8)()
+        lmax = (C.c_double * 8)()
+        its = C.c_int64(0)
+        _ffi.check(_ffi.lib().tdg_mg_info(self._h, C.byref(n), 8, deg, bs, lmax, C.byref(its)))
+        k = n.value
+        return dict(levels=k, degrees=list(deg[:k]), block_sizes=list(bs[:k]), lambda_max=list(lmax[:k]),
+                    coarse_iterations=its.value)
+
+    def mg_level_matrix(self, level: int) -> tuple[np.ndarray, np.ndarray]:
+        """Galerkin operator of a coarse level: blocks [E, NB, bs, bs] (row, column) and the
+        neighbour table [E, NB] (slot 0 the element, 1 + f across face f, -1 none)."""
+        info = self.mg_info()
+        bs = info["block_sizes"][level]
+        NB = self.dim + 2
+        blocks = np.zeros((self.E, NB, bs, bs))
+        nbr = np.zeros((self.E, NB), dtype=np.int32)
+        _ffi.check(_ffi.lib().tdg_mg_level_matrix(self._h, level, blocks.ctypes.data, nbr.ctypes.data))
+        return np.ascontiguousarray(blocks.transpose(0, 1, 3, 2)), nbr
+
     def rhs(self, force_Q: np.ndarray | None = None, bc_q: np.ndarray | None = None) -> np.ndarray:
         """Right-hand side (DGOperator::rhs): force_Q [E, Q, Nq], bc_q [F, Q, nq]."""
         b = np.zeros(self.ndof)
@@ -326,3 +373,20 @@ def greens_function(op: DGOperator, fault: Fault, precision: int = FP64, rtol: f
         fault.traction(x, slip, T, n)
         G[:, s:s + n] = T.T
     return G, stats
+
+
+def mg_level_degrees(strategy: str, coarse_degree: int, degree: int) -> list[int]:
+    """Level degrees, coarsest first (MGConfig::levels)."""
+    out = (C.c_int * 16)()
+    n = _ffi.lib().tdg_mg_level_degrees(MG_STRATEGIES.index(strategy), coarse_degree, degree, out)
+    if n < 0:
+        _ffi.check(n)
+    return list(out[:n])
+
+
+def mg_interpolation(dim: int, kind: int, n_to: int, n_from: int) -> np.ndarray:
+    """Reference interpolation matrix of one component, [Nbf(n_to), Nbf(n_from)]."""
+    from math import comb
+    out = np.zeros((comb(n_to + dim, dim), comb(n_from + dim, dim)))
+    _ffi.check(_ffi.lib().tdg_mg_interpolation(dim, kind, n_to, n_from, out.ctypes.data))
+    return out
