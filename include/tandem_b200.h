@@ -225,6 +225,9 @@ int tdg_solve_segmented(tdg_op* op, const double* b, double* x, int nseg, const 
 #define TDG_MG_LOGARITHMIC 1
 #define TDG_MG_FULL 2
 
+#define TDG_MG_COARSE_DG 0
+#define TDG_MG_COARSE_P1 1
+
 typedef struct {
     int32_t strategy;        /* TDG_MG_TWOLEVEL / LOGARITHMIC / FULL (MGStrategy; default logarithmic) */
     int32_t coarse_degree;   /* degree of the coarsest level (MGConfig coarse_level; default 1) */
@@ -236,6 +239,11 @@ typedef struct {
     int32_t coarse_max_it;   /* coarsest-level CG iteration cap (default 1000) */
     int32_t smooth_precision; /* TDG_FP64, or TDG_MIXED: FP32 arithmetic for the finest level's
                                  smoother applies (the level operators stay FP64) */
+    int32_t coarse_space;    /* TDG_MG_COARSE_DG: the coarse CG works on the coarsest DG level (as
+                                tandem's -mg_coarse_ksp_type cg).  TDG_MG_COARSE_P1 (default): the
+                                coarsest DG level is smoothed too and corrected from the continuous
+                                P1 space on the mesh vertices (Galerkin R^T A R, rigid-body modes
+                                included), where the coarse CG runs -- in place of tandem's GAMG */
 } tdg_mg_opts;
 
 /* Builds the p-multigrid hierarchy: level degrees from the strategy; the element interpolation
@@ -243,9 +251,10 @@ typedef struct {
  * ModalInterpolation.h:40-44, NodalInterpolation.cpp:8-36); Galerkin coarse operators
  * A_l = I^T A_{l+1} I (the first by probing the matrix-free operator with a distance-2 element
  * colouring, the others by block triple products) stored element block-sparse on the device;
- * point-Jacobi diagonals; the lambda_max estimates of the Chebyshev smoothers; block-Jacobi
- * inverses of the coarsest level.  opts may be NULL (defaults).  Does not select the
- * preconditioner (tdg_set_preconditioner). */
+ * point-Jacobi diagonals; the lambda_max estimates of the Chebyshev smoothers; the coarse system
+ * (see coarse_space) with its block-Jacobi inverses.  opts may be NULL (defaults: logarithmic,
+ * coarse degree 1, continuous P1 coarse space).  Does not select the preconditioner
+ * (tdg_set_preconditioner). */
 int tdg_mg_setup(tdg_op* op, const tdg_mg_opts* opts, void* stream);
 /* z = M r, one V-cycle per right-hand side (PCMG's apply): Chebyshev pre-smoothing from zero,
  * restriction of the residual, the coarser levels, prolongation, Chebyshev post-smoothing; CG with

@@ -92,7 +92,8 @@ TDG_MG_TWOLEVEL, TDG_MG_LOGARITHMIC, TDG_MG_FULL = 0, 1, 2
 class MgOpts(C.Structure):
     _fields_ = [("strategy", C.c_int32), ("coarse_degree", C.c_int32), ("smooth_its", C.c_int32),
                 ("esteig_lo", C.c_double), ("esteig_hi", C.c_double), ("esteig_steps", C.c_int32),
-                ("coarse_rtol", C.c_double), ("coarse_max_it", C.c_int32), ("smooth_precision", C.c_int32)]
+                ("coarse_rtol", C.c_double), ("coarse_max_it", C.c_int32), ("smooth_precision", C.c_int32),
+                ("coarse_space", C.c_int32)]
 
 
 class SolveStats(C.Structure):

@@ -148,7 +148,23 @@ struct MgHierarchy {
     int nchunks = 0;
     int* status = nullptr;
     int64_t coarse_its = 0;
+    // the coarse system the CG solves: the coarsest DG level, or (aux) the continuous P1 level
+    // below it; cn unknowns, block-Jacobi blocks of cbs x cbs, cnb of them
+    bool aux = false;
+    MgAux ax{};
+    double *ab = nullptr, *axv = nullptr;
+    int64_t cn = 0, cnb = 0;
+    int cbs = 0;
+    // coarsest-level CG: a block of kCoarseBlock iterations captured once (its vectors never move)
+    cudaGraphExec_t coarse_exec = nullptr;
+    void reset_graph() {
+        if (coarse_exec) cudaGraphExecDestroy(coarse_exec);
+        coarse_exec = nullptr;
+    }
+    ~MgHierarchy() { reset_graph(); }
 };
+
+constexpr int kCoarseBlock = 8;
 
 }  // namespace
 
@@ -440,15 +456,21 @@ struct SegPlan {
     int64_t op_ld = 0;
 };
 
+// Chunk length: about four chunks per SM over all segments (so short vectors still occupy the
+// whole GPU), a multiple of the CTA size, between kChunkMin and kChunk entries.
 void plan_chunks(std::vector<int64_t> const& seg_begin, std::vector<int64_t> const& seg_end, std::vector<Chunk>& chunks,
                  std::vector<int>& seg_chunk) {
+    int64_t total = 0;
+    for (size_t sgi = 0; sgi < seg_begin.size(); ++sgi) total += seg_end[sgi] - seg_begin[sgi];
+    const int64_t target = (total / (4 * static_cast<int64_t>(device_sm_count())) + kVecThreads - 1) / kVecThreads * kVecThreads;
+    const int64_t len = std::max<int64_t>(kChunkMin, std::min<int64_t>(kChunk, target));
     chunks.clear();
     seg_chunk.assign(1, 0);
     for (size_t sgi = 0; sgi < seg_begin.size(); ++sgi) {
-        for (int64_t b = seg_begin[sgi]; b < seg_end[sgi]; b += kChunk) {
+        for (int64_t b = seg_begin[sgi]; b < seg_end[sgi]; b += len) {
             Chunk c;
             c.begin = b;
-            c.end = std::min(seg_end[sgi], b + kChunk);
+            c.end = std::min(seg_end[sgi], b + len);
             c.seg = static_cast<int>(sgi);
             c.pad = 0;
             chunks.push_back(c);
@@ -528,24 +550,44 @@ int mg_read_scalars(tdg_op* op, double* hs, cudaStream_t s) {
     return 0;
 }
 
-// Coarsest level: CG with the block-Jacobi inverses from x = 0 until ||r|| <= coarse_rtol ||b||
-// (checked every 4 iterations) or coarse_max_it iterations.
-int mg_coarse_solve(tdg_op* op, const double* b, double* x, cudaStream_t s) {
+// kCoarseBlock CG iterations of the coarsest level with device-resident scalars.
+int mg_coarse_block(tdg_op* op, SegPlan const& sp, double* x, cudaStream_t s) {
     auto& mg = op->mg;
     auto const& L = mg.lv[0];
+    for (int k = 0; k < kCoarseBlock; ++k) {
+        if (mg.aux)
+            TDG_TRY(mgk(launch_aux_apply(mg.ax, mg.cp, nullptr, mg.cq, s), "coarse A"));
+        else
+            TDG_TRY(mgk(launch_mg_bsr_apply(op->h.E, mg.NB, L.bs, mg.nbr, L.A, mg.cp, nullptr, mg.cq, s), "coarse A"));
+        TDG_TRY(dots<double>(sp, mg.cp, mg.cq, nullptr, nullptr, mg.partial, mg.scal, kPQ, -1, s));
+        k_cg_xr<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, mg.cr, mg.cp, mg.cq, mg.scal);
+        TDG_TRY(mgk(launch_bjac_apply<double, double>(mg.cbs, mg.cnb, mg.cinv, mg.cr, mg.cz, 1, mg.cn, s), "coarse PC"));
+        TDG_TRY(dots<double>(sp, mg.cr, mg.cz, mg.cr, mg.cr, mg.partial, mg.scal, kRZnew, kRR, s));
+        k_cg_p<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, mg.cp, mg.cz, mg.scal);
+        k_cg_shift<<<1, 128, 0, s>>>(mg.scal, 1);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "multigrid: coarse CG kernels");
+}
+
+// Coarsest level: CG with the block-Jacobi inverses from x = 0 until ||r|| <= coarse_rtol ||b||
+// (checked every kCoarseBlock iterations, the blocks replayed from a CUDA graph on a non-default
+// stream) or coarse_max_it iterations.  x is always the coarse system's own vector (the coarsest
+// DG level's, or the continuous P1 level's).
+int mg_coarse_solve(tdg_op* op, const double* b, double* x, cudaStream_t s) {
+    auto& mg = op->mg;
     SegPlan sp;
     sp.nseg = 1;
     sp.nchunks = mg.nchunks;
     sp.chunks = mg.chunks;
     sp.seg_chunk = mg.seg_chunk;
     sp.op_nrhs = 1;
-    sp.op_ld = L.n;
+    sp.op_ld = mg.cn;
     double hs[kScal] = {};
     hs[kActive] = 1.0;
-    TDG_CUDA_TRY(cudaMemsetAsync(x, 0, L.n * sizeof(double), s));
-    TDG_CUDA_TRY(cudaMemcpyAsync(mg.cr, b, L.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    TDG_CUDA_TRY(cudaMemsetAsync(x, 0, mg.cn * sizeof(double), s));
+    TDG_CUDA_TRY(cudaMemcpyAsync(mg.cr, b, mg.cn * sizeof(double), cudaMemcpyDeviceToDevice, s));
     TDG_CUDA_TRY(cudaMemcpyAsync(mg.scal, hs, sizeof(hs), cudaMemcpyHostToDevice, s));
-    TDG_TRY(mgk(launch_bjac_apply<double, double>(L.bs, op->h.E, mg.cinv, mg.cr, mg.cz, 1, L.n, s), "coarse PC"));
+    TDG_TRY(mgk(launch_bjac_apply<double, double>(mg.cbs, mg.cnb, mg.cinv, mg.cr, mg.cz, 1, mg.cn, s), "coarse PC"));
     k_copy<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, mg.cz, mg.cp);
     TDG_TRY(dots<double>(sp, mg.cr, mg.cz, mg.cr, mg.cr, mg.partial, mg.scal, kRZ, kRR, s));
     TDG_TRY(mg_read_scalars(op, hs, s));
@@ -553,16 +595,24 @@ int mg_coarse_solve(tdg_op* op, const double* b, double* x, cudaStream_t s) {
     if (!(hs[kRR] > 0.0)) return 0;
     int it = 0;
     while (it < mg.opts.coarse_max_it) {
-        for (int k = 0; k < 4; ++k) {
-            TDG_TRY(mgk(launch_mg_bsr_apply(op->h.E, mg.NB, L.bs, mg.nbr, L.A, mg.cp, nullptr, mg.cq, s), "coarse A"));
-            TDG_TRY(dots<double>(sp, mg.cp, mg.cq, nullptr, nullptr, mg.partial, mg.scal, kPQ, -1, s));
-            k_cg_xr<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, mg.cr, mg.cp, mg.cq, mg.scal);
-            TDG_TRY(mgk(launch_bjac_apply<double, double>(L.bs, op->h.E, mg.cinv, mg.cr, mg.cz, 1, L.n, s), "coarse PC"));
-            TDG_TRY(dots<double>(sp, mg.cr, mg.cz, mg.cr, mg.cr, mg.partial, mg.scal, kRZnew, kRR, s));
-            k_cg_p<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, mg.cp, mg.cz, mg.scal);
-            k_cg_shift<<<1, 128, 0, s>>>(mg.scal, 1);
+        if (s != nullptr && !mg.coarse_exec) {
+            cudaGraph_t graph = nullptr;
+            TDG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            int rc = mg_coarse_block(op, sp, x, s);
+            cudaError_t ce = cudaStreamEndCapture(s, &graph);
+            if (rc == 0 && ce == cudaSuccess) ce = cudaGraphInstantiate(&mg.coarse_exec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (rc) return rc;
+            if (ce != cudaSuccess) {
+                mg.coarse_exec = nullptr;
+                return fail(TDG_E_CUDA, std::string("multigrid: coarse CG graph: ") + cudaGetErrorString(ce));
+            }
         }
-        it += 4;
+        if (mg.coarse_exec)
+            TDG_CUDA_TRY(cudaGraphLaunch(mg.coarse_exec, s));
+        else
+            TDG_TRY(mg_coarse_block(op, sp, x, s));
+        it += kCoarseBlock;
         TDG_TRY(mg_read_scalars(op, hs, s));
         if (!std::isfinite(hs[kRR])) return fail(TDG_E_DIVERGED, "multigrid: coarse CG diverged");
         if (hs[kRR] <= tol2) break;
@@ -571,18 +621,25 @@ int mg_coarse_solve(tdg_op* op, const double* b, double* x, cudaStream_t s) {
     return 0;
 }
 
-// One V-cycle on level l: x = M_l b.
+// One V-cycle on level l: x = M_l b.  Below the coarsest DG level sits either the coarse solve
+// itself or, with the auxiliary space, a smoothed DG level corrected from the continuous P1 level.
 int mg_vcycle(tdg_op* op, int l, const double* b, double* x, cudaStream_t s) {
-    if (l == 0) return mg_coarse_solve(op, b, x, s);
     auto& mg = op->mg;
+    if (l == 0 && !mg.aux) return mg_coarse_solve(op, b, x, s);
     auto& L = mg.lv[static_cast<size_t>(l)];
-    auto& C = mg.lv[static_cast<size_t>(l - 1)];
     const int64_t E = op->h.E;
     TDG_TRY(mg_smooth(op, l, b, x, true, s));
     TDG_TRY(mg_level_apply(op, l, x, L.r, b, s));
-    TDG_TRY(mgk(launch_mg_restrict(E, C.ip, L.r, C.b, s), "restriction"));
-    TDG_TRY(mg_vcycle(op, l - 1, C.b, C.x, s));
-    TDG_TRY(mgk(launch_mg_prolong_add(E, C.ip, C.x, x, s), "prolongation"));
+    if (l == 0) {
+        TDG_TRY(mgk(launch_aux_restrict(mg.ax, L.r, mg.ab, s), "restriction to P1"));
+        TDG_TRY(mg_coarse_solve(op, mg.ab, mg.axv, s));
+        TDG_TRY(mgk(launch_aux_prolong_add(mg.ax, E, mg.axv, x, s), "prolongation from P1"));
+    } else {
+        auto& C = mg.lv[static_cast<size_t>(l - 1)];
+        TDG_TRY(mgk(launch_mg_restrict(E, C.ip, L.r, C.b, s), "restriction"));
+        TDG_TRY(mg_vcycle(op, l - 1, C.b, C.x, s));
+        TDG_TRY(mgk(launch_mg_prolong_add(E, C.ip, C.x, x, s), "prolongation"));
+    }
     return mg_smooth(op, l, b, x, false, s);
 }
 
@@ -699,6 +756,71 @@ int mg_probe(tdg_op* op, cudaStream_t s) {
     return rc;
 }
 
+// Continuous P1 level below the coarsest DG level: vertex numbering, the Galerkin operator
+// R^T A_0 R assembled on the host from the coarsest DG level's blocks, its Q x Q diagonal blocks
+// inverted for the block-Jacobi CG.
+int mg_setup_aux(tdg_op* op, cudaStream_t s) {
+    auto& h = op->h;
+    auto& mg = op->mg;
+    auto& L0 = mg.lv[0];
+    const int64_t E = h.E;
+    const int NVe = h.D + 1, Nbf0 = L0.bs / h.Q;
+    std::vector<double> A0(static_cast<size_t>(E) * mg.NB * L0.bs * L0.bs);
+    TDG_CUDA_TRY(cudaMemcpyAsync(A0.data(), L0.A, A0.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    std::vector<int32_t> nbr(static_cast<size_t>(E) * mg.NB);
+    TDG_CUDA_TRY(cudaMemcpyAsync(nbr.data(), mg.nbr, nbr.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    TDG_CUDA_TRY(cudaStreamSynchronize(s));
+    int64_t nv = 0;
+    std::vector<int32_t> vid = vertex_numbering(h, &nv);
+    Dense T = linear_to_space(h.D, h.kind, L0.degree);
+    VertexCsr c = vertex_galerkin(A0, nbr, E, mg.NB, h.D, Nbf0, h.Q, T, vid, nv);
+    A0.clear();
+    A0.shrink_to_fit();
+    const int64_t* dptr = nullptr;
+    const int32_t *dcol = nullptr, *dvinc = nullptr, *dvid = nullptr;
+    const double *dval = nullptr, *dT = nullptr;
+    const int64_t* dvp = nullptr;
+    TDG_CUDA_TRY(mg.arena.upload(&dptr, c.ptr));
+    TDG_CUDA_TRY(mg.arena.upload(&dcol, c.col));
+    TDG_CUDA_TRY(mg.arena.upload(&dval, c.val));
+    TDG_CUDA_TRY(mg.arena.upload(&dvp, c.vinc_ptr));
+    TDG_CUDA_TRY(mg.arena.upload(&dvinc, c.vinc));
+    TDG_CUDA_TRY(mg.arena.upload(&dvid, vid));
+    TDG_CUDA_TRY(mg.arena.upload(&dT, T.a));
+    mg.ax.ptr = dptr;
+    mg.ax.col = dcol;
+    mg.ax.val = dval;
+    mg.ax.vinc_ptr = dvp;
+    mg.ax.vinc = dvinc;
+    mg.ax.vid = dvid;
+    mg.ax.T = dT;
+    mg.ax.nv = nv;
+    mg.ax.Q = h.Q;
+    mg.ax.Nbf = Nbf0;
+    mg.ax.NV = NVe;
+    mg.cn = nv * h.Q;
+    mg.cbs = h.Q;
+    mg.cnb = nv;
+    TDG_CUDA_TRY(mg.arena.alloc(&mg.ab, static_cast<size_t>(mg.cn)));
+    TDG_CUDA_TRY(mg.arena.alloc(&mg.axv, static_cast<size_t>(mg.cn)));
+    // diagonal blocks, column-major, for the block-Jacobi inversion
+    const int Q = h.Q;
+    std::vector<double> diag(static_cast<size_t>(nv) * Q * Q, 0.0);
+    for (int64_t v = 0; v < nv; ++v) {
+        const int32_t* c0 = c.col.data() + c.ptr[static_cast<size_t>(v)];
+        const int32_t* c1 = c.col.data() + c.ptr[static_cast<size_t>(v) + 1];
+        const int32_t* it = std::lower_bound(c0, c1, static_cast<int32_t>(v));
+        if (it == c1 || *it != v) return fail(TDG_E_NOT_SPD, "multigrid: a P1 vertex without a diagonal block");
+        const double* blk = &c.val[static_cast<size_t>(it - c.col.data()) * Q * Q];
+        for (int p = 0; p < Q; ++p)
+            for (int q = 0; q < Q; ++q) diag[static_cast<size_t>(v) * Q * Q + q * Q + p] = blk[p * Q + q];
+    }
+    const double* ddiag = nullptr;
+    TDG_CUDA_TRY(mg.arena.upload(&ddiag, diag));
+    TDG_CUDA_TRY(mg.arena.alloc(&mg.cinv, diag.size()));
+    return mgk(launch_bjac_invert<double>(Q, nv, ddiag, mg.cinv, mg.status, s), "P1 block inversion");
+}
+
 int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
     auto& h = op->h;
     auto& mg = op->mg;
@@ -721,12 +843,15 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
     }
     if (deg.size() < 2) return fail(TDG_E_INVALID, "multigrid: needs at least two levels");
     // a fresh hierarchy
+    mg.reset_graph();
     mg.arena.release();
     mg.lv.clear();
     mg.ready = false;
     mg.coarse_its = 0;
     mg.opts = o;
     mg.fine_prec = o.smooth_precision;
+    // the continuous P1 level embeds in the coarsest DG level only from degree 1 on
+    mg.aux = o.coarse_space == TDG_MG_COARSE_P1 && deg[0] >= 1;
     TDG_TRY(ensure_uploaded(op, TDG_FP64));
     if (mg.fine_prec == TDG_MIXED) TDG_TRY(ensure_uploaded(op, TDG_FP32));
     TDG_TRY(ensure_blocks(op, s));
@@ -764,9 +889,6 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
         TDG_CUDA_TRY(mg.arena.alloc(&L.y, n));
         TDG_CUDA_TRY(mg.arena.alloc(&L.w, n));
     }
-    // dot partials: the level dots (kDotBlocks + a result slot) and the coarsest CG's chunk pairs
-    const size_t nchunk_max = static_cast<size_t>(mg.lv[0].n / kChunk) + 2;
-    TDG_CUDA_TRY(mg.arena.alloc(&mg.partial, std::max<size_t>(kDotBlocks + 8, 2 * nchunk_max)));
     TDG_CUDA_TRY(mg.arena.alloc(&mg.status, 1));
     TDG_CUDA_TRY(cudaMemsetAsync(mg.status, 0, sizeof(int), s));
     // Galerkin operators: probing below the finest level, triple products further down
@@ -785,9 +907,14 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
             TDG_TRY(mgk(launch_mg_diag_inv(E, L.bs, static_cast<int64_t>(mg.NB) * L.bs * L.bs, L.A, L.dinv, mg.status, s),
                         "diagonal"));
     }
-    // coarsest level: block-Jacobi inverses, CG vectors and plan
+    // the coarse system: block-Jacobi inverses, CG vectors and plan
     auto& L0 = mg.lv[0];
-    {
+    if (mg.aux) {
+        TDG_TRY(mg_setup_aux(op, s));
+    } else {
+        mg.cn = L0.n;
+        mg.cbs = L0.bs;
+        mg.cnb = E;
         double* blk0 = nullptr;
         TDG_CUDA_TRY(cudaMalloc(&blk0, sizeof(double) * E * L0.bs * L0.bs));
         int rc = mgk(launch_mg_self_blocks(E, mg.NB, L0.bs, L0.A, blk0, s), "coarse blocks");
@@ -804,11 +931,11 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
     TDG_CUDA_TRY(cudaMemcpyAsync(&st, mg.status, sizeof(int), cudaMemcpyDeviceToHost, s));
     TDG_CUDA_TRY(cudaStreamSynchronize(s));
     if (st) return fail(TDG_E_NOT_SPD, "multigrid: a level diagonal or coarse block is not positive definite");
-    for (double** v : {&mg.cr, &mg.cz, &mg.cp, &mg.cq}) TDG_CUDA_TRY(mg.arena.alloc(v, static_cast<size_t>(L0.n)));
+    for (double** v : {&mg.cr, &mg.cz, &mg.cp, &mg.cq}) TDG_CUDA_TRY(mg.arena.alloc(v, static_cast<size_t>(mg.cn)));
     {
         std::vector<Chunk> hc;
         std::vector<int> hsc;
-        plan_chunks({0}, {L0.n}, hc, hsc);
+        plan_chunks({0}, {mg.cn}, hc, hsc);
         const Chunk* dch = nullptr;
         const int* dsc = nullptr;
         TDG_CUDA_TRY(mg.arena.upload(&dch, hc));
@@ -817,9 +944,11 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
         mg.seg_chunk = const_cast<int*>(dsc);
         mg.nchunks = static_cast<int>(hc.size());
         TDG_CUDA_TRY(mg.arena.alloc(&mg.scal, static_cast<size_t>(kScal)));
+        // dot partials: the level dots (kDotBlocks + a result slot) and the coarsest CG's chunk pairs
+        TDG_CUDA_TRY(mg.arena.alloc(&mg.partial, std::max<size_t>(kDotBlocks + 8, 2 * hc.size())));
     }
     // Chebyshev bounds of the smoothed levels
-    for (int l = 1; l < nl; ++l) TDG_TRY(mg_estimate_lmax(op, l, s));
+    for (int l = mg.aux ? 0 : 1; l < nl; ++l) TDG_TRY(mg_estimate_lmax(op, l, s));
     mg.ready = true;
     return 0;
 }
@@ -1655,6 +1784,7 @@ extern "C" int tdg_mg_setup(tdg_op* op, const tdg_mg_opts* opts, void* stream) {
     } else {
         o.strategy = TDG_MG_LOGARITHMIC;
         o.coarse_degree = 1;
+        o.coarse_space = TDG_MG_COARSE_P1;
     }
     try {
         return mg_setup(op, o, static_cast<cudaStream_t>(stream));

@@ -581,4 +581,138 @@ std::vector<int32_t> distance2_colouring(std::vector<int32_t> const& nbr, int64_
     return col;
 }
 
+std::vector<int32_t> vertex_numbering(HostOperator const& h, int64_t* nv) {
+    const int NV = h.D + 1;
+    const int64_t n = h.E * NV;
+    std::vector<int64_t> parent(static_cast<size_t>(n));
+    for (int64_t i = 0; i < n; ++i) parent[static_cast<size_t>(i)] = i;
+    auto find = [&](int64_t a) {
+        while (parent[static_cast<size_t>(a)] != a) {
+            parent[static_cast<size_t>(a)] = parent[static_cast<size_t>(parent[static_cast<size_t>(a)])];
+            a = parent[static_cast<size_t>(a)];
+        }
+        return a;
+    };
+    auto fv = facet_vertices(h.D);
+    for (int64_t f = 0; f < h.F; ++f) {
+        const int64_t e0 = h.up[static_cast<size_t>(2 * f)], e1 = h.up[static_cast<size_t>(2 * f + 1)];
+        if (e0 == e1) continue;
+        const int l0 = h.loc[static_cast<size_t>(2 * f)], l1 = h.loc[static_cast<size_t>(2 * f + 1)];
+        for (int k = 0; k < h.D; ++k) {
+            int64_t a = find(e0 * NV + fv[static_cast<size_t>(l0)][static_cast<size_t>(k)]);
+            int64_t b = find(e1 * NV + fv[static_cast<size_t>(l1)][static_cast<size_t>(k)]);
+            if (a != b) parent[static_cast<size_t>(std::max(a, b))] = std::min(a, b);
+        }
+    }
+    std::vector<int32_t> vid(static_cast<size_t>(n));
+    std::vector<int32_t> id_of_root(static_cast<size_t>(n), -1);
+    int32_t next = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t r = find(i);
+        if (id_of_root[static_cast<size_t>(r)] < 0) id_of_root[static_cast<size_t>(r)] = next++;
+        vid[static_cast<size_t>(i)] = id_of_root[static_cast<size_t>(r)];
+    }
+    *nv = next;
+    return vid;
+}
+
+Dense linear_to_space(int D, int kind, int p) {
+    Points nodes = warp_blend_nodes(D, p);
+    RefSpace sp = (kind == kPoisson) ? RefSpace::modal(D, p) : RefSpace::nodal(D, p, nodes);
+    Dense Eb = sp.eval(nodes);  // [Nbf][Nnodes]
+    const int nb = Eb.rows;
+    Dense V(nb, nb);
+    for (int j = 0; j < nb; ++j)
+        for (int k = 0; k < nb; ++k) V(j, k) = Eb(k, j);
+    Dense Vi = invert(V);
+    Dense T(nb, D + 1);
+    for (int j = 0; j < nb; ++j) {
+        const double* x = &nodes[static_cast<size_t>(j) * D];
+        double lam[4];
+        lam[0] = 1.0;
+        for (int d = 0; d < D; ++d) {
+            lam[d + 1] = x[d];
+            lam[0] -= x[d];
+        }
+        for (int k = 0; k < nb; ++k)
+            for (int i = 0; i <= D; ++i) T(k, i) += Vi(k, j) * lam[i];
+    }
+    return T;
+}
+
+VertexCsr vertex_galerkin(std::vector<double> const& A, std::vector<int32_t> const& nbr, int64_t E, int NB, int D,
+                          int Nbf, int Q, Dense const& T, std::vector<int32_t> const& vid, int64_t nv) {
+    const int NV = D + 1, bs = Nbf * Q, m = NV * Q;
+    VertexCsr c;
+    c.nv = nv;
+    c.Q = Q;
+    // sparsity: every (corner of e, corner of t) pair of a present block (e, s)
+    std::vector<int64_t> keys;
+    keys.reserve(static_cast<size_t>(E) * NB * NV * NV);
+    for (int64_t e = 0; e < E; ++e)
+        for (int s = 0; s < NB; ++s) {
+            const int32_t t = nbr[static_cast<size_t>(e * NB + s)];
+            if (t < 0) continue;
+            for (int i = 0; i < NV; ++i)
+                for (int j = 0; j < NV; ++j)
+                    keys.push_back(static_cast<int64_t>(vid[static_cast<size_t>(e * NV + i)]) * nv +
+                                   vid[static_cast<size_t>(static_cast<int64_t>(t) * NV + j)]);
+        }
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    c.ptr.assign(static_cast<size_t>(nv) + 1, 0);
+    c.col.resize(keys.size());
+    for (size_t k = 0; k < keys.size(); ++k) {
+        ++c.ptr[static_cast<size_t>(keys[k] / nv) + 1];
+        c.col[k] = static_cast<int32_t>(keys[k] % nv);
+    }
+    for (int64_t v = 0; v < nv; ++v) c.ptr[static_cast<size_t>(v) + 1] += c.ptr[static_cast<size_t>(v)];
+    c.val.assign(keys.size() * Q * Q, 0.0);
+    // values: B = R_e^T A_es R_t per block, scattered by vertex pair
+    std::vector<double> AT(static_cast<size_t>(bs) * m), B(static_cast<size_t>(m) * m);
+    for (int64_t e = 0; e < E; ++e)
+        for (int s = 0; s < NB; ++s) {
+            const int32_t t = nbr[static_cast<size_t>(e * NB + s)];
+            if (t < 0) continue;
+            const double* a = &A[static_cast<size_t>((e * NB + s) * bs) * bs];  // a[col * bs + row]
+            // AT[row][(j, q)] = sum_k' A[row][k' + q Nbf] T(k', j)
+            for (int row = 0; row < bs; ++row)
+                for (int q = 0; q < Q; ++q)
+                    for (int j = 0; j < NV; ++j) {
+                        double acc = 0.0;
+                        for (int kk = 0; kk < Nbf; ++kk) acc += a[static_cast<size_t>(kk + q * Nbf) * bs + row] * T(kk, j);
+                        AT[static_cast<size_t>(row) * m + j * Q + q] = acc;
+                    }
+            // B[(i, p)][(j, q)] = sum_k T(k, i) AT[k + p Nbf][(j, q)]
+            for (int i = 0; i < NV; ++i)
+                for (int p = 0; p < Q; ++p)
+                    for (int jq = 0; jq < m; ++jq) {
+                        double acc = 0.0;
+                        for (int k = 0; k < Nbf; ++k) acc += T(k, i) * AT[static_cast<size_t>(k + p * Nbf) * m + jq];
+                        B[static_cast<size_t>(i * Q + p) * m + jq] = acc;
+                    }
+            for (int i = 0; i < NV; ++i) {
+                const int64_t v = vid[static_cast<size_t>(e * NV + i)];
+                const int32_t* c0 = c.col.data() + c.ptr[static_cast<size_t>(v)];
+                const int32_t* c1 = c.col.data() + c.ptr[static_cast<size_t>(v) + 1];
+                for (int j = 0; j < NV; ++j) {
+                    const int32_t w = vid[static_cast<size_t>(static_cast<int64_t>(t) * NV + j)];
+                    const size_t pos = static_cast<size_t>(std::lower_bound(c0, c1, w) - c.col.data());
+                    double* out = &c.val[pos * Q * Q];
+                    for (int p = 0; p < Q; ++p)
+                        for (int q = 0; q < Q; ++q) out[p * Q + q] += B[static_cast<size_t>(i * Q + p) * m + j * Q + q];
+                }
+            }
+        }
+    // incidences (element, corner) per vertex
+    c.vinc_ptr.assign(static_cast<size_t>(nv) + 1, 0);
+    for (int64_t k = 0; k < E * NV; ++k) ++c.vinc_ptr[static_cast<size_t>(vid[static_cast<size_t>(k)]) + 1];
+    for (int64_t v = 0; v < nv; ++v) c.vinc_ptr[static_cast<size_t>(v) + 1] += c.vinc_ptr[static_cast<size_t>(v)];
+    c.vinc.resize(static_cast<size_t>(E * NV));
+    std::vector<int64_t> fill(c.vinc_ptr.begin(), c.vinc_ptr.end() - 1);
+    for (int64_t k = 0; k < E * NV; ++k)
+        c.vinc[static_cast<size_t>(fill[static_cast<size_t>(vid[static_cast<size_t>(k)])]++)] = static_cast<int32_t>(k);
+    return c;
+}
+
 }  // namespace tdg

@@ -113,4 +113,32 @@ std::vector<int32_t> element_neighbours(HostOperator const& h);
 // most once.  Returns the colour per element and sets ncolors.
 std::vector<int32_t> distance2_colouring(std::vector<int32_t> const& nbr, int64_t E, int NB, int* ncolors);
 
+// ---- continuous P1 auxiliary coarse space (below the coarsest DG level) ---------------------------
+
+// Global vertex numbers vid[e][i] of the element corners, from the facet connectivity alone: the
+// corners of a facet are identified across its two elements (both list a facet's corners in the
+// same order, as element corners are sorted by global id), so vertices are shared exactly within
+// facet-connected parts of the mesh (independent problems of a mesh union stay apart).
+std::vector<int32_t> vertex_numbering(HostOperator const& h, int64_t* nv);
+
+// T [Nbf(p)][D+1]: coefficients in the operator's degree-p space (modal Dubiner or nodal warp &
+// blend) of the linear function with value 1 at corner i and 0 at the others.
+Dense linear_to_space(int D, int kind, int p);
+
+// Galerkin operator R^T A R of the continuous P1 space for the element block-sparse matrix A
+// [E][NB][bs][bs] (column-major blocks, bs = Nbf(p) Q), R_e = T per component on element e's
+// corners.  Rows of Q x Q blocks by vertex, CSR: ptr [nv + 1], col [nnzb], val [nnzb][Q][Q]
+// (row-major).  vinc_ptr/vinc: the (element, corner) incidences of each vertex (e * (D+1) + i).
+struct VertexCsr {
+    int64_t nv = 0;
+    int Q = 0;
+    std::vector<int64_t> ptr;
+    std::vector<int32_t> col;
+    std::vector<double> val;
+    std::vector<int64_t> vinc_ptr;
+    std::vector<int32_t> vinc;
+};
+VertexCsr vertex_galerkin(std::vector<double> const& A, std::vector<int32_t> const& nbr, int64_t E, int NB, int D,
+                          int Nbf, int Q, Dense const& T, std::vector<int32_t> const& vid, int64_t nv);
+
 }  // namespace tdg

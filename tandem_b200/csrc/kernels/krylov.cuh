@@ -3,7 +3,8 @@
 // Vectors are split into *segments*, each with its own Krylov scalars: the right-hand sides of a
 // multi-RHS solve (segment r = [r * ld, r * ld + n)) or the independent problems of a block-
 // diagonal batch (segment s = the DOF range of problem s).  The host cuts every segment into
-// chunks of at most kChunk entries; chunk i is processed by CTA i, so no CTA straddles two
+// chunks of kChunkMin to kChunk entries (about four per SM over the whole vector); chunk i is
+// processed by CTA i, so no CTA straddles two
 // segments and a segment's dot product is the sum of its chunks' partial sums (deterministic).
 // Every scalar the iteration needs (alpha, beta, residual norms) lives in device memory, one row
 // of kScal doubles per segment, so an iteration is a fixed sequence of launches that can be
@@ -21,6 +22,7 @@ constexpr int kScal = 10;
 enum ScalSlot { kRZ = 0, kPQ = 1, kRZnew = 2, kRR = 3, kActive = 4, kBB = 5, kTmp = 6, kRepl = 7, kZQ = 8 };
 constexpr int kVecThreads = 256;
 constexpr int64_t kChunk = 32 * 1024;
+constexpr int64_t kChunkMin = 1024;
 
 struct Chunk {
     int64_t begin, end;  // entries [begin, end) of the stacked vector

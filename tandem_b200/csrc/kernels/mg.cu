@@ -112,6 +112,28 @@ __global__ void __launch_bounds__(kT)
     }
 }
 
+// The same with the block size known at compile time: the column loop unrolls, so every thread
+// issues its block row's loads back to back.
+template <int BS>
+__global__ void __launch_bounds__(kT)
+    k_bsr_apply_t(int64_t E, int NB, const int32_t* __restrict__ nbr, const double* __restrict__ A,
+                  const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y) {
+    TDG_GRID_LOOP(g, E * BS) {
+        const int row = static_cast<int>(g % BS);
+        const int64_t n = g / BS;
+        double acc = 0.0;
+        for (int s = 0; s < NB; ++s) {
+            const int32_t t = nbr[n * NB + s];
+            if (t < 0) continue;
+            const double* blk = A + (n * NB + s) * (BS * BS) + row;
+            const double* xt = x + static_cast<int64_t>(t) * BS;
+#pragma unroll
+            for (int col = 0; col < BS; ++col) acc += blk[col * BS] * xt[col];
+        }
+        y[g] = b ? b[g] - acc : acc;
+    }
+}
+
 __global__ void __launch_bounds__(kT)
     k_diag_inv(int64_t E, int bs, int64_t stride, const double* __restrict__ blocks, double* __restrict__ dinv,
                int* __restrict__ status) {
@@ -161,6 +183,51 @@ __global__ void __launch_bounds__(kT)
         double acc = 0.0;
         for (int k = 0; k < ip.N1; ++k) acc += ip.I[k * ip.N2 + l] * f[k];
         rc[g] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(kT)
+    k_aux_apply(MgAux a, const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y) {
+    const int Q = a.Q, QQ = a.Q * a.Q;
+    TDG_GRID_LOOP(g, a.nv * Q) {
+        const int64_t v = g / Q;
+        const int p = static_cast<int>(g % Q);
+        double acc = 0.0;
+        for (int64_t k = a.ptr[v]; k < a.ptr[v + 1]; ++k) {
+            const double* blk = a.val + k * QQ + p * Q;
+            const double* xw = x + static_cast<int64_t>(a.col[k]) * Q;
+            for (int q = 0; q < Q; ++q) acc += blk[q] * xw[q];
+        }
+        y[g] = b ? b[g] - acc : acc;
+    }
+}
+
+__global__ void __launch_bounds__(kT) k_aux_restrict(MgAux a, const double* __restrict__ r0, double* __restrict__ rc) {
+    const int Q = a.Q, bs = a.Nbf * a.Q;
+    TDG_GRID_LOOP(g, a.nv * Q) {
+        const int64_t v = g / Q;
+        const int p = static_cast<int>(g % Q);
+        double acc = 0.0;
+        for (int64_t k = a.vinc_ptr[v]; k < a.vinc_ptr[v + 1]; ++k) {
+            const int32_t inc = a.vinc[k];
+            const int64_t e = inc / a.NV;
+            const int i = inc % a.NV;
+            const double* r = r0 + e * bs + p * a.Nbf;
+            for (int kk = 0; kk < a.Nbf; ++kk) acc += a.T[kk * a.NV + i] * r[kk];
+        }
+        rc[g] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(kT)
+    k_aux_prolong_add(MgAux a, int64_t E, const double* __restrict__ xc, double* __restrict__ x0) {
+    const int bs = a.Nbf * a.Q;
+    TDG_GRID_LOOP(g, E * bs) {  // g = e * bs + p * Nbf + kk
+        const int64_t e = g / bs;
+        const int p = static_cast<int>((g % bs) / a.Nbf), kk = static_cast<int>(g % a.Nbf);
+        double acc = 0.0;
+        for (int i = 0; i < a.NV; ++i) acc += a.T[kk * a.NV + i] * xc[static_cast<int64_t>(a.vid[e * a.NV + i]) * a.Q + p];
+        x0[g] += acc;
     }
 }
 
@@ -268,7 +335,15 @@ int launch_mg_triple(int64_t E, int NB, const int32_t* nbr, MgInterp ip, const d
 
 int launch_mg_bsr_apply(int64_t E, int NB, int bs, const int32_t* nbr, const double* A, const double* x,
                         const double* b, double* y, cudaStream_t s) {
-    k_bsr_apply<<<grid_for(E * bs), kT, 0, s>>>(E, NB, bs, nbr, A, x, b, y);
+    const unsigned g = grid_for(E * bs);
+    switch (bs) {
+#define TDG_BSR_CASE(B) \
+    case B: k_bsr_apply_t<B><<<g, kT, 0, s>>>(E, NB, nbr, A, x, b, y); break;
+        TDG_BSR_CASE(1) TDG_BSR_CASE(2) TDG_BSR_CASE(3) TDG_BSR_CASE(4) TDG_BSR_CASE(6) TDG_BSR_CASE(10)
+        TDG_BSR_CASE(12) TDG_BSR_CASE(20) TDG_BSR_CASE(30) TDG_BSR_CASE(60)
+#undef TDG_BSR_CASE
+        default: k_bsr_apply<<<g, kT, 0, s>>>(E, NB, bs, nbr, A, x, b, y);
+    }
     return launched();
 }
 
@@ -290,6 +365,21 @@ int launch_mg_prolong_add(int64_t E, MgInterp ip, const double* xc, double* xf, 
 
 int launch_mg_restrict(int64_t E, MgInterp ip, const double* rf, double* rc, cudaStream_t s) {
     k_restrict<<<grid_for(E * ip.Q * ip.N2), kT, 0, s>>>(E, ip, rf, rc);
+    return launched();
+}
+
+int launch_aux_apply(MgAux const& a, const double* x, const double* b, double* y, cudaStream_t s) {
+    k_aux_apply<<<grid_for(a.nv * a.Q), kT, 0, s>>>(a, x, b, y);
+    return launched();
+}
+
+int launch_aux_restrict(MgAux const& a, const double* r0, double* rc, cudaStream_t s) {
+    k_aux_restrict<<<grid_for(a.nv * a.Q), kT, 0, s>>>(a, r0, rc);
+    return launched();
+}
+
+int launch_aux_prolong_add(MgAux const& a, int64_t E, const double* xc, double* x0, cudaStream_t s) {
+    k_aux_prolong_add<<<grid_for(E * a.Nbf * a.Q), kT, 0, s>>>(a, E, xc, x0);
     return launched();
 }
 

@@ -43,6 +43,25 @@ int launch_mg_self_blocks(int64_t E, int NB, int bs, const double* A, double* bl
 int launch_mg_prolong_add(int64_t E, MgInterp ip, const double* xc, double* xf, cudaStream_t s);
 int launch_mg_restrict(int64_t E, MgInterp ip, const double* rf, double* rc, cudaStream_t s);
 
+// Continuous P1 auxiliary level: R maps vertex values to the coarsest DG level (on element e, corner
+// values through T [Nbf][NV] per component); its Galerkin operator is CSR over vertices with Q x Q
+// blocks (row-major).  The restriction gathers over each vertex's (element, corner) incidences, so
+// it needs no atomics and is deterministic.
+struct MgAux {
+    const int64_t* ptr = nullptr;
+    const int32_t* col = nullptr;
+    const double* val = nullptr;
+    const int64_t* vinc_ptr = nullptr;
+    const int32_t* vinc = nullptr;  // e * NV + corner
+    const int32_t* vid = nullptr;   // [E][NV]
+    const double* T = nullptr;      // [Nbf][NV]
+    int64_t nv = 0;
+    int Q = 0, Nbf = 0, NV = 0;
+};
+int launch_aux_apply(MgAux const& a, const double* x, const double* b, double* y, cudaStream_t s);
+int launch_aux_restrict(MgAux const& a, const double* r0, double* rc, cudaStream_t s);
+int launch_aux_prolong_add(MgAux const& a, int64_t E, const double* xc, double* x0, cudaStream_t s);
+
 // Chebyshev iteration (Saad, "Iterative Methods for Sparse Linear Systems", 2nd ed., Alg. 12.1,
 // preconditioned with Dinv): first step d = c Dinv r, x = d (x_zero) or x += d; later steps
 // r -= y (y = A d), d = c1 d + c2 Dinv r, x += d.

@@ -22,6 +22,7 @@ FP64, FP32, MIXED = _ffi.TDG_FP64, _ffi.TDG_FP32, _ffi.TDG_MIXED
 FAMILIES = ("tensor", "simt", "face")
 MG_STRATEGIES = ("twolevel", "logarithmic", "full")  # MGStrategy (app/common/MGConfig.h:8)
 PRECONDITIONERS = ("bjacobi", "mg")
+MG_COARSE_SPACES = ("dg", "p1")
 
 
 def _c(a: np.ndarray, dtype) -> np.ndarray:
@@ -202,13 +203,16 @@ class DGOperator:
     # -- p-multigrid preconditioner (PetscLinearSolver::setup_mg + mg_cheby.cfg) -------------------
     def mg_setup(self, strategy: str = "logarithmic", coarse_degree: int = 1, smooth_its: int = 10,
                  esteig: tuple[float, float] = (0.01, 1.1), esteig_steps: int = 10, coarse_rtol: float = 0.1,
-                 coarse_max_it: int = 1000, smooth_precision: int = FP64, stream=None) -> None:
+                 coarse_max_it: int = 1000, smooth_precision: int = FP64, coarse_space: str = "p1",
+                 stream=None) -> None:
         """Builds the p-multigrid hierarchy (tdg_mg_setup): levels by MGConfig strategy, Galerkin
-        coarse operators, Chebyshev smoothers on esteig x lambda_max(D^-1 A) with point Jacobi, CG
-        with block Jacobi on the coarsest level.  smooth_precision MIXED runs the finest level's
+        coarse operators, Chebyshev smoothers on esteig x lambda_max(D^-1 A) with point Jacobi, and
+        a block-Jacobi CG coarse solve -- on the coarsest DG level (coarse_space "dg") or on the
+        continuous P1 space below it ("p1").  smooth_precision MIXED runs the finest level's
         smoother applies in FP32 arithmetic."""
         o = _ffi.MgOpts(MG_STRATEGIES.index(strategy), coarse_degree, smooth_its, esteig[0], esteig[1],
-                        esteig_steps, coarse_rtol, coarse_max_it, smooth_precision)
+                        esteig_steps, coarse_rtol, coarse_max_it, smooth_precision,
+                        MG_COARSE_SPACES.index(coarse_space))
         _ffi.check(_ffi.lib().tdg_mg_setup(self._h, C.byref(o), _stream(stream)))
 
     def mg_apply(self, r, z, nrhs: int = 1, ld: int | None = None, stream=None) -> None:

@@ -4,7 +4,8 @@
   P^T A P of the oracle's dense operator to 1e-12 relative (max norm).
 * The Lanczos estimates of lambda_max(D^-1 A_l) lie in [0.7, 1 + 1e-9] x the exact value.
 * One V-cycle equals the dense restatement of PCMG's V-cycle (oracle.DenseMultigrid, exact
-  coarse solve; the device's coarse CG runs to 1e-13) to 1e-9 relative.
+  coarse solve; the device's coarse CG runs to 1e-13) to 1e-9 relative, with the coarse solve on
+  the coarsest DG level or on the continuous P1 level below it.
 * Multigrid-preconditioned (flexible) CG solves reach the 1e-10 residual target, checked with the
   oracle's operator, in far fewer iterations than block Jacobi: single problems (FP64 and mixed),
   a segmented batch and multiple right-hand sides."""
@@ -40,6 +41,27 @@ def dense(orc, n):
 def prolongations(op, kind, dim, degrees):
     return [element_interpolation(op.E, op.Q, oracle.mg_interpolation(dim, kind, degrees[l + 1], degrees[l]))
             for l in range(len(degrees) - 1)]
+
+
+def p1_embedding(m, op, kind, dim, degree0):
+    """Dense R: continuous P1 (mesh vertices, Q components) -> the coarsest DG level; on element e
+    corner i of the (sorted) element, coefficient k of component p gets T[k, i], T the DG basis
+    coefficients of the corner's hat function (inverse basis Vandermonde at the warp & blend
+    nodes times the barycentric coordinates of those nodes)."""
+    from tandem_b200.refelem import MODAL, WARP_BLEND, ref_basis, ref_nodes
+    nodes = ref_nodes(dim, degree0)
+    Eb = ref_basis(dim, degree0, MODAL if kind == POISSON else WARP_BLEND, nodes)
+    Eb = Eb[0] if isinstance(Eb, tuple) else Eb
+    lam = np.concatenate([1.0 - nodes.sum(axis=1, keepdims=True), nodes], axis=1)
+    T = np.linalg.solve(Eb.T, lam)
+    nbf, Q = T.shape[0], op.Q
+    nv = int(m.elements.max()) + 1
+    R = np.zeros((op.E * nbf * Q, nv * Q))
+    for e in range(op.E):
+        for i, v in enumerate(m.elements[e]):
+            for p in range(Q):
+                R[e * nbf * Q + p * nbf:e * nbf * Q + (p + 1) * nbf, v * Q + p] += T[:, i]
+    return R
 
 
 def level_dense(op, level):
@@ -96,15 +118,23 @@ def test_chebyshev_bounds_from_lanczos():
         assert 0.7 * lam <= est <= lam * (1 + 1e-9), (l, est, lam)
 
 
+@pytest.mark.parametrize("coarse_space", ["dg", "p1"])
 @pytest.mark.parametrize("case", [(POISSON, 2, 3, 4, "full"), (ELASTICITY, 2, 3, 4, "logarithmic"),
-                                  (ELASTICITY, 3, 1, 3, "full")], ids=lambda c: "k{}d{}n{}p{}{}".format(*c))
-def test_vcycle_matches_dense_restatement(case):
+                                  (ELASTICITY, 3, 1, 3, "full"), (POISSON, 3, 2, 2, "twolevel")],
+                         ids=lambda c: "k{}d{}n{}p{}{}".format(*c))
+def test_vcycle_matches_dense_restatement(case, coarse_space):
+    """coarse_space "p1": the restatement's coarsest level is the continuous P1 space of the
+    mesh's own vertex numbering (the V-cycle does not depend on how the vertices are numbered)."""
     kind, dim, n, N, strategy = case
-    _, op, orc = product_and_oracle(kind, dim, n, N, True, True)
-    op.mg_setup(strategy=strategy, coarse_rtol=1e-13, coarse_max_it=20000)
+    m, op, orc = product_and_oracle(kind, dim, n, N, True, True)
+    op.mg_setup(strategy=strategy, coarse_rtol=1e-13, coarse_max_it=20000, coarse_space=coarse_space)
     info = op.mg_info()
     P = prolongations(op, kind, dim, info["degrees"])
-    dm = DenseMultigrid(dense(orc, op.ndof), P, info["lambda_max"], smooth_its=10, esteig=(0.01, 1.1))
+    lmax = list(info["lambda_max"])
+    if coarse_space == "p1":
+        P = [p1_embedding(m, op, kind, dim, info["degrees"][0])] + P
+        lmax = [0.0] + lmax
+    dm = DenseMultigrid(dense(orc, op.ndof), P, lmax, smooth_its=10, esteig=(0.01, 1.1))
     r = np.random.default_rng(5).standard_normal(op.ndof)
     z = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
     op.mg_apply(dev(r), z)
@@ -121,13 +151,14 @@ def _bj_iterations(op, b):
 
 @pytest.mark.parametrize("kind,dim,n", [(POISSON, 2, 8), (ELASTICITY, 2, 6), (ELASTICITY, 3, 2)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_mg_solve_reaches_target(kind, dim, n, precision):
+@pytest.mark.parametrize("coarse_space", ["dg", "p1"])
+def test_mg_solve_reaches_target(kind, dim, n, precision, coarse_space):
     prec = FP64 if precision == "fp64" else MIXED
     _, op, orc = product_and_oracle(kind, dim, n, 4, True, True)
     _, _, _, f, g = mms_inputs(op, kind, dim, True)
     b = op.rhs(f, g)
     its_bj = _bj_iterations(op, b)
-    op.mg_setup(smooth_precision=prec)
+    op.mg_setup(smooth_precision=prec, coarse_space=coarse_space)
     op.set_preconditioner("mg")
     if prec == MIXED:
         op.bjacobi_setup(FP32)
