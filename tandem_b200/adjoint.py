@@ -24,10 +24,12 @@ class LameProblem:
     """Elasticity solve u(lambda, mu) on a fixed mesh, forcing and boundary data.
 
     lam, mu: per-element constants [E].  force_Q: [E, D, Nq] or None; bc_q: [F, D, nq] Dirichlet
-    and fault slip data or None.  Solves are block-Jacobi CG to `rtol` in `precision`."""
+    and fault slip data or None.  Solves are CG to `rtol` in `precision`, preconditioned by block
+    Jacobi or (preconditioner="mg") by the p-multigrid V-cycle, rebuilt whenever the parameters
+    change."""
 
     def __init__(self, op: DGOperator, force_Q=None, bc_q=None, rtol: float = 1e-12, precision: int = FP64,
-                 **solve_kw):
+                 preconditioner: str = "bjacobi", **solve_kw):
         import torch
         if op.kind != 1:
             raise ValueError("LameProblem needs an elasticity operator")
@@ -38,6 +40,9 @@ class LameProblem:
         self.rtol = rtol
         self.precision = precision
         self.pc_precision = FP64 if precision != FP32 else FP32
+        if preconditioner not in ("bjacobi", "mg") or (preconditioner == "mg" and precision == FP32):
+            raise ValueError("preconditioner: 'bjacobi', or 'mg' with FP64 / MIXED solves")
+        self.preconditioner = preconditioner
         self.solve_kw = solve_kw
         self._theta = None
         self.last_stats: list[dict] = []
@@ -52,7 +57,12 @@ class LameProblem:
             return
         ones = np.ones((1, self.op.Nq))
         self.op.set_material(lam[:, None] * ones, mu[:, None] * ones)
-        self.op.bjacobi_setup(self.pc_precision)
+        if self.preconditioner == "mg":
+            self.op.mg_setup(smooth_precision=self.precision)
+            self.op.set_preconditioner("mg")
+        else:
+            self.op.set_preconditioner("bjacobi")
+            self.op.bjacobi_setup(self.pc_precision)
         self._theta = key
 
     def rhs(self):

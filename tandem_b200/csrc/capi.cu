@@ -118,10 +118,11 @@ namespace {
 // One level of the p-multigrid hierarchy.  Coarse levels hold their Galerkin operator as element
 // block-sparse blocks A [E][NB][bs][bs]; the finest level is the matrix-free operator.  ip is the
 // interpolation from this level to the next finer one.  x, b are the level's solution and
-// right-hand side (the caller's z and r on the finest level), r, d, y, w work vectors.
+// right-hand side (the caller's z and r on the finest level), r, d, y, w work vectors; every
+// vector holds up to `cap` columns at stride ld (the caller's ld on the finest level, n below).
 struct MgLevel {
     int degree = 0, bs = 0;
-    int64_t n = 0;
+    int64_t n = 0, ld = 0;
     double* A = nullptr;
     double* dinv = nullptr;
     MgInterp ip{};
@@ -135,31 +136,37 @@ struct MgHierarchy {
     int fine_prec = TDG_FP64;
     int NB = 0, ncolours = 0;
     std::vector<MgLevel> lv;  // coarsest first; lv.back() is the matrix-free operator
-    DevArena arena;
+    DevArena arena;           // operators, diagonals, interpolation, topology
+    DevArena ws;              // work vectors, sized for cap right-hand sides
+    int cap = 0;
+    int64_t fine_ld = 0;
     int32_t* nbr = nullptr;
     int32_t* colour = nullptr;
-    // coarsest-level CG: block-Jacobi inverses, vectors, single-segment plan and scalars
+    int* status = nullptr;
+    int64_t coarse_its = 0;
+    // the coarse system the CG solves: the coarsest DG level, or (aux) the continuous P1 level
+    // below it; cn unknowns per right-hand side, block-Jacobi blocks of cbs x cbs, cnb of them
+    bool aux = false;
+    MgAux ax{};
+    double *ab = nullptr, *axv = nullptr;
+    int64_t cn = 0, cnb = 0;
+    int cbs = 0;
+    // coarse CG: block-Jacobi inverses, vectors of cap columns, one segment (own scalars and
+    // stopping test) per column, chunk plan (seg_chunk_h: its host copy)
     double* cinv = nullptr;
     double *cr = nullptr, *cz = nullptr, *cp = nullptr, *cq = nullptr;
     double* partial = nullptr;
     double* scal = nullptr;
     Chunk* chunks = nullptr;
     int* seg_chunk = nullptr;
-    int nchunks = 0;
-    int* status = nullptr;
-    int64_t coarse_its = 0;
-    // the coarse system the CG solves: the coarsest DG level, or (aux) the continuous P1 level
-    // below it; cn unknowns, block-Jacobi blocks of cbs x cbs, cnb of them
-    bool aux = false;
-    MgAux ax{};
-    double *ab = nullptr, *axv = nullptr;
-    int64_t cn = 0, cnb = 0;
-    int cbs = 0;
-    // coarsest-level CG: a block of kCoarseBlock iterations captured once (its vectors never move)
+    std::vector<int> seg_chunk_h;
+    // coarse CG: a block of kCoarseBlock iterations captured for graph_nrhs columns
     cudaGraphExec_t coarse_exec = nullptr;
+    int graph_nrhs = 0;
     void reset_graph() {
         if (coarse_exec) cudaGraphExecDestroy(coarse_exec);
         coarse_exec = nullptr;
+        graph_nrhs = 0;
     }
     ~MgHierarchy() { reset_graph(); }
 };
@@ -510,95 +517,114 @@ int ensure_blocks(tdg_op* op, cudaStream_t s) {
 
 int mgk(int rc, const char* what) { return rc ? fail(rc, std::string("multigrid: ") + what) : 0; }
 
-// y = A_l x, or y = b - A_l x when b != nullptr.
-int mg_level_apply(tdg_op* op, int l, const double* x, double* y, const double* b, cudaStream_t s) {
+// y = A_l x, or y = b - A_l x when b != nullptr, for nrhs columns at the level's stride.
+int mg_level_apply(tdg_op* op, int l, const double* x, double* y, const double* b, int nrhs, cudaStream_t s) {
     auto& mg = op->mg;
     auto const& L = mg.lv[static_cast<size_t>(l)];
     if (l + 1 == static_cast<int>(mg.lv.size())) {
-        TDG_TRY(tdg_apply(op, mg.fine_prec, x, y, 1, L.n, s));
-        if (b) TDG_TRY(mgk(launch_vec_sub(L.n, b, y, y, s), "residual"));
+        TDG_TRY(tdg_apply(op, mg.fine_prec, x, y, nrhs, L.ld, s));
+        if (b) TDG_TRY(mgk(launch_vec_rsub_cols(L.n, nrhs, L.ld, b, y, s), "residual"));
         return 0;
     }
-    return mgk(launch_mg_bsr_apply(op->h.E, mg.NB, L.bs, mg.nbr, L.A, x, b, y, s), "level apply");
+    return mgk(launch_mg_bsr_apply(op->h.E, mg.NB, L.bs, mg.nbr, L.A, x, b, y, nrhs, L.ld, s), "level apply");
 }
 
 // Chebyshev smoothing of A_l x = b on [esteig_lo, esteig_hi] x lambda_max(D^-1 A_l), smooth_its
 // steps (Saad, Alg. 12.1, with the point-Jacobi preconditioner), from x = 0 or from the given x.
-int mg_smooth(tdg_op* op, int l, const double* b, double* x, bool x_zero, cudaStream_t s) {
+int mg_smooth(tdg_op* op, int l, const double* b, double* x, bool x_zero, int nrhs, cudaStream_t s) {
     auto& mg = op->mg;
     auto& L = mg.lv[static_cast<size_t>(l)];
     const double emax = mg.opts.esteig_hi * L.lmax, emin = mg.opts.esteig_lo * L.lmax;
     const double theta = 0.5 * (emax + emin), delta = 0.5 * (emax - emin), sigma = theta / delta;
     double rho = 1.0 / sigma;
     if (x_zero)
-        TDG_TRY(mgk(launch_vec_axpby(L.n, 1.0, b, 0.0, L.r, s), "copy"));
+        TDG_TRY(mgk(launch_vec_copy_cols(L.n, nrhs, L.ld, b, L.r, s), "copy"));
     else
-        TDG_TRY(mg_level_apply(op, l, x, L.r, b, s));
-    TDG_TRY(mgk(launch_cheb_first(L.n, L.dinv, L.r, L.d, x, 1.0 / theta, x_zero ? 1 : 0, s), "Chebyshev"));
+        TDG_TRY(mg_level_apply(op, l, x, L.r, b, nrhs, s));
+    TDG_TRY(mgk(launch_cheb_first(L.n, nrhs, L.ld, L.dinv, L.r, L.d, x, 1.0 / theta, x_zero ? 1 : 0, s), "Chebyshev"));
     for (int k = 1; k < mg.opts.smooth_its; ++k) {
-        TDG_TRY(mg_level_apply(op, l, L.d, L.y, nullptr, s));
+        TDG_TRY(mg_level_apply(op, l, L.d, L.y, nullptr, nrhs, s));
         const double rho1 = 1.0 / (2.0 * sigma - rho);
-        TDG_TRY(mgk(launch_cheb_step(L.n, L.dinv, L.y, L.r, L.d, x, rho1 * rho, 2.0 * rho1 / delta, s), "Chebyshev"));
+        TDG_TRY(mgk(launch_cheb_step(L.n, nrhs, L.ld, L.dinv, L.y, L.r, L.d, x, rho1 * rho, 2.0 * rho1 / delta, s),
+                    "Chebyshev"));
         rho = rho1;
     }
     return 0;
 }
 
-int mg_read_scalars(tdg_op* op, double* hs, cudaStream_t s) {
-    TDG_CUDA_TRY(cudaMemcpyAsync(hs, op->mg.scal, kScal * sizeof(double), cudaMemcpyDeviceToHost, s));
+int mg_read_scalars(tdg_op* op, std::vector<double>& hs, int nrhs, cudaStream_t s) {
+    hs.resize(static_cast<size_t>(nrhs) * kScal);
+    TDG_CUDA_TRY(cudaMemcpyAsync(hs.data(), op->mg.scal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     TDG_CUDA_TRY(cudaStreamSynchronize(s));
     return 0;
 }
 
-// kCoarseBlock CG iterations of the coarsest level with device-resident scalars.
-int mg_coarse_block(tdg_op* op, SegPlan const& sp, double* x, cudaStream_t s) {
+// kCoarseBlock CG iterations of the coarse system with device-resident scalars, nrhs columns.
+int mg_coarse_block(tdg_op* op, SegPlan const& sp, double* x, int nrhs, cudaStream_t s) {
     auto& mg = op->mg;
     auto const& L = mg.lv[0];
     for (int k = 0; k < kCoarseBlock; ++k) {
         if (mg.aux)
-            TDG_TRY(mgk(launch_aux_apply(mg.ax, mg.cp, nullptr, mg.cq, s), "coarse A"));
+            TDG_TRY(mgk(launch_aux_apply(mg.ax, mg.cp, nullptr, mg.cq, nrhs, s), "coarse A"));
         else
-            TDG_TRY(mgk(launch_mg_bsr_apply(op->h.E, mg.NB, L.bs, mg.nbr, L.A, mg.cp, nullptr, mg.cq, s), "coarse A"));
+            TDG_TRY(mgk(launch_mg_bsr_apply(op->h.E, mg.NB, L.bs, mg.nbr, L.A, mg.cp, nullptr, mg.cq, nrhs, mg.cn, s),
+                        "coarse A"));
         TDG_TRY(dots<double>(sp, mg.cp, mg.cq, nullptr, nullptr, mg.partial, mg.scal, kPQ, -1, s));
         k_cg_xr<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, mg.cr, mg.cp, mg.cq, mg.scal);
-        TDG_TRY(mgk(launch_bjac_apply<double, double>(mg.cbs, mg.cnb, mg.cinv, mg.cr, mg.cz, 1, mg.cn, s), "coarse PC"));
+        TDG_TRY(mgk(launch_bjac_apply<double, double>(mg.cbs, mg.cnb, mg.cinv, mg.cr, mg.cz, nrhs, mg.cn, s),
+                    "coarse PC"));
         TDG_TRY(dots<double>(sp, mg.cr, mg.cz, mg.cr, mg.cr, mg.partial, mg.scal, kRZnew, kRR, s));
         k_cg_p<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, mg.cp, mg.cz, mg.scal);
-        k_cg_shift<<<1, 128, 0, s>>>(mg.scal, 1);
+        k_cg_shift<<<(nrhs + 127) / 128, 128, 0, s>>>(mg.scal, nrhs);
     }
     return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "multigrid: coarse CG kernels");
 }
 
-// Coarsest level: CG with the block-Jacobi inverses from x = 0 until ||r|| <= coarse_rtol ||b||
-// (checked every kCoarseBlock iterations, the blocks replayed from a CUDA graph on a non-default
-// stream) or coarse_max_it iterations.  x is always the coarse system's own vector (the coarsest
-// DG level's, or the continuous P1 level's).
-int mg_coarse_solve(tdg_op* op, const double* b, double* x, cudaStream_t s) {
+// Coarse solve of nrhs columns (contiguous, cn entries each): CG with the block-Jacobi inverses
+// from x = 0, one segment per column, until every column has ||r|| <= coarse_rtol ||b|| (checked
+// every kCoarseBlock iterations, the blocks replayed from a CUDA graph on a non-default stream) or
+// coarse_max_it iterations.  x is always the coarse system's own vector (the coarsest DG level's,
+// or the continuous P1 level's).
+int mg_coarse_solve(tdg_op* op, const double* b, double* x, int nrhs, cudaStream_t s) {
     auto& mg = op->mg;
     SegPlan sp;
-    sp.nseg = 1;
-    sp.nchunks = mg.nchunks;
+    sp.nseg = nrhs;
+    sp.nchunks = mg.seg_chunk_h[static_cast<size_t>(nrhs)];
     sp.chunks = mg.chunks;
     sp.seg_chunk = mg.seg_chunk;
-    sp.op_nrhs = 1;
+    sp.op_nrhs = nrhs;
     sp.op_ld = mg.cn;
-    double hs[kScal] = {};
-    hs[kActive] = 1.0;
-    TDG_CUDA_TRY(cudaMemsetAsync(x, 0, mg.cn * sizeof(double), s));
-    TDG_CUDA_TRY(cudaMemcpyAsync(mg.cr, b, mg.cn * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    TDG_CUDA_TRY(cudaMemcpyAsync(mg.scal, hs, sizeof(hs), cudaMemcpyHostToDevice, s));
-    TDG_TRY(mgk(launch_bjac_apply<double, double>(mg.cbs, mg.cnb, mg.cinv, mg.cr, mg.cz, 1, mg.cn, s), "coarse PC"));
+    const size_t nc = static_cast<size_t>(mg.cn) * nrhs;
+    std::vector<double> hs(static_cast<size_t>(nrhs) * kScal, 0.0);
+    for (int c = 0; c < nrhs; ++c) hs[static_cast<size_t>(c) * kScal + kActive] = 1.0;
+    TDG_CUDA_TRY(cudaMemsetAsync(x, 0, nc * sizeof(double), s));
+    TDG_CUDA_TRY(cudaMemcpyAsync(mg.cr, b, nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    TDG_CUDA_TRY(cudaMemcpyAsync(mg.scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    TDG_TRY(mgk(launch_bjac_apply<double, double>(mg.cbs, mg.cnb, mg.cinv, mg.cr, mg.cz, nrhs, mg.cn, s), "coarse PC"));
     k_copy<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, mg.cz, mg.cp);
     TDG_TRY(dots<double>(sp, mg.cr, mg.cz, mg.cr, mg.cr, mg.partial, mg.scal, kRZ, kRR, s));
-    TDG_TRY(mg_read_scalars(op, hs, s));
-    const double tol2 = mg.opts.coarse_rtol * mg.opts.coarse_rtol * hs[kRR];
-    if (!(hs[kRR] > 0.0)) return 0;
+    TDG_TRY(mg_read_scalars(op, hs, nrhs, s));
+    std::vector<double> tol2(static_cast<size_t>(nrhs));
+    bool any = false, changed = false;
+    for (int c = 0; c < nrhs; ++c) {
+        double* sc = &hs[static_cast<size_t>(c) * kScal];
+        tol2[static_cast<size_t>(c)] = mg.opts.coarse_rtol * mg.opts.coarse_rtol * sc[kRR];
+        if (!(sc[kRR] > 0.0)) {
+            sc[kActive] = 0.0;
+            changed = true;
+        } else {
+            any = true;
+        }
+    }
+    if (!any) return 0;
+    if (changed) TDG_CUDA_TRY(cudaMemcpyAsync(mg.scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     int it = 0;
     while (it < mg.opts.coarse_max_it) {
-        if (s != nullptr && !mg.coarse_exec) {
+        if (s != nullptr && (!mg.coarse_exec || mg.graph_nrhs != nrhs)) {
+            mg.reset_graph();
             cudaGraph_t graph = nullptr;
             TDG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            int rc = mg_coarse_block(op, sp, x, s);
+            int rc = mg_coarse_block(op, sp, x, nrhs, s);
             cudaError_t ce = cudaStreamEndCapture(s, &graph);
             if (rc == 0 && ce == cudaSuccess) ce = cudaGraphInstantiate(&mg.coarse_exec, graph, 0);
             if (graph) cudaGraphDestroy(graph);
@@ -607,40 +633,102 @@ int mg_coarse_solve(tdg_op* op, const double* b, double* x, cudaStream_t s) {
                 mg.coarse_exec = nullptr;
                 return fail(TDG_E_CUDA, std::string("multigrid: coarse CG graph: ") + cudaGetErrorString(ce));
             }
+            mg.graph_nrhs = nrhs;
         }
         if (mg.coarse_exec)
             TDG_CUDA_TRY(cudaGraphLaunch(mg.coarse_exec, s));
         else
-            TDG_TRY(mg_coarse_block(op, sp, x, s));
+            TDG_TRY(mg_coarse_block(op, sp, x, nrhs, s));
         it += kCoarseBlock;
-        TDG_TRY(mg_read_scalars(op, hs, s));
-        if (!std::isfinite(hs[kRR])) return fail(TDG_E_DIVERGED, "multigrid: coarse CG diverged");
-        if (hs[kRR] <= tol2) break;
+        TDG_TRY(mg_read_scalars(op, hs, nrhs, s));
+        any = false;
+        changed = false;
+        for (int c = 0; c < nrhs; ++c) {
+            double* sc = &hs[static_cast<size_t>(c) * kScal];
+            if (sc[kActive] == 0.0) continue;
+            if (!std::isfinite(sc[kRR])) return fail(TDG_E_DIVERGED, "multigrid: coarse CG diverged");
+            if (sc[kRR] <= tol2[static_cast<size_t>(c)]) {
+                sc[kActive] = 0.0;
+                changed = true;
+            } else {
+                any = true;
+            }
+        }
+        if (!any) break;
+        if (changed) TDG_CUDA_TRY(cudaMemcpyAsync(mg.scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     }
     mg.coarse_its += it;
     return 0;
 }
 
-// One V-cycle on level l: x = M_l b.  Below the coarsest DG level sits either the coarse solve
-// itself or, with the auxiliary space, a smoothed DG level corrected from the continuous P1 level.
-int mg_vcycle(tdg_op* op, int l, const double* b, double* x, cudaStream_t s) {
+// One V-cycle on level l for nrhs columns: x = M_l b.  Below the coarsest DG level sits either the
+// coarse solve itself or, with the auxiliary space, a smoothed DG level corrected from the
+// continuous P1 level.
+int mg_vcycle(tdg_op* op, int l, const double* b, double* x, int nrhs, cudaStream_t s) {
     auto& mg = op->mg;
-    if (l == 0 && !mg.aux) return mg_coarse_solve(op, b, x, s);
+    if (l == 0 && !mg.aux) return mg_coarse_solve(op, b, x, nrhs, s);
     auto& L = mg.lv[static_cast<size_t>(l)];
     const int64_t E = op->h.E;
-    TDG_TRY(mg_smooth(op, l, b, x, true, s));
-    TDG_TRY(mg_level_apply(op, l, x, L.r, b, s));
+    TDG_TRY(mg_smooth(op, l, b, x, true, nrhs, s));
+    TDG_TRY(mg_level_apply(op, l, x, L.r, b, nrhs, s));
     if (l == 0) {
-        TDG_TRY(mgk(launch_aux_restrict(mg.ax, L.r, mg.ab, s), "restriction to P1"));
-        TDG_TRY(mg_coarse_solve(op, mg.ab, mg.axv, s));
-        TDG_TRY(mgk(launch_aux_prolong_add(mg.ax, E, mg.axv, x, s), "prolongation from P1"));
+        TDG_TRY(mgk(launch_aux_restrict(mg.ax, L.r, L.ld, mg.ab, nrhs, s), "restriction to P1"));
+        TDG_TRY(mg_coarse_solve(op, mg.ab, mg.axv, nrhs, s));
+        TDG_TRY(mgk(launch_aux_prolong_add(mg.ax, E, mg.axv, x, L.ld, nrhs, s), "prolongation from P1"));
     } else {
         auto& C = mg.lv[static_cast<size_t>(l - 1)];
-        TDG_TRY(mgk(launch_mg_restrict(E, C.ip, L.r, C.b, s), "restriction"));
-        TDG_TRY(mg_vcycle(op, l - 1, C.b, C.x, s));
-        TDG_TRY(mgk(launch_mg_prolong_add(E, C.ip, C.x, x, s), "prolongation"));
+        TDG_TRY(mgk(launch_mg_restrict(E, C.ip, L.r, L.ld, C.b, C.ld, nrhs, s), "restriction"));
+        TDG_TRY(mg_vcycle(op, l - 1, C.b, C.x, nrhs, s));
+        TDG_TRY(mgk(launch_mg_prolong_add(E, C.ip, C.x, C.ld, x, L.ld, nrhs, s), "prolongation"));
     }
-    return mg_smooth(op, l, b, x, false, s);
+    return mg_smooth(op, l, b, x, false, nrhs, s);
+}
+
+// Work vectors for nrhs right-hand sides with the finest level's leading dimension ld (grown on
+// demand; reallocation waits for the stream and drops the coarse CG graph).
+int mg_ensure_ws(tdg_op* op, int nrhs, int64_t ld, cudaStream_t s) {
+    auto& mg = op->mg;
+    if (nrhs <= mg.cap && ld == mg.fine_ld) return 0;
+    TDG_CUDA_TRY(cudaStreamSynchronize(s));
+    mg.reset_graph();
+    mg.ws.release();
+    const int cap = std::max(nrhs, mg.cap);
+    const int nl = static_cast<int>(mg.lv.size());
+    for (int l = 0; l < nl; ++l) {
+        auto& L = mg.lv[static_cast<size_t>(l)];
+        L.ld = (l + 1 == nl) ? ld : L.n;
+        const size_t sz = static_cast<size_t>(cap) * static_cast<size_t>(L.ld);
+        if (l + 1 < nl) {
+            TDG_CUDA_TRY(mg.ws.alloc(&L.x, sz));
+            TDG_CUDA_TRY(mg.ws.alloc(&L.b, sz));
+        }
+        for (double** v : {&L.r, &L.d, &L.y, &L.w}) TDG_CUDA_TRY(mg.ws.alloc(v, sz));
+    }
+    const size_t csz = static_cast<size_t>(cap) * static_cast<size_t>(mg.cn);
+    for (double** v : {&mg.cr, &mg.cz, &mg.cp, &mg.cq}) TDG_CUDA_TRY(mg.ws.alloc(v, csz));
+    if (mg.aux) {
+        TDG_CUDA_TRY(mg.ws.alloc(&mg.ab, csz));
+        TDG_CUDA_TRY(mg.ws.alloc(&mg.axv, csz));
+    }
+    std::vector<int64_t> sb(static_cast<size_t>(cap)), se(static_cast<size_t>(cap));
+    for (int c = 0; c < cap; ++c) {
+        sb[static_cast<size_t>(c)] = c * mg.cn;
+        se[static_cast<size_t>(c)] = c * mg.cn + mg.cn;
+    }
+    std::vector<Chunk> hc;
+    plan_chunks(sb, se, hc, mg.seg_chunk_h);
+    const Chunk* dch = nullptr;
+    const int* dsc = nullptr;
+    TDG_CUDA_TRY(mg.ws.upload(&dch, hc));
+    TDG_CUDA_TRY(mg.ws.upload(&dsc, mg.seg_chunk_h));
+    mg.chunks = const_cast<Chunk*>(dch);
+    mg.seg_chunk = const_cast<int*>(dsc);
+    TDG_CUDA_TRY(mg.ws.alloc(&mg.scal, static_cast<size_t>(cap) * kScal));
+    // dot partials: the level dots (kDotBlocks + a result slot) and the coarse CG's chunk pairs
+    TDG_CUDA_TRY(mg.ws.alloc(&mg.partial, std::max<size_t>(kDotBlocks + 8, 2 * hc.size())));
+    mg.cap = cap;
+    mg.fine_ld = ld;
+    return 0;
 }
 
 // Largest eigenvalue of the symmetric tridiagonal matrix (a diagonal, c off-diagonal) by Sturm
@@ -696,7 +784,7 @@ int mg_estimate_lmax(tdg_op* op, int l, cudaStream_t s) {
     TDG_TRY(dot(r, z, &rz));
     std::vector<double> alpha, beta;
     for (int k = 0; k < mg.opts.esteig_steps && rz > 0.0; ++k) {
-        TDG_TRY(mg_level_apply(op, l, p, q, nullptr, s));
+        TDG_TRY(mg_level_apply(op, l, p, q, nullptr, 1, s));
         double pq = 0.0;
         TDG_TRY(dot(p, q, &pq));
         if (!(pq > 0.0)) break;
@@ -801,8 +889,6 @@ int mg_setup_aux(tdg_op* op, cudaStream_t s) {
     mg.cn = nv * h.Q;
     mg.cbs = h.Q;
     mg.cnb = nv;
-    TDG_CUDA_TRY(mg.arena.alloc(&mg.ab, static_cast<size_t>(mg.cn)));
-    TDG_CUDA_TRY(mg.arena.alloc(&mg.axv, static_cast<size_t>(mg.cn)));
     // diagonal blocks, column-major, for the block-Jacobi inversion
     const int Q = h.Q;
     std::vector<double> diag(static_cast<size_t>(nv) * Q * Q, 0.0);
@@ -844,6 +930,7 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
     if (deg.size() < 2) return fail(TDG_E_INVALID, "multigrid: needs at least two levels");
     // a fresh hierarchy
     mg.reset_graph();
+    mg.ws.release();
     mg.arena.release();
     mg.lv.clear();
     mg.ready = false;
@@ -872,22 +959,15 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
         L.degree = deg[static_cast<size_t>(l)];
         L.bs = num_basis(h.D, L.degree) * h.Q;
         L.n = E * L.bs;
-        const size_t n = static_cast<size_t>(L.n);
         if (l + 1 < nl) {
             TDG_CUDA_TRY(mg.arena.alloc(&L.A, static_cast<size_t>(E) * mg.NB * L.bs * L.bs));
             TDG_CUDA_TRY(cudaMemsetAsync(L.A, 0, sizeof(double) * E * mg.NB * L.bs * L.bs, s));
-            TDG_CUDA_TRY(mg.arena.alloc(&L.x, n));
-            TDG_CUDA_TRY(mg.arena.alloc(&L.b, n));
             Dense I = interpolation_matrix(h.D, h.kind, deg[static_cast<size_t>(l + 1)], L.degree);
             const double* dI = nullptr;
             TDG_CUDA_TRY(mg.arena.upload(&dI, I.a));
             L.ip = MgInterp{dI, I.rows, I.cols, h.Q};
         }
-        TDG_CUDA_TRY(mg.arena.alloc(&L.dinv, n));
-        TDG_CUDA_TRY(mg.arena.alloc(&L.r, n));
-        TDG_CUDA_TRY(mg.arena.alloc(&L.d, n));
-        TDG_CUDA_TRY(mg.arena.alloc(&L.y, n));
-        TDG_CUDA_TRY(mg.arena.alloc(&L.w, n));
+        TDG_CUDA_TRY(mg.arena.alloc(&L.dinv, static_cast<size_t>(L.n)));
     }
     TDG_CUDA_TRY(mg.arena.alloc(&mg.status, 1));
     TDG_CUDA_TRY(cudaMemsetAsync(mg.status, 0, sizeof(int), s));
@@ -931,22 +1011,10 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
     TDG_CUDA_TRY(cudaMemcpyAsync(&st, mg.status, sizeof(int), cudaMemcpyDeviceToHost, s));
     TDG_CUDA_TRY(cudaStreamSynchronize(s));
     if (st) return fail(TDG_E_NOT_SPD, "multigrid: a level diagonal or coarse block is not positive definite");
-    for (double** v : {&mg.cr, &mg.cz, &mg.cp, &mg.cq}) TDG_CUDA_TRY(mg.arena.alloc(v, static_cast<size_t>(mg.cn)));
-    {
-        std::vector<Chunk> hc;
-        std::vector<int> hsc;
-        plan_chunks({0}, {mg.cn}, hc, hsc);
-        const Chunk* dch = nullptr;
-        const int* dsc = nullptr;
-        TDG_CUDA_TRY(mg.arena.upload(&dch, hc));
-        TDG_CUDA_TRY(mg.arena.upload(&dsc, hsc));
-        mg.chunks = const_cast<Chunk*>(dch);
-        mg.seg_chunk = const_cast<int*>(dsc);
-        mg.nchunks = static_cast<int>(hc.size());
-        TDG_CUDA_TRY(mg.arena.alloc(&mg.scal, static_cast<size_t>(kScal)));
-        // dot partials: the level dots (kDotBlocks + a result slot) and the coarsest CG's chunk pairs
-        TDG_CUDA_TRY(mg.arena.alloc(&mg.partial, std::max<size_t>(kDotBlocks + 8, 2 * hc.size())));
-    }
+    // work vectors for one right-hand side (grown by tdg_mg_apply on demand)
+    mg.cap = 0;
+    mg.fine_ld = 0;
+    TDG_TRY(mg_ensure_ws(op, 1, mg.lv.back().n, s));
     // Chebyshev bounds of the smoothed levels
     for (int l = mg.aux ? 0 : 1; l < nl; ++l) TDG_TRY(mg_estimate_lmax(op, l, s));
     mg.ready = true;
@@ -957,9 +1025,8 @@ int mg_apply(tdg_op* op, const double* r, double* z, int nrhs, int64_t ld, cudaS
     auto& mg = op->mg;
     if (!mg.ready) return fail(TDG_E_STATE, "tdg_mg_setup not called");
     if (nrhs < 1 || ld < mg.lv.back().n) return fail(TDG_E_INVALID, "nrhs < 1 or ld < E * bs");
-    const int top = static_cast<int>(mg.lv.size()) - 1;
-    for (int k = 0; k < nrhs; ++k) TDG_TRY(mg_vcycle(op, top, r + k * ld, z + k * ld, s));
-    return 0;
+    TDG_TRY(mg_ensure_ws(op, nrhs, ld, s));
+    return mg_vcycle(op, static_cast<int>(mg.lv.size()) - 1, r, z, nrhs, s);
 }
 
 // z = M r with the preconditioner the solves use (multigrid for FP64 vectors when selected).

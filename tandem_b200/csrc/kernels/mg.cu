@@ -94,21 +94,26 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+// Column c of x, b, y starts at c * ld (nrhs columns).
 __global__ void __launch_bounds__(kT)
     k_bsr_apply(int64_t E, int NB, int bs, const int32_t* __restrict__ nbr, const double* __restrict__ A,
-                const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y) {
-    TDG_GRID_LOOP(g, E * bs) {
-        const int row = static_cast<int>(g % bs);
-        const int64_t n = g / bs;
+                const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y, int nrhs,
+                int64_t ld) {
+    const int64_t n = E * bs;
+    TDG_GRID_LOOP(g, n * nrhs) {
+        const int64_t c = g / n, gi = g % n;
+        const int row = static_cast<int>(gi % bs);
+        const int64_t e = gi / bs;
+        const double* xc = x + c * ld;
         double acc = 0.0;
         for (int s = 0; s < NB; ++s) {
-            const int32_t t = nbr[n * NB + s];
+            const int32_t t = nbr[e * NB + s];
             if (t < 0) continue;
-            const double* blk = A + (n * NB + s) * bs * bs;
-            const double* xt = x + static_cast<int64_t>(t) * bs;
+            const double* blk = A + (e * NB + s) * bs * bs;
+            const double* xt = xc + static_cast<int64_t>(t) * bs;
             for (int col = 0; col < bs; ++col) acc += blk[col * bs + row] * xt[col];
         }
-        y[g] = b ? b[g] - acc : acc;
+        y[c * ld + gi] = b ? b[c * ld + gi] - acc : acc;
     }
 }
 
@@ -117,20 +122,24 @@ __global__ void __launch_bounds__(kT)
 template <int BS>
 __global__ void __launch_bounds__(kT)
     k_bsr_apply_t(int64_t E, int NB, const int32_t* __restrict__ nbr, const double* __restrict__ A,
-                  const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y) {
-    TDG_GRID_LOOP(g, E * BS) {
-        const int row = static_cast<int>(g % BS);
-        const int64_t n = g / BS;
+                  const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y, int nrhs,
+                  int64_t ld) {
+    const int64_t n = E * BS;
+    TDG_GRID_LOOP(g, n * nrhs) {
+        const int64_t c = g / n, gi = g % n;
+        const int row = static_cast<int>(gi % BS);
+        const int64_t e = gi / BS;
+        const double* xc = x + c * ld;
         double acc = 0.0;
         for (int s = 0; s < NB; ++s) {
-            const int32_t t = nbr[n * NB + s];
+            const int32_t t = nbr[e * NB + s];
             if (t < 0) continue;
-            const double* blk = A + (n * NB + s) * (BS * BS) + row;
-            const double* xt = x + static_cast<int64_t>(t) * BS;
+            const double* blk = A + (e * NB + s) * (BS * BS) + row;
+            const double* xt = xc + static_cast<int64_t>(t) * BS;
 #pragma unroll
             for (int col = 0; col < BS; ++col) acc += blk[col * BS] * xt[col];
         }
-        y[g] = b ? b[g] - acc : acc;
+        y[c * ld + gi] = b ? b[c * ld + gi] - acc : acc;
     }
 }
 
@@ -159,60 +168,75 @@ __global__ void __launch_bounds__(kT)
 }
 
 __global__ void __launch_bounds__(kT)
-    k_prolong_add(int64_t E, MgInterp ip, const double* __restrict__ xc, double* __restrict__ xf) {
+    k_prolong_add(int64_t E, MgInterp ip, const double* __restrict__ xc, int64_t ldc, double* __restrict__ xf,
+                  int64_t ldf, int nrhs) {
     const int bsc = ip.N2 * ip.Q;
-    TDG_GRID_LOOP(g, E * ip.Q * ip.N1) {  // g = e * bsf + p * N1 + k
-        const int k = static_cast<int>(g % ip.N1);
-        const int p = static_cast<int>((g / ip.N1) % ip.Q);
-        const int64_t e = g / (static_cast<int64_t>(ip.N1) * ip.Q);
-        const double* c = xc + e * bsc + p * ip.N2;
+    const int64_t nf = E * ip.Q * ip.N1;
+    TDG_GRID_LOOP(g, nf * nrhs) {  // gi = e * bsf + p * N1 + k
+        const int64_t col = g / nf, gi = g % nf;
+        const int k = static_cast<int>(gi % ip.N1);
+        const int p = static_cast<int>((gi / ip.N1) % ip.Q);
+        const int64_t e = gi / (static_cast<int64_t>(ip.N1) * ip.Q);
+        const double* c = xc + col * ldc + e * bsc + p * ip.N2;
         double acc = 0.0;
         for (int l = 0; l < ip.N2; ++l) acc += ip.I[k * ip.N2 + l] * c[l];
-        xf[g] += acc;
+        xf[col * ldf + gi] += acc;
     }
 }
 
 __global__ void __launch_bounds__(kT)
-    k_restrict(int64_t E, MgInterp ip, const double* __restrict__ rf, double* __restrict__ rc) {
+    k_restrict(int64_t E, MgInterp ip, const double* __restrict__ rf, int64_t ldf, double* __restrict__ rc,
+               int64_t ldc, int nrhs) {
     const int bsf = ip.N1 * ip.Q;
-    TDG_GRID_LOOP(g, E * ip.Q * ip.N2) {  // g = e * bsc + p * N2 + l
-        const int l = static_cast<int>(g % ip.N2);
-        const int p = static_cast<int>((g / ip.N2) % ip.Q);
-        const int64_t e = g / (static_cast<int64_t>(ip.N2) * ip.Q);
-        const double* f = rf + e * bsf + p * ip.N1;
+    const int64_t nc = E * ip.Q * ip.N2;
+    TDG_GRID_LOOP(g, nc * nrhs) {  // gi = e * bsc + p * N2 + l
+        const int64_t col = g / nc, gi = g % nc;
+        const int l = static_cast<int>(gi % ip.N2);
+        const int p = static_cast<int>((gi / ip.N2) % ip.Q);
+        const int64_t e = gi / (static_cast<int64_t>(ip.N2) * ip.Q);
+        const double* f = rf + col * ldf + e * bsf + p * ip.N1;
         double acc = 0.0;
         for (int k = 0; k < ip.N1; ++k) acc += ip.I[k * ip.N2 + l] * f[k];
-        rc[g] = acc;
+        rc[col * ldc + gi] = acc;
     }
 }
 
+// The P1 vectors have nrhs contiguous columns of nv * Q entries; the DG level's columns start at
+// multiples of ld0.
 __global__ void __launch_bounds__(kT)
-    k_aux_apply(MgAux a, const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y) {
+    k_aux_apply(MgAux a, const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y,
+                int nrhs) {
     const int Q = a.Q, QQ = a.Q * a.Q;
-    TDG_GRID_LOOP(g, a.nv * Q) {
-        const int64_t v = g / Q;
-        const int p = static_cast<int>(g % Q);
+    const int64_t n = a.nv * Q;
+    TDG_GRID_LOOP(g, n * nrhs) {
+        const int64_t col = g / n, gi = g % n;
+        const int64_t v = gi / Q;
+        const int p = static_cast<int>(gi % Q);
+        const double* xcol = x + col * n;
         double acc = 0.0;
         for (int64_t k = a.ptr[v]; k < a.ptr[v + 1]; ++k) {
             const double* blk = a.val + k * QQ + p * Q;
-            const double* xw = x + static_cast<int64_t>(a.col[k]) * Q;
+            const double* xw = xcol + static_cast<int64_t>(a.col[k]) * Q;
             for (int q = 0; q < Q; ++q) acc += blk[q] * xw[q];
         }
         y[g] = b ? b[g] - acc : acc;
     }
 }
 
-__global__ void __launch_bounds__(kT) k_aux_restrict(MgAux a, const double* __restrict__ r0, double* __restrict__ rc) {
+__global__ void __launch_bounds__(kT)
+    k_aux_restrict(MgAux a, const double* __restrict__ r0, int64_t ld0, double* __restrict__ rc, int nrhs) {
     const int Q = a.Q, bs = a.Nbf * a.Q;
-    TDG_GRID_LOOP(g, a.nv * Q) {
-        const int64_t v = g / Q;
-        const int p = static_cast<int>(g % Q);
+    const int64_t n = a.nv * Q;
+    TDG_GRID_LOOP(g, n * nrhs) {
+        const int64_t col = g / n, gi = g % n;
+        const int64_t v = gi / Q;
+        const int p = static_cast<int>(gi % Q);
         double acc = 0.0;
         for (int64_t k = a.vinc_ptr[v]; k < a.vinc_ptr[v + 1]; ++k) {
             const int32_t inc = a.vinc[k];
             const int64_t e = inc / a.NV;
             const int i = inc % a.NV;
-            const double* r = r0 + e * bs + p * a.Nbf;
+            const double* r = r0 + col * ld0 + e * bs + p * a.Nbf;
             for (int kk = 0; kk < a.Nbf; ++kk) acc += a.T[kk * a.NV + i] * r[kk];
         }
         rc[g] = acc;
@@ -220,36 +244,59 @@ __global__ void __launch_bounds__(kT) k_aux_restrict(MgAux a, const double* __re
 }
 
 __global__ void __launch_bounds__(kT)
-    k_aux_prolong_add(MgAux a, int64_t E, const double* __restrict__ xc, double* __restrict__ x0) {
+    k_aux_prolong_add(MgAux a, int64_t E, const double* __restrict__ xc, double* __restrict__ x0, int64_t ld0,
+                      int nrhs) {
     const int bs = a.Nbf * a.Q;
-    TDG_GRID_LOOP(g, E * bs) {  // g = e * bs + p * Nbf + kk
-        const int64_t e = g / bs;
-        const int p = static_cast<int>((g % bs) / a.Nbf), kk = static_cast<int>(g % a.Nbf);
+    const int64_t n0 = E * bs, nc = a.nv * a.Q;
+    TDG_GRID_LOOP(g, n0 * nrhs) {  // gi = e * bs + p * Nbf + kk
+        const int64_t col = g / n0, gi = g % n0;
+        const int64_t e = gi / bs;
+        const int p = static_cast<int>((gi % bs) / a.Nbf), kk = static_cast<int>(gi % a.Nbf);
+        const double* xcol = xc + col * nc;
         double acc = 0.0;
-        for (int i = 0; i < a.NV; ++i) acc += a.T[kk * a.NV + i] * xc[static_cast<int64_t>(a.vid[e * a.NV + i]) * a.Q + p];
-        x0[g] += acc;
+        for (int i = 0; i < a.NV; ++i) acc += a.T[kk * a.NV + i] * xcol[static_cast<int64_t>(a.vid[e * a.NV + i]) * a.Q + p];
+        x0[col * ld0 + gi] += acc;
     }
 }
 
+// Chebyshev kernels over nrhs columns of n entries at stride ld (the diagonal is shared).
 __global__ void __launch_bounds__(kT)
-    k_cheb_first(int64_t n, const double* __restrict__ dinv, const double* __restrict__ r, double* __restrict__ d,
-                 double* __restrict__ x, double c, int x_zero) {
-    TDG_GRID_LOOP(i, n) {
-        const double di = c * dinv[i] * r[i];
+    k_cheb_first(int64_t n, int nrhs, int64_t ld, const double* __restrict__ dinv, const double* __restrict__ r,
+                 double* __restrict__ d, double* __restrict__ x, double c, int x_zero) {
+    TDG_GRID_LOOP(g, n * nrhs) {
+        const int64_t j = g % n, i = (g / n) * ld + j;
+        const double di = c * dinv[j] * r[i];
         d[i] = di;
         x[i] = x_zero ? di : x[i] + di;
     }
 }
 
 __global__ void __launch_bounds__(kT)
-    k_cheb_step(int64_t n, const double* __restrict__ dinv, const double* __restrict__ y, double* __restrict__ r,
-                double* __restrict__ d, double* __restrict__ x, double c1, double c2) {
-    TDG_GRID_LOOP(i, n) {
+    k_cheb_step(int64_t n, int nrhs, int64_t ld, const double* __restrict__ dinv, const double* __restrict__ y,
+                double* __restrict__ r, double* __restrict__ d, double* __restrict__ x, double c1, double c2) {
+    TDG_GRID_LOOP(g, n * nrhs) {
+        const int64_t j = g % n, i = (g / n) * ld + j;
         const double ri = r[i] - y[i];
-        const double di = c1 * d[i] + c2 * dinv[i] * ri;
+        const double di = c1 * d[i] + c2 * dinv[j] * ri;
         r[i] = ri;
         d[i] = di;
         x[i] += di;
+    }
+}
+
+// y = x over nrhs columns of n entries at stride ld; y = a - y likewise.
+__global__ void __launch_bounds__(kT)
+    k_copy_cols(int64_t n, int nrhs, int64_t ld, const double* __restrict__ x, double* __restrict__ y) {
+    TDG_GRID_LOOP(g, n * nrhs) {
+        const int64_t i = (g / n) * ld + g % n;
+        y[i] = x[i];
+    }
+}
+
+__global__ void __launch_bounds__(kT) k_rsub_cols(int64_t n, int nrhs, int64_t ld, const double* a, double* y) {
+    TDG_GRID_LOOP(g, n * nrhs) {
+        const int64_t i = (g / n) * ld + g % n;
+        y[i] = a[i] - y[i];
     }
 }
 
@@ -334,15 +381,15 @@ int launch_mg_triple(int64_t E, int NB, const int32_t* nbr, MgInterp ip, const d
 }
 
 int launch_mg_bsr_apply(int64_t E, int NB, int bs, const int32_t* nbr, const double* A, const double* x,
-                        const double* b, double* y, cudaStream_t s) {
-    const unsigned g = grid_for(E * bs);
+                        const double* b, double* y, int nrhs, int64_t ld, cudaStream_t s) {
+    const unsigned g = grid_for(E * bs * nrhs);
     switch (bs) {
 #define TDG_BSR_CASE(B) \
-    case B: k_bsr_apply_t<B><<<g, kT, 0, s>>>(E, NB, nbr, A, x, b, y); break;
+    case B: k_bsr_apply_t<B><<<g, kT, 0, s>>>(E, NB, nbr, A, x, b, y, nrhs, ld); break;
         TDG_BSR_CASE(1) TDG_BSR_CASE(2) TDG_BSR_CASE(3) TDG_BSR_CASE(4) TDG_BSR_CASE(6) TDG_BSR_CASE(10)
         TDG_BSR_CASE(12) TDG_BSR_CASE(20) TDG_BSR_CASE(30) TDG_BSR_CASE(60)
 #undef TDG_BSR_CASE
-        default: k_bsr_apply<<<g, kT, 0, s>>>(E, NB, bs, nbr, A, x, b, y);
+        default: k_bsr_apply<<<g, kT, 0, s>>>(E, NB, bs, nbr, A, x, b, y, nrhs, ld);
     }
     return launched();
 }
@@ -358,40 +405,53 @@ int launch_mg_self_blocks(int64_t E, int NB, int bs, const double* A, double* bl
     return launched();
 }
 
-int launch_mg_prolong_add(int64_t E, MgInterp ip, const double* xc, double* xf, cudaStream_t s) {
-    k_prolong_add<<<grid_for(E * ip.Q * ip.N1), kT, 0, s>>>(E, ip, xc, xf);
+int launch_mg_prolong_add(int64_t E, MgInterp ip, const double* xc, int64_t ldc, double* xf, int64_t ldf, int nrhs,
+                          cudaStream_t s) {
+    k_prolong_add<<<grid_for(E * ip.Q * ip.N1 * nrhs), kT, 0, s>>>(E, ip, xc, ldc, xf, ldf, nrhs);
     return launched();
 }
 
-int launch_mg_restrict(int64_t E, MgInterp ip, const double* rf, double* rc, cudaStream_t s) {
-    k_restrict<<<grid_for(E * ip.Q * ip.N2), kT, 0, s>>>(E, ip, rf, rc);
+int launch_mg_restrict(int64_t E, MgInterp ip, const double* rf, int64_t ldf, double* rc, int64_t ldc, int nrhs,
+                       cudaStream_t s) {
+    k_restrict<<<grid_for(E * ip.Q * ip.N2 * nrhs), kT, 0, s>>>(E, ip, rf, ldf, rc, ldc, nrhs);
     return launched();
 }
 
-int launch_aux_apply(MgAux const& a, const double* x, const double* b, double* y, cudaStream_t s) {
-    k_aux_apply<<<grid_for(a.nv * a.Q), kT, 0, s>>>(a, x, b, y);
+int launch_aux_apply(MgAux const& a, const double* x, const double* b, double* y, int nrhs, cudaStream_t s) {
+    k_aux_apply<<<grid_for(a.nv * a.Q * nrhs), kT, 0, s>>>(a, x, b, y, nrhs);
     return launched();
 }
 
-int launch_aux_restrict(MgAux const& a, const double* r0, double* rc, cudaStream_t s) {
-    k_aux_restrict<<<grid_for(a.nv * a.Q), kT, 0, s>>>(a, r0, rc);
+int launch_aux_restrict(MgAux const& a, const double* r0, int64_t ld0, double* rc, int nrhs, cudaStream_t s) {
+    k_aux_restrict<<<grid_for(a.nv * a.Q * nrhs), kT, 0, s>>>(a, r0, ld0, rc, nrhs);
     return launched();
 }
 
-int launch_aux_prolong_add(MgAux const& a, int64_t E, const double* xc, double* x0, cudaStream_t s) {
-    k_aux_prolong_add<<<grid_for(E * a.Nbf * a.Q), kT, 0, s>>>(a, E, xc, x0);
+int launch_aux_prolong_add(MgAux const& a, int64_t E, const double* xc, double* x0, int64_t ld0, int nrhs,
+                           cudaStream_t s) {
+    k_aux_prolong_add<<<grid_for(E * a.Nbf * a.Q * nrhs), kT, 0, s>>>(a, E, xc, x0, ld0, nrhs);
     return launched();
 }
 
-int launch_cheb_first(int64_t n, const double* dinv, const double* r, double* d, double* x, double c, int x_zero,
-                      cudaStream_t s) {
-    k_cheb_first<<<grid_for(n), kT, 0, s>>>(n, dinv, r, d, x, c, x_zero);
+int launch_cheb_first(int64_t n, int nrhs, int64_t ld, const double* dinv, const double* r, double* d, double* x,
+                      double c, int x_zero, cudaStream_t s) {
+    k_cheb_first<<<grid_for(n * nrhs), kT, 0, s>>>(n, nrhs, ld, dinv, r, d, x, c, x_zero);
     return launched();
 }
 
-int launch_cheb_step(int64_t n, const double* dinv, const double* y, double* r, double* d, double* x, double c1,
-                     double c2, cudaStream_t s) {
-    k_cheb_step<<<grid_for(n), kT, 0, s>>>(n, dinv, y, r, d, x, c1, c2);
+int launch_cheb_step(int64_t n, int nrhs, int64_t ld, const double* dinv, const double* y, double* r, double* d,
+                     double* x, double c1, double c2, cudaStream_t s) {
+    k_cheb_step<<<grid_for(n * nrhs), kT, 0, s>>>(n, nrhs, ld, dinv, y, r, d, x, c1, c2);
+    return launched();
+}
+
+int launch_vec_copy_cols(int64_t n, int nrhs, int64_t ld, const double* x, double* y, cudaStream_t s) {
+    k_copy_cols<<<grid_for(n * nrhs), kT, 0, s>>>(n, nrhs, ld, x, y);
+    return launched();
+}
+
+int launch_vec_rsub_cols(int64_t n, int nrhs, int64_t ld, const double* a, double* y, cudaStream_t s) {
+    k_rsub_cols<<<grid_for(n * nrhs), kT, 0, s>>>(n, nrhs, ld, a, y);
     return launched();
 }
 

@@ -30,18 +30,20 @@ int launch_mg_probe_extract(int64_t E, int NB, const int32_t* nbr, const int32_t
 // Ac[n][s] = I^T Af[n][s] I for every present block.
 int launch_mg_triple(int64_t E, int NB, const int32_t* nbr, MgInterp ip, const double* Af, double* Ac,
                      cudaStream_t s);
-// y = A x (b == nullptr) or y = b - A x.
+// y = A x (b == nullptr) or y = b - A x, for nrhs columns starting at multiples of ld.
 int launch_mg_bsr_apply(int64_t E, int NB, int bs, const int32_t* nbr, const double* A, const double* x,
-                        const double* b, double* y, cudaStream_t s);
+                        const double* b, double* y, int nrhs, int64_t ld, cudaStream_t s);
 // dinv[e][i] = 1 / blocks[e * stride + i * bs + i] (point Jacobi); status set on a non-positive
 // diagonal entry.
 int launch_mg_diag_inv(int64_t E, int bs, int64_t stride, const double* blocks, double* dinv, int* status,
                        cudaStream_t s);
 // blk[e] = A[e][0] (self blocks, contiguous, for the block-Jacobi inversion).
 int launch_mg_self_blocks(int64_t E, int NB, int bs, const double* A, double* blk, cudaStream_t s);
-// xf += I xc; rc = I^T rf.
-int launch_mg_prolong_add(int64_t E, MgInterp ip, const double* xc, double* xf, cudaStream_t s);
-int launch_mg_restrict(int64_t E, MgInterp ip, const double* rf, double* rc, cudaStream_t s);
+// xf += I xc; rc = I^T rf (nrhs columns, leading dimensions ldc / ldf).
+int launch_mg_prolong_add(int64_t E, MgInterp ip, const double* xc, int64_t ldc, double* xf, int64_t ldf, int nrhs,
+                          cudaStream_t s);
+int launch_mg_restrict(int64_t E, MgInterp ip, const double* rf, int64_t ldf, double* rc, int64_t ldc, int nrhs,
+                       cudaStream_t s);
 
 // Continuous P1 auxiliary level: R maps vertex values to the coarsest DG level (on element e, corner
 // values through T [Nbf][NV] per component); its Galerkin operator is CSR over vertices with Q x Q
@@ -58,17 +60,22 @@ struct MgAux {
     int64_t nv = 0;
     int Q = 0, Nbf = 0, NV = 0;
 };
-int launch_aux_apply(MgAux const& a, const double* x, const double* b, double* y, cudaStream_t s);
-int launch_aux_restrict(MgAux const& a, const double* r0, double* rc, cudaStream_t s);
-int launch_aux_prolong_add(MgAux const& a, int64_t E, const double* xc, double* x0, cudaStream_t s);
+// P1 vectors: nrhs contiguous columns of nv * Q; DG level columns at multiples of ld0.
+int launch_aux_apply(MgAux const& a, const double* x, const double* b, double* y, int nrhs, cudaStream_t s);
+int launch_aux_restrict(MgAux const& a, const double* r0, int64_t ld0, double* rc, int nrhs, cudaStream_t s);
+int launch_aux_prolong_add(MgAux const& a, int64_t E, const double* xc, double* x0, int64_t ld0, int nrhs,
+                           cudaStream_t s);
 
 // Chebyshev iteration (Saad, "Iterative Methods for Sparse Linear Systems", 2nd ed., Alg. 12.1,
 // preconditioned with Dinv): first step d = c Dinv r, x = d (x_zero) or x += d; later steps
-// r -= y (y = A d), d = c1 d + c2 Dinv r, x += d.
-int launch_cheb_first(int64_t n, const double* dinv, const double* r, double* d, double* x, double c, int x_zero,
-                      cudaStream_t s);
-int launch_cheb_step(int64_t n, const double* dinv, const double* y, double* r, double* d, double* x, double c1,
-                     double c2, cudaStream_t s);
+// r -= y (y = A d), d = c1 d + c2 Dinv r, x += d.  nrhs columns of n entries at stride ld.
+int launch_cheb_first(int64_t n, int nrhs, int64_t ld, const double* dinv, const double* r, double* d, double* x,
+                      double c, int x_zero, cudaStream_t s);
+int launch_cheb_step(int64_t n, int nrhs, int64_t ld, const double* dinv, const double* y, double* r, double* d,
+                     double* x, double c1, double c2, cudaStream_t s);
+// y = x and y = a - y over nrhs columns of n entries at stride ld (padding untouched).
+int launch_vec_copy_cols(int64_t n, int nrhs, int64_t ld, const double* x, double* y, cudaStream_t s);
+int launch_vec_rsub_cols(int64_t n, int nrhs, int64_t ld, const double* a, double* y, cudaStream_t s);
 
 // Vector helpers of the level solvers (grid-stride).  dot: deterministic two-pass sum into
 // out[0] (partial holds kDotBlocks doubles).
