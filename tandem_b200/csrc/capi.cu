@@ -1697,8 +1697,10 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     plan_chunks(seg_begin, seg_end, hchunks, hseg);
     const int nseg = static_cast<int>(seg_begin.size());
     const size_t vec = vec_entries;
+    // every carve below is rounded up to 256 bytes: one 256-byte unit of slack per carve (9 FP64
+    // carves, 5 more for the FP32 vectors)
     size_t need = 5 * vec * sizeof(double) + hchunks.size() * (2 * sizeof(double) + sizeof(Chunk)) +
-                  (hseg.size()) * sizeof(int) + 2 * static_cast<size_t>(nseg) * kScal * sizeof(double) + 8 * 256;
+                  (hseg.size()) * sizeof(int) + static_cast<size_t>(nseg) * kScal * sizeof(double) + 9 * 256;
     if (prec == TDG_FP32) need += 5 * vec * sizeof(float) + 5 * 256;
     if (op->ws_bytes < need) {
         op->arena_ws.release();
@@ -1724,7 +1726,6 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     Chunk* dchunks = reinterpret_cast<Chunk*>(take(hchunks.size() * sizeof(Chunk)));
     int* dseg = reinterpret_cast<int*>(take(hseg.size() * sizeof(int)));
     double* scal = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * kScal * sizeof(double)));
-    double* scal_out = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * kScal * sizeof(double)));
     TDG_CUDA_TRY(cudaMemcpyAsync(dchunks, hchunks.data(), hchunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice, s));
     TDG_CUDA_TRY(cudaMemcpyAsync(dseg, hseg.data(), hseg.size() * sizeof(int), cudaMemcpyHostToDevice, s));
     SegPlan sp;
