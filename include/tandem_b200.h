@@ -254,7 +254,8 @@ typedef struct {
  * point-Jacobi diagonals; the lambda_max estimates of the Chebyshev smoothers; the coarse system
  * (see coarse_space) with its block-Jacobi inverses.  opts may be NULL (defaults: logarithmic,
  * coarse degree 1, continuous P1 coarse space).  Does not select the preconditioner
- * (tdg_set_preconditioner). */
+ * (tdg_set_preconditioner).  tdg_set_material invalidates the hierarchy (as it does the
+ * block-Jacobi inverses): call tdg_mg_setup again before the next multigrid solve. */
 int tdg_mg_setup(tdg_op* op, const tdg_mg_opts* opts, void* stream);
 /* z = M r, one V-cycle per right-hand side (PCMG's apply): Chebyshev pre-smoothing from zero,
  * restriction of the residual, the coarser levels, prolongation, Chebyshev post-smoothing; CG with

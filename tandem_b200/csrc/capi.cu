@@ -690,9 +690,13 @@ int mg_ensure_ws(tdg_op* op, int nrhs, int64_t ld, cudaStream_t s) {
     auto& mg = op->mg;
     if (nrhs <= mg.cap && ld == mg.fine_ld) return 0;
     TDG_CUDA_TRY(cudaStreamSynchronize(s));
+    const int cap = std::max(nrhs, mg.cap);
+    // until every vector is in place the hierarchy has no work space (a failed allocation must not
+    // leave stale pointers that a later call with the same shape would reuse)
     mg.reset_graph();
     mg.ws.release();
-    const int cap = std::max(nrhs, mg.cap);
+    mg.cap = 0;
+    mg.fine_ld = 0;
     const int nl = static_cast<int>(mg.lv.size());
     for (int l = 0; l < nl; ++l) {
         auto& L = mg.lv[static_cast<size_t>(l)];
@@ -1127,6 +1131,7 @@ int tdg_set_material(tdg_op* op, const double* c0_Q, const double* c1_Q) {
     op->blk = nullptr;
     op->inv = nullptr;
     op->inv_precision = -1;
+    op->mg.ready = false;  // the hierarchy's Galerkin operators and bounds belong to the old material
     op->status = nullptr;
     return 0;
 }
