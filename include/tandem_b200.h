@@ -279,6 +279,13 @@ int tdg_mg_level_matrix(tdg_op* op, int level, double* blocks, int32_t* nbr);
  * be NULL) and the reference interpolation matrix [Nbf(n_to)][Nbf(n_from)] of one component. */
 int tdg_mg_level_degrees(int strategy, int coarse_degree, int degree, int* degrees);
 int tdg_mg_interpolation(int dim, int kind, int n_to, int n_from, double* out);
+/* Host utilities of an operator (no device work, no tdg_set_material needed):
+ * the element colouring the Galerkin probing uses (distance 2 across interior facets: an element's
+ * neighbours and their neighbours all differ from it), colour [E], *ncolours;
+ * the vertex numbering of the continuous P1 coarse space (corners identified across interior
+ * facets only), vid [E][dim + 1] in the element's corner order, *nv. */
+int tdg_mg_colouring(const tdg_op* op, int32_t* colour, int* ncolours);
+int tdg_mg_vertex_numbering(const tdg_op* op, int32_t* vid, int64_t* nv);
 
 /* --- explicit wave operator (Elasticity::wave_rhs, app/localoperator/Elasticity.cpp:865-880) -- */
 

@@ -1920,6 +1920,21 @@ extern "C" int tdg_mg_level_degrees(int strategy, int coarse_degree, int degree,
     }
 }
 
+extern "C" int tdg_mg_colouring(const tdg_op* op, int32_t* colour, int* ncolours) {
+    if (!op || !colour || !ncolours) return fail(TDG_E_INVALID, "null argument");
+    std::vector<int32_t> nbr = element_neighbours(op->h);
+    std::vector<int32_t> col = distance2_colouring(nbr, op->h.E, 1 + op->h.nfaces, ncolours);
+    std::copy(col.begin(), col.end(), colour);
+    return 0;
+}
+
+extern "C" int tdg_mg_vertex_numbering(const tdg_op* op, int32_t* vid, int64_t* nv) {
+    if (!op || !vid || !nv) return fail(TDG_E_INVALID, "null argument");
+    std::vector<int32_t> v = vertex_numbering(op->h, nv);
+    std::copy(v.begin(), v.end(), vid);
+    return 0;
+}
+
 extern "C" int tdg_mg_interpolation(int dim, int kind, int n_to, int n_from, double* out) {
     if (!out || dim < 2 || dim > 3 || (kind != TDG_POISSON && kind != TDG_ELASTICITY))
         return fail(TDG_E_INVALID, "bad argument");

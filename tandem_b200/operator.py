@@ -237,6 +237,20 @@ class DGOperator:
         return dict(levels=k, degrees=list(deg[:k]), block_sizes=list(bs[:k]), lambda_max=list(lmax[:k]),
                     coarse_iterations=its.value)
 
+    def mg_colouring(self) -> tuple[np.ndarray, int]:
+        """Distance-2 element colouring of the Galerkin probing (host only): colour [E], count."""
+        out = np.zeros(self.E, dtype=np.int32)
+        n = C.c_int(0)
+        _ffi.check(_ffi.lib().tdg_mg_colouring(self._h, out.ctypes.data, C.byref(n)))
+        return out, n.value
+
+    def mg_vertex_numbering(self) -> tuple[np.ndarray, int]:
+        """Vertices of the continuous P1 coarse space (host only): vid [E, dim + 1], count."""
+        out = np.zeros((self.E, self.dim + 1), dtype=np.int32)
+        n = C.c_int64(0)
+        _ffi.check(_ffi.lib().tdg_mg_vertex_numbering(self._h, out.ctypes.data, C.byref(n)))
+        return out, n.value
+
     def mg_level_matrix(self, level: int) -> tuple[np.ndarray, np.ndarray]:
         """Galerkin operator of a coarse level: blocks [E, NB, bs, bs] (row, column) and the
         neighbour table [E, NB] (slot 0 the element, 1 + f across face f, -1 none)."""

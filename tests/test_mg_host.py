@@ -60,3 +60,51 @@ def test_nodal_interpolation_embeds_the_coarse_space(dim):
 def test_modal_interpolation_is_injection():
     I = mg_interpolation(3, POISSON, 4, 2)
     assert np.array_equal(I[:10], np.eye(10)) and not I[10:].any()
+
+
+def _op(m, dim, degree=2):
+    from cases import tandem_quadrature
+    from tandem_b200.operator import DGOperator
+    return DGOperator(m, degree, ELASTICITY, tandem_quadrature(dim, degree))
+
+
+def _closed_neighbourhoods(m):
+    E = m.num_elements
+    nb = [{e} for e in range(E)]
+    for a, b in m.facet_up:
+        if a != b:
+            nb[a].add(int(b))
+            nb[b].add(int(a))
+    return nb
+
+
+@pytest.mark.parametrize("dim,n", [(2, 5), (3, 3)])
+def test_probing_colouring_is_distance_two(dim, n):
+    """Every closed neighbourhood (an element and the elements across its interior facets) holds
+    each colour at most once, which is what lets one probe recover every block of a colour."""
+    from tandem_b200 import mesh as M
+    m = M.build(M.square_mesh(n) if dim == 2 else M.cube_mesh(n), 2)
+    col, nc = _op(m, dim).mg_colouring()
+    assert col.min() == 0 and col.max() == nc - 1
+    for hood in _closed_neighbourhoods(m):
+        cs = [col[e] for e in hood]
+        assert len(set(cs)) == len(cs)
+
+
+def test_vertex_numbering_follows_facet_connectivity():
+    """Connected mesh: the numbering is the mesh's own vertex ids up to renaming.  Mesh union of
+    overlapping copies: no vertex is shared between problems (they stay independent)."""
+    from tandem_b200 import mesh as M
+    m = M.build(M.square_mesh(4), 2)
+    vid, nv = _op(m, 2).mg_vertex_numbering()
+    pairs = set(zip(m.elements.ravel().tolist(), vid.ravel().tolist()))
+    assert nv == len(np.unique(m.elements)) == len(pairs)
+    meshes = [M.build(M.square_mesh(k), 2) for k in (3, 2, 3)]
+    um, eoff = M.union(meshes)
+    vid, nv = _op(um, 2).mg_vertex_numbering()
+    seen = []
+    for i in range(len(meshes)):
+        part = vid[eoff[i]:eoff[i + 1]]
+        assert len(np.unique(part)) == len(np.unique(meshes[i].elements))
+        seen.append(set(part.ravel().tolist()))
+    assert sum(len(s) for s in seen) == nv == len(set().union(*seen))
