@@ -200,9 +200,11 @@ typedef struct {
 } tdg_solve_stats;
 
 /* Solves A x = b (device double arrays, nrhs stacked with leading dimension ld) with
- * block-Jacobi preconditioned CG (reliable updates: the recurrence residual is periodically
- * replaced by the FP64 residual b - A x, keeping the search direction).  x holds the initial guess.  tdg_bjacobi_setup must have
- * been called with the precision the solve needs (FP64 for TDG_FP64, FP32 for TDG_FP32). */
+ * preconditioned CG (reliable updates: the recurrence residual is periodically replaced by the
+ * FP64 residual b - A x, keeping the search direction).  x holds the initial guess.  The
+ * preconditioner is the one tdg_set_preconditioner selected: block Jacobi (default;
+ * tdg_bjacobi_setup must have been called with the precision the solve needs, FP64 for TDG_FP64,
+ * FP32 for TDG_FP32) or the multigrid V-cycle (tdg_mg_setup; TDG_FP64 or TDG_MIXED; flexible CG). */
 int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64_t ld,
               const tdg_solve_opts* opts, tdg_solve_stats* stats, void* stream);
 

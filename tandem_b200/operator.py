@@ -274,9 +274,11 @@ class DGOperator:
     def solve(self, b, x, precision: int = FP64, rtol: float = 1e-10, max_iterations: int = 20000,
               inner_rtol: float = 0.0, max_outer: int = 0, use_graphs: bool = True, nrhs: int = 1,
               ld: int | None = None, stream=None, check: bool = True) -> dict:
-        """Block-Jacobi preconditioned CG on the device: FP64; MIXED (FP64 recurrence around the
-        FP32 tensor-core operator and FP32 block inverses); or FP32 (operator, preconditioner and
-        recurrence in FP32).  The solution and the true residual are FP64 in every mode (reliable
+        """Preconditioned CG on the device: FP64; MIXED (FP64 recurrence around the FP32
+        tensor-core operator and FP32 block inverses or FP32 fine-level multigrid smoothing); or
+        FP32 (operator, preconditioner and recurrence in FP32; block Jacobi only).  The
+        preconditioner is block Jacobi or, after set_preconditioner("mg"), the multigrid V-cycle
+        (flexible CG).  The solution and the true residual are FP64 in every mode (reliable
         updates).  inner_rtol: reliable-update threshold (0 = default).  Raises on
         non-convergence unless check=False (then the stats report it)."""
         ld = self.ndof if ld is None else ld
