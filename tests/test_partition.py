@@ -7,7 +7,8 @@ blocks.
   codes and facet sides from the global mesh) and of the local right-hand side (volume and facet
   data sliced to the local elements and facets) equal the global rows to 1e-12, on a mesh with
   Dirichlet, natural, boundary-fault and interior-fault facets.
-* With 2 and 3 gloo ranks: the exchange fills ghost blocks that start out zero, the distributed
+* With 2 and 3 gloo ranks: the exchange fills ghost blocks that start out zero (one vector, and two
+  right-hand sides at a padded leading dimension whose padding it leaves alone), the distributed
   apply equals the global apply on the owned rows, and distributed block-Jacobi CG reaches the
   1e-10 relative residual of the global (oracle) operator."""
 import os
@@ -128,6 +129,17 @@ def _dd_worker(rank, world, port, q, kind, dim, n, degree):
         y = torch.zeros_like(xl)
         A.apply(xl, y)
         ghosts_ok = np.array_equal(xl.numpy().reshape(-1, bs)[lm.n_owned:], xg.reshape(-1, bs)[lm.elements[lm.n_owned:]])
+        # two right-hand sides at a padded leading dimension: ghosts filled, padding untouched
+        ld = A.n_local + 5
+        X = torch.full((2, ld), -1.0, dtype=torch.float64)
+        X[0, :A.n_local] = 0.0
+        X[1, :A.n_local] = 0.0
+        X[0, :A.n_owned] = torch.from_numpy(xg.reshape(-1, bs)[own].ravel())
+        X[1, :A.n_owned] = 2.0 * X[0, :A.n_owned]
+        A.halo.exchange(X.reshape(-1), nrhs=2, ld=ld)
+        gl = xg.reshape(-1, bs)[lm.elements[lm.n_owned:]].ravel()
+        ghosts_ok = ghosts_ok and np.array_equal(X[0, A.n_owned:A.n_local].numpy(), gl) \
+            and np.array_equal(X[1, A.n_owned:A.n_local].numpy(), 2.0 * gl) and bool(torch.all(X[:, A.n_local:] == -1.0))
         ref = glob.apply(xg).reshape(-1, bs)[own]
         apply_err = float(np.abs(y.numpy().reshape(-1, bs)[:lm.n_owned] - ref).max() / np.abs(ref).max())
         # distributed block-Jacobi CG on the manufactured problem
