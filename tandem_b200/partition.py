@@ -152,6 +152,7 @@ class HaloExchange:
     def __init__(self, plan: HaloPlan, bs: int, group=None):
         self.plan, self.bs, self.group = plan, bs, group
         self._idx = {}
+        self._started = False
 
     def _entries(self, which: str, q: int, nrhs: int, ld: int, device):
         """Vector entries of the element list plan.<which>[q] over nrhs columns (cached)."""
@@ -164,20 +165,26 @@ class HaloExchange:
         return self._idx[key]
 
     def exchange(self, x, nrhs: int = 1, ld: int | None = None) -> None:
+        """The sends and receives go out as one batch (batch_isend_irecv: grouped under nccl, so
+        two ranks that send to each other before receiving cannot block each other).  The first
+        exchange starts with a barrier, since a rank without peers has nothing to batch and a
+        group's first batch must include every rank."""
         import torch
         import torch.distributed as dist
         ld = x.numel() // nrhs if ld is None else ld
-        reqs, sends, recvs = [], [], []
+        ops, recvs = [], []
         for q in sorted(self.plan.send):
             buf = x.index_select(0, self._entries("send", q, nrhs, ld, x.device)).contiguous()
-            sends.append(buf)  # alive until the waits below
-            reqs.append(dist.isend(buf, q, group=self.group, tag=1))
+            ops.append(dist.P2POp(dist.isend, buf, q, self.group))
         for q in sorted(self.plan.recv):
             idx = self._entries("recv", q, nrhs, ld, x.device)
             buf = torch.empty(idx.numel(), dtype=x.dtype, device=x.device)
-            reqs.append(dist.irecv(buf, q, group=self.group, tag=1))
+            ops.append(dist.P2POp(dist.irecv, buf, q, self.group))
             recvs.append((idx, buf))
-        for r in reqs:
+        if not self._started:
+            dist.barrier(group=self.group)
+            self._started = True
+        for r in (dist.batch_isend_irecv(ops) if ops else []):
             r.wait()
         for idx, buf in recvs:
             x.index_copy_(0, idx, buf)
