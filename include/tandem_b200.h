@@ -287,6 +287,10 @@ int tdg_mg_interpolation(int dim, int kind, int n_to, int n_from, double* out);
  * the vertex numbering of the continuous P1 coarse space (corners identified across interior
  * facets only), vid [E][dim + 1] in the element's corner order, *nv. */
 int tdg_mg_colouring(const tdg_op* op, int32_t* colour, int* ncolours);
+/* The continuous P1 coarse space's element embedding (host only): out [Nbf(degree)][dim + 1], the
+ * coefficients in the degree-`degree` space of `kind` (modal for TDG_POISSON, nodal for
+ * TDG_ELASTICITY) of the linear function that is 1 at corner i and 0 at the other corners. */
+int tdg_mg_p1_embedding(int dim, int kind, int degree, double* out);
 int tdg_mg_vertex_numbering(const tdg_op* op, int32_t* vid, int64_t* nv);
 
 /* --- explicit wave operator (Elasticity::wave_rhs, app/localoperator/Elasticity.cpp:865-880) -- */

@@ -1935,6 +1935,18 @@ extern "C" int tdg_mg_vertex_numbering(const tdg_op* op, int32_t* vid, int64_t* 
     return 0;
 }
 
+extern "C" int tdg_mg_p1_embedding(int dim, int kind, int degree, double* out) {
+    if (!out || dim < 2 || dim > 3 || degree < 1 || (kind != TDG_POISSON && kind != TDG_ELASTICITY))
+        return fail(TDG_E_INVALID, "bad argument");
+    try {
+        Dense T = linear_to_space(dim, kind, degree);
+        std::copy(T.a.begin(), T.a.end(), out);
+        return 0;
+    } catch (std::exception const& e) {
+        return fail(TDG_E_INVALID, e.what());
+    }
+}
+
 extern "C" int tdg_mg_interpolation(int dim, int kind, int n_to, int n_from, double* out) {
     if (!out || dim < 2 || dim > 3 || (kind != TDG_POISSON && kind != TDG_ELASTICITY))
         return fail(TDG_E_INVALID, "bad argument");

@@ -410,3 +410,11 @@ def mg_interpolation(dim: int, kind: int, n_to: int, n_from: int) -> np.ndarray:
     out = np.zeros((comb(n_to + dim, dim), comb(n_from + dim, dim)))
     _ffi.check(_ffi.lib().tdg_mg_interpolation(dim, kind, n_to, n_from, out.ctypes.data))
     return out
+
+
+def mg_p1_embedding(dim: int, kind: int, degree: int) -> np.ndarray:
+    """Coefficients [Nbf(degree), dim + 1] of each corner's hat function in the operator's space."""
+    from math import comb
+    out = np.zeros((comb(degree + dim, dim), dim + 1))
+    _ffi.check(_ffi.lib().tdg_mg_p1_embedding(dim, kind, degree, out.ctypes.data))
+    return out

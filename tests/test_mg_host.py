@@ -108,3 +108,19 @@ def test_vertex_numbering_follows_facet_connectivity():
         assert len(np.unique(part)) == len(np.unique(meshes[i].elements))
         seen.append(set(part.ravel().tolist()))
     assert sum(len(s) for s in seen) == nv == len(set().union(*seen))
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("kind", [POISSON, ELASTICITY])
+def test_p1_embedding_reproduces_hat_functions(dim, kind):
+    """Evaluated at random points, the degree-p function with the embedding's coefficients equals
+    the corner's barycentric coordinate (exact for every p >= 1)."""
+    from tandem_b200.operator import mg_p1_embedding
+    from tandem_b200.refelem import MODAL, WARP_BLEND, ref_basis
+    rng = np.random.default_rng(dim + 10 * kind)
+    pts = rng.dirichlet(np.ones(dim + 1), size=20)[:, 1:]
+    lam = np.concatenate([1.0 - pts.sum(axis=1, keepdims=True), pts], axis=1)  # [np, dim + 1]
+    for p in range(1, 5):
+        T = mg_p1_embedding(dim, kind, p)
+        Eb = ref_basis(dim, p, MODAL if kind == POISSON else WARP_BLEND, pts)  # [Nbf, np]
+        assert np.abs(Eb.T @ T - lam).max() < 1e-12, p
