@@ -361,6 +361,20 @@ int tdg_fault_slip_rhs(tdg_fault* fault, const double* slip, int64_t ld_slip, do
 int tdg_fault_traction(tdg_fault* fault, const double* u, int64_t ld, const double* slip, int64_t ld_slip,
                        double* traction, int64_t ld_t, int nrhs, void* stream);
 
+/* --- error norms (Error<D>::L2 / H1_semi, src/form/Error.cpp; host post-processing) ---------- */
+
+/* tandem integrates the error with its own rule (simplexQuadratureRule<D>(20)); the caller passes
+ * the rule here: np points on the unit simplex [np][dim] and weights [np] (tdg_conical_rule gives
+ * tandem's conical product rules).  tdg_rule_coords maps the points to every element, out
+ * [E][np][dim], for the caller to evaluate its reference solution there.  x: the solution on the
+ * host [E][bs].  ref: reference values [E][Q][np]; refgrad: reference physical gradients
+ * [E][Q][dim][np].  *out: the norm (square root of the summed integrals). */
+int tdg_rule_coords(const tdg_op* op, int np, const double* points, double* out);
+int tdg_error_l2(const tdg_op* op, const double* x, int np, const double* points, const double* weights,
+                 const double* ref, double* out);
+int tdg_error_h1_semi(const tdg_op* op, const double* x, int np, const double* points, const double* weights,
+                      const double* refgrad, double* out);
+
 /* --- host utilities: reference-element tables (no device work) ---------------------------- */
 
 /* Reference nodes of degree N on the unit simplex: family 0 = warp & blend

@@ -1935,6 +1935,26 @@ extern "C" int tdg_mg_vertex_numbering(const tdg_op* op, int32_t* vid, int64_t* 
     return 0;
 }
 
+extern "C" int tdg_rule_coords(const tdg_op* op, int np, const double* points, double* out) {
+    if (!op || !points || !out || np < 1) return fail(TDG_E_INVALID, "bad argument");
+    op->h.rule_coords(np, points, out);
+    return 0;
+}
+
+extern "C" int tdg_error_l2(const tdg_op* op, const double* x, int np, const double* points, const double* weights,
+                            const double* ref, double* out) {
+    if (!op || !x || !points || !weights || !ref || !out || np < 1) return fail(TDG_E_INVALID, "bad argument");
+    *out = op->h.error_l2(x, np, points, weights, ref);
+    return 0;
+}
+
+extern "C" int tdg_error_h1_semi(const tdg_op* op, const double* x, int np, const double* points,
+                                 const double* weights, const double* refgrad, double* out) {
+    if (!op || !x || !points || !weights || !refgrad || !out || np < 1) return fail(TDG_E_INVALID, "bad argument");
+    *out = op->h.error_h1_semi(x, np, points, weights, refgrad);
+    return 0;
+}
+
 extern "C" int tdg_mg_p1_embedding(int dim, int kind, int degree, double* out) {
     if (!out || dim < 2 || dim > 3 || degree < 1 || (kind != TDG_POISSON && kind != TDG_ELASTICITY))
         return fail(TDG_E_INVALID, "bad argument");

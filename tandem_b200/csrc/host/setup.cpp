@@ -506,6 +506,97 @@ int64_t HostOperator::bytes_apply(int s) const {
     return E * per_el * s + F * (per_f * s + 20);
 }
 
+// ---- error norms at a caller-chosen rule --------------------------------------------------------
+
+namespace {
+
+// Geometry of element el at the rule's points: |det J| and J^-1 (Ji[e * D + i] = d xi_e / d x_i).
+void rule_geometry(HostOperator const& h, int64_t el, std::vector<double> const& gd, int np, int q, double* Ji,
+                   double* absdet) {
+    const int D = h.D;
+    double const* X = &h.geo_nodes[static_cast<std::size_t>(el) * h.Ngeo * D];
+    double J[9];
+    for (int i = 0; i < D; ++i)
+        for (int e = 0; e < D; ++e) {
+            double acc = 0.0;
+            for (int n = 0; n < h.Ngeo; ++n) acc += X[n * D + i] * gd[(static_cast<std::size_t>(n) * D + e) * np + q];
+            J[i * D + e] = acc;
+        }
+    *absdet = std::fabs(inv_det(D, J, Ji));
+}
+
+}  // namespace
+
+void HostOperator::rule_coords(int np, double const* pts, double* out) const {
+    Dense ge = geo_space.eval(Points(pts, pts + static_cast<std::size_t>(np) * D));
+#pragma omp parallel for schedule(static)
+    for (int64_t el = 0; el < E; ++el) {
+        double const* X = &geo_nodes[static_cast<std::size_t>(el) * Ngeo * D];
+        for (int q = 0; q < np; ++q)
+            for (int i = 0; i < D; ++i) {
+                double acc = 0.0;
+                for (int n = 0; n < Ngeo; ++n) acc += X[n * D + i] * ge(n, q);
+                out[(static_cast<std::size_t>(el) * np + q) * D + i] = acc;
+            }
+    }
+}
+
+double HostOperator::error_l2(double const* x, int np, double const* pts, double const* w, double const* ref) const {
+    Points P(pts, pts + static_cast<std::size_t>(np) * D);
+    Dense Eb = space.eval(P);
+    std::vector<double> gd = geo_space.grad(P);
+    std::vector<double> part(static_cast<std::size_t>(E), 0.0);
+#pragma omp parallel for schedule(static)
+    for (int64_t el = 0; el < E; ++el) {
+        double acc = 0.0;
+        for (int q = 0; q < np; ++q) {
+            double Ji[9], ad;
+            rule_geometry(*this, el, gd, np, q, Ji, &ad);
+            for (int j = 0; j < Q; ++j) {
+                double u = 0.0;
+                for (int k = 0; k < Nbf; ++k) u += Eb(k, q) * x[el * bs + k + j * Nbf];
+                const double e = ref[(static_cast<std::size_t>(el) * Q + j) * np + q] - u;
+                acc += w[q] * ad * e * e;
+            }
+        }
+        part[static_cast<std::size_t>(el)] = acc;
+    }
+    double err = 0.0;
+    for (double v : part) err += v;
+    return std::sqrt(err);
+}
+
+double HostOperator::error_h1_semi(double const* x, int np, double const* pts, double const* w,
+                                   double const* refgrad) const {
+    Points P(pts, pts + static_cast<std::size_t>(np) * D);
+    std::vector<double> Gb = space.grad(P);  // [(k * D + e) * np + q]
+    std::vector<double> gd = geo_space.grad(P);
+    std::vector<double> part(static_cast<std::size_t>(E), 0.0);
+#pragma omp parallel for schedule(static)
+    for (int64_t el = 0; el < E; ++el) {
+        double acc = 0.0;
+        for (int q = 0; q < np; ++q) {
+            double Ji[9], ad;
+            rule_geometry(*this, el, gd, np, q, Ji, &ad);
+            for (int j = 0; j < Q; ++j)
+                for (int d = 0; d < D; ++d) {
+                    double g = 0.0;
+                    for (int k = 0; k < Nbf; ++k) {
+                        double dx = 0.0;
+                        for (int e = 0; e < D; ++e) dx += Ji[e * D + d] * Gb[(static_cast<std::size_t>(k) * D + e) * np + q];
+                        g += dx * x[el * bs + k + j * Nbf];
+                    }
+                    const double e = refgrad[((static_cast<std::size_t>(el) * Q + j) * D + d) * np + q] - g;
+                    acc += w[q] * ad * e * e;
+                }
+        }
+        part[static_cast<std::size_t>(el)] = acc;
+    }
+    double err = 0.0;
+    for (double v : part) err += v;
+    return std::sqrt(err);
+}
+
 // ---- p-multigrid set-up ----------------------------------------------------------------------
 
 Dense interpolation_matrix(int D, int kind, int n_to, int n_from) {

@@ -88,6 +88,15 @@ struct HostOperator {
 
     int64_t flops_apply() const;
     int64_t bytes_apply(int scalar_bytes) const;
+
+    // Error<D>::L2 / H1_semi (src/form/Error.cpp:13-48, 120-170) of the solution x [E][bs] against a
+    // reference given at the np points (unit simplex, [np][D]) of a caller-chosen rule with weights
+    // w (tandem integrates with simplexQuadratureRule<D>(20)): ref [E][Q][np] values, refgrad
+    // [E][Q][D][np] physical gradients.  rule_coords: the points mapped to every element, out
+    // [E][np][D], where the caller evaluates its reference.
+    void rule_coords(int np, double const* pts, double* out) const;
+    double error_l2(double const* x, int np, double const* pts, double const* w, double const* ref) const;
+    double error_h1_semi(double const* x, int np, double const* pts, double const* w, double const* refgrad) const;
 };
 
 // ---- p-multigrid set-up (tandem's PCMG path, app/common/PetscLinearSolver.cpp:53-114) ----------

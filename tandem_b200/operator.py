@@ -237,6 +237,43 @@ class DGOperator:
         return dict(levels=k, degrees=list(deg[:k]), block_sizes=list(bs[:k]), lambda_max=list(lmax[:k]),
                     coarse_iterations=its.value)
 
+    # -- error norms (Error<D>::L2 / H1_semi; host post-processing) ------------------------------
+    def rule_coords(self, points: np.ndarray) -> np.ndarray:
+        """Physical coordinates [E, np, dim] of unit-simplex points [np, dim] on every element."""
+        pts = _c(points, np.float64).reshape(-1, self.dim)
+        out = np.zeros((self.E, pts.shape[0], self.dim))
+        _ffi.check(_ffi.lib().tdg_rule_coords(self._h, pts.shape[0], pts.ctypes.data, out.ctypes.data))
+        return out
+
+    @staticmethod
+    def _host_solution(x) -> np.ndarray:
+        if hasattr(x, "detach"):
+            x = x.detach().cpu().numpy()
+        return _c(x, np.float64)
+
+    def error_l2(self, x, points: np.ndarray, weights: np.ndarray, ref: np.ndarray) -> float:
+        """||x - ref||_L2 with the given rule; ref [E, Q, np] at rule_coords(points) (tandem's
+        Error::L2 uses simplexQuadratureRule(20), e.g. conical_rule(dim, 20))."""
+        pts = _c(points, np.float64).reshape(-1, self.dim)
+        w = _c(weights, np.float64)
+        r = _c(ref, np.float64).reshape(self.E, self.Q, pts.shape[0])
+        xs = self._host_solution(x)
+        out = C.c_double(0.0)
+        _ffi.check(_ffi.lib().tdg_error_l2(self._h, xs.ctypes.data, pts.shape[0], pts.ctypes.data, w.ctypes.data,
+                                           r.ctypes.data, C.byref(out)))
+        return out.value
+
+    def error_h1_semi(self, x, points: np.ndarray, weights: np.ndarray, refgrad: np.ndarray) -> float:
+        """|x - ref|_H1 (gradient L2 norm) with the given rule; refgrad [E, Q, dim, np]."""
+        pts = _c(points, np.float64).reshape(-1, self.dim)
+        w = _c(weights, np.float64)
+        r = _c(refgrad, np.float64).reshape(self.E, self.Q, self.dim, pts.shape[0])
+        xs = self._host_solution(x)
+        out = C.c_double(0.0)
+        _ffi.check(_ffi.lib().tdg_error_h1_semi(self._h, xs.ctypes.data, pts.shape[0], pts.ctypes.data,
+                                                w.ctypes.data, r.ctypes.data, C.byref(out)))
+        return out.value
+
     def mg_colouring(self) -> tuple[np.ndarray, int]:
         """Distance-2 element colouring of the Galerkin probing (host only): colour [E], count."""
         out = np.zeros(self.E, dtype=np.int32)
