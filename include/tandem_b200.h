@@ -361,6 +361,16 @@ int tdg_fault_slip_rhs(tdg_fault* fault, const double* slip, int64_t ld_slip, do
 int tdg_fault_traction(tdg_fault* fault, const double* u, int64_t ld, const double* slip, int64_t ld_slip,
                        double* traction, int64_t ld_t, int nrhs, void* stream);
 
+/* --- projection and evaluation (host; AbstractDGOperator::project / solution) -------------------- */
+
+/* y [E][bs] = the projection of values at the volume points U_Q [E][Q][Nq] (Elasticity::project,
+ * app/localoperator/Elasticity.cpp:882-911: weight-adjusted inverse mass of E_Q W |J| U_Q; exact
+ * for the discrete space on affine elements; here for both kinds). */
+int tdg_project(const tdg_op* op, const double* U_Q, double* y);
+/* The discrete function x [E][bs] (host) at np unit-simplex points [np][dim] of every element:
+ * out [E][Q][np] (DGOperator::solution + FiniteElementFunction::map). */
+int tdg_evaluate(const tdg_op* op, const double* x, int np, const double* points, double* out);
+
 /* --- error norms (Error<D>::L2 / H1_semi, src/form/Error.cpp; host post-processing) ---------- */
 
 /* tandem integrates the error with its own rule (simplexQuadratureRule<D>(20)); the caller passes

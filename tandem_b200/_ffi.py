@@ -57,6 +57,8 @@ SYMBOLS = {
     "tdg_mg_colouring": (C.c_int, [_p, _p, _p]),
     "tdg_mg_p1_embedding": (C.c_int, [C.c_int, C.c_int, C.c_int, _p]),
     "tdg_rule_coords": (C.c_int, [_p, C.c_int, _p, _p]),
+    "tdg_project": (C.c_int, [_p, _p, _p]),
+    "tdg_evaluate": (C.c_int, [_p, _p, C.c_int, _p, _p]),
     "tdg_error_l2": (C.c_int, [_p, _p, C.c_int, _p, _p, _p, _p]),
     "tdg_error_h1_semi": (C.c_int, [_p, _p, C.c_int, _p, _p, _p, _p]),
     "tdg_mg_vertex_numbering": (C.c_int, [_p, _p, _p]),

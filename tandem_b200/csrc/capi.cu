@@ -1935,6 +1935,18 @@ extern "C" int tdg_mg_vertex_numbering(const tdg_op* op, int32_t* vid, int64_t* 
     return 0;
 }
 
+extern "C" int tdg_project(const tdg_op* op, const double* U_Q, double* y) {
+    if (!op || !U_Q || !y) return fail(TDG_E_INVALID, "null argument");
+    op->h.project(U_Q, y);
+    return 0;
+}
+
+extern "C" int tdg_evaluate(const tdg_op* op, const double* x, int np, const double* points, double* out) {
+    if (!op || !x || !points || !out || np < 1) return fail(TDG_E_INVALID, "bad argument");
+    op->h.evaluate(x, np, points, out);
+    return 0;
+}
+
 extern "C" int tdg_rule_coords(const tdg_op* op, int np, const double* points, double* out) {
     if (!op || !points || !out || np < 1) return fail(TDG_E_INVALID, "bad argument");
     op->h.rule_coords(np, points, out);

@@ -541,6 +541,56 @@ void HostOperator::rule_coords(int np, double const* pts, double* out) const {
     }
 }
 
+void HostOperator::project(double const* U_Q, double* y) const {
+    const int nb = Nbf;
+#pragma omp parallel for schedule(static)
+    for (int64_t el = 0; el < E; ++el) {
+        double const* J = &vAbsDetJ[static_cast<std::size_t>(el) * Nq];
+        std::vector<double> u(static_cast<std::size_t>(nb)), t(static_cast<std::size_t>(nb)),
+            v(static_cast<std::size_t>(Nq)), r(static_cast<std::size_t>(nb));
+        for (int p = 0; p < Q; ++p) {
+            double const* f = &U_Q[(static_cast<std::size_t>(el) * Q + p) * Nq];
+            for (int k = 0; k < nb; ++k) {  // U = E_Q W |J| U_Q
+                double acc = 0.0;
+                for (int q = 0; q < Nq; ++q) acc += E_Q(k, q) * W[q] * J[q] * f[q];
+                u[k] = acc;
+            }
+            for (int s = 0; s < nb; ++s) {  // MinvRef U
+                double acc = 0.0;
+                for (int l = 0; l < nb; ++l) acc += Minv_ref(s, l) * u[l];
+                t[s] = acc;
+            }
+            for (int q = 0; q < Nq; ++q) {  // (W / |J|) E_Q^T (MinvRef U)
+                double acc = 0.0;
+                for (int s = 0; s < nb; ++s) acc += E_Q(s, q) * t[s];
+                v[q] = W[q] / J[q] * acc;
+            }
+            for (int rr = 0; rr < nb; ++rr) {
+                double acc = 0.0;
+                for (int q = 0; q < Nq; ++q) acc += E_Q(rr, q) * v[q];
+                r[rr] = acc;
+            }
+            for (int k = 0; k < nb; ++k) {  // MinvRef (...)
+                double acc = 0.0;
+                for (int rr = 0; rr < nb; ++rr) acc += Minv_ref(k, rr) * r[rr];
+                y[el * bs + k + p * nb] = acc;
+            }
+        }
+    }
+}
+
+void HostOperator::evaluate(double const* x, int np, double const* pts, double* out) const {
+    Dense Eb = space.eval(Points(pts, pts + static_cast<std::size_t>(np) * D));
+#pragma omp parallel for schedule(static)
+    for (int64_t el = 0; el < E; ++el)
+        for (int p = 0; p < Q; ++p)
+            for (int q = 0; q < np; ++q) {
+                double acc = 0.0;
+                for (int k = 0; k < Nbf; ++k) acc += Eb(k, q) * x[el * bs + k + p * Nbf];
+                out[(static_cast<std::size_t>(el) * Q + p) * np + q] = acc;
+            }
+}
+
 double HostOperator::error_l2(double const* x, int np, double const* pts, double const* w, double const* ref) const {
     Points P(pts, pts + static_cast<std::size_t>(np) * D);
     Dense Eb = space.eval(P);

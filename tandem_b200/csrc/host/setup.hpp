@@ -95,6 +95,15 @@ struct HostOperator {
     // [E][Q][D][np] physical gradients.  rule_coords: the points mapped to every element, out
     // [E][np][D], where the caller evaluates its reference.
     void rule_coords(int np, double const* pts, double* out) const;
+
+    // Elasticity::project (app/localoperator/Elasticity.cpp:882-911): y [E][bs] from values at the
+    // volume points U_Q [E][Q][Nq]: the weight-adjusted inverse mass (kernel apply_inverse_mass
+    // with weights W/|J|, app/kernels/elasticity.py:236-237) of E_Q W |J| U_Q (project_u_rhs);
+    // exact for the discrete space on affine elements.  Offered for both kinds.
+    void project(double const* U_Q, double* y) const;
+    // The discrete function x [E][bs] at unit-simplex points pts [np][D] of every element, out
+    // [E][Q][np] (FiniteElementFunction::map over DGOperator::solution).
+    void evaluate(double const* x, int np, double const* pts, double* out) const;
     double error_l2(double const* x, int np, double const* pts, double const* w, double const* ref) const;
     double error_h1_semi(double const* x, int np, double const* pts, double const* w, double const* refgrad) const;
 };

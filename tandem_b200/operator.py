@@ -237,6 +237,23 @@ class DGOperator:
         return dict(levels=k, degrees=list(deg[:k]), block_sizes=list(bs[:k]), lambda_max=list(lmax[:k]),
                     coarse_iterations=its.value)
 
+    # -- projection and evaluation (AbstractDGOperator::project / solution; host) ---------------
+    def project(self, U_Q: np.ndarray) -> np.ndarray:
+        """Coefficients [ndof] of values at the volume points U_Q [E, Q, Nq] (Elasticity::project:
+        weight-adjusted inverse mass of the L2 right-hand side)."""
+        u = _c(U_Q, np.float64).reshape(self.E, self.Q, self.Nq)
+        y = np.zeros(self.ndof)
+        _ffi.check(_ffi.lib().tdg_project(self._h, u.ctypes.data, y.ctypes.data))
+        return y
+
+    def evaluate(self, x, points: np.ndarray) -> np.ndarray:
+        """The discrete function x at unit-simplex points [np, dim] of every element: [E, Q, np]."""
+        pts = _c(points, np.float64).reshape(-1, self.dim)
+        xs = self._host_solution(x)
+        out = np.zeros((self.E, self.Q, pts.shape[0]))
+        _ffi.check(_ffi.lib().tdg_evaluate(self._h, xs.ctypes.data, pts.shape[0], pts.ctypes.data, out.ctypes.data))
+        return out
+
     # -- error norms (Error<D>::L2 / H1_semi; host post-processing) ------------------------------
     def rule_coords(self, points: np.ndarray) -> np.ndarray:
         """Physical coordinates [E, np, dim] of unit-simplex points [np, dim] on every element."""

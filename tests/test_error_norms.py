@@ -4,7 +4,9 @@
   solutions against the manufactured reference, curved and straight, 2D and 3D, both kinds), and
   the rule's points map to the operator's volume coordinates;
 * with tandem's error rule (order 20) the errors of oracle solves converge at tandem's bounds
-  (L2 order in (N, N+1), H1 semi-norm in (N-1, N); test/conftest.py:61-75)."""
+  (L2 order in (N, N+1), H1 semi-norm in (N-1, N); test/conftest.py:61-75);
+* projection (Elasticity::project) equals the oracle's weighted inverse mass of the L2 right-hand
+  side, and projection / evaluation round-trip discrete functions on affine elements."""
 import numpy as np
 import pytest
 
@@ -77,3 +79,30 @@ def test_mms_rates_with_tandems_error_rule(kind, N):
     r1 = np.log2(errs[0][1] / errs[1][1])
     assert N - 0.2 < r0 < N + 1.2, (r0, errs)
     assert N - 1.2 < r1 < N + 0.2, (r1, errs)
+
+
+@pytest.mark.parametrize("dim,curved", [(2, True), (3, True), (2, False)])
+def test_projection_is_the_weighted_inverse_mass_of_the_l2_rhs(dim, curved):
+    """project(U_Q) = -apply_inverse_mass(rhs(U_Q)) of the oracle at density 1 (the oracle's
+    inverse mass carries the wave operator's -1/rho W/|J|)."""
+    n = 3 if dim == 2 else 1
+    _, op, orc = product_and_oracle(ELASTICITY, dim, n, 3, curved, True)
+    U = np.random.default_rng(dim).standard_normal((op.E, dim, op.Nq))
+    ref = -orc.apply_inverse_mass(orc.rhs(U, None))
+    np.testing.assert_allclose(op.project(U), ref, atol=1e-12 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("kind,dim", [(POISSON, 2), (ELASTICITY, 2), (POISSON, 3), (ELASTICITY, 3)])
+def test_project_evaluate_round_trip_on_affine_elements(kind, dim):
+    """On straight elements the projection of a discrete function's values at the volume points
+    returns its coefficients, and evaluate() at the volume points gives those values."""
+    n = 3 if dim == 2 else 2
+    m = make_mesh(dim, n, 3, False)
+    q = tandem_quadrature(dim, 3)
+    op = DGOperator(m, 3, kind, q)
+    x = np.random.default_rng(kind + dim).standard_normal(op.ndof)
+    U = op.evaluate(x, q.vol_x)
+    np.testing.assert_allclose(op.project(U), x, atol=1e-11)
+    # independent check of evaluate(): the oracle's own error of x against those values vanishes
+    orc = Oracle(m, 3, kind, q)
+    assert orc.error_L2(x, np.ascontiguousarray(U.transpose(0, 2, 1))) <= 1e-12 * np.linalg.norm(x)
