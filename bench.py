@@ -35,7 +35,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "DOF/s of matrix-free DG apply; solve time to 1e-10 rel. residual, mixed vs FP64"
-FP64_NOMINAL_TFLOPS = 37.0  # B200 nominal FP64 (no measured FP64 peak is available)
+FP64_PROBES = ("dfma", "dmma_m8n8k4", "dmma_m16n8k4", "dmma_m16n8k8", "dmma_m16n8k16")
 # solve arms: (name, solve precision, preconditioner precision, preconditioner).  Block Jacobi:
 # FP64 CG; mixed = FP64 recurrence around the FP32 tensor-core operator with FP32 (or FP64) block
 # inverses; fp32_recurrence = FP32 vectors and recurrence with FP64 reliable updates.  Multigrid:
@@ -45,6 +45,8 @@ BJ_ARMS = (("fp64", 0, 0, "bjacobi"), ("mixed", 2, 1, "bjacobi"), ("mixed_fp64_p
            ("fp32_recurrence", 1, 1, "bjacobi"))
 MG_ARMS = (("mg_fp64", 0, 0, "mg"), ("mg_mixed", 2, 2, "mg"))
 SOLVE_ARMS = BJ_ARMS + MG_ARMS
+# the default cube leg: tandem's FP64 configuration (block-Jacobi CG) and the two multigrid arms
+DEFAULT_CUBE_ARMS = BJ_ARMS[:1] + MG_ARMS
 
 
 def select_arms(args, default=SOLVE_ARMS):
@@ -90,6 +92,23 @@ KERNEL_NAMES = {"tensor": "apply_mma_kernel<Shape<3,4,Elasticity>> (FP64 mma.syn
                 "face": "vol_mma_kernel + face_mma_kernel<Shape<3,4,Elasticity>> (FP64 mma.sync m8n8k4, "
                         "face-centric; roofline over both launches of one apply)",
                 "simt": "apply_kernel<Shape<3,4,Elasticity>, double> (SIMT)"}
+
+
+def fp64_peaks(stream) -> dict:
+    """Measured FP64 throughput of this GPU (tdg_probe_fp64_peak): every FP64 path (CUDA-core FMA
+    and the tensor pipe's f64 mma.sync shapes) at 2 and 4 CTAs of 256 threads per SM, best of three
+    20 ms launches each.  The roofline denominator of the FP64 apply is the largest of them."""
+    import ctypes as C
+    from tandem_b200 import _ffi
+    out = {}
+    for kind, name in enumerate(FP64_PROBES):
+        best = 0.0
+        for ctas in (2, 4):
+            v = C.c_double(0.0)
+            _ffi.check(_ffi.lib().tdg_probe_fp64_peak(kind, ctas, C.c_void_p(stream.cuda_stream), C.byref(v)))
+            best = max(best, v.value)
+        out[name] = best
+    return out
 
 
 def peaks():
@@ -175,13 +194,13 @@ class ClockSampler:
 def cpu_apply_sample(wl, target_s: float, threads: int, max_elements: int | None = None):
     """Times the oracle's element-centric apply on a contiguous slice of elements."""
     from oracle import Oracle
-    orc = Oracle(wl.mesh, wl.degree, wl.kind, wl.quad)
+    orc = getattr(wl, "orc", None) or Oracle(wl.mesh, wl.degree, wl.kind, wl.quad)
     orc.set_material(wl.c0, wl.c1)
     x = np.random.default_rng(1).standard_normal(orc.ndof)
     y = np.zeros_like(x)
     E = orc.E
-    n = min(512, E)
     e0 = E // 3
+    n = min(512, E - e0)
     t = time.perf_counter()
     orc.apply_range(e0, e0 + n, x, y)
     dt = time.perf_counter() - t
@@ -209,14 +228,31 @@ def cpu_solve_sample(wl, iterations: int = 20) -> dict:
             "pc_setup_seconds": t1 - t0, "cores": os.cpu_count(), "kind": "port"}
 
 
+def oracle_elasticity_cube(n: int, degree: int):
+    """The cube workload of elasticity_cube (same mesh, curved boundary, material fields and seeds)
+    built with the oracle alone: geometry nodes from the oracle's reference tables, quadrature-point
+    coordinates from the oracle, so the CPU arm neither loads the product library nor touches a GPU."""
+    from types import SimpleNamespace
+    from oracle import Oracle, Tables
+    from tandem_b200 import mesh as M
+    from tandem_b200.scenarios import RandomField
+    quad = tandem_quadrature(3, degree)
+    m = M.build(M.cube_mesh(n), degree, curve=M.box_boundary_surface(0.02), tables=Tables)
+    orc = Oracle(m, degree, 1, quad)
+    X = orc.volume_coords()
+    c0, c1 = RandomField(3, 2024, ell=0.2)(X), RandomField(3, 2025, ell=0.2)(X)
+    name = (f"3D isotropic elasticity p{degree}, unit cube {n}^3 x 6 tets ({m.num_elements:,}), curved P2 boundary, "
+            "log-normal lambda/mu")
+    return SimpleNamespace(name=name, mesh=m, quad=quad, kind=1, degree=degree, c0=c0, c1=c1, orc=orc)
+
+
 def run_reference(args):
     """CPU reference arm: tandem's element-centric apply restated (the oracle), all host cores,
     each step a bounded slice of the workload's elements."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from tandem_b200.workloads import elasticity_cube
-    wl = elasticity_cube(args.n, 4, tandem_quadrature(3, 4))
+    wl = oracle_elasticity_cube(args.n, 4)
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     orc, x, y, e0, n = cpu_apply_sample(wl, target_s=3.0, threads=threads)
     for _ in range(args.warmup):
@@ -272,7 +308,9 @@ def run_ours(args):
     x = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
     y = torch.empty_like(x)
 
-    # ---- the fastest FP64 launch configuration for this mesh, then the device-resident apply ----
+    # ---- measured FP64 peaks (roofline denominator), the fastest FP64 launch configuration for
+    # this mesh, then the device-resident apply ----
+    probes = fp64_peaks(stream)
     tune64 = op.autotune(FP64, stream=stream)
     best64 = min(tune64, key=lambda e: e["ms"])
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -332,7 +370,7 @@ def run_ours(args):
     ms32 = max_over_ranks(e0.elapsed_time(e1)) / args.steps
 
     solve = None
-    arms = select_arms(args) if args.solve or args.arms else (() if args.no_solve else MG_ARMS)
+    arms = select_arms(args) if args.solve or args.arms else (() if args.no_solve else DEFAULT_CUBE_ARMS)
     if arms:
         b = torch.as_tensor(op.rhs(wl.force, wl.bc), device="cuda")
         solve = {}
@@ -368,17 +406,23 @@ def run_ours(args):
     bytes_apply = op.bytes_apply(FP64)
     flops_apply = op.flops_apply()
     achieved = bytes_apply / (ms * 1e-3) / 1e9
+    tflops = flops_apply / (ms * 1e-3) / 1e12
+    fp64_peak = max(probes.values())
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
         traffic = json.loads(tfile.read_text()).get(f"apply_fp64_{best64['family']}_cube{args.n}")
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+    # 3D p4 elasticity runs at ~15 FLOP/B, right of the FP64 ridge (~40 TF/s over ~6.5 TB/s):
+    # the FP64 pipe binds, HBM is reported beside it
+    roofline = {"bound": "fp64", "achieved": tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": tflops / fp64_peak, "traffic": traffic,
+                "peak_source": "measured in this run (tdg_probe_fp64_peak, best FP64 path: "
+                               + max(probes, key=probes.get) + ")",
+                "fp64_probes_tflops": probes,
                 "kernel": KERNEL_NAMES[best64["family"]],
-                "algorithmic_bytes_per_launch": bytes_apply,
-                "fp64": {"achieved_tflops": flops_apply / (ms * 1e-3) / 1e12, "peak_tflops": FP64_NOMINAL_TFLOPS,
-                         "frac": flops_apply / (ms * 1e-3) / 1e12 / FP64_NOMINAL_TFLOPS,
-                         "peak_source": "nominal B200 FP64 (not measured)", "algorithmic_flops_per_launch": flops_apply}}
+                "algorithmic_flops_per_launch": flops_apply, "algorithmic_bytes_per_launch": bytes_apply,
+                "hbm": {"achieved_gbs": achieved, "peak_gbs": hbm, "frac": achieved / hbm,
+                        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}}
     cpu = None
     if world == 1 and not args.no_cpu:
         threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
@@ -654,21 +698,35 @@ def run_adjoint(args):
     gl, gm = lam.grad.numpy().copy(), mu.grad.numpy().copy()
     u0 = u.detach().clone()
 
-    # finite differences (mixed solves: FP64 recurrence and residual around the FP32 operator; block
-    # Jacobi, whose set-up per parameter change costs milliseconds)
+    # central finite differences.  Each side replaces the base material by tdg_update_material,
+    # which keeps the base point's preconditioner (the perturbation is one element by a factor
+    # 1 +- h), and solves for the correction A(theta') du = b(theta') - A(theta') u0 from the
+    # converged u0 to fd_rtol relative to that (O(h)) right-hand side; the minus side starts from
+    # -du of the plus side (they agree to O(h^2)).
     from tandem_b200.operator import MIXED
-    pb.precision, pb.pc_precision, pb.rtol, pb._theta = MIXED, FP64, args.fd_rtol, None
-    pb.preconditioner = "bjacobi"
+    fd_prec = {"fp64": FP64, "mixed": MIXED}[args.fd_precision]
     sel = np.random.Generator(np.random.PCG64(args.seed + 3)).choice(op.E, size=args.fd_elements, replace=False)
     h = 1e-4
+    ones = np.ones((1, op.Nq))
+    au = torch.empty_like(u0)
+    fd_its = []
 
-    def misfit_at(lv, mv):
-        pb.set_parameters(lv, mv)
-        r = torch.as_tensor(op.rhs(f, g), device="cuda")
-        au = torch.empty_like(u0)
-        op.apply(u0, au)
-        du = pb.solve(r - au)
-        return 0.5 * float(torch.sum((P.apply(u0 + du) - d) ** 2))
+    def misfit_pair(e, comp):
+        vals, du_prev = [], None
+        for sgn in (1.0, -1.0):
+            lv, mv = lam0.copy(), mu0.copy()
+            (lv if comp == "lambda" else mv)[e] *= 1.0 + sgn * h
+            op.update_material(lv[:, None] * ones, mv[:, None] * ones)
+            r = torch.as_tensor(op.rhs(f, g), device="cuda")
+            op.apply(u0, au)
+            r -= au
+            du = torch.zeros_like(u0) if du_prev is None else -du_prev
+            st = op.solve(r, du, precision=fd_prec, rtol=args.fd_rtol, max_iterations=args.max_iterations,
+                          check=False)
+            fd_its.append(st["iterations"])
+            du_prev = du
+            vals.append(0.5 * float(torch.sum((P.apply(u0 + du) - d) ** 2)))
+        return vals
 
     errs = {"lambda": [], "mu": []}
     absd = {"lambda": [], "mu": []}
@@ -676,11 +734,7 @@ def run_adjoint(args):
     f0 = time.perf_counter()
     for e in sel:
         for comp, grad in (("lambda", gl), ("mu", gm)):
-            vals = []
-            for sgn in (1.0, -1.0):
-                lv, mv = lam0.copy(), mu0.copy()
-                (lv if comp == "lambda" else mv)[e] *= 1.0 + sgn * h
-                vals.append(misfit_at(lv, mv))
+            vals = misfit_pair(e, comp)
             step = h * (lam0[e] if comp == "lambda" else mu0[e])
             fd = (vals[0] - vals[1]) / (2.0 * step)
             errs[comp].append(abs(grad[e] - fd) / abs(fd))
@@ -693,6 +747,8 @@ def run_adjoint(args):
            "config": {"workload": f"3D elasticity p4, unit cube {args.adj_n}^3 x 6 tets ({op.E:,}), curved P2 boundary, "
                                   f"512 observation points in [0.1,0.9]^3", "dofs": int(op.ndof),
                       "fd_elements": int(args.fd_elements), "fd_step_rel": h, "fd_solve_rtol": args.fd_rtol,
+                      "fd_solve_precision": args.fd_precision,
+                      "fd_preconditioner": f"{args.adj_pc} of the base point (kept by tdg_update_material)",
                       "gradient_solve_rtol": args.grad_rtol, "gradient_preconditioner": args.adj_pc,
                       "setup_seconds": setup_s},
            "misfit": float(J.detach()), "gradient_solves": solves,
@@ -700,7 +756,46 @@ def run_adjoint(args):
                   "median_rel_err_lambda": float(np.median(errs["lambda"])),
                   "median_rel_err_mu": float(np.median(errs["mu"])),
                   "max_err_rel_to_largest_lambda": max(absd["lambda"]) / scale["lambda"],
-                  "max_err_rel_to_largest_mu": max(absd["mu"]) / scale["mu"], "seconds": fd_s}}
+                  "max_err_rel_to_largest_mu": max(absd["mu"]) / scale["mu"], "seconds": fd_s,
+                  "max_rel_err": max(max(errs["lambda"]), max(errs["mu"])),
+                  "solve_iterations_mean": float(np.mean(fd_its))}}
+    print(json.dumps(out), flush=True)
+
+
+def run_vcycle(args):
+    """One multigrid V-cycle of the cube workload (logarithmic p1-p2-p4 levels, continuous P1 coarse
+    space, --mg-smooth-its Chebyshev steps, FP64) after one warm-up V-cycle, with the CUDA profiler
+    range (torch.cuda.profiler start / stop) around the timed one, so that a launch-list capture
+    (ncu --profile-from-start off) sees exactly one V-cycle."""
+    import torch
+    from tandem_b200.operator import FP64
+    from tandem_b200.workloads import elasticity_cube
+
+    torch.cuda.set_device(0)
+    wl = elasticity_cube(args.n, 4, tandem_quadrature(3, 4))
+    op = wl.op
+    stream = torch.cuda.current_stream()
+    tune = op.autotune(FP64, stream=stream)
+    op.mg_setup(smooth_its=MG_SMOOTH_ITS)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    r = torch.randn(op.ndof, dtype=torch.float64, device="cuda", generator=g)
+    z = torch.zeros_like(r)
+    op.mg_apply(r, z, stream=stream)
+    torch.cuda.synchronize()
+    c0 = op.mg_info()["coarse_iterations"]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.profiler.start()
+    e0.record(stream)
+    op.mg_apply(r, z, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    info = op.mg_info()
+    out = {"metric": "multigrid V-cycle time", "value": e0.elapsed_time(e1), "unit": "ms", "higher_is_better": False,
+           "n_gpus": 1, "dtype": "f64", "data": "synthetic (seeded mesh, random-field material)",
+           "config": {"workload": wl.name, "dofs": int(op.ndof), "levels": info["degrees"],
+                      "smooth_its": MG_SMOOTH_ITS, "coarse_space": "continuous P1"},
+           "coarse_iterations": info["coarse_iterations"] - c0, "apply_config": min(tune, key=lambda e: e["ms"])}
     print(json.dumps(out), flush=True)
 
 
@@ -722,17 +817,19 @@ def main():
     ap.add_argument("--max-iterations", type=int, default=30000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", choices=["cube", "batch", "gf", "poisson", "adjoint"], default="cube",
+    ap.add_argument("--workload", choices=["cube", "batch", "gf", "poisson", "adjoint", "vcycle"], default="cube",
                     help="cube: the apply benchmark (default); batch: uneven batch of 2D elasticity "
                          "solves; gf: discrete Green's function columns; poisson: 2D Poisson p4 "
-                         "64x64x2; adjoint: Lame gradient vs finite differences")
+                         "64x64x2; adjoint: Lame gradient vs finite differences; vcycle: one multigrid "
+                         "V-cycle of the cube inside a profiler range")
     ap.add_argument("--count", type=int, default=48, help="batch: number of problems")
     ap.add_argument("--columns", type=int, default=0, help="gf: columns to solve (0 = all)")
     ap.add_argument("--batch", type=int, default=256, help="gf: right-hand sides per solve")
     ap.add_argument("--square", type=int, default=64, help="poisson: cells per direction")
     ap.add_argument("--adj-n", type=int, default=16, help="adjoint: cube cells per direction")
-    ap.add_argument("--fd-elements", type=int, default=16, help="adjoint: elements checked by FD")
-    ap.add_argument("--fd-rtol", type=float, default=1e-10, help="adjoint: FD correction solve tolerance")
+    ap.add_argument("--fd-elements", type=int, default=64, help="adjoint: elements checked by FD")
+    ap.add_argument("--fd-rtol", type=float, default=1e-12, help="adjoint: FD correction solve tolerance")
+    ap.add_argument("--fd-precision", choices=["fp64", "mixed"], default="fp64", help="adjoint: FD solve precision")
     ap.add_argument("--grad-rtol", type=float, default=1e-12, help="adjoint: forward / adjoint solve tolerance")
     ap.add_argument("--adj-pc", choices=["bjacobi", "mg"], default="mg", help="adjoint: gradient solves' preconditioner")
     ap.add_argument("--seed", type=int, default=11)
@@ -748,6 +845,8 @@ def main():
         run_poisson(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "vcycle":
+        run_vcycle(args)
     else:
         run_ours(args)
 

@@ -111,6 +111,14 @@ int tdg_facet_normals(const tdg_op* op, double* out);
  * uploads everything to the current device. */
 int tdg_set_material(tdg_op* op, const double* c0_Q, const double* c1_Q);
 
+/* Replaces the material as tdg_set_material does but keeps the preconditioner built for the
+ * previous material (block-Jacobi inverses and the multigrid hierarchy, whichever exist), which
+ * then approximates the new operator's preconditioner.  For nearby materials -- finite-difference
+ * checks, line searches of an inversion -- where rebuilding the preconditioner costs more than the
+ * Krylov iterations it saves (no counterpart in tandem, which rebuilds on every change).
+ * TDG_E_STATE when no material or no preconditioner has been set up yet. */
+int tdg_update_material(tdg_op* op, const double* c0_Q, const double* c1_Q);
+
 /* Nodal material coefficients [E][Nbf] for c = 0, 1 (after projection). */
 int tdg_material_nodal(const tdg_op* op, int c, double* out);
 /* Penalty per facet [F]. */
@@ -163,6 +171,14 @@ int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_ent
 /* Sets the apply configuration of `precision` (TDG_FP64 / TDG_FP32; TDG_MIXED follows TDG_FP32)
  * explicitly: kernel family as in tdg_tune_entry and persistent CTAs per SM. */
 int tdg_set_apply_config(tdg_op* op, int precision, int family, int ctas_per_sm);
+
+/* Measured FP64 throughput of the current device (no counterpart in tandem; the denominator of the
+ * FP64 apply's roofline): kind 0 = FP64 FMA on the CUDA cores, 1..4 = the FP64 tensor pipe through
+ * mma.sync of shape m8n8k4, m16n8k4, m16n8k8, m16n8k16; ctas_per_sm CTAs of 256 threads per SM
+ * (0 = 2), every warp with 8 independent accumulators.  Times 3 launches of about 20 ms with CUDA
+ * events on `stream` after a warm-up and returns the best rate in *tflops.  Allocates and frees
+ * two small device buffers; synchronises `stream`. */
+int tdg_probe_fp64_peak(int kind, int ctas_per_sm, void* stream, double* tflops);
 
 /* --- right-hand side (DGOperator::rhs, src/form/DGOperator.h:189-237) ---------------------- */
 
@@ -321,19 +337,22 @@ int tdg_adjoint_lame_gradient(tdg_op* op, const double* u, const double* p, cons
                               void* stream);
 
 /* Allocation-free variant of tdg_adjoint_lame_gradient (no counterpart in tandem).  Same inputs,
- * output and arithmetic; it calls no device or host allocator.  For callers that cannot allocate
- * device memory at the time of the call: a process whose caching allocator (torch, PETSc pools)
- * already holds the device memory, where a fresh cudaMallocAsync can fail with out-of-memory in the
- * middle of an optimisation loop, or a caller running inside an allocator or memory-pool callback.
- * The per-facet penalty derivatives go through a fixed device scratch, a static __device__ array
- * of 2^20 doubles (8 MiB) per device: meshes with 4 F + 2 E > 2^20 (about 120,000 tetrahedra or
- * 170,000 triangles) return TDG_E_INVALID with the sizes in tdg_last_error.  Every scratch entry
- * the kernel reads is written by the call, so nothing needs clearing.  The operator's FP64 data
- * must already be resident (one FP64 tdg_apply after tdg_set_material), else TDG_E_STATE.
- * Calls on one device share the scratch: overlapping calls (two host threads, or two streams)
- * race and must be serialised by the caller.  The call synchronises `stream` before returning.
- * The first call on each device looks up the scratch address (cudaGetSymbolAddress, with that
- * device current); make it before any stream capture begins. */
+ * output and arithmetic; on success it calls no device or host allocator.  For callers that cannot
+ * allocate device memory at the time of the call: a process whose caching allocator (torch, PETSc
+ * pools) already holds the device memory, where a fresh cudaMallocAsync can fail with out-of-memory
+ * in the middle of an optimisation loop, or a caller running inside an allocator or memory-pool
+ * callback.  The per-facet penalty derivatives go through a fixed device scratch, a static
+ * __device__ array of 2^20 doubles (8 MiB) per device, staged from a static host buffer of 2^16
+ * doubles: meshes with 4 F + 2 E > 2^20 (about 120,000 tetrahedra or 170,000 triangles) return
+ * TDG_E_INVALID with the sizes in tdg_last_error.  Every scratch entry the kernel reads is written
+ * by the call, so nothing needs clearing.  The operator's FP64 data must already be resident (one
+ * FP64 tdg_apply after tdg_set_material), else TDG_E_STATE: that upload, on the device current at
+ * the time, also looks up the scratch address (cudaGetSymbolAddress) and loads the gradient kernel,
+ * the two steps that can place the scratch or code in device memory, so this call itself does
+ * neither.  Calls on one device share the scratch (and all calls the host buffer): overlapping
+ * calls (two host threads, or two streams) race on the device and must be serialised by the
+ * caller.  The call synchronises `stream` before returning.  A failing call records its message
+ * for tdg_last_error in a thread-local string, which may allocate host memory. */
 int tdg_adjoint_lame_gradient_noalloc(tdg_op* op, const double* u, const double* p, const double* bc_q,
                                       double* grad, void* stream);
 
@@ -360,6 +379,17 @@ int tdg_fault_slip_rhs(tdg_fault* fault, const double* slip, int64_t ld_slip, do
  * device [nrhs][ld_t] with ld_t >= num_fault * nbf. */
 int tdg_fault_traction(tdg_fault* fault, const double* u, int64_t ld, const double* slip, int64_t ld_slip,
                        double* traction, int64_t ld_t, int nrhs, void* stream);
+
+/* Traction update of the discrete Green's function operator
+ * (SeasQDDiscreteGreenOperator::update_traction, app/form/SeasQDDiscreteGreenOperator.cpp:115-127:
+ * MatMult(G_, S, traction) followed by VecAXPY(traction, time, t_boundary_)) in one kernel, for k
+ * slip states at once: out[j * ldo + i] = sum_c G[i * ldg + c] S[j * lds + c] + time t_boundary[i],
+ * i < n, c < m, j < k.  G: device, dense row-major n x m (leading dimension ldg >= m), read once
+ * per group of 4 states; S: device [k][lds]; t_boundary: device [n] or NULL (no boundary term);
+ * out: device [k][ldo], must not overlap S.  m <= 7264 (the states of a group sit in shared
+ * memory). */
+int tdg_gf_traction_update(int64_t n, int64_t m, const double* G, int64_t ldg, const double* S, int64_t lds,
+                           int k, const double* t_boundary, double time, double* out, int64_t ldo, void* stream);
 
 /* --- projection and evaluation (host; AbstractDGOperator::project / solution) -------------------- */
 

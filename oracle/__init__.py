@@ -45,12 +45,35 @@ def lib() -> C.CDLL:
             "orc_fault_traction": (None, [_p, C.c_long, _p, _p, _p, C.c_int, _p, _p, _p]),
             "orc_mg_interpolation": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _p]),
             "orc_mg_levels": (C.c_int, [C.c_int, C.c_int, C.c_int, _p]),
+            "orc_ref_nodes": (C.c_int, [C.c_int, C.c_int, C.c_int, _p]),
+            "orc_ref_basis": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _p, _p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
             fn.restype, fn.argtypes = res, args
         _lib = L
     return _lib
+
+
+class Tables:
+    """Reference nodes and nodal basis values from the oracle library, with the signatures of
+    tandem_b200.refelem's ref_nodes / ref_basis, so that test-side code can build a mesh's geometry
+    nodes (tandem_b200.mesh.build(..., tables=Tables)) without loading the product library."""
+
+    @staticmethod
+    def ref_nodes(dim: int, degree: int, family: int = 0) -> np.ndarray:
+        out = np.zeros((comb(degree + dim, dim), dim))
+        lib().orc_ref_nodes(dim, degree, family, out.ctypes.data)
+        return out
+
+    @staticmethod
+    def ref_basis(dim: int, degree: int, family: int, points: np.ndarray, grad: bool = False):
+        if grad:
+            raise ValueError("the oracle's tables give basis values only")
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, dim)
+        E = np.zeros((comb(degree + dim, dim), pts.shape[0]))
+        lib().orc_ref_basis(dim, degree, family, pts.shape[0], pts.ctypes.data, E.ctypes.data)
+        return E
 
 
 def ref_lib() -> C.CDLL | None:

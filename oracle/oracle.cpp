@@ -1193,3 +1193,25 @@ int orc_mg_levels(int strategy, int coarse, int N, int* out) {
 }
 
 }  // extern "C"
+
+// ---- reference-element tables for building geometry nodes on the test side ------------------------
+extern "C" {
+
+// Nodes of degree N (family 0 warp & blend, 1 equidistant) [Nbf][D], and the nodal basis values at
+// np points [Nbf][np]: what a test-side mesh builder needs to place Curvilinear's geometry nodes
+// without the product library.
+int orc_ref_nodes(int D, int N, int family, double* out) {
+    Points p = family == 0 ? tdg::warp_blend_nodes(D, N) : tdg::equidistant_nodes(D, N);
+    std::memcpy(out, p.data(), p.size() * sizeof(double));
+    return 0;
+}
+
+int orc_ref_basis(int D, int N, int family, int np, const double* points, double* E) {
+    RefSpace sp = RefSpace::nodal(D, N, family == 0 ? tdg::warp_blend_nodes(D, N) : tdg::equidistant_nodes(D, N));
+    Points pts(points, points + static_cast<size_t>(np) * D);
+    Dense e = sp.eval(pts);
+    std::memcpy(E, e.a.data(), e.a.size() * sizeof(double));
+    return 0;
+}
+
+}  // extern "C"

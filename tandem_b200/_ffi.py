@@ -29,6 +29,7 @@ SYMBOLS = {
     "tdg_facet_coords": (C.c_int, [_p, _p]),
     "tdg_facet_normals": (C.c_int, [_p, _p]),
     "tdg_set_material": (C.c_int, [_p, _p, _p]),
+    "tdg_update_material": (C.c_int, [_p, _p, _p]),
     "tdg_material_nodal": (C.c_int, [_p, C.c_int, _p]),
     "tdg_penalty": (C.c_int, [_p, _p]),
     "tdg_apply": (C.c_int, [_p, C.c_int, _p, _p, C.c_int, _i64, _p]),
@@ -44,6 +45,7 @@ SYMBOLS = {
     "tdg_adjoint_lame_gradient_noalloc": (C.c_int, [_p, _p, _p, _p, _p, _p]),
     "tdg_autotune": (C.c_int, [_p, C.c_int, C.c_int, _p, _p, C.c_int, _p]),
     "tdg_set_apply_config": (C.c_int, [_p, C.c_int, C.c_int, C.c_int]),
+    "tdg_probe_fp64_peak": (C.c_int, [C.c_int, C.c_int, _p, C.POINTER(C.c_double)]),
     "tdg_set_density": (C.c_int, [_p, _p]),
     "tdg_apply_inverse_mass": (C.c_int, [_p, _p, _p, C.c_int, _i64, _p]),
     "tdg_wave_rhs": (C.c_int, [_p, _p, _p, _p, C.c_int, _i64, _p]),
@@ -62,6 +64,7 @@ SYMBOLS = {
     "tdg_error_l2": (C.c_int, [_p, _p, C.c_int, _p, _p, _p, _p]),
     "tdg_error_h1_semi": (C.c_int, [_p, _p, C.c_int, _p, _p, _p, _p]),
     "tdg_mg_vertex_numbering": (C.c_int, [_p, _p, _p]),
+    "tdg_gf_traction_update": (C.c_int, [_i64, _i64, _p, _i64, _p, _i64, C.c_int, _p, C.c_double, _p, _i64, _p]),
     "tdg_fault_create": (C.c_int, [_p, _i64, _p, _p, C.POINTER(_p)]),
     "tdg_fault_destroy": (None, [_p]),
     "tdg_fault_sizes": (C.c_int, [_p, _p]),

@@ -97,9 +97,10 @@ class LameProblem:
 
     def gradient_noalloc(self, u, p, grad, stream=None):
         """Allocation-free gradient into the caller's grad [E, 2] (CUDA float64): no device or host
-        allocation inside the call.  Meshes up to 4 F + 2 E <= 2^20 (fixed 8 MiB device scratch);
-        the FP64 operator data must be resident (an FP64 apply after set_material).  Calls on one
-        device must not overlap."""
+        allocation inside a successful call, for loops that cannot allocate device memory (their
+        process's caching pool holds it).  Meshes up to 4 F + 2 E <= 2^20 (fixed 8 MiB device
+        scratch); the FP64 operator data must be resident (an FP64 apply after set_material, which
+        also prepares the scratch and the kernel).  Calls on one device must not overlap."""
         _check_vec(u, FP64, self.op.ndof)
         _check_vec(p, FP64, self.op.ndof)
         _check_vec(grad, FP64, 2 * self.op.E)

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <exception>
 #include <limits>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -440,6 +441,10 @@ int ensure_uploaded(tdg_op* op, int precision) {
         if (!op->uploaded64) {
             TDG_TRY(upload_precision<double>(op, op->arena64, op->op64));
             op->uploaded64 = true;
+            // the allocation-free gradient entry point of elasticity operators reads these data:
+            // resolve its fixed scratch and load its kernel now, while allocating is allowed (a
+            // failure here is reported by that entry point when it repeats the lookup)
+            if (op->h.kind == 1 && adjoint_prepare(op->h.D, op->h.N)) cudaGetLastError();
         }
         return 0;
     }
@@ -1133,6 +1138,27 @@ int tdg_set_material(tdg_op* op, const double* c0_Q, const double* c1_Q) {
     op->inv_precision = -1;
     op->mg.ready = false;  // the hierarchy's Galerkin operators and bounds belong to the old material
     op->status = nullptr;
+    return 0;
+}
+
+int tdg_update_material(tdg_op* op, const double* c0_Q, const double* c1_Q) {
+    if (!op) return fail(TDG_E_INVALID, "null operator");
+    const bool pc_ready = op->inv != nullptr || op->mg.ready;
+    if (!op->h.has_material || !pc_ready)
+        return fail(TDG_E_STATE, "tdg_update_material needs a material and a preconditioner set up for it");
+    try {
+        op->h.set_material(c0_Q, c1_Q);
+    } catch (std::exception const& e) {
+        return fail(TDG_E_INVALID, e.what());
+    }
+    // the operator's own data (both precisions, the penalty) follow the new material on the next
+    // upload; the block-Jacobi inverses (arena_pc) and the multigrid hierarchy stay as they are
+    op->arena64.release();
+    op->arena32.release();
+    op->arena_common.release();
+    op->uploaded64 = op->uploaded32 = false;
+    op->penalty = nullptr;
+    op->sides = nullptr;
     return 0;
 }
 
@@ -2106,6 +2132,20 @@ extern "C" int tdg_fault_traction(tdg_fault* fault, const double* u, int64_t ld,
     return rc ? fail(rc, "fault traction launch failed") : 0;
 }
 
+extern "C" int tdg_gf_traction_update(int64_t n, int64_t m, const double* G, int64_t ldg, const double* S,
+                                      int64_t lds, int k, const double* t_boundary, double time, double* out,
+                                      int64_t ldo, void* stream) {
+    if (!G || !S || !out || n < 0 || m < 0 || k < 0) return fail(TDG_E_INVALID, "null argument or negative size");
+    if (n == 0 || k == 0) return 0;
+    if (ldg < m || (k > 1 && (lds < m || ldo < n))) return fail(TDG_E_INVALID, "leading dimension too small");
+    if (m == 0) return fail(TDG_E_INVALID, "G has no columns");
+    if ((out < S + lds * (k - 1) + m && S < out + ldo * (k - 1) + n))
+        return fail(TDG_E_INVALID, "out must not overlap the slip states");
+    int rc = launch_gf_traction(n, m, G, ldg, S, lds, k, t_boundary, time, out, ldo, static_cast<cudaStream_t>(stream));
+    if (rc == TDG_E_INVALID) return fail(rc, "G has too many columns for the shared-memory slip states (m <= 7264)");
+    return rc ? fail(rc, std::string("traction update launch failed: ") + cudaGetErrorString(cudaGetLastError())) : 0;
+}
+
 // ------------------------------------------------------------------------------------------------
 // adjoint gradient with respect to per-element Lame parameters
 // ------------------------------------------------------------------------------------------------
@@ -2177,14 +2217,35 @@ extern "C" int tdg_adjoint_lame_gradient(tdg_op* op, const double* u, const doub
 }
 
 // Allocation-free variant: the penalty derivatives go through the fixed device scratch of
-// adjoint.cu in chunks staged on the stack; the operator's FP64 data must already be resident.
+// adjoint.cu, staged in chunks through a static host buffer; the operator's FP64 data must already
+// be resident (its upload resolved the scratch address and loaded the kernel).
+namespace {
+constexpr size_t kNoallocStage = size_t(1) << 16;  // doubles; a multiple of 4 (facet) and 2 (element)
+double g_noalloc_stage[kNoallocStage];
+std::mutex g_noalloc_mutex;
+
+// lam, mu of element e: the mean of its nodal coefficients (constant per element, checked).
+inline void element_lame(HostOperator const& h, int nm, int64_t e, double& lam, double& mu) {
+    const double* a = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 0) * nm];
+    const double* b = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 1) * nm];
+    double sa = 0.0, sb = 0.0;
+    for (int i = 0; i < nm; ++i) {
+        sa += a[i];
+        sb += b[i];
+    }
+    lam = sa / nm;
+    mu = sb / nm;
+}
+}  // namespace
+
 extern "C" int tdg_adjoint_lame_gradient_noalloc(tdg_op* op, const double* u, const double* p, const double* bc_q,
                                                  double* grad, void* stream) {
     if (!op || !u || !p || !grad) return fail(TDG_E_INVALID, "null argument");
     auto const& h = op->h;
     if (h.kind != 1) return fail(TDG_E_INVALID, "the Lame gradient needs an elasticity operator");
     if (!h.has_material) return fail(TDG_E_STATE, "no material");
-    const size_t need = static_cast<size_t>(h.F) * 4 + static_cast<size_t>(h.E) * 2;
+    const size_t nfct = static_cast<size_t>(h.F) * 4;
+    const size_t need = nfct + static_cast<size_t>(h.E) * 2;
     if (need > kAdjointScratchDoubles) {
         char msg[256];
         std::snprintf(msg, sizeof msg,
@@ -2197,20 +2258,9 @@ extern "C" int tdg_adjoint_lame_gradient_noalloc(tdg_op* op, const double* u, co
         return fail(TDG_E_STATE, "FP64 operator data not resident: call tdg_apply (FP64) once after tdg_set_material");
     const int nm = h.mat_space.num_basis();
     const int D = h.D;
-    auto lam_mu = [&](int64_t e, double& lam, double& mu) {
-        const double* a = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 0) * nm];
-        const double* b = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 1) * nm];
-        double sa = 0.0, sb = 0.0;
-        for (int i = 0; i < nm; ++i) {
-            sa += a[i];
-            sb += b[i];
-        }
-        lam = sa / nm;
-        mu = sb / nm;
-    };
     for (int64_t e = 0; e < h.E; ++e) {
         double lam, mu;
-        lam_mu(e, lam, mu);
+        element_lame(h, nm, e, lam, mu);
         const double* a = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 0) * nm];
         const double* b = &h.mat_nodal[(static_cast<size_t>(e) * 2 + 1) * nm];
         for (int i = 0; i < nm; ++i)
@@ -2220,33 +2270,43 @@ extern "C" int tdg_adjoint_lame_gradient_noalloc(tdg_op* op, const double* u, co
     double* scratch = nullptr;
     if (adjoint_scratch(&scratch)) return fail(TDG_E_CUDA, "looking up the fixed scratch failed");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    // the same values as lame_gradient_inputs, produced entry by entry
+    // the values of lame_gradient_inputs: per facet both sides' penalty derivatives (each side's
+    // lam, mu computed once per facet), then per element (lam, mu)
     const double cN1 = h.N * (h.N - 1.0 + D) / static_cast<double>(D);
-    auto entry = [&](size_t i) -> double {
-        if (i >= static_cast<size_t>(h.F) * 4) {
-            const size_t j = i - static_cast<size_t>(h.F) * 4;
-            double lam, mu;
-            lam_mu(static_cast<int64_t>(j / 2), lam, mu);
-            return (j % 2) ? mu : lam;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    for (size_t c0 = 0; c0 < need; c0 += kNoallocStage) {
+        const size_t n = std::min(kNoallocStage, need - c0);
+        double* st = g_noalloc_stage;
+        for (size_t i = c0; i < c0 + n;) {
+            if (i < nfct) {  // chunk boundaries are multiples of 4: a facet never straddles two
+                const int64_t f = static_cast<int64_t>(i / 4);
+                const bool interior = h.up[2 * f] != h.up[2 * f + 1];
+                const double scale = interior ? 0.25 : 1.0;
+                for (int sd = 0; sd < 2; ++sd) {
+                    double dl = 0.0, dm = 0.0;
+                    if (sd == 0 || interior) {
+                        const int64_t e = h.up[2 * f + sd];
+                        double lam, mu;
+                        element_lame(h, nm, e, lam, mu);
+                        const double K = (D + 1) * cN1 * h.area[f] / h.volume[e];
+                        const double c0v = 2.0 * mu, c1v = D * lam + 2.0 * mu;
+                        dl = scale * K * 2.0 * c1v * D / c0v;
+                        dm = scale * K * (4.0 * c1v / c0v - 2.0 * c1v * c1v / (c0v * c0v));
+                    }
+                    st[i - c0 + 2 * sd] = dl;
+                    st[i - c0 + 2 * sd + 1] = dm;
+                }
+                i += 4;
+            } else {
+                const int64_t e = static_cast<int64_t>((i - nfct) / 2);
+                double lam, mu;
+                element_lame(h, nm, e, lam, mu);
+                st[i - c0] = lam;
+                st[i - c0 + 1] = mu;
+                i += 2;
+            }
         }
-        const int64_t f = static_cast<int64_t>(i / 4);
-        const int side = static_cast<int>((i % 4) / 2);
-        const bool interior = h.up[2 * f] != h.up[2 * f + 1];
-        if (side == 1 && !interior) return 0.0;
-        const int64_t e = h.up[2 * f + side];
-        double lam, mu;
-        lam_mu(e, lam, mu);
-        const double K = (D + 1) * cN1 * h.area[f] / h.volume[e];
-        const double c0 = 2.0 * mu, c1 = D * lam + 2.0 * mu;
-        const double scale = interior ? 0.25 : 1.0;
-        return (i % 2) ? scale * K * (4.0 * c1 / c0 - 2.0 * c1 * c1 / (c0 * c0)) : scale * K * 2.0 * c1 * D / c0;
-    };
-    constexpr size_t kStage = 2048;
-    double stage[kStage];
-    for (size_t c0 = 0; c0 < need; c0 += kStage) {
-        const size_t n = std::min(kStage, need - c0);
-        for (size_t k = 0; k < n; ++k) stage[k] = entry(c0 + k);
-        TDG_CUDA_TRY(cudaMemcpyAsync(scratch + c0, stage, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        TDG_CUDA_TRY(cudaMemcpyAsync(scratch + c0, st, n * sizeof(double), cudaMemcpyHostToDevice, s));
         TDG_CUDA_TRY(cudaStreamSynchronize(s));  // the stage is reused
     }
     int rc = launch_adjoint_lame(h.D, h.N, op->op64, u, p, bc_q, scratch, grad, s);

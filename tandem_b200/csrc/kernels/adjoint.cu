@@ -67,4 +67,24 @@ int adjoint_scratch(double** ptr) {
     return 0;
 }
 
+namespace {
+template <int D, int N>
+cudaError_t load_adj() {
+    cudaFuncAttributes a{};
+    return cudaFuncGetAttributes(&a, adjoint_lame_kernel<Shape<D, N, kElasticity>>);
+}
+}  // namespace
+
+int adjoint_prepare(int D, int N) {
+    // Under lazy module loading the module image (and with it the static scratch) and the kernel's
+    // code are placed in device memory on first use; doing both here, while the caller is still
+    // allowed to allocate, keeps the allocation-free entry point free of them.
+    double* p = nullptr;
+    if (adjoint_scratch(&p)) return TDG_E_CUDA;
+    cudaError_t e = cudaErrorInvalidValue;
+    if (D == 2 && N >= 1 && N <= 4) e = N == 1 ? load_adj<2, 1>() : N == 2 ? load_adj<2, 2>() : N == 3 ? load_adj<2, 3>() : load_adj<2, 4>();
+    if (D == 3 && N >= 1 && N <= 4) e = N == 1 ? load_adj<3, 1>() : N == 2 ? load_adj<3, 2>() : N == 3 ? load_adj<3, 3>() : load_adj<3, 4>();
+    return e == cudaSuccess ? 0 : TDG_E_CUDA;
+}
+
 }  // namespace tdg

@@ -67,15 +67,23 @@ int launch_adjoint_lame(int D, int N, DevOp<double> const& op, const double* u, 
 
 // Fixed device scratch of tdg_adjoint_lame_gradient_noalloc: 2^20 doubles (8 MiB) per device, a
 // static __device__ array.  adjoint_scratch returns its address on the current device (looked up
-// once per device); TDG_E_CUDA when the lookup fails.
+// once per device); TDG_E_CUDA when the lookup fails.  adjoint_prepare(D, N) looks the address up
+// and loads the gradient kernel of that shape on the current device (both may place code or the
+// module image in device memory under lazy loading), so that later calls allocate nothing.
 constexpr size_t kAdjointScratchDoubles = size_t(1) << 20;
 int adjoint_scratch(double** ptr);
+int adjoint_prepare(int D, int N);
 
 // y = Minv_rho (x - b) (elasticity inverse mass of the wave operator, wave.cuh); b may be null,
 // y may alias x.
 struct WaveData;
 int launch_inverse_mass(int D, int N, WaveData const& wd, int64_t E, int Nq, const double* x, const double* b,
                         double* y, int nrhs, int64_t ld, cudaStream_t s);
+
+// out[:, j] = G S[:, j] + t tb for k states (Green's-function traction update, gf_traction.cu);
+// G row-major [n][ldg], S / out [k][lds / ldo], tb may be null.
+int launch_gf_traction(int64_t n, int64_t m, const double* G, int64_t ldg, const double* S, int64_t lds, int k,
+                       const double* tb, double t, double* out, int64_t ldo, cudaStream_t s);
 
 // Number of resident CTAs of a kernel on the current device times the SM count, cached.
 int device_sm_count();

@@ -6,8 +6,8 @@
   optional checkpoint after every batch;
 * ``compute_boundary_traction``: the traction of the zero-slip solve with the boundary / body data
   at time 1 (compute_boundary_traction, :129-150);
-* ``update_traction``: traction = G S + time t_boundary (update_traction, :115-127) as one FP64
-  GEMM (cuBLAS through torch) over any number of slip states;
+* ``update_traction``: traction = G S + time t_boundary (update_traction, :115-127) as one kernel
+  of the library (tdg_gf_traction_update) over any number of slip states;
 * ``save`` / ``load``: a checkpoint that does not depend on how the fault was partitioned or
   ordered (write_discrete_greens_operator / load_discrete_greens_operator, :201-237, :432-491):
   G is stored with the global facet labels of its block rows and columns and the set of computed
@@ -117,12 +117,28 @@ class DiscreteGreensOperator:
         self.fault.traction(x, slip, out)
         self.t_boundary = out
 
-    def update_traction(self, slip, time: float = 0.0):
-        """traction = G slip + time t_boundary for slip [n] or [n, k] (k slip states at once)."""
+    def update_traction(self, slip, time: float = 0.0, stream=None):
+        """traction = G slip + time t_boundary for slip [n] or [n, k] (k slip states at once), one
+        kernel of the library (tdg_gf_traction_update: G read once per group of 4 states, the
+        boundary term fused)."""
+        import ctypes as C
+        import torch
+        from . import _ffi
+        from .operator import _stream
         if self.current != self.n:
             raise RuntimeError(f"G has {self.current} of {self.n} columns")
-        t = self.G @ slip
-        return t + time * (self.t_boundary if t.dim() == 1 else self.t_boundary[:, None])
+        if slip.dtype != torch.float64 or not slip.is_cuda or slip.shape[0] != self.n or slip.dim() > 2:
+            raise ValueError(f"slip must be a CUDA float64 tensor [{self.n}] or [{self.n}, k]")
+        k = 1 if slip.dim() == 1 else slip.shape[1]
+        S = slip.reshape(self.n, k).T.contiguous()  # [k][n]: one state per row
+        G = self.G.contiguous()
+        tb = self.t_boundary.contiguous()
+        out = torch.empty(k, self.n, dtype=torch.float64, device=slip.device)
+        _ffi.check(_ffi.lib().tdg_gf_traction_update(self.n, self.n, C.c_void_p(G.data_ptr()), self.n,
+                                                     C.c_void_p(S.data_ptr()), self.n, k, C.c_void_p(tb.data_ptr()),
+                                                     float(time), C.c_void_p(out.data_ptr()), self.n,
+                                                     _stream(stream)))
+        return out[0] if slip.dim() == 1 else out.T
 
     def save(self, path: str) -> None:
         save_checkpoint(path, self.G.cpu().numpy(), self.done, self.labels, self.fault.nbf)

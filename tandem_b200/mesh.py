@@ -235,16 +235,18 @@ def _same_boundary_plane(a: np.ndarray, b: np.ndarray, tol: float = 1e-12) -> np
 
 
 def geometry_nodes(mesh: SimplexMesh, degree: int, p2: np.ndarray | None = None,
-                   transform: Callable[[np.ndarray], np.ndarray] | None = None) -> SimplexMesh:
-    """Degree-N warp & blend geometry nodes of every element (Curvilinear::vertices)."""
+                   transform: Callable[[np.ndarray], np.ndarray] | None = None, tables=None) -> SimplexMesh:
+    """Degree-N warp & blend geometry nodes of every element (Curvilinear::vertices).  tables: an
+    object with ref_nodes / ref_basis of this module's signatures (default: the native library's)."""
     D = mesh.dim
-    xi = ref_nodes(D, degree, WARP_BLEND)  # [Ngeo, D]
+    rn, rb = (ref_nodes, ref_basis) if tables is None else (tables.ref_nodes, tables.ref_basis)
+    xi = rn(D, degree, WARP_BLEND)  # [Ngeo, D]
     if p2 is None:
         lam = np.concatenate([(1.0 - xi.sum(axis=1))[:, None], xi], axis=1)  # [Ngeo, D+1]
         X = mesh.vertices[mesh.elements]  # [E, D+1, D]
         nodes = np.einsum("nv,evd->end", lam, X)
     else:
-        phi = ref_basis(D, 2, EQUIDISTANT, xi)  # [nP2, Ngeo]
+        phi = rb(D, 2, EQUIDISTANT, xi)  # [nP2, Ngeo]
         nodes = np.einsum("jn,ejd->end", phi, p2)
         mesh.p2_nodes = p2
     if transform is not None:
@@ -273,11 +275,11 @@ def box_boundary_surface(amplitude: float = 0.02):
 
 
 def build(mesh: SimplexMesh, degree: int, boundary_bc=BC_DIRICHLET, interior_bc=None, curve=None,
-          transform=None) -> SimplexMesh:
+          transform=None, tables=None) -> SimplexMesh:
     """Topology + geometry nodes in one call; curve is a boundary displacement (P2 geometry)."""
     topology(mesh, boundary_bc, interior_bc)
     p2 = p2_nodes(mesh, curve) if curve is not None else None
-    return geometry_nodes(mesh, degree, p2, transform)
+    return geometry_nodes(mesh, degree, p2, transform, tables)
 
 
 def union(meshes: list[SimplexMesh]) -> tuple[SimplexMesh, np.ndarray]:

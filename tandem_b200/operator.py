@@ -118,6 +118,14 @@ class DGOperator:
         self._mat = (a, b)
         _ffi.check(_ffi.lib().tdg_set_material(self._h, a.ctypes.data, None if b is None else b.ctypes.data))
 
+    def update_material(self, c0_Q: np.ndarray, c1_Q: np.ndarray | None = None) -> None:
+        """Replaces the material but keeps the preconditioner set up for the previous one
+        (tdg_update_material): for nearby materials (finite differences, line searches)."""
+        a = _c(c0_Q, np.float64).reshape(self.E, self.Nq)
+        b = None if c1_Q is None else _c(c1_Q, np.float64).reshape(self.E, self.Nq)
+        self._mat = (a, b)
+        _ffi.check(_ffi.lib().tdg_update_material(self._h, a.ctypes.data, None if b is None else b.ctypes.data))
+
     def material_nodal(self, c: int) -> np.ndarray:
         out = np.zeros((self.E, self.nbf))
         _ffi.check(_ffi.lib().tdg_material_nodal(self._h, c, out.ctypes.data))

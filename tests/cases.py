@@ -38,6 +38,44 @@ def make_mesh(dim: int, n: int, degree: int, curved: bool = False, bc=M.BC_DIRIC
                    curve=M.box_boundary_surface(0.02) if curved else None)
 
 
+def mixed_bc_codes(dim: int):
+    """Boundary and interior facet codes that exercise every branch of tandem's facet loop
+    (Poisson.cpp:591-631, Elasticity.cpp:752-801) on the unit square / cube (n even):
+    boundary x=0 Dirichlet, x=1 Natural, y=0 Fault, y=1 None (the element is its own neighbour),
+    in 3D also z=0 Dirichlet, z=1 Natural; interior facets on x=0.5 Fault, and a crack of interior
+    Natural facets on y=0.5 for x < 0.5 (no flux across it); all other interior facets None."""
+    tol = 1e-9
+
+    def on(c, d, v):
+        return np.all(np.abs(c[:, :, d] - v) < tol, axis=1)
+
+    def boundary_bc(c):
+        out = np.full(c.shape[0], M.BC_DIRICHLET, dtype=np.int32)
+        out[on(c, 0, 1.0)] = M.BC_NATURAL
+        out[on(c, 1, 0.0)] = M.BC_FAULT
+        out[on(c, 1, 1.0)] = M.BC_NONE
+        if dim == 3:
+            out[on(c, 2, 1.0)] = M.BC_NATURAL
+        out[on(c, 0, 0.0)] = M.BC_DIRICHLET
+        return out
+
+    def interior_bc(c):
+        out = np.full(c.shape[0], M.BC_NONE, dtype=np.int32)
+        out[on(c, 0, 0.5)] = M.BC_FAULT
+        crack = on(c, 1, 0.5) & np.all(c[:, :, 0] <= 0.5 + tol, axis=1)
+        out[crack] = M.BC_NATURAL
+        return out
+
+    return boundary_bc, interior_bc
+
+
+def mixed_bc_mesh(dim: int, n: int, degree: int, curved: bool = False):
+    """make_mesh with the facet codes of mixed_bc_codes (n even)."""
+    assert n % 2 == 0
+    bb, ib = mixed_bc_codes(dim)
+    return make_mesh(dim, n, degree, curved, bc=bb, interior_bc=ib)
+
+
 def material(kind: int, dim: int, X: np.ndarray, variable: bool, seed: int = 1, ell: float = 0.5):
     if kind == 0:
         if variable:
@@ -71,9 +109,10 @@ def mms_inputs(op, kind: int, dim: int, variable: bool):
     return sc, c0, c1, np.ascontiguousarray(f), np.ascontiguousarray(g)
 
 
-def product_and_oracle(kind: int, dim: int, n: int, degree: int, curved: bool, variable: bool, **mesh_kw):
+def product_and_oracle(kind: int, dim: int, n: int, degree: int, curved: bool, variable: bool,
+                       mixed_bc: bool = False, **mesh_kw):
     from oracle import Oracle
-    m = make_mesh(dim, n, degree, curved, **mesh_kw)
+    m = mixed_bc_mesh(dim, n, degree, curved) if mixed_bc else make_mesh(dim, n, degree, curved, **mesh_kw)
     q = tandem_quadrature(dim, degree)
     op = DGOperator(m, degree, kind, q)
     orc = Oracle(m, degree, kind, q)

@@ -91,6 +91,19 @@ def test_product_rhs_matches_oracle(kind, dim):
     np.testing.assert_allclose(b_op, b_or, rtol=0, atol=1e-12 * np.abs(b_or).max())
 
 
+@pytest.mark.parametrize("kind,dim,degree", [(POISSON, 2, 4), (POISSON, 3, 2), (ELASTICITY, 2, 4),
+                                             (ELASTICITY, 3, 3)])
+def test_product_rhs_matches_oracle_mixed_bc(kind, dim, degree):
+    """Every facet code at once (boundary Dirichlet / Natural / Fault / None, interior Fault and
+    Natural): the volume load plus the lift terms of rhs_skeleton / rhs_boundary (Poisson.cpp:387-549,
+    Elasticity.cpp:521-696), boundary faults with the halved slip."""
+    m, op, orc = product_and_oracle(kind, dim, 4 if dim == 2 else 2, degree, True, True, mixed_bc=True)
+    sc, c0, c1, f, g = mms_inputs(op, kind, dim, True)
+    b_op = op.rhs(f, g)
+    b_or = orc.rhs(f, g)
+    np.testing.assert_allclose(b_op, b_or, rtol=0, atol=1e-12 * np.abs(b_or).max())
+
+
 def test_fault_facets_rhs():
     """A fault line through the square: interior facets with BC::Fault use the skeleton lift on
     both sides (Poisson.cpp:434-482); the product's host RHS matches the oracle."""

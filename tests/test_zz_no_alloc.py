@@ -1,7 +1,10 @@
 """tdg_adjoint_lame_gradient_noalloc (fixed device scratch, no allocation) against the allocating
 tdg_adjoint_lame_gradient: two calls in a row agree with it to 1e-13 relative (same kernel and
-inputs; only where the penalty derivatives are staged differs).  Collected last on purpose: it
-must pass after every other test has run in the process, and alone."""
+inputs; only where the penalty derivatives are staged differs), and a first call made before any
+allocating gradient call leaves the device's free memory unchanged.  The entry point serves
+callers that cannot allocate at the time of the call, e.g. an inversion loop in a process whose
+caching allocator already holds the device memory.  Collected last on purpose: it must pass after
+every other test has run in the process, and alone."""
 import numpy as np
 import pytest
 import torch
@@ -56,6 +59,24 @@ def test_noalloc_gradient_matches_allocating_entry(dim, n, degree, with_bc):
         pb.gradient_noalloc(u, p, g)
         torch.cuda.synchronize()
         assert (g - ref).abs().max().item() <= 1e-13 * scale
+
+
+@pytest.mark.parametrize("dim,n,degree", [(3, 2, 4), (2, 5, 2)])
+def test_noalloc_gradient_first_call_allocates_nothing(dim, n, degree):
+    """A fresh operator: one FP64 apply (which uploads the operator, resolves the scratch and loads
+    the gradient kernel), then the allocation-free call before any allocating gradient call.  The
+    device's free memory is the same before and after it; the result then matches the allocating
+    entry point."""
+    op, pb, u, p = _problem(dim, n, degree, True)
+    g = torch.full((op.E, 2), float("nan"), dtype=torch.float64, device=DEV)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    pb.gradient_noalloc(u, p, g)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 >= free0, (free0, free1)
+    ref = pb.gradient(u, p)
+    assert (g - ref).abs().max().item() <= 1e-13 * ref.abs().max().item()
 
 
 def test_noalloc_gradient_needs_resident_operator_data():
