@@ -1208,13 +1208,19 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
                                       static_cast<float*>(y), nrhs, ld, s, op->ctas[1]);
     if (precision == TDG_MIXED) {
         if (!op->use_mma) return fail(TDG_E_INVALID, "TDG_MIXED needs the tensor-core kernels");
-        if (face32)
-            rc = launch_apply_face_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, op->face32,
-                                                static_cast<const double*>(x), static_cast<double*>(y), nrhs, ld, s,
-                                                op->ctas[1]);
-        else
-            rc = launch_apply_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const double*>(x),
-                                           static_cast<double*>(y), nrhs, ld, s, op->ctas[1]);
+        // the selected tensor-core family, else the other one (a shape whose element-centric tile
+        // does not fit shared memory runs face-centric, and the reverse)
+        auto face = [&] {
+            return launch_apply_face_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, op->face32,
+                                                  static_cast<const double*>(x), static_cast<double*>(y), nrhs, ld, s,
+                                                  op->ctas[1]);
+        };
+        auto elem = [&] {
+            return launch_apply_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const double*>(x),
+                                             static_cast<double*>(y), nrhs, ld, s, op->ctas[1]);
+        };
+        rc = face32 ? face() : elem();
+        if (rc == TDG_E_INVALID) rc = face32 ? elem() : face();
         if (rc) return fail(rc, std::string("mixed apply launch failed: ") + cudaGetErrorString(cudaGetLastError()));
         return 0;
     }
