@@ -41,12 +41,16 @@ FP64_PROBES = ("dfma", "dmma_m8n8k4", "dmma_m16n8k4", "dmma_m16n8k8", "dmma_m16n
 # inverses; fp32_recurrence = FP32 vectors and recurrence with FP64 reliable updates.  Multigrid:
 # p-multigrid (tandem's mg_cheby configuration, continuous P1 coarse space) under flexible CG,
 # all FP64, or mixed = FP32 arithmetic in the finest level's smoother and the outer operator.
-BJ_ARMS = (("fp64", 0, 0, "bjacobi"), ("mixed", 2, 1, "bjacobi"), ("mixed_fp64_pc", 2, 0, "bjacobi"),
-           ("fp32_recurrence", 1, 1, "bjacobi"))
-MG_ARMS = (("mg_fp64", 0, 0, "mg"), ("mg_mixed", 2, 2, "mg"))
-SOLVE_ARMS = BJ_ARMS + MG_ARMS
-# the default cube leg: tandem's FP64 configuration (block-Jacobi CG) and the two multigrid arms
-DEFAULT_CUBE_ARMS = BJ_ARMS[:1] + MG_ARMS
+# The fifth entry is the Krylov method: CG, or flexible GMRES(30) as tandem's multigrid
+# configuration runs it (examples/options/mg_cheby.cfg: -ksp_type fgmres).
+BJ_ARMS = (("fp64", 0, 0, "bjacobi", "cg"), ("mixed", 2, 1, "bjacobi", "cg"), ("mixed_fp64_pc", 2, 0, "bjacobi", "cg"),
+           ("fp32_recurrence", 1, 1, "bjacobi", "cg"))
+MG_ARMS = (("mg_fp64", 0, 0, "mg", "cg"), ("mg_mixed", 2, 2, "mg", "cg"))
+GMRES_ARMS = (("mg_fgmres_fp64", 0, 0, "mg", "fgmres"), ("mg_fgmres_mixed", 2, 2, "mg", "fgmres"))
+SOLVE_ARMS = BJ_ARMS + MG_ARMS + GMRES_ARMS
+# the default cube leg: tandem's FP64 configuration (block-Jacobi CG), the two multigrid CG arms
+# and multigrid FGMRES in FP64 (tandem's multigrid configuration)
+DEFAULT_CUBE_ARMS = BJ_ARMS[:1] + MG_ARMS + GMRES_ARMS[:1]
 
 
 def select_arms(args, default=SOLVE_ARMS):
@@ -375,10 +379,11 @@ def run_ours(args):
         b = torch.as_tensor(op.rhs(wl.force, wl.bc), device="cuda")
         solve = {}
         x_first = None
-        for name, prec, pcp, pc in arms:
+        for name, prec, pcp, pc, method in arms:
             setup_s = max_over_ranks(prepare_arm(op, pcp, pc))
             xs = torch.zeros_like(b)
-            st = op.solve(b, xs, precision=prec, rtol=1e-10, max_iterations=args.max_iterations, check=False)
+            st = op.solve(b, xs, precision=prec, rtol=1e-10, max_iterations=args.max_iterations, check=False,
+                          method=method)
             solve[name] = {"seconds": max_over_ranks(st["seconds"]), "iterations": st["iterations"],
                            "reliable_updates": st["outer"], "fp64_continuation_iterations": st["fp64_iterations"],
                            "rel_residual": st["rel_residual"], "pc_setup_seconds": setup_s}
@@ -441,8 +446,9 @@ def run_ours(args):
                       "quadrature": f"tandem volRule {op.Nq} / fctRule {op.nq} points",
                       "l2": "inputs larger than L2 (x, y 165 MB each, geometry 2.8 GB per apply)",
                       "parallelism": f"replicas x{world}",
-                      "solve": "to 1e-10 rel. FP64 residual; multigrid arms: logarithmic p1-p2-p4, continuous P1 "
-                               f"coarse space, {MG_SMOOTH_ITS} Chebyshev steps per smoothing"},
+                      "solve": "to 1e-10 rel. FP64 residual; fp64 = block-Jacobi CG (tandem's default solver); "
+                               "multigrid arms: logarithmic p1-p2-p4, continuous P1 coarse space, "
+                               f"{MG_SMOOTH_ITS} Chebyshev steps per smoothing, flexible CG or FGMRES(30)"},
            "clocks": clk.summary(), "e2e": e2e,
            "gpu_launches": args.steps * (2 if best64["family"] == "face" else 1),
            "apply_config": best64, "autotune": tune64,
@@ -496,7 +502,7 @@ def run_batch(args):
     solve = {}
     sol = {}
     arms = select_arms(args)
-    for name, prec, pcp, pc in arms:
+    for name, prec, pcp, pc, method in arms:
         setup_s = prepare_arm(op, pcp, pc)
         rhs = rhs_h.to("cuda", non_blocking=True)
         xs = torch.zeros(n, dtype=torch.float64, device="cuda")
@@ -505,7 +511,7 @@ def run_batch(args):
         e0.record(stream)
         rhs = rhs_h.to("cuda", non_blocking=True)
         st, rel = solve_segmented(op, rhs, xs, b.elem_offsets, precision=prec, rtol=1e-10,
-                                  max_iterations=args.max_iterations, check=False)
+                                  max_iterations=args.max_iterations, check=False, method=method)
         xh = xs.to("cpu")
         e1.record(stream)
         torch.cuda.synchronize()
@@ -517,7 +523,7 @@ def run_batch(args):
                        "rel_residual_per_problem": [float(v) for v in rel], "pc_setup_seconds": setup_s}
         del xh
     op.set_preconditioner("bjacobi")
-    for name, _, _, _ in arms[1:]:
+    for name, _, _, _, _ in arms[1:]:
         d = []
         for i in range(args.count):
             sl = slice(int(b.elem_offsets[i]) * op.bs, int(b.elem_offsets[i + 1]) * op.bs)
@@ -560,12 +566,12 @@ def run_gf(args):
             "fp32": op.autotune(FP32, nrhs=min(args.batch, ncols))}
     res, Gs = {}, {}
     arms = select_arms(args)
-    for name, prec, pcp, pc in arms:
+    for name, prec, pcp, pc, method in arms:
         setup_s = prepare_arm(op, pcp, pc)
         torch.cuda.synchronize()
         w0 = time.perf_counter()
         G, stats = greens_function(op, fl, precision=prec, rtol=1e-10, columns=cols, batch=args.batch,
-                                   max_iterations=args.max_iterations)
+                                   max_iterations=args.max_iterations, method=method)
         torch.cuda.synchronize()
         wall = time.perf_counter() - w0
         Gs[name] = G
@@ -576,7 +582,7 @@ def run_gf(args):
                      "max_rel_residual": max(s["rel_residual"] for s in stats), "pc_setup_seconds": setup_s}
     op.set_preconditioner("bjacobi")
     first = arms[0][0]
-    for name, _, _, _ in arms[1:]:
+    for name, _, _, _, _ in arms[1:]:
         diff = torch.norm(Gs[name] - Gs[first], dim=0) / torch.norm(Gs[first], dim=0)
         res[name][f"max_column_rel_diff_vs_{first}"] = float(diff.max())
     add_speedups(res)
@@ -612,10 +618,11 @@ def run_poisson(args):
     b = torch.as_tensor(op.rhs(wl.force, wl.bc), device="cuda")
     solve, sol = {}, {}
     arms = select_arms(args)
-    for name, prec, pcp, pc in arms:
+    for name, prec, pcp, pc, method in arms:
         setup_s = prepare_arm(op, pcp, pc)
         xs = torch.zeros_like(b)
-        st = op.solve(b, xs, precision=prec, rtol=1e-10, max_iterations=args.max_iterations, check=False)
+        st = op.solve(b, xs, precision=prec, rtol=1e-10, max_iterations=args.max_iterations, check=False,
+                      method=method)
         sol[name] = xs
         solve[name] = {"seconds": st["seconds"], "iterations": st["iterations"], "reliable_updates": st["outer"],
                        "fp64_continuation_iterations": st["fp64_iterations"], "rel_residual": st["rel_residual"],

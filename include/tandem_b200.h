@@ -204,7 +204,19 @@ typedef struct {
                                (0 = default: 0.1) */
     int32_t max_outer;      /* cap on reliable updates (0 = none) */
     int32_t use_graphs;     /* capture iteration blocks in CUDA graphs */
+    int32_t method;         /* TDG_KSP_CG (default) or TDG_KSP_FGMRES */
+    int32_t restart;        /* FGMRES restart length m (0 = 30; at most 64) */
 } tdg_solve_opts;
+
+/* Krylov methods of tdg_solve / tdg_solve_segmented (KSPCG, and KSPFGMRES as tandem's multigrid
+ * configuration selects it, examples/options/mg_cheby.cfg:2).  TDG_KSP_FGMRES: restarted flexible
+ * GMRES(m) with right preconditioning, FP64 vectors, one Arnoldi process per right-hand side or
+ * problem; classical Gram-Schmidt applied twice, each pass one batched multi-dot reduction; every
+ * cycle starts from the FP64 residual b - A x.  Precision TDG_FP64 or TDG_MIXED (the operator and
+ * the preconditioner in FP32 arithmetic inside the FP64 cycles).  In tdg_solve_stats, iterations
+ * counts Arnoldi steps and outer the restart cycles. */
+#define TDG_KSP_CG 0
+#define TDG_KSP_FGMRES 1
 
 typedef struct {
     int32_t iterations;     /* total Krylov iterations */

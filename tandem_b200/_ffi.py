@@ -93,7 +93,11 @@ class TuneEntry(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("max_iterations", C.c_int32), ("rtol", C.c_double),
-                ("inner_rtol", C.c_double), ("max_outer", C.c_int32), ("use_graphs", C.c_int32)]
+                ("inner_rtol", C.c_double), ("max_outer", C.c_int32), ("use_graphs", C.c_int32),
+                ("method", C.c_int32), ("restart", C.c_int32)]
+
+
+TDG_KSP_CG, TDG_KSP_FGMRES = 0, 1
 
 
 TDG_PC_BJACOBI, TDG_PC_MG = 0, 1

@@ -9,6 +9,7 @@
 #include "kernels/wave.cuh"
 #include "kernels/dispatch.hpp"
 #include "kernels/krylov.cuh"
+#include "kernels/gmres.cuh"
 #include "kernels/mg.cuh"
 
 #include <algorithm>
@@ -1711,6 +1712,122 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
     return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "solve kernels");
 }
 
+// Restarted flexible GMRES(m) with right preconditioning (gmres.cuh), FP64 vectors; prec selects
+// the operator / preconditioner arithmetic (TDG_MIXED: FP32 arithmetic inside FP64 vectors).
+// Every cycle starts from the true FP64 residual b - A x, so the Arnoldi process of an inexact
+// (mixed) operator acts as an inner solver of an iterative refinement; a cycle of a segment ends
+// when its residual estimate meets max(tol, inner * beta) (inner = 1e-6 for TDG_MIXED, about the
+// FP32 operator's relative error; 0 for FP64), when its new basis vector vanishes, or after m
+// steps.  The host looks at the per-segment activity every kCheck steps (every step under
+// multigrid, which synchronises anyway) and ends a cycle early once no segment is active.
+struct GmWork {
+    double *V, *Z, *w, *dots, *H, *cs, *sn, *g, *y, *st, *gpart;
+    int gstride;  // columns of gpart per chunk: m + 2
+};
+
+int fgmres(tdg_op* op, int prec, SegPlan const& sp, const double* b, double* x, size_t vec, int m, GmWork const& gw,
+           double* r64, double* t64, double* partial, double* scal, double rtol, int max_it, cudaStream_t s,
+           std::vector<double>& rn, std::vector<double>& bn, int* iters, int* cycles, bool* diverged) {
+    const int nseg = sp.nseg;
+    const int kCheck = op->pc == TDG_PC_MG ? 1 : 4;
+    const double inner = prec == TDG_MIXED ? 1e-6 : 0.0;
+    const int ds = m + 2;  // columns of gw.dots per segment
+    std::vector<double> tol(nseg), hst(static_cast<size_t>(nseg) * kGm), hg(static_cast<size_t>(nseg) * (m + 1));
+    std::vector<double> last(nseg, HUGE_VAL);
+    int stagnant = 0;
+    *iters = 0;
+    *cycles = 0;
+    *diverged = false;
+    auto ngroups = [](int nv) { return (nv + kGmGroup - 1) / kGmGroup; };
+    for (;;) {
+        TDG_TRY(residual64(op, sp, b, x, r64, t64, partial, scal, rn, bn, s));
+        bool any = false, progress = false;
+        for (int i = 0; i < nseg; ++i) {
+            if (!std::isfinite(rn[i])) *diverged = true;
+            tol[i] = rtol * bn[i];
+            const bool act = rn[i] > tol[i];
+            any = any || act;
+            if (act && rn[i] < 0.999 * last[i]) progress = true;
+            last[i] = rn[i];
+            double* sg = &hst[static_cast<size_t>(i) * kGm];
+            std::fill(sg, sg + kGm, 0.0);
+            sg[kGmBeta] = rn[i];
+            sg[kGmActive] = act ? 1.0 : 0.0;
+            sg[kGmTol] = std::max(tol[i], inner * rn[i]);
+            sg[kGmEst] = rn[i];
+            double* gs = &hg[static_cast<size_t>(i) * (m + 1)];
+            std::fill(gs, gs + m + 1, 0.0);
+            gs[0] = rn[i];
+        }
+        if (*diverged || !any || *iters >= max_it) break;
+        stagnant = progress ? 0 : stagnant + 1;
+        if (stagnant >= 3) break;  // three cycles without a 0.1 % gain: the attainable accuracy
+        TDG_CUDA_TRY(cudaMemcpyAsync(gw.st, hst.data(), hst.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        TDG_CUDA_TRY(cudaMemcpyAsync(gw.g, hg.data(), hg.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        TDG_CUDA_TRY(cudaMemsetAsync(gw.H, 0, static_cast<size_t>(nseg) * (m + 1) * m * sizeof(double), s));
+        k_gm_start<<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, r64, gw.V, gw.st);
+        int j = 0;
+        while (j < m && *iters < max_it) {
+            double* vj = gw.V + static_cast<size_t>(j) * vec;
+            double* zj = gw.Z + static_cast<size_t>(j) * vec;
+            TDG_TRY(precondition<double>(op, prec, vj, zj, sp.op_nrhs, sp.op_ld, s));
+            TDG_TRY(tdg_apply(op, prec, zj, gw.w, sp.op_nrhs, sp.op_ld, s));
+            const int nv = j + 1;
+            const int ng = ngroups(nv);
+            // pass 1: h1 = V^T w, w -= V h1
+            for (int q = 0; q < ng; ++q) {
+                const int k0 = q * kGmGroup, nk = std::min(kGmGroup, nv - k0);
+                k_gm_dots<kGmGroup><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, gw.V + static_cast<size_t>(k0) * vec,
+                                                                      static_cast<int64_t>(vec), nk, gw.w, 0, gw.gpart,
+                                                                      gw.gstride, k0);
+            }
+            k_gm_reduce<<<nseg, 64, 0, s>>>(gw.gpart, gw.gstride, sp.seg_chunk, nv, gw.dots, ds);
+            k_gm_pass1<<<nseg, 64, 0, s>>>(gw.dots, ds, gw.H, m, j, nseg, gw.st);
+            for (int q = 0; q < ng; ++q) {
+                const int k0 = q * kGmGroup, nk = std::min(kGmGroup, nv - k0);
+                k_gm_update<kGmGroup><<<sp.nchunks, kVecThreads, 0, s>>>(
+                    sp.chunks, gw.V + static_cast<size_t>(k0) * vec, static_cast<int64_t>(vec), nk, gw.w, gw.dots + k0,
+                    ds, gw.st, nullptr);
+            }
+            // pass 2: h2 = V^T w and w.w, H[:, j] += h2, rotations; v_{j+1} = (w - V h2) / h_{j+1,j}
+            for (int q = 0; q < ng; ++q) {
+                const int k0 = q * kGmGroup, nk = std::min(kGmGroup, nv - k0);
+                k_gm_dots<kGmGroup><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, gw.V + static_cast<size_t>(k0) * vec,
+                                                                      static_cast<int64_t>(vec), nk, gw.w,
+                                                                      q == ng - 1 ? 1 : 0, gw.gpart, gw.gstride, k0);
+            }
+            k_gm_reduce<<<nseg, 64, 0, s>>>(gw.gpart, gw.gstride, sp.seg_chunk, nv + 1, gw.dots, ds);
+            k_gm_pass2<<<(nseg + 127) / 128, 128, 0, s>>>(gw.dots, ds, gw.H, gw.cs, gw.sn, gw.g, m, j, nseg, gw.st);
+            for (int q = 0; q < ng; ++q) {
+                const int k0 = q * kGmGroup, nk = std::min(kGmGroup, nv - k0);
+                k_gm_update<kGmGroup><<<sp.nchunks, kVecThreads, 0, s>>>(
+                    sp.chunks, gw.V + static_cast<size_t>(k0) * vec, static_cast<int64_t>(vec), nk, gw.w, gw.dots + k0,
+                    ds, gw.st, q == ng - 1 ? gw.V + static_cast<size_t>(j + 1) * vec : nullptr);
+            }
+            TDG_CUDA_TRY(cudaGetLastError());
+            ++j;
+            ++*iters;
+            if (j % kCheck == 0 && j < m) {
+                TDG_CUDA_TRY(cudaMemcpyAsync(hst.data(), gw.st, hst.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+                TDG_CUDA_TRY(cudaStreamSynchronize(s));
+                bool live = false;
+                for (int i = 0; i < nseg; ++i) live = live || hst[static_cast<size_t>(i) * kGm + kGmActive] != 0.0;
+                if (!live) break;
+            }
+        }
+        // x += Z y with y = R^-1 g over each segment's steps of this cycle
+        k_gm_solve_y<<<(nseg + 127) / 128, 128, 0, s>>>(gw.H, gw.g, gw.y, m, nseg, gw.st);
+        for (int q = 0; q < ngroups(j); ++q) {
+            const int k0 = q * kGmGroup, nk = std::min(kGmGroup, j - k0);
+            k_gm_update_x<kGmGroup><<<sp.nchunks, kVecThreads, 0, s>>>(
+                sp.chunks, gw.Z + static_cast<size_t>(k0) * vec, static_cast<int64_t>(vec), nk, x, gw.y + k0, m);
+        }
+        TDG_CUDA_TRY(cudaGetLastError());
+        ++*cycles;
+    }
+    return 0;
+}
+
 // Shared solve driver over a segment plan.  seg_rel (optional) receives each segment's final
 // relative residual.
 int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> const& seg_begin,
@@ -1718,6 +1835,11 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
                    const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel, cudaStream_t s) {
     const int prec = opts->precision;
     if (prec != TDG_FP64 && prec != TDG_FP32 && prec != TDG_MIXED) return fail(TDG_E_INVALID, "bad precision");
+    const bool gmres = opts->method == TDG_KSP_FGMRES;
+    if (opts->method != TDG_KSP_CG && !gmres) return fail(TDG_E_INVALID, "method must be TDG_KSP_CG or TDG_KSP_FGMRES");
+    const int m = opts->restart > 0 ? opts->restart : 30;
+    if (gmres && prec == TDG_FP32) return fail(TDG_E_INVALID, "FGMRES runs with TDG_FP64 or TDG_MIXED");
+    if (gmres && m > kGmMaxRestart) return fail(TDG_E_INVALID, "FGMRES restart length above 64");
     if (op->pc == TDG_PC_MG) {
         if (!op->mg.ready) return fail(TDG_E_STATE, "tdg_mg_setup must be called before a multigrid solve");
         if (prec == TDG_FP32) return fail(TDG_E_INVALID, "the multigrid preconditioner needs TDG_FP64 or TDG_MIXED");
@@ -1739,6 +1861,13 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     size_t need = 5 * vec * sizeof(double) + hchunks.size() * (2 * sizeof(double) + sizeof(Chunk)) +
                   (hseg.size()) * sizeof(int) + static_cast<size_t>(nseg) * kScal * sizeof(double) + 9 * 256;
     if (prec == TDG_FP32) need += 5 * vec * sizeof(float) + 5 * 256;
+    // FGMRES: V (m + 1 vectors), Z (m), w; per segment the dots, H, rotations, g, y, state; chunk
+    // partials of the multi-dots (m + 2 columns)
+    const size_t gm_seg = static_cast<size_t>(nseg) *
+                          ((m + 2) + static_cast<size_t>(m + 1) * m + 2 * m + (m + 1) + m + kGm);
+    if (gmres)
+        need += (2 * static_cast<size_t>(m) + 2) * vec * sizeof(double) + gm_seg * sizeof(double) +
+                hchunks.size() * (m + 2) * sizeof(double) + 12 * 256;
     if (op->ws_bytes < need) {
         op->arena_ws.release();
         op->ws = nullptr;
@@ -1785,7 +1914,25 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     int total_it = 0, updates = 0;
     bool diverged = false;
     auto rel_of = [&](int i) { return bn[i] > 0 ? rn[i] / bn[i] : 0.0; };
-    if (prec == TDG_FP64 || prec == TDG_MIXED) {
+    if (gmres) {
+        GmWork gw;
+        gw.V = reinterpret_cast<double*>(take((m + 1) * vec * sizeof(double)));
+        gw.Z = reinterpret_cast<double*>(take(static_cast<size_t>(m) * vec * sizeof(double)));
+        gw.w = reinterpret_cast<double*>(take(vec * sizeof(double)));
+        gw.dots = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * (m + 2) * sizeof(double)));
+        gw.H = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * (m + 1) * m * sizeof(double)));
+        gw.cs = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * m * sizeof(double)));
+        gw.sn = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * m * sizeof(double)));
+        gw.g = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * (m + 1) * sizeof(double)));
+        gw.y = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * m * sizeof(double)));
+        gw.st = reinterpret_cast<double*>(take(static_cast<size_t>(nseg) * kGm * sizeof(double)));
+        gw.gstride = m + 2;
+        gw.gpart = reinterpret_cast<double*>(take(hchunks.size() * (m + 2) * sizeof(double)));
+        int cycles = 0;
+        TDG_TRY(fgmres(op, prec, sp, b, x, vec, m, gw, r64, t64, partial, scal, rtol, max_it, s, rn, bn, &total_it,
+                       &cycles, &diverged));
+        updates = cycles;
+    } else if (prec == TDG_FP64 || prec == TDG_MIXED) {
         // FP64 recurrence: the recurrence residual is r64 itself and x accumulates directly; the
         // mixed mode applies the operator in FP32 arithmetic and the FP32 inverses, so its
         // recurrence residual drifts from the true one and is replaced more often.  Multigrid

@@ -23,6 +23,7 @@ FAMILIES = ("tensor", "simt", "face")
 MG_STRATEGIES = ("twolevel", "logarithmic", "full")  # MGStrategy (app/common/MGConfig.h:8)
 PRECONDITIONERS = ("bjacobi", "mg")
 MG_COARSE_SPACES = ("dg", "p1")
+KSP_METHODS = ("cg", "fgmres")  # TDG_KSP_CG, TDG_KSP_FGMRES
 
 
 def _c(a: np.ndarray, dtype) -> np.ndarray:
@@ -335,18 +336,21 @@ class DGOperator:
 
     def solve(self, b, x, precision: int = FP64, rtol: float = 1e-10, max_iterations: int = 20000,
               inner_rtol: float = 0.0, max_outer: int = 0, use_graphs: bool = True, nrhs: int = 1,
-              ld: int | None = None, stream=None, check: bool = True) -> dict:
+              ld: int | None = None, stream=None, check: bool = True, method: str = "cg",
+              restart: int = 30) -> dict:
         """Preconditioned CG on the device: FP64; MIXED (FP64 recurrence around the FP32
         tensor-core operator and FP32 block inverses or FP32 fine-level multigrid smoothing); or
         FP32 (operator, preconditioner and recurrence in FP32; block Jacobi only).  The
         preconditioner is block Jacobi or, after set_preconditioner("mg"), the multigrid V-cycle
         (flexible CG).  The solution and the true residual are FP64 in every mode (reliable
-        updates).  inner_rtol: reliable-update threshold (0 = default).  Raises on
-        non-convergence unless check=False (then the stats report it)."""
+        updates).  inner_rtol: reliable-update threshold (0 = default).  method "fgmres": restarted
+        flexible GMRES(restart) (FP64 or MIXED; iterations = Arnoldi steps, outer = cycles).  Raises
+        on non-convergence unless check=False (then the stats report it)."""
         ld = self.ndof if ld is None else ld
         _check_vec(b, FP64, nrhs * ld)
         _check_vec(x, FP64, nrhs * ld)
-        opts = _ffi.SolveOpts(precision, max_iterations, rtol, inner_rtol, max_outer, int(use_graphs))
+        opts = _ffi.SolveOpts(precision, max_iterations, rtol, inner_rtol, max_outer, int(use_graphs),
+                              KSP_METHODS.index(method), restart)
         st = _ffi.SolveStats()
         rc = _ffi.lib().tdg_solve(self._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), nrhs, ld,
                                   C.byref(opts), C.byref(st), _stream(stream))
@@ -359,7 +363,8 @@ class DGOperator:
 
 def solve_segmented(op: DGOperator, b, x, elem_offsets, precision: int = FP64, rtol: float = 1e-10,
                     max_iterations: int = 20000, inner_rtol: float = 0.0, max_outer: int = 0,
-                    use_graphs: bool = True, stream=None, check: bool = True):
+                    use_graphs: bool = True, stream=None, check: bool = True, method: str = "cg",
+                    restart: int = 30):
     """Independent problems held in one block-diagonal operator (a mesh union): one apply and one
     preconditioner launch per iteration cover every problem, each problem has its own CG scalars
     and stopping test.  Returns (aggregate stats, per-problem relative residuals); with
@@ -368,7 +373,8 @@ def solve_segmented(op: DGOperator, b, x, elem_offsets, precision: int = FP64, r
     nseg = len(off) - 1
     _check_vec(b, FP64, op.ndof)
     _check_vec(x, FP64, op.ndof)
-    opts = _ffi.SolveOpts(precision, max_iterations, rtol, inner_rtol, max_outer, int(use_graphs))
+    opts = _ffi.SolveOpts(precision, max_iterations, rtol, inner_rtol, max_outer, int(use_graphs),
+                          KSP_METHODS.index(method), restart)
     st = _ffi.SolveStats()
     rel = np.zeros(nseg)
     rc = _ffi.lib().tdg_solve_segmented(op._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), nseg,
