@@ -35,7 +35,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "DOF/s of matrix-free DG apply; solve time to 1e-10 rel. residual, mixed vs FP64"
-FP64_PROBES = ("dfma", "dmma_m8n8k4", "dmma_m16n8k4", "dmma_m16n8k8", "dmma_m16n8k16")
+FP64_PROBES = ("dfma", "dmma_m8n8k4", "dmma_m16n8k4", "dmma_m16n8k8", "dmma_m16n8k16", "dfma_and_dmma")
 # solve arms: (name, solve precision, preconditioner precision, preconditioner).  Block Jacobi:
 # FP64 CG; mixed = FP64 recurrence around the FP32 tensor-core operator with FP32 (or FP64) block
 # inverses; fp32_recurrence = FP32 vectors and recurrence with FP64 reliable updates.  Multigrid:
@@ -95,6 +95,9 @@ def add_speedups(res: dict, key: str = "seconds") -> None:
 KERNEL_NAMES = {"tensor": "apply_mma_kernel<Shape<3,4,Elasticity>> (FP64 mma.sync m8n8k4, element-centric)",
                 "face": "vol_mma_kernel + face_mma_kernel<Shape<3,4,Elasticity>> (FP64 mma.sync m8n8k4, "
                         "face-centric; roofline over both launches of one apply)",
+                "face2": "vol2_kernel + face2_kernel<Shape<3,4,Elasticity>> (FP64 mma.sync m8n8k4, face-centric, "
+                         "cp.async double-buffered coefficient blocks, tile-ordered geometry; roofline over both "
+                         "launches of one apply)",
                 "simt": "apply_kernel<Shape<3,4,Elasticity>, double> (SIMT)"}
 
 
@@ -412,7 +415,8 @@ def run_ours(args):
     flops_apply = op.flops_apply()
     achieved = bytes_apply / (ms * 1e-3) / 1e9
     tflops = flops_apply / (ms * 1e-3) / 1e12
-    fp64_peak = max(probes.values())
+    # the denominator: the best single FP64 path (the concurrent probe is reported beside it)
+    fp64_peak = max(v for k, v in probes.items() if k != "dfma_and_dmma")
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
@@ -422,7 +426,7 @@ def run_ours(args):
     roofline = {"bound": "fp64", "achieved": tflops, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": tflops / fp64_peak, "traffic": traffic,
                 "peak_source": "measured in this run (tdg_probe_fp64_peak, best FP64 path: "
-                               + max(probes, key=probes.get) + ")",
+                               + max((k for k in probes if k != "dfma_and_dmma"), key=probes.get) + ")",
                 "fp64_probes_tflops": probes,
                 "kernel": KERNEL_NAMES[best64["family"]],
                 "algorithmic_flops_per_launch": flops_apply, "algorithmic_bytes_per_launch": bytes_apply,

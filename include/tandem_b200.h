@@ -155,7 +155,9 @@ int tdg_bjacobi_blocks(tdg_op* op, double* out);
 
 typedef struct {
     int family;       /* 0 = element-centric tensor-core kernel, 1 = SIMT kernel, 2 = face-centric
-                         tensor-core kernels (volume kernel + one pass over the facets) */
+                         tensor-core kernels (volume kernel + one pass over the facets), 3 = the
+                         face-centric pair software-pipelined (FP64: asynchronous copies of the next
+                         tile's coefficient blocks, tile-ordered geometry; FP32 runs family 2) */
     int ctas_per_sm;  /* persistent CTAs per SM requested (0 = default) */
     double ms;        /* measured time of one apply */
 } tdg_tune_entry;
@@ -174,7 +176,8 @@ int tdg_set_apply_config(tdg_op* op, int precision, int family, int ctas_per_sm)
 
 /* Measured FP64 throughput of the current device (no counterpart in tandem; the denominator of the
  * FP64 apply's roofline): kind 0 = FP64 FMA on the CUDA cores, 1..4 = the FP64 tensor pipe through
- * mma.sync of shape m8n8k4, m16n8k4, m16n8k8, m16n8k16; ctas_per_sm CTAs of 256 threads per SM
+ * mma.sync of shape m8n8k4, m16n8k4, m16n8k8, m16n8k16, 5 = half the warps on each of the two
+ * (whether they run concurrently); ctas_per_sm CTAs of 256 threads per SM
  * (0 = 2), every warp with 8 independent accumulators.  Times 3 launches of about 20 ms with CUDA
  * events on `stream` after a warm-up and returns the best rate in *tflops.  Allocates and frees
  * two small device buffers; synchronises `stream`. */

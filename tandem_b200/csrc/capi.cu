@@ -6,6 +6,7 @@
 #include "kernels/apply_tc32.cuh"
 #include "kernels/apply_face.cuh"
 #include "kernels/apply_face_tc32.cuh"
+#include "kernels/apply_face2.cuh"
 #include "kernels/wave.cuh"
 #include "kernels/dispatch.hpp"
 #include "kernels/krylov.cuh"
@@ -187,6 +188,7 @@ struct tdg_op {
     Tc32Tiles tc32;         // FP32 tensor-core apply (3xTF32): packed tables and signature tiles
     FaceTiles face;         // face-centric FP64 apply: facet tiles grouped by (l0, l1, mode)
     FaceTiles face32;       // face-centric FP32 apply: the same grouping with the FP32 tile size
+    TileGeo tgeo;           // software-pipelined face-centric FP64 apply: tile-ordered geometry
     // explicit wave operator: basis at the volume points, reference inverse mass, -rhoInv W / |J|
     DevArena arena_wave;
     WaveData wave;
@@ -270,6 +272,71 @@ void facet_tiles(HostOperator const& h, int TE, std::vector<int4>& finfo, std::v
     }
 }
 
+// Geometry and coefficients of the software-pipelined face-centric apply (apply_face2.cuh) in tile
+// order: per element tile of TE consecutive elements [field][Nq][TE] (J^-1, then the volume
+// coefficients), per facet tile [field][nq][TE] (n, n_unit, then Poisson K G0, K G1 or elasticity
+// G0, G1, lam0, mu0, lam1, mu1) and the penalty [TE]; unused slots zero.  The same values as the
+// reference-layout arrays, read with the tile's elements or facets fastest.
+int upload_tile_geometry(tdg_op* op, DevArena& arena, std::vector<int> const& fids, std::vector<int4> const& ftiles) {
+    auto const& h = op->h;
+    const int D = h.D, DD = D * D, Nq = h.Nq, nq = h.nq;
+    const int TE = mma_tile_elements(D, h.N, h.Q);
+    const bool poisson = h.kind == 0;
+    const int ncoef = poisson ? 1 : 2;
+    const int vf = DD + ncoef;
+    const int64_t vtiles = (h.E + TE - 1) / TE;
+    std::vector<double> vol(static_cast<size_t>(vtiles) * vf * Nq * TE, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < h.E; ++e) {
+        const int64_t t = e / TE;
+        const int te = static_cast<int>(e % TE);
+        double* base = &vol[static_cast<size_t>(t) * vf * Nq * TE];
+        for (int c = 0; c < DD; ++c)
+            for (int q = 0; q < Nq; ++q)
+                base[(static_cast<size_t>(c) * Nq + q) * TE + te] = h.vG[(static_cast<size_t>(e) * DD + c) * Nq + q];
+        for (int c = 0; c < ncoef; ++c)
+            for (int q = 0; q < Nq; ++q)
+                base[(static_cast<size_t>(DD + c) * Nq + q) * TE + te] =
+                    h.vCoef[(static_cast<size_t>(e) * ncoef + c) * Nq + q];
+    }
+    const int ff = 2 * D + 2 * DD + (poisson ? 0 : 4);
+    const size_t nft = ftiles.size();
+    std::vector<double> fct(nft * ff * nq * TE, 0.0), pen(nft * TE, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < static_cast<int64_t>(nft); ++t) {
+        const int4 td = ftiles[t];
+        double* base = &fct[static_cast<size_t>(t) * ff * nq * TE];
+        for (int te = 0; te < td.y; ++te) {
+            const int64_t f = fids[td.x + te];
+            auto put = [&](int field, int q, double v) { base[(static_cast<size_t>(field) * nq + q) * TE + te] = v; };
+            for (int q = 0; q < nq; ++q) {
+                for (int i = 0; i < D; ++i) {
+                    put(i, q, h.fN[(static_cast<size_t>(f) * D + i) * nq + q]);
+                    put(D + i, q, h.fNunit[(static_cast<size_t>(f) * D + i) * nq + q]);
+                }
+                if (poisson) {
+                    for (int side = 0; side < 2; ++side)
+                        for (int c = 0; c < DD; ++c)
+                            put(2 * D + side * DD + c, q, h.fCoef[((static_cast<size_t>(f) * 2 + side) * DD + c) * nq + q]);
+                } else {
+                    for (int c = 0; c < DD; ++c) {
+                        put(2 * D + c, q, h.fG0[(static_cast<size_t>(f) * DD + c) * nq + q]);
+                        put(2 * D + DD + c, q, h.fG1[(static_cast<size_t>(f) * DD + c) * nq + q]);
+                    }
+                    for (int c = 0; c < 4; ++c) put(2 * D + 2 * DD + c, q, h.fCoef[(static_cast<size_t>(f) * 4 + c) * nq + q]);
+                }
+            }
+            pen[static_cast<size_t>(t) * TE + te] = h.penalty[f];
+        }
+    }
+    TDG_CUDA_TRY(arena.upload(&op->tgeo.vol, vol));
+    if (nft) {
+        TDG_CUDA_TRY(arena.upload(&op->tgeo.fct, fct));
+        TDG_CUDA_TRY(arena.upload(&op->tgeo.pen, pen));
+    }
+    return 0;
+}
+
 int upload_mma(tdg_op* op, DevArena& arena) {
     auto const& h = op->h;
     const int D = h.D, NBF = h.Nbf, Nq = h.Nq, nq = h.nq, NF = h.nfaces;
@@ -308,6 +375,7 @@ int upload_mma(tdg_op* op, DevArena& arena) {
     TDG_CUDA_TRY(arena.upload(&op->face.finfo, finfo));
     op->face.nftiles = static_cast<int>(ftiles.size());
     op->face.tables = op->mma.tables + static_cast<size_t>(MV) * LDT;
+    TDG_TRY(upload_tile_geometry(op, arena, fids, ftiles));
     return 0;
 }
 
@@ -1190,7 +1258,10 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
     int rc = TDG_E_INVALID;
     const int pi = precision == TDG_FP64 ? 0 : 1;
     const bool tensor = op->use_mma && op->family[pi] == 0;
-    if (precision == TDG_FP64 && op->use_mma && op->family[0] == 2)
+    if (precision == TDG_FP64 && op->use_mma && op->family[0] == 3)
+        rc = launch_apply_face2(h.D, h.N, h.kind, op->op64, op->mma, op->face, op->tgeo,
+                                static_cast<const double*>(x), static_cast<double*>(y), nrhs, ld, s, op->ctas[0]);
+    if (precision == TDG_FP64 && op->use_mma && (op->family[0] == 2 || (op->family[0] == 3 && rc == TDG_E_INVALID)))
         rc = launch_apply_face(h.D, h.N, h.kind, op->op64, op->mma, op->face, static_cast<const double*>(x),
                                static_cast<double*>(y), nrhs, ld, s, op->ctas[0]);
     else if (precision == TDG_FP64 && tensor)
@@ -1199,7 +1270,7 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
     if (precision == TDG_FP64 && rc == TDG_E_INVALID)
         rc = launch_apply<double>(h.D, h.N, h.kind, op->op64, static_cast<const double*>(x),
                                   static_cast<double*>(y), nrhs, ld, s);
-    const bool face32 = op->use_mma && op->family[1] == 2;
+    const bool face32 = op->use_mma && op->family[1] >= 2;  // face-centric (the FP32 kernels have one form)
     if (precision == TDG_FP32 && face32)
         rc = launch_apply_face_tc32<float>(h.D, h.N, h.kind, op->op32, op->tc32, op->face32,
                                            static_cast<const float*>(x), static_cast<float*>(y), nrhs, ld, s,
@@ -1233,7 +1304,7 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
 }
 
 int tdg_set_apply_config(tdg_op* op, int precision, int family, int ctas_per_sm) {
-    if (!op || (precision != TDG_FP64 && precision != TDG_FP32) || family < 0 || family > 2 || ctas_per_sm < 0)
+    if (!op || (precision != TDG_FP64 && precision != TDG_FP32) || family < 0 || family > 3 || ctas_per_sm < 0)
         return fail(TDG_E_INVALID, "bad argument");
     const int pi = precision == TDG_FP64 ? 0 : 1;
     op->family[pi] = family;
@@ -1268,6 +1339,8 @@ int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_ent
         for (int c = 1; c <= 4; ++c) cands.push_back({0, c});
     if (op->use_mma)
         for (int c = 1; c <= 4; ++c) cands.push_back({2, c});
+    if (op->use_mma && precision == TDG_FP64)
+        for (int c = 1; c <= 2; ++c) cands.push_back({3, c});
     cands.push_back({1, 0});
     const int fam0 = op->family[pi], ct0 = op->ctas[pi];
     cudaEvent_t e0, e1;

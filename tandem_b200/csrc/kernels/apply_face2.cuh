@@ -1,0 +1,665 @@
+// Face-centric FP64 apply, software-pipelined: the operator of apply_face.cuh (volume kernel +
+// one pass over the facets, tandem's apply_volume / flux / apply_facet einsums,
+// app/kernels/elasticity.py:201-234, poisson.py:123-140; the facet loop of Poisson.cpp:586-631 and
+// Elasticity.cpp:734-801 with every facet evaluated once for both sides) with the memory traffic of
+// a tile taken off the critical path:
+//
+//  * the coefficient blocks of the next tile are copied into shared memory with cp.async while the
+//    current tile computes (double buffer), element-major as x holds them -- each element's Q
+//    component runs of Nbf values land at a component stride KS and an element stride LDU chosen
+//    so that the m8n8k4 B-fragment loads of every half warp hit 16 distinct 8-byte banks;
+//  * the per-point geometry and coefficients are read from copies laid out per tile, point-major
+//    with the tile's elements (or facets) fastest, so the pointwise phase's loads are coalesced;
+//  * the facet flux evaluates the averaged stress once for both sides (the side-1 view of tandem's
+//    flux, Elasticity.cpp:734-747, shares it: the side-1 value row is the negated side-0 row and the
+//    gradient rows differ only in the side's J^-1 and Lame parameters).
+//
+// The tables (basis derivatives / values at the points) and the GEMM tiling are those of
+// apply_mma.cuh.  Results agree with the other FP64 kernels to rounding (atomics into y).
+#pragma once
+
+#include "apply_face.cuh"
+
+namespace tdg {
+
+// ---- staged coefficient blocks --------------------------------------------------------------------
+
+// True when the B-fragment addresses (k = t, n = nt * 8 + g; address (n / Q) * ldu + (n % Q) * ks
+// + k) of both half warps are distinct modulo 16 doubles, for every n-tile.
+__host__ __device__ constexpr bool staged_conflict_free(int Q, int ks, int ldu, int ntn) {
+    for (int nt = 0; nt < ntn; ++nt)
+        for (int half = 0; half < 2; ++half) {
+            bool used[16] = {};
+            for (int g = 4 * half; g < 4 * half + 4; ++g)
+                for (int t = 0; t < 4; ++t) {
+                    const int n = nt * 8 + g;
+                    const int a = ((n / Q) * ldu + (n % Q) * ks + t) % 16;
+                    if (used[a]) return false;
+                    used[a] = true;
+                }
+        }
+    return true;
+}
+
+// Element stride of the staged blocks: the smallest >= Q * ks (at most 16 more) that is conflict
+// free, else Q * ks + 4.
+__host__ __device__ constexpr int staged_ldu(int Q, int ks, int ntn) {
+    for (int l = Q * ks; l < Q * ks + 16; ++l)
+        if (staged_conflict_free(Q, ks, l, ntn)) return l;
+    return Q * ks + 4;
+}
+
+// Component stride: the padded Nbf, or 4, 8 or 12 more where no element stride is conflict free
+// with it (2D p4 elasticity: a stride of 16 puts both components' k on the same banks).
+__host__ __device__ constexpr int staged_ks(int Q, int kp, int ntn) {
+    for (int ks = kp; ks < kp + 16; ks += 4)
+        if (staged_conflict_free(Q, ks, staged_ldu(Q, ks, ntn), ntn)) return ks;
+    return kp;
+}
+
+template <class S>
+struct Staged {
+    using L = MmaTile<S>;
+    static constexpr int KS = staged_ks(S::Q, L::KP, L::NTN);       // component stride
+    static constexpr int LDU = staged_ldu(S::Q, KS, L::NTN);       // element stride
+    static constexpr int UE = (L::NP + S::Q - 1) / S::Q;           // elements per staged tile
+    static constexpr int USZ = UE * LDU;                           // doubles per staged tile
+};
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// C[M x NP] = A[M x K] U for rows [0, mrows), U staged element-major (Staged<S>): as
+// cta_gemm_store with the B fragments read from the staged layout.  Two GEMMs of the same shape
+// at once when A1 != nullptr (C1 = A1 U1).
+template <class S>
+__device__ __forceinline__ void cta_gemm_store_staged(const double* A0, const double* U0, double* C0,
+                                                      const double* A1, const double* U1, double* C1, int mrows,
+                                                      int ksteps, int warp, int lane) {
+    using L = MmaTile<S>;
+    using SU = Staged<S>;
+    constexpr int Q = S::Q;
+    const int g = lane >> 2, t = lane & 3;
+    const int per = (mrows / 8) * L::NTN;
+    const int ntiles = A1 ? 2 * per : per;
+    for (int t0 = warp; t0 < ntiles; t0 += 4 * L::GW) {
+        double acc[4][2];
+        const double* ap[4];
+        const double* bp[4];
+        int cnt = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            acc[j][0] = acc[j][1] = 0.0;
+            const int tile = t0 + j * L::GW;
+            const int tt = tile < ntiles ? tile : t0;
+            const int which = tt / per, loc = tt % per;
+            const int mt = loc / L::NTN, nt = loc % L::NTN;
+            const int n = nt * 8 + g;
+            ap[j] = (which ? A1 : A0) + (mt * 8 + g) * L::LDT + t;
+            bp[j] = (which ? U1 : U0) + (n / Q) * SU::LDU + (n % Q) * SU::KS + t;
+            cnt += tile < ntiles;
+        }
+        for (int ks = 0; ks < ksteps; ++ks) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (j < cnt) dmma(acc[j], ap[j][ks * 4], bp[j][ks * 4]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (j < cnt) {
+                const int tile = t0 + j * L::GW;
+                const int which = tile / per, loc = tile % per;
+                const int mt = loc / L::NTN, nt = loc % L::NTN;
+                double* c = (which ? C1 : C0) + (mt * 8 + g) * L::LDN + nt * 8 + 2 * t;
+                c[0] = acc[j][0];
+                c[1] = acc[j][1];
+            }
+        }
+    }
+}
+
+// Issues the cp.async copies of the coefficient blocks of up to UE elements (el[te] < 0: skipped)
+// from xr into the staged buffer U.
+template <class S, int NT>
+__device__ __forceinline__ void stage_blocks(const double* __restrict__ xr, const int* el, double* U, int tid) {
+    using SU = Staged<S>;
+    constexpr int per_el = S::Q * S::NBF;
+    for (int i = tid; i < SU::UE * per_el; i += NT) {
+        const int te = i / per_el, w = i % per_el;
+        const int r = w / S::NBF, k = w % S::NBF;
+        const int e = el[te];
+        if (e >= 0) cp_async8(U + te * SU::LDU + r * SU::KS + k, xr + static_cast<int64_t>(e) * S::BS + w);
+    }
+}
+
+// ---- tile-ordered geometry ------------------------------------------------------------------------
+
+// Volume data per element tile, [tile][field][q][te] with fields J^-1 (DD) then the coefficients
+// (Poisson |J| W K; elasticity lam W |J|, mu W |J|): the tile's elements are fastest.
+// Facet data per facet tile, [tile][field][q][te] with fields n (D), n_unit (D), then Poisson
+// K G0, K G1 (DD each) or elasticity G0, G1 (DD each), lam0, mu0, lam1, mu1; penalty [tile][te].
+struct TileGeo {
+    const double* vol = nullptr;
+    const double* fct = nullptr;
+    const double* pen = nullptr;
+};
+
+template <class S>
+__host__ __device__ constexpr int vol_fields() {
+    return S::DD + (S::KIND == kPoisson ? 1 : 2);
+}
+template <class S>
+__host__ __device__ constexpr int fct_fields() {
+    return 2 * S::D + 2 * S::DD + (S::KIND == kPoisson ? 0 : 4);
+}
+
+// Lift inputs of both sides of an interior facet point (mode 1; mode 3 passes the element's own
+// data as side 1): the same values facet_lift gives for side 0 (n, u0 own) and side 1 (-n, u1 own),
+// with the averaged stress / flux computed once.
+template <class S>
+__device__ __forceinline__ void facet_lift_pair(const double* n, const double* nu, double pen, double wq,
+                                                const double (&u0)[S::Q], const double (&g0)[S::D][S::Q],
+                                                const double (&u1)[S::Q], const double (&g1)[S::D][S::Q],
+                                                const double* G0, const double* G1, const double* c0,
+                                                const double* c1, double (&ga0)[S::D][S::Q], double (&gb0)[S::Q],
+                                                double (&ga1)[S::D][S::Q], double (&gb1)[S::Q]) {
+    constexpr int D = S::D;
+    if constexpr (S::KIND == kPoisson) {
+        const double uh = 0.5 * (u1[0] - u0[0]);
+        const double pj = pen * (u0[0] - u1[0]);
+        double bsum = 0.0;
+#pragma unroll
+        for (int p = 0; p < D; ++p) {
+            double s = 0.0;
+#pragma unroll
+            for (int a = 0; a < D; ++a) s += c0[a * D + p] * g0[a][0] + c1[a * D + p] * g1[a][0];
+            bsum += n[p] * (0.5 * s - pj * nu[p]);
+        }
+        gb0[0] = -wq * bsum;
+        gb1[0] = wq * bsum;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                s0 += n[r] * c0[a * D + r];
+                s1 += n[r] * c1[a * D + r];
+            }
+            ga0[a][0] = wq * uh * s0;
+            ga1[a][0] = wq * uh * s1;
+        }
+    } else {
+        const double lam0 = c0[0], mu0 = c0[1], lam1 = c1[0], mu1 = c1[1];
+        double sg[D][D];
+        {
+            double J[D][D];
+#pragma unroll
+            for (int s = 0; s < D; ++s)
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int a = 0; a < D; ++a) acc += G0[a * D + s] * g0[a][r];
+                    J[s][r] = acc;
+                }
+            double d = 0.0;
+#pragma unroll
+            for (int r = 0; r < D; ++r) d += J[r][r];
+#pragma unroll
+            for (int i = 0; i < D; ++i)
+#pragma unroll
+                for (int j = 0; j < D; ++j) sg[i][j] = mu0 * (J[i][j] + J[j][i]) + ((i == j) ? lam0 * d : 0.0);
+        }
+        {
+            double J[D][D];
+#pragma unroll
+            for (int s = 0; s < D; ++s)
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int a = 0; a < D; ++a) acc += G1[a * D + s] * g1[a][r];
+                    J[s][r] = acc;
+                }
+            double d = 0.0;
+#pragma unroll
+            for (int r = 0; r < D; ++r) d += J[r][r];
+#pragma unroll
+            for (int i = 0; i < D; ++i) {
+                const double pj = pen * (u0[i] - u1[i]);
+#pragma unroll
+                for (int j = 0; j < D; ++j) {
+                    const double s1 = mu1 * (J[i][j] + J[j][i]) + ((i == j) ? lam1 * d : 0.0);
+                    sg[i][j] = 0.5 * (sg[i][j] + s1) - pj * nu[j];
+                }
+            }
+        }
+        double uhm[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) uhm[i] = 0.5 * (u1[i] - u0[i]);
+        double un = 0.0;
+#pragma unroll
+        for (int r = 0; r < D; ++r) un += uhm[r] * n[r];
+#pragma unroll
+        for (int uu = 0; uu < D; ++uu) {
+            double X0[D], X1[D];
+#pragma unroll
+            for (int j = 0; j < D; ++j) {
+                const double sym = uhm[uu] * n[j] + uhm[j] * n[uu];
+                X0[j] = mu0 * sym + ((uu == j) ? lam0 * un : 0.0);
+                X1[j] = mu1 * sym + ((uu == j) ? lam1 * un : 0.0);
+            }
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                for (int j = 0; j < D; ++j) {
+                    s0 += G0[a * D + j] * X0[j];
+                    s1 += G1[a * D + j] * X1[j];
+                }
+                ga0[a][uu] = wq * s0;
+                ga1[a][uu] = wq * s1;
+            }
+            double bsum = 0.0;
+#pragma unroll
+            for (int j = 0; j < D; ++j) bsum += n[j] * sg[uu][j];
+            gb0[uu] = -wq * bsum;
+            gb1[uu] = wq * bsum;
+        }
+    }
+}
+
+// ---- volume kernel ----------------------------------------------------------------------------------
+
+template <class S>
+struct Vol2Layout {
+    int MV, off_U, off_R, total;
+};
+template <class S>
+__host__ __device__ inline Vol2Layout<S> vol2_layout(int Nq) {
+    using L = MmaTile<S>;
+    Vol2Layout<S> l;
+    l.MV = round8(S::D * Nq);
+    l.off_U = l.MV * L::LDT;
+    l.off_R = l.off_U + 2 * Staged<S>::USZ;
+    l.total = l.off_R + L::QC * S::D * L::LDN;
+    return l;
+}
+
+template <class S>
+__global__ void __launch_bounds__(MmaTile<S>::NT, 2)
+    vol2_kernel(DevOp<double> op, TileGeo tg, const double* __restrict__ tv, const double* __restrict__ x,
+                double* __restrict__ y, int64_t ld, int nrhs) {
+    using L = MmaTile<S>;
+    using SU = Staged<S>;
+    constexpr int D = S::D, NBF = S::NBF, Q = S::Q, BS = S::BS, DD = S::DD;
+    constexpr int TE = L::TE, NT = L::NT, LDN = L::LDN, LDT = L::LDT;
+    constexpr int NFLD = vol_fields<S>();
+    const int Nq = op.Nq;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const Vol2Layout<S> lay = vol2_layout<S>(Nq);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sm = reinterpret_cast<double*>(smem_raw);
+    double* TV = sm;
+    double* Ub = sm + lay.off_U;
+    double* R0 = sm + lay.off_R;
+    __shared__ int s_el[2][SU::UE];
+    for (int i = tid; i < lay.MV * LDT; i += NT) sm[i] = tv[i];
+    for (int i = tid; i < 2 * SU::USZ; i += NT) Ub[i] = 0.0;  // padding stays zero, stale columns finite
+
+    const int64_t ntiles = (op.E + TE - 1) / TE;
+    const int64_t nwork = ntiles * nrhs;
+    auto stage = [&](int64_t work, int buf) {
+        const int64_t tile = work % ntiles;
+        const double* xr = x + (work / ntiles) * ld;
+        if (tid < SU::UE) {
+            const int64_t e = tile * TE + tid;
+            s_el[buf][tid] = (tid < TE && e < op.E) ? static_cast<int>(e) : -1;
+        }
+        __syncthreads();
+        stage_blocks<S, NT>(xr, s_el[buf], Ub + buf * SU::USZ, tid);
+        cp_async_commit();
+    };
+    __syncthreads();
+    int buf = 0;
+    if (static_cast<int64_t>(blockIdx.x) < nwork) stage(blockIdx.x, 0);
+    for (int64_t work = blockIdx.x; work < nwork; work += gridDim.x, buf ^= 1) {
+        const int64_t tile = work % ntiles;
+        double* yr = y + (work / ntiles) * ld;
+        const int64_t next = work + gridDim.x;
+        __syncthreads();  // the previous tile is done with the other buffer
+        if (next < nwork) {
+            stage(next, buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double* U = Ub + buf * SU::USZ;
+        const int* el = s_el[buf];
+        const double* geo = tg.vol + tile * static_cast<int64_t>(NFLD) * Nq * TE;
+        double yacc[L::YPW][2][2];
+#pragma unroll
+        for (int j = 0; j < L::YPW; ++j) yacc[j][0][0] = yacc[j][0][1] = yacc[j][1][0] = yacc[j][1][1] = 0.0;
+        for (int q0 = 0; q0 < Nq; q0 += L::QC) {
+            const int nqc = (Nq - q0 < L::QC) ? (Nq - q0) : L::QC;
+            const int rows = round8(nqc * D);
+            cta_gemm_store_staged<S>(TV + q0 * D * LDT, U, R0, nullptr, nullptr, nullptr, rows, L::KP / 4, warp, lane);
+            __syncthreads();
+            for (int it = tid; it < TE * nqc; it += NT) {
+                const int te = it % TE, qq = it / TE;
+                if (el[te] < 0) continue;
+                const double* gp = geo + static_cast<int64_t>(q0 + qq) * TE + te;  // field f at gp[f * Nq * TE]
+                double G[DD];
+#pragma unroll
+                for (int c = 0; c < DD; ++c) G[c] = gp[static_cast<int64_t>(c) * Nq * TE];
+                double* rr = R0 + (qq * D) * LDN + te * Q;
+                if constexpr (S::KIND == kPoisson) {
+                    const double jwk = gp[static_cast<int64_t>(DD) * Nq * TE];
+                    double gx[D];
+#pragma unroll
+                    for (int i = 0; i < D; ++i) {
+                        double s = 0.0;
+#pragma unroll
+                        for (int a = 0; a < D; ++a) s += G[a * D + i] * rr[a * LDN];
+                        gx[i] = jwk * s;
+                    }
+#pragma unroll
+                    for (int a = 0; a < D; ++a) {
+                        double s = 0.0;
+#pragma unroll
+                        for (int i = 0; i < D; ++i) s += G[a * D + i] * gx[i];
+                        rr[a * LDN] = s;
+                    }
+                } else {
+                    const double lam = gp[static_cast<int64_t>(DD) * Nq * TE];
+                    const double mu = gp[static_cast<int64_t>(DD + 1) * Nq * TE];
+                    double Ju[D][D];
+#pragma unroll
+                    for (int s = 0; s < D; ++s)
+#pragma unroll
+                        for (int r = 0; r < D; ++r) {
+                            double acc = 0.0;
+#pragma unroll
+                            for (int a = 0; a < D; ++a) acc += G[a * D + s] * rr[a * LDN + r];
+                            Ju[s][r] = acc;
+                        }
+                    double div = 0.0;
+#pragma unroll
+                    for (int r = 0; r < D; ++r) div += Ju[r][r];
+                    double T[D][D];
+#pragma unroll
+                    for (int uu = 0; uu < D; ++uu) {
+                        double sg[D];
+#pragma unroll
+                        for (int j = 0; j < D; ++j) sg[j] = mu * (Ju[uu][j] + Ju[j][uu]) + ((uu == j) ? lam * div : 0.0);
+#pragma unroll
+                        for (int a = 0; a < D; ++a) {
+                            double s = 0.0;
+#pragma unroll
+                            for (int j = 0; j < D; ++j) s += G[a * D + j] * sg[j];
+                            T[a][uu] = s;
+                        }
+                    }
+#pragma unroll
+                    for (int a = 0; a < D; ++a)
+#pragma unroll
+                        for (int uu = 0; uu < D; ++uu) rr[a * LDN + uu] = T[a][uu];
+                }
+            }
+            __syncthreads();
+            cta_gemm_acc_t<L>(TV + q0 * D * LDT, R0, yacc, rows, warp, lane);
+            __syncthreads();
+        }
+        const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+        for (int j = 0; j < L::YPW; ++j) {
+            const int tl = warp + j * L::GW;
+            if (tl < L::YT) {
+                const int ym = tl % L::MYT, yn = tl / L::MYT;
+                const int k = ym * 8 + g;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = yn * 8 + 2 * t + h;
+                    if (k < NBF && c < L::NC) {
+                        const int te = c / Q, r = c % Q;
+                        const int e = el[te];
+                        if (e >= 0) yr[static_cast<int64_t>(e) * BS + k + NBF * r] = yacc[j][0][h] + yacc[j][1][h];
+                    }
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
+// ---- facet kernel -----------------------------------------------------------------------------------
+
+template <class S>
+struct Face2Layout {
+    int MF, off_TB, off_U, off_R0, off_R1, total;
+};
+template <class S>
+__host__ __device__ inline Face2Layout<S> face2_layout(int nq) {
+    using L = MmaTile<S>;
+    Face2Layout<S> l;
+    l.MF = round8((S::D + 1) * nq);
+    l.off_TB = l.MF * L::LDT;
+    l.off_U = l.off_TB + l.MF * L::LDT;
+    l.off_R0 = l.off_U + 4 * Staged<S>::USZ;  // [buffer][side]
+    l.off_R1 = l.off_R0 + l.MF * L::LDN;
+    l.total = l.off_R1 + l.MF * L::LDN;
+    return l;
+}
+
+template <class S, int MINB>
+__global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
+    face2_kernel(DevOp<double> op, FaceTiles ft, TileGeo tg, const double* __restrict__ x, double* __restrict__ y,
+                 int64_t ld, int nrhs) {
+    using L = MmaTile<S>;
+    using SU = Staged<S>;
+    constexpr int D = S::D, NBF = S::NBF, Q = S::Q, BS = S::BS, DD = S::DD;
+    constexpr int TE = L::TE, NT = L::NT, LDN = L::LDN;
+    constexpr int NFLD = fct_fields<S>();
+    const int nq = op.nq;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const Face2Layout<S> lay = face2_layout<S>(nq);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sm = reinterpret_cast<double*>(smem_raw);
+    double* TA = sm;
+    double* TB = sm + lay.off_TB;
+    double* Ub = sm + lay.off_U;
+    double* R0 = sm + lay.off_R0;
+    double* R1 = sm + lay.off_R1;
+    __shared__ int s_f[2][SU::UE], s_e0[2][SU::UE], s_e1[2][SU::UE];
+    const int tab = lay.MF * L::LDT;
+    for (int i = tid; i < 4 * SU::USZ; i += NT) Ub[i] = 0.0;
+
+    // contiguous work ranges per CTA keep the table pair mostly unchanged
+    const int64_t nwork = static_cast<int64_t>(ft.nftiles) * nrhs;
+    const int64_t per = (nwork + gridDim.x - 1) / gridDim.x;
+    const int64_t w0 = static_cast<int64_t>(blockIdx.x) * per;
+    const int64_t w1 = (w0 + per < nwork) ? w0 + per : nwork;
+    auto stage = [&](int64_t work, int buf) {
+        const int tile = static_cast<int>(work % ft.nftiles);
+        const double* xr = x + (work / ft.nftiles) * ld;
+        const int4 td = ft.ftiles[tile];
+        const bool two = (td.z >> 4) == 1;
+        if (tid < SU::UE) {
+            int f = -1, e0 = -1, e1 = -1;
+            if (tid < TE && tid < td.y) {
+                f = ft.fperm[td.x + tid];
+                const int4 fi = ft.finfo[f];
+                e0 = fi.x;
+                e1 = two ? fi.y : -1;
+            }
+            s_f[buf][tid] = f;
+            s_e0[buf][tid] = e0;
+            s_e1[buf][tid] = e1;
+        }
+        __syncthreads();
+        stage_blocks<S, NT>(xr, s_e0[buf], Ub + (2 * buf) * SU::USZ, tid);
+        if (two) stage_blocks<S, NT>(xr, s_e1[buf], Ub + (2 * buf + 1) * SU::USZ, tid);
+        cp_async_commit();
+    };
+    int cur_a = -1, cur_b = -1;  // face tables held in TA / TB
+    __syncthreads();
+    if (w0 < w1) stage(w0, 0);
+    int buf = 0;
+    for (int64_t work = w0; work < w1; ++work, buf ^= 1) {
+        const int tile = static_cast<int>(work % ft.nftiles);
+        double* yr = y + (work / ft.nftiles) * ld;
+        const int4 td = ft.ftiles[tile];
+        const int key = td.z;
+        const int l0 = key & 3, l1 = (key >> 2) & 3, mode = key >> 4;
+        const bool two = (mode == 1);
+        __syncthreads();  // the previous tile is done with R, the tables and the other buffer
+        if (work + 1 < w1) stage(work + 1, buf ^ 1);
+        if (l0 != cur_a) {
+            for (int i = tid; i < tab; i += NT) TA[i] = ft.tables[static_cast<int64_t>(l0) * tab + i];
+            cur_a = l0;
+        }
+        if (two && l1 != cur_b) {
+            for (int i = tid; i < tab; i += NT) TB[i] = ft.tables[static_cast<int64_t>(l1) * tab + i];
+            cur_b = l1;
+        }
+        if (work + 1 < w1)
+            cp_async_wait<1>();
+        else
+            cp_async_wait<0>();
+        __syncthreads();
+        const double* U0 = Ub + (2 * buf) * SU::USZ;
+        const double* U1 = Ub + (2 * buf + 1) * SU::USZ;
+        const int* sf = s_f[buf];
+        const int* se0 = s_e0[buf];
+        const int* se1 = s_e1[buf];
+        if (two)
+            cta_gemm_store_staged<S>(TA, U0, R0, TB, U1, R1, lay.MF, L::KP / 4, warp, lane);
+        else
+            cta_gemm_store_staged<S>(TA, U0, R0, nullptr, nullptr, nullptr, lay.MF, L::KP / 4, warp, lane);
+        __syncthreads();
+        const double* geo = tg.fct + static_cast<int64_t>(tile) * NFLD * nq * TE;
+        const double* pens = tg.pen + static_cast<int64_t>(tile) * TE;
+        for (int it = tid; it < TE * nq; it += NT) {
+            const int te = it % TE, q = it / TE;
+            if (sf[te] < 0) continue;
+            const double* gp = geo + it;  // field f at gp[f * nq * TE]
+            const int64_t fs = static_cast<int64_t>(nq) * TE;
+            double* ga0p = R0 + (q * D) * LDN + te * Q;
+            double* gb0p = R0 + (D * nq + q) * LDN + te * Q;
+            double* ga1p = R1 + (q * D) * LDN + te * Q;
+            double* gb1p = R1 + (D * nq + q) * LDN + te * Q;
+            double u0[Q], u1[Q], g0[D][Q], g1[D][Q];
+#pragma unroll
+            for (int r = 0; r < Q; ++r) {
+                u0[r] = gb0p[r];
+#pragma unroll
+                for (int a = 0; a < D; ++a) g0[a][r] = ga0p[a * LDN + r];
+                if (two) {
+                    u1[r] = gb1p[r];
+#pragma unroll
+                    for (int a = 0; a < D; ++a) g1[a][r] = ga1p[a * LDN + r];
+                } else if (mode == 3) {  // own neighbour: the other side is the element itself
+                    u1[r] = u0[r];
+#pragma unroll
+                    for (int a = 0; a < D; ++a) g1[a][r] = g0[a][r];
+                } else {
+                    u1[r] = 0.0;
+#pragma unroll
+                    for (int a = 0; a < D; ++a) g1[a][r] = 0.0;
+                }
+            }
+            double n[D], nu[D];
+#pragma unroll
+            for (int i = 0; i < D; ++i) {
+                n[i] = gp[i * fs];
+                nu[i] = gp[(D + i) * fs];
+            }
+            double Gs0[DD], Gs1[DD], cs0[DD], cs1[DD];
+            if constexpr (S::KIND == kPoisson) {
+#pragma unroll
+                for (int c = 0; c < DD; ++c) {
+                    cs0[c] = gp[(2 * D + c) * fs];
+                    cs1[c] = gp[(2 * D + DD + c) * fs];
+                    Gs0[c] = Gs1[c] = 0.0;
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < DD; ++c) {
+                    Gs0[c] = gp[(2 * D + c) * fs];
+                    Gs1[c] = gp[(2 * D + DD + c) * fs];
+                }
+                cs0[0] = gp[(2 * D + 2 * DD + 0) * fs];
+                cs0[1] = gp[(2 * D + 2 * DD + 1) * fs];
+                cs1[0] = gp[(2 * D + 2 * DD + 2) * fs];
+                cs1[1] = gp[(2 * D + 2 * DD + 3) * fs];
+            }
+            const double pen = pens[te];
+            const double wq = op.w[q];
+            double ga[D][Q], gb[Q];
+            if (mode == 2) {
+                facet_lift<S, double>(2, n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs1, cs0, cs1, ga, gb);
+            } else {
+                double ha[D][Q], hb[Q];
+                if (mode == 3)
+                    facet_lift_pair<S>(n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs0, cs0, cs0, ga, gb, ha, hb);
+                else
+                    facet_lift_pair<S>(n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs1, cs0, cs1, ga, gb, ha, hb);
+                if (two) {
+#pragma unroll
+                    for (int r = 0; r < Q; ++r) {
+                        gb1p[r] = hb[r];
+#pragma unroll
+                        for (int a = 0; a < D; ++a) ga1p[a * LDN + r] = ha[a][r];
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < Q; ++r) {
+                gb0p[r] = gb[r];
+#pragma unroll
+                for (int a = 0; a < D; ++a) ga0p[a * LDN + r] = ga[a][r];
+            }
+        }
+        __syncthreads();
+        double y0[L::YPW][2][2], y1[L::YPW][2][2];
+#pragma unroll
+        for (int j = 0; j < L::YPW; ++j)
+#pragma unroll
+            for (int a = 0; a < 2; ++a) y0[j][a][0] = y0[j][a][1] = y1[j][a][0] = y1[j][a][1] = 0.0;
+        cta_gemm_acc_t<L>(TA, R0, y0, lay.MF, warp, lane);
+        if (two) cta_gemm_acc_t<L>(TB, R1, y1, lay.MF, warp, lane);
+        const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+        for (int j = 0; j < L::YPW; ++j) {
+            const int tl = warp + j * L::GW;
+            if (tl < L::YT) {
+                const int ym = tl % L::MYT, yn = tl / L::MYT;
+                const int k = ym * 8 + g;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = yn * 8 + 2 * t + h;
+                    if (k < NBF && c < L::NC) {
+                        const int te = c / Q, r = c % Q;
+                        if (sf[te] >= 0) {
+                            atomicAdd(&yr[static_cast<int64_t>(se0[te]) * BS + k + NBF * r], y0[j][0][h] + y0[j][1][h]);
+                            if (two)
+                                atomicAdd(&yr[static_cast<int64_t>(se1[te]) * BS + k + NBF * r],
+                                          y1[j][0][h] + y1[j][1][h]);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
+}  // namespace tdg

@@ -30,6 +30,13 @@ struct FaceTiles;
 int launch_apply_face(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft,
                       const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas = 0);
 
+// Software-pipelined face-centric FP64 apply (apply_face2.cuh): cp.async double-buffered
+// coefficient blocks, tile-ordered geometry (TileGeo), both sides' fluxes from one stress.
+struct TileGeo;
+int launch_apply_face2(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft,
+                       TileGeo const& tg, const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s,
+                       int ctas = 0);
+
 // Face-centric FP32 apply (apply_face_tc32.cuh), TX = float or double vectors.
 struct Tc32Tiles;
 template <typename TX>

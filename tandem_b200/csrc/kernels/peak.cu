@@ -110,6 +110,43 @@ __global__ void __launch_bounds__(kThreads) k_peak_dmma(const double* __restrict
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// Half the warps on the FMA pipe, half on the tensor pipe (m8n8k4): whether the two FP64 paths
+// run concurrently.
+__global__ void __launch_bounds__(kThreads) k_peak_both(const double* __restrict__ seed, double* __restrict__ out,
+                                                        int iters) {
+    const int warp = threadIdx.x >> 5;
+    double s = 0.0;
+    if (warp & 1) {
+        using M = MmaF64<1>;
+        double a[1] = {seed[0] * (1.0 + 1e-3 * (threadIdx.x & 7))}, b[1] = {seed[1]}, c[kChains][2] = {};
+        for (int it = 0; it < iters; ++it) {
+#pragma unroll
+            for (int r = 0; r < kUnroll; ++r)
+#pragma unroll
+                for (int j = 0; j < kChains; ++j) M::run(c[j], a, b);
+        }
+#pragma unroll
+        for (int j = 0; j < kChains; ++j) s += c[j][0] + c[j][1];
+    } else {
+        const double a = seed[0], b = seed[1];
+        double c[kChains];
+#pragma unroll
+        for (int j = 0; j < kChains; ++j) c[j] = seed[2] * (threadIdx.x + j);
+        // 4 x the trips: per trip a tensor warp does 32 m8n8k4 (8,192 FMA), an FMA warp 4 x 32 x
+        // 32 = 4,096 FMA, so with separate pipes the FMA half ends first and the rate reads ~1.5 x
+        // the tensor pipe's; with one shared pipe it stays at the single-pipe rate
+        for (int it = 0; it < iters * 4; ++it) {
+#pragma unroll
+            for (int r = 0; r < kUnroll; ++r)
+#pragma unroll
+                for (int j = 0; j < kChains; ++j) c[j] = fma(c[j], a, b);
+        }
+#pragma unroll
+        for (int j = 0; j < kChains; ++j) s += c[j];
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 template <int SHAPE>
 constexpr double dmma_flops_per_warp_iter() {
     return static_cast<double>(MmaF64<SHAPE>::kFlops) * kUnroll * kChains;
@@ -122,7 +159,7 @@ constexpr double dmma_flops_per_warp_iter() {
 using namespace tdg;
 
 extern "C" int tdg_probe_fp64_peak(int kind, int ctas_per_sm, void* stream, double* tflops) {
-    if (!tflops || kind < 0 || kind > 4 || ctas_per_sm < 0 || ctas_per_sm > 8) return TDG_E_INVALID;
+    if (!tflops || kind < 0 || kind > 5 || ctas_per_sm < 0 || ctas_per_sm > 8) return TDG_E_INVALID;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -144,7 +181,11 @@ extern "C" int tdg_probe_fp64_peak(int kind, int ctas_per_sm, void* stream, doub
         case 1: per_iter = warps * dmma_flops_per_warp_iter<1>(); break;
         case 2: per_iter = warps * dmma_flops_per_warp_iter<2>(); break;
         case 3: per_iter = warps * dmma_flops_per_warp_iter<3>(); break;
-        default: per_iter = warps * dmma_flops_per_warp_iter<4>(); break;
+        case 4: per_iter = warps * dmma_flops_per_warp_iter<4>(); break;
+        default:  // half the warps: m8n8k4 per trip; the other half: 4 x the FMA loop per trip
+            per_iter = 0.5 * warps * dmma_flops_per_warp_iter<1>() +
+                       0.5 * static_cast<double>(grid) * kThreads * kUnroll * kChains * 2.0 * 4.0;
+            break;
     }
     // about 20 ms per launch at 40 TFLOP/s
     const int iters = std::max(16, static_cast<int>(8e11 / per_iter));
@@ -154,7 +195,8 @@ extern "C" int tdg_probe_fp64_peak(int kind, int ctas_per_sm, void* stream, doub
             case 1: k_peak_dmma<1><<<grid, kThreads, 0, s>>>(seed, out, iters); break;
             case 2: k_peak_dmma<2><<<grid, kThreads, 0, s>>>(seed, out, iters); break;
             case 3: k_peak_dmma<3><<<grid, kThreads, 0, s>>>(seed, out, iters); break;
-            default: k_peak_dmma<4><<<grid, kThreads, 0, s>>>(seed, out, iters); break;
+            case 4: k_peak_dmma<4><<<grid, kThreads, 0, s>>>(seed, out, iters); break;
+            default: k_peak_both<<<grid, kThreads, 0, s>>>(seed, out, iters); break;
         }
     };
     cudaEvent_t e0, e1;

@@ -275,12 +275,13 @@ def test_mixed_solve_reaches_fp64_target(kind, dim, n, curved):
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: "k{}d{}n{}p{}c{}v{}".format(*c))
 @pytest.mark.parametrize("ctas", [1, 2])
-def test_apply_face_centric_matches_oracle(case, ctas):
-    """Face-centric FP64 apply (volume kernel + one pass over the facets with atomics) against
-    the oracle, 1e-12 like the element-centric kernel."""
+@pytest.mark.parametrize("family", ["face", "face2"])
+def test_apply_face_centric_matches_oracle(case, ctas, family):
+    """Face-centric FP64 apply (volume kernel + one pass over the facets with atomics; face2: the
+    software-pipelined pair) against the oracle, 1e-12 like the element-centric kernel."""
     kind, dim, n, N, curved, var = case
     _, op, orc = product_and_oracle(kind, dim, n, N, curved, var)
-    op.set_apply_config(FP64, "face", ctas)
+    op.set_apply_config(FP64, family, ctas)
     x = np.random.default_rng(7).standard_normal(op.ndof)
     y = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
     op.apply(dev(x), y)
@@ -288,9 +289,10 @@ def test_apply_face_centric_matches_oracle(case, ctas):
     assert rel(y.cpu().numpy(), orc.apply(x)) < 1e-12
 
 
-def test_face_centric_multi_rhs_and_solve():
+@pytest.mark.parametrize("family", ["face", "face2"])
+def test_face_centric_multi_rhs_and_solve(family):
     _, op, orc = product_and_oracle(ELASTICITY, 3, 2, 4, True, True)
-    op.set_apply_config(FP64, "face")
+    op.set_apply_config(FP64, family)
     nrhs, ld = 3, op.ndof + 37
     X = torch.randn(nrhs, ld, dtype=torch.float64, device=DEV)
     Y = torch.full((nrhs, ld), 7.0, dtype=torch.float64, device=DEV)

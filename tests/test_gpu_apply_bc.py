@@ -3,8 +3,8 @@ on (Poisson.cpp:591-631, Elasticity.cpp:752-801): boundary Dirichlet, Natural (n
 None (the element as its own neighbour), interior Fault (skeleton flux) and interior Natural (a
 crack: no flux), see cases.mixed_bc_codes.
 
-Every kernel family is pinned separately (set_apply_config): the face-centric tensor-core pair,
-the element-centric tensor-core kernel and the SIMT kernel.  Tolerances: FP64 1e-12 relative
+Every kernel family is pinned separately (set_apply_config): the face-centric tensor-core pair
+(and its software-pipelined form, FP64), the element-centric tensor-core kernel and the SIMT kernel.  Tolerances: FP64 1e-12 relative
 (max-norm over the vector; summation order differs), FP32 and mixed (FP32 arithmetic on FP64
 vectors) 2e-5 relative in the 2-norm."""
 import numpy as np
@@ -47,7 +47,7 @@ def case(request):
     return op, orc, x, orc.apply(x)
 
 
-@pytest.mark.parametrize("family", ["face", "tensor", "simt"])
+@pytest.mark.parametrize("family", ["face", "face2", "tensor", "simt"])
 def test_apply_fp64_mixed_bc(case, family):
     op, orc, x, ref = case
     op.set_apply_config(FP64, family)
