@@ -318,8 +318,13 @@ def run_ours(args):
     # ---- measured FP64 peaks (roofline denominator), the fastest FP64 launch configuration for
     # this mesh, then the device-resident apply ----
     probes = fp64_peaks(stream)
-    tune64 = op.autotune(FP64, stream=stream)
-    best64 = min(tune64, key=lambda e: e["ms"])
+    if args.family:
+        # a fixed launch configuration (profiling runs): no autotuner candidates before the apply
+        op.set_apply_config(FP64, args.family, args.ctas)
+        tune64 = [{"family": args.family, "ctas_per_sm": args.ctas, "ms": None}]
+    else:
+        tune64 = op.autotune(FP64, stream=stream)
+    best64 = min(tune64, key=lambda e: e["ms"] or 0.0)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         for _ in range(args.warmup):
@@ -827,6 +832,9 @@ def main():
                     + ", ".join(a[0] for a in SOLVE_ARMS))
     ap.add_argument("--max-iterations", type=int, default=30000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--family", choices=["tensor", "face", "face2", "simt"], default="",
+                    help="cube: FP64 apply kernel family to use instead of the autotuner's pick")
+    ap.add_argument("--ctas", type=int, default=2, help="cube: persistent CTAs per SM with --family")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", choices=["cube", "batch", "gf", "poisson", "adjoint", "vcycle"], default="cube",
                     help="cube: the apply benchmark (default); batch: uneven batch of 2D elasticity "

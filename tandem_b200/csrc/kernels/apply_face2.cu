@@ -25,7 +25,7 @@ template <class S>
 int run_face2(DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, TileGeo const& tg, const double* x,
               double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas) {
     using L = MmaTile<S>;
-    const Vol2Layout<S> vl = vol2_layout<S>(op.Nq);
+    const Vol2Layout<S> vl = vol2_layout_auto<S>(op.Nq);
     const Face2Layout<S> fl = face2_layout<S>(op.nq);
     const size_t vsmem = sizeof(double) * static_cast<size_t>(vl.total);
     const size_t fsmem = sizeof(double) * static_cast<size_t>(fl.total);
@@ -54,7 +54,7 @@ int run_face2(DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, 
     int64_t vg = static_cast<int64_t>(sms) * ((ctas > 0 && ctas < vper) ? ctas : vper);
     if (vg > vwork) vg = vwork;
     if (vg < 1) vg = 1;
-    vk<<<static_cast<unsigned>(vg), L::NT, vsmem, s>>>(op, tg, mt.tables, x, y, ld, nrhs);
+    vk<<<static_cast<unsigned>(vg), L::NT, vsmem, s>>>(op, tg, mt.tables, x, y, ld, nrhs, vl.qc);
     if (cudaGetLastError() != cudaSuccess) return TDG_E_CUDA;
     if (ft.nftiles > 0) {
         const int64_t fwork = static_cast<int64_t>(ft.nftiles) * nrhs;

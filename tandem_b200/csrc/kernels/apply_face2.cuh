@@ -79,7 +79,7 @@ __device__ __forceinline__ void cp_async_wait() {
 // C[M x NP] = A[M x K] U for rows [0, mrows), U staged element-major (Staged<S>): as
 // cta_gemm_store with the B fragments read from the staged layout.  Two GEMMs of the same shape
 // at once when A1 != nullptr (C1 = A1 U1).
-template <class S>
+template <class S, int CH = 8>
 __device__ __forceinline__ void cta_gemm_store_staged(const double* A0, const double* U0, double* C0,
                                                       const double* A1, const double* U1, double* C1, int mrows,
                                                       int ksteps, int warp, int lane) {
@@ -89,13 +89,14 @@ __device__ __forceinline__ void cta_gemm_store_staged(const double* A0, const do
     const int g = lane >> 2, t = lane & 3;
     const int per = (mrows / 8) * L::NTN;
     const int ntiles = A1 ? 2 * per : per;
-    for (int t0 = warp; t0 < ntiles; t0 += 4 * L::GW) {
-        double acc[4][2];
-        const double* ap[4];
-        const double* bp[4];
+    // a warp advances up to CH of its output tiles together (independent accumulators)
+    for (int t0 = warp; t0 < ntiles; t0 += CH * L::GW) {
+        double acc[CH][2];
+        const double* ap[CH];
+        const double* bp[CH];
         int cnt = 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < CH; ++j) {
             acc[j][0] = acc[j][1] = 0.0;
             const int tile = t0 + j * L::GW;
             const int tt = tile < ntiles ? tile : t0;
@@ -108,11 +109,11 @@ __device__ __forceinline__ void cta_gemm_store_staged(const double* A0, const do
         }
         for (int ks = 0; ks < ksteps; ++ks) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < CH; ++j)
                 if (j < cnt) dmma(acc[j], ap[j][ks * 4], bp[j][ks * 4]);
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < CH; ++j) {
             if (j < cnt) {
                 const int tile = t0 + j * L::GW;
                 const int which = tile / per, loc = tile % per;
@@ -122,6 +123,53 @@ __device__ __forceinline__ void cta_gemm_store_staged(const double* A0, const do
                 c[1] = acc[j][1];
             }
         }
+    }
+}
+
+// y0 += A0^T B0 and y1 += A1^T B1 (the two lift-backs of a facet tile) in one k loop: both sides'
+// Y tiles of a warp advance together, so twice as many independent accumulators are in flight as
+// in two cta_gemm_acc_t calls.  Layouts as cta_gemm_acc_t.
+template <class L>
+__device__ __forceinline__ void cta_gemm_acc_t2(const double* A0, const double* B0, double (&y0)[L::YPW][2][2],
+                                                const double* A1, const double* B1, double (&y1)[L::YPW][2][2],
+                                                int krows, int warp, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    // side 1 reads at fixed distances from side 0's fragments (same table and buffer layouts)
+    const ptrdiff_t da = A1 - A0, db = B1 - B0;
+    const double *a0[L::YPW], *b0[L::YPW];
+    bool on[L::YPW];
+#pragma unroll
+    for (int j = 0; j < L::YPW; ++j) {
+        const int tile = warp + j * L::GW;
+        on[j] = tile < L::YT;
+        const int tt = on[j] ? tile : 0;
+        const int ym = tt % L::MYT, yn = tt / L::MYT;
+        a0[j] = A0 + t * L::LDT + ym * 8 + g;
+        b0[j] = B0 + t * L::LDN + yn * 8 + g;
+    }
+    const int ks_n = krows / 4;
+    int ks = 0;
+    for (; ks + 1 < ks_n; ks += 2) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int j = 0; j < L::YPW; ++j)
+                if (on[j]) {
+                    const double* ap = a0[j] + (ks + h) * 4 * L::LDT;
+                    const double* bp = b0[j] + (ks + h) * 4 * L::LDN;
+                    dmma(y0[j][h], ap[0], bp[0]);
+                    dmma(y1[j][h], ap[da], bp[db]);
+                }
+    }
+    if (ks < ks_n) {
+#pragma unroll
+        for (int j = 0; j < L::YPW; ++j)
+            if (on[j]) {
+                const double* ap = a0[j] + ks * 4 * L::LDT;
+                const double* bp = b0[j] + ks * 4 * L::LDN;
+                dmma(y0[j][0], ap[0], bp[0]);
+                dmma(y1[j][0], ap[da], bp[db]);
+            }
     }
 }
 
@@ -278,25 +326,33 @@ __device__ __forceinline__ void facet_lift_pair(const double* n, const double* n
 
 // ---- volume kernel ----------------------------------------------------------------------------------
 
+// qc: volume points per pass (all Nq where the buffer fits two CTAs per SM, else MmaTile::QC);
+// fewer passes mean fewer barriers per tile and more pointwise items per pass.
 template <class S>
 struct Vol2Layout {
-    int MV, off_U, off_R, total;
+    int MV, qc, off_U, off_R, total;
 };
 template <class S>
-__host__ __device__ inline Vol2Layout<S> vol2_layout(int Nq) {
+__host__ __device__ inline Vol2Layout<S> vol2_layout(int Nq, int qc) {
     using L = MmaTile<S>;
     Vol2Layout<S> l;
     l.MV = round8(S::D * Nq);
+    l.qc = qc;
     l.off_U = l.MV * L::LDT;
     l.off_R = l.off_U + 2 * Staged<S>::USZ;
-    l.total = l.off_R + L::QC * S::D * L::LDN;
+    l.total = l.off_R + round8(qc * S::D) * L::LDN;
     return l;
+}
+template <class S>
+__host__ inline Vol2Layout<S> vol2_layout_auto(int Nq) {
+    const Vol2Layout<S> full = vol2_layout<S>(Nq, Nq);
+    return full.total * sizeof(double) <= 112 * 1024 ? full : vol2_layout<S>(Nq, MmaTile<S>::QC);
 }
 
 template <class S>
 __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
     vol2_kernel(DevOp<double> op, TileGeo tg, const double* __restrict__ tv, const double* __restrict__ x,
-                double* __restrict__ y, int64_t ld, int nrhs) {
+                double* __restrict__ y, int64_t ld, int nrhs, int qc) {
     using L = MmaTile<S>;
     using SU = Staged<S>;
     constexpr int D = S::D, NBF = S::NBF, Q = S::Q, BS = S::BS, DD = S::DD;
@@ -304,7 +360,7 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
     constexpr int NFLD = vol_fields<S>();
     const int Nq = op.Nq;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const Vol2Layout<S> lay = vol2_layout<S>(Nq);
+    const Vol2Layout<S> lay = vol2_layout<S>(Nq, qc);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sm = reinterpret_cast<double*>(smem_raw);
     double* TV = sm;
@@ -348,8 +404,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
         double yacc[L::YPW][2][2];
 #pragma unroll
         for (int j = 0; j < L::YPW; ++j) yacc[j][0][0] = yacc[j][0][1] = yacc[j][1][0] = yacc[j][1][1] = 0.0;
-        for (int q0 = 0; q0 < Nq; q0 += L::QC) {
-            const int nqc = (Nq - q0 < L::QC) ? (Nq - q0) : L::QC;
+        for (int q0 = 0; q0 < Nq; q0 += qc) {
+            const int nqc = (Nq - q0 < qc) ? (Nq - q0) : qc;
             const int rows = round8(nqc * D);
             cta_gemm_store_staged<S>(TV + q0 * D * LDT, U, R0, nullptr, nullptr, nullptr, rows, L::KP / 4, warp, lane);
             __syncthreads();
@@ -478,7 +534,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     double* Ub = sm + lay.off_U;
     double* R0 = sm + lay.off_R0;
     double* R1 = sm + lay.off_R1;
-    __shared__ int s_f[2][SU::UE], s_e0[2][SU::UE], s_e1[2][SU::UE];
+    // facet / element ids of three tiles in flight: the current one, the one being copied in, and
+    // the one after it (written one iteration ahead, so the copies never wait for them)
+    __shared__ int s_f[3][SU::UE], s_e0[3][SU::UE], s_e1[3][SU::UE];
     const int tab = lay.MF * L::LDT;
     for (int i = tid; i < 4 * SU::USZ; i += NT) Ub[i] = 0.0;
 
@@ -487,59 +545,62 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     const int64_t per = (nwork + gridDim.x - 1) / gridDim.x;
     const int64_t w0 = static_cast<int64_t>(blockIdx.x) * per;
     const int64_t w1 = (w0 + per < nwork) ? w0 + per : nwork;
-    auto stage = [&](int64_t work, int buf) {
-        const int tile = static_cast<int>(work % ft.nftiles);
-        const double* xr = x + (work / ft.nftiles) * ld;
-        const int4 td = ft.ftiles[tile];
+    auto write_ids = [&](int64_t work, int slot) {  // threads tid < UE
+        const int4 td = ft.ftiles[static_cast<int>(work % ft.nftiles)];
         const bool two = (td.z >> 4) == 1;
-        if (tid < SU::UE) {
-            int f = -1, e0 = -1, e1 = -1;
-            if (tid < TE && tid < td.y) {
-                f = ft.fperm[td.x + tid];
-                const int4 fi = ft.finfo[f];
-                e0 = fi.x;
-                e1 = two ? fi.y : -1;
-            }
-            s_f[buf][tid] = f;
-            s_e0[buf][tid] = e0;
-            s_e1[buf][tid] = e1;
+        int f = -1, e0 = -1, e1 = -1;
+        if (tid < TE && tid < td.y) {
+            f = ft.fperm[td.x + tid];
+            const int4 fi = ft.finfo[f];
+            e0 = fi.x;
+            e1 = two ? fi.y : -1;
         }
-        __syncthreads();
-        stage_blocks<S, NT>(xr, s_e0[buf], Ub + (2 * buf) * SU::USZ, tid);
-        if (two) stage_blocks<S, NT>(xr, s_e1[buf], Ub + (2 * buf + 1) * SU::USZ, tid);
+        s_f[slot][tid] = f;
+        s_e0[slot][tid] = e0;
+        s_e1[slot][tid] = e1;
+    };
+    auto stage = [&](int64_t work, int slot, int buf) {  // every thread; ids of `slot` visible
+        const double* xr = x + (work / ft.nftiles) * ld;
+        stage_blocks<S, NT>(xr, s_e0[slot], Ub + (2 * buf) * SU::USZ, tid);
+        stage_blocks<S, NT>(xr, s_e1[slot], Ub + (2 * buf + 1) * SU::USZ, tid);
         cp_async_commit();
     };
     int cur_a = -1, cur_b = -1;  // face tables held in TA / TB
+    if (tid < SU::UE) {
+        if (w0 < w1) write_ids(w0, 0);
+        if (w0 + 1 < w1) write_ids(w0 + 1, 1);
+    }
     __syncthreads();
-    if (w0 < w1) stage(w0, 0);
-    int buf = 0;
-    for (int64_t work = w0; work < w1; ++work, buf ^= 1) {
+    if (w0 < w1) stage(w0, 0, 0);
+    int buf = 0, slot = 0;
+    for (int64_t work = w0; work < w1; ++work, buf ^= 1, slot = (slot == 2 ? 0 : slot + 1)) {
         const int tile = static_cast<int>(work % ft.nftiles);
         double* yr = y + (work / ft.nftiles) * ld;
         const int4 td = ft.ftiles[tile];
         const int key = td.z;
         const int l0 = key & 3, l1 = (key >> 2) & 3, mode = key >> 4;
         const bool two = (mode == 1);
-        __syncthreads();  // the previous tile is done with R, the tables and the other buffer
-        if (work + 1 < w1) stage(work + 1, buf ^ 1);
-        if (l0 != cur_a) {
-            for (int i = tid; i < tab; i += NT) TA[i] = ft.tables[static_cast<int64_t>(l0) * tab + i];
-            cur_a = l0;
-        }
-        if (two && l1 != cur_b) {
-            for (int i = tid; i < tab; i += NT) TB[i] = ft.tables[static_cast<int64_t>(l1) * tab + i];
-            cur_b = l1;
-        }
-        if (work + 1 < w1)
-            cp_async_wait<1>();
-        else
-            cp_async_wait<0>();
+        // own copies of this tile landed; after the barrier everybody's have, and the previous
+        // tile is done with R, the tables, the other buffer and its ids
+        cp_async_wait<0>();
         __syncthreads();
+        const int slot1 = slot == 2 ? 0 : slot + 1, slot2 = slot1 == 2 ? 0 : slot1 + 1;
+        if (work + 1 < w1) stage(work + 1, slot1, buf ^ 1);
+        if (work + 2 < w1 && tid < SU::UE) write_ids(work + 2, slot2);
+        if (l0 != cur_a || (two && l1 != cur_b)) {  // uniform: the key is the CTA's
+            if (l0 != cur_a)
+                for (int i = tid; i < tab; i += NT) TA[i] = ft.tables[static_cast<int64_t>(l0) * tab + i];
+            if (two && l1 != cur_b)
+                for (int i = tid; i < tab; i += NT) TB[i] = ft.tables[static_cast<int64_t>(l1) * tab + i];
+            cur_a = l0;
+            if (two) cur_b = l1;
+            __syncthreads();
+        }
         const double* U0 = Ub + (2 * buf) * SU::USZ;
         const double* U1 = Ub + (2 * buf + 1) * SU::USZ;
-        const int* sf = s_f[buf];
-        const int* se0 = s_e0[buf];
-        const int* se1 = s_e1[buf];
+        const int* sf = s_f[slot];
+        const int* se0 = s_e0[slot];
+        const int* se1 = s_e1[slot];
         if (two)
             cta_gemm_store_staged<S>(TA, U0, R0, TB, U1, R1, lay.MF, L::KP / 4, warp, lane);
         else
@@ -634,8 +695,10 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         for (int j = 0; j < L::YPW; ++j)
 #pragma unroll
             for (int a = 0; a < 2; ++a) y0[j][a][0] = y0[j][a][1] = y1[j][a][0] = y1[j][a][1] = 0.0;
-        cta_gemm_acc_t<L>(TA, R0, y0, lay.MF, warp, lane);
-        if (two) cta_gemm_acc_t<L>(TB, R1, y1, lay.MF, warp, lane);
+        if (two)
+            cta_gemm_acc_t2<L>(TA, R0, y0, TB, R1, y1, lay.MF, warp, lane);
+        else
+            cta_gemm_acc_t<L>(TA, R0, y0, lay.MF, warp, lane);
         const int g = lane >> 2, t = lane & 3;
 #pragma unroll
         for (int j = 0; j < L::YPW; ++j) {
