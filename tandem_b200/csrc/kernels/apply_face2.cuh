@@ -126,52 +126,12 @@ __device__ __forceinline__ void cta_gemm_store_staged(const double* A0, const do
     }
 }
 
-// y0 += A0^T B0 and y1 += A1^T B1 (the two lift-backs of a facet tile) in one k loop: both sides'
-// Y tiles of a warp advance together, so twice as many independent accumulators are in flight as
-// in two cta_gemm_acc_t calls.  Layouts as cta_gemm_acc_t.
-template <class L>
-__device__ __forceinline__ void cta_gemm_acc_t2(const double* A0, const double* B0, double (&y0)[L::YPW][2][2],
-                                                const double* A1, const double* B1, double (&y1)[L::YPW][2][2],
-                                                int krows, int warp, int lane) {
-    const int g = lane >> 2, t = lane & 3;
-    // side 1 reads at fixed distances from side 0's fragments (same table and buffer layouts)
-    const ptrdiff_t da = A1 - A0, db = B1 - B0;
-    const double *a0[L::YPW], *b0[L::YPW];
-    bool on[L::YPW];
-#pragma unroll
-    for (int j = 0; j < L::YPW; ++j) {
-        const int tile = warp + j * L::GW;
-        on[j] = tile < L::YT;
-        const int tt = on[j] ? tile : 0;
-        const int ym = tt % L::MYT, yn = tt / L::MYT;
-        a0[j] = A0 + t * L::LDT + ym * 8 + g;
-        b0[j] = B0 + t * L::LDN + yn * 8 + g;
-    }
-    const int ks_n = krows / 4;
-    int ks = 0;
-    for (; ks + 1 < ks_n; ks += 2) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int j = 0; j < L::YPW; ++j)
-                if (on[j]) {
-                    const double* ap = a0[j] + (ks + h) * 4 * L::LDT;
-                    const double* bp = b0[j] + (ks + h) * 4 * L::LDN;
-                    dmma(y0[j][h], ap[0], bp[0]);
-                    dmma(y1[j][h], ap[da], bp[db]);
-                }
-    }
-    if (ks < ks_n) {
-#pragma unroll
-        for (int j = 0; j < L::YPW; ++j)
-            if (on[j]) {
-                const double* ap = a0[j] + ks * 4 * L::LDT;
-                const double* bp = b0[j] + ks * 4 * L::LDN;
-                dmma(y0[j][0], ap[0], bp[0]);
-                dmma(y1[j][0], ap[da], bp[db]);
-            }
-    }
-}
+// Output tiles a warp advances together in the trace GEMMs (independent accumulators).  Measured on
+// the 32^3 p4 elasticity apply (B200, 2 CTAs per SM, 16 warps per SM): volume 1 / facets 2 ran
+// 3.10 ms, 4 / 4 3.25 ms, 8 / 8 3.75 ms -- with 16 warps per SM the other warps hide the mma
+// latency, and more chains per warp only add live registers and shared-memory traffic in flight.
+constexpr int kVolChains = 1;
+constexpr int kFaceChains = 2;
 
 // Issues the cp.async copies of the coefficient blocks of up to UE elements (el[te] < 0: skipped)
 // from xr into the staged buffer U.
@@ -407,7 +367,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
         for (int q0 = 0; q0 < Nq; q0 += qc) {
             const int nqc = (Nq - q0 < qc) ? (Nq - q0) : qc;
             const int rows = round8(nqc * D);
-            cta_gemm_store_staged<S>(TV + q0 * D * LDT, U, R0, nullptr, nullptr, nullptr, rows, L::KP / 4, warp, lane);
+            cta_gemm_store_staged<S, kVolChains>(TV + q0 * D * LDT, U, R0, nullptr, nullptr, nullptr, rows, L::KP / 4,
+                                                 warp, lane);
             __syncthreads();
             for (int it = tid; it < TE * nqc; it += NT) {
                 const int te = it % TE, qq = it / TE;
@@ -602,9 +563,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         const int* se0 = s_e0[slot];
         const int* se1 = s_e1[slot];
         if (two)
-            cta_gemm_store_staged<S>(TA, U0, R0, TB, U1, R1, lay.MF, L::KP / 4, warp, lane);
+            cta_gemm_store_staged<S, kFaceChains>(TA, U0, R0, TB, U1, R1, lay.MF, L::KP / 4, warp, lane);
         else
-            cta_gemm_store_staged<S>(TA, U0, R0, nullptr, nullptr, nullptr, lay.MF, L::KP / 4, warp, lane);
+            cta_gemm_store_staged<S, kFaceChains>(TA, U0, R0, nullptr, nullptr, nullptr, lay.MF, L::KP / 4, warp, lane);
         __syncthreads();
         const double* geo = tg.fct + static_cast<int64_t>(tile) * NFLD * nq * TE;
         const double* pens = tg.pen + static_cast<int64_t>(tile) * TE;
@@ -695,10 +656,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         for (int j = 0; j < L::YPW; ++j)
 #pragma unroll
             for (int a = 0; a < 2; ++a) y0[j][a][0] = y0[j][a][1] = y1[j][a][0] = y1[j][a][1] = 0.0;
-        if (two)
-            cta_gemm_acc_t2<L>(TA, R0, y0, TB, R1, y1, lay.MF, warp, lane);
-        else
-            cta_gemm_acc_t<L>(TA, R0, y0, lay.MF, warp, lane);
+        cta_gemm_acc_t<L>(TA, R0, y0, lay.MF, warp, lane);
+        if (two) cta_gemm_acc_t<L>(TB, R1, y1, lay.MF, warp, lane);
         const int g = lane >> 2, t = lane & 3;
 #pragma unroll
         for (int j = 0; j < L::YPW; ++j) {
