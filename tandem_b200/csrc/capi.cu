@@ -329,6 +329,18 @@ int upload_tile_geometry(tdg_op* op, DevArena& arena, std::vector<int> const& fi
             pen[static_cast<size_t>(t) * TE + te] = h.penalty[f];
         }
     }
+    // the facet and element ids of every tile slot, in one load per slot
+    std::vector<int4> tids(nft * TE, make_int4(-1, -1, -1, 0));
+    for (size_t t = 0; t < nft; ++t) {
+        const int4 td = ftiles[t];
+        const bool two = (td.z >> 4) == 1;
+        for (int te = 0; te < td.y; ++te) {
+            const int64_t f = fids[td.x + te];
+            tids[t * TE + te] = make_int4(static_cast<int>(f), static_cast<int>(h.up[2 * f]),
+                                          two ? static_cast<int>(h.up[2 * f + 1]) : -1, 0);
+        }
+    }
+    if (nft) TDG_CUDA_TRY(arena.upload(&op->face.tids, tids));
     TDG_CUDA_TRY(arena.upload(&op->tgeo.vol, vol));
     if (nft) {
         TDG_CUDA_TRY(arena.upload(&op->tgeo.fct, fct));

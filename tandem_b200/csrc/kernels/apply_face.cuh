@@ -28,6 +28,8 @@ struct FaceTiles {
     const int* fperm = nullptr;    // facet ids grouped by key
     const int4* finfo = nullptr;   // per facet: {up0, up1, l0 | l1 << 8, mode}
     const double* tables = nullptr;  // the face tables of the FP64 tensor kernel, [NF][MF][LDT]
+    const int4* tids = nullptr;    // per tile slot [ntiles][TE]: {facet, side-0 element, side-1 element
+                                   // (-1 unless mode 1), 0}, facet -1 for unused slots
     int nftiles = 0;
 };
 

@@ -90,7 +90,7 @@ int face2_deg(int N, int kind, DevOp<double> const& op, MmaTiles const& mt, Face
 
 int launch_apply_face2(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft,
                        TileGeo const& tg, const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas) {
-    if (nrhs < 1 || !mt.tables || !tg.vol || (ft.nftiles > 0 && !tg.fct)) return TDG_E_INVALID;
+    if (nrhs < 1 || !mt.tables || !tg.vol || (ft.nftiles > 0 && (!tg.fct || !ft.tids))) return TDG_E_INVALID;
     if (D == 2) return face2_deg<2>(N, kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas);
     if (D == 3) return face2_deg<3>(N, kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas);
     return TDG_E_INVALID;

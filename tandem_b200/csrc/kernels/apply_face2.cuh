@@ -70,6 +70,10 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -495,9 +499,11 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     double* Ub = sm + lay.off_U;
     double* R0 = sm + lay.off_R0;
     double* R1 = sm + lay.off_R1;
-    // facet / element ids of three tiles in flight: the current one, the one being copied in, and
-    // the one after it (written one iteration ahead, so the copies never wait for them)
-    __shared__ int s_f[3][SU::UE], s_e0[3][SU::UE], s_e1[3][SU::UE];
+    // tile descriptors and {facet, element 0, element 1} ids of three tiles in flight: the current
+    // one, the one whose blocks are being copied in, and the one after it (copied asynchronously one
+    // iteration ahead, so nothing waits for them)
+    __shared__ int4 s_td[3];
+    __shared__ int4 s_ids[3][SU::UE];
     const int tab = lay.MF * L::LDT;
     for (int i = tid; i < 4 * SU::USZ; i += NT) Ub[i] = 0.0;
 
@@ -506,48 +512,49 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     const int64_t per = (nwork + gridDim.x - 1) / gridDim.x;
     const int64_t w0 = static_cast<int64_t>(blockIdx.x) * per;
     const int64_t w1 = (w0 + per < nwork) ? w0 + per : nwork;
-    auto write_ids = [&](int64_t work, int slot) {  // threads tid < UE
-        const int4 td = ft.ftiles[static_cast<int>(work % ft.nftiles)];
-        const bool two = (td.z >> 4) == 1;
-        int f = -1, e0 = -1, e1 = -1;
-        if (tid < TE && tid < td.y) {
-            f = ft.fperm[td.x + tid];
-            const int4 fi = ft.finfo[f];
-            e0 = fi.x;
-            e1 = two ? fi.y : -1;
-        }
-        s_f[slot][tid] = f;
-        s_e0[slot][tid] = e0;
-        s_e1[slot][tid] = e1;
+    auto ids_async = [&](int64_t work, int slot) {  // the descriptor and ids of tile `work`
+        const int tile = static_cast<int>(work % ft.nftiles);
+        if (tid < TE) cp_async16(&s_ids[slot][tid], &ft.tids[static_cast<int64_t>(tile) * TE + tid]);
+        if (tid == TE) cp_async16(&s_td[slot], &ft.ftiles[tile]);
     };
     auto stage = [&](int64_t work, int slot, int buf) {  // every thread; ids of `slot` visible
         const double* xr = x + (work / ft.nftiles) * ld;
-        stage_blocks<S, NT>(xr, s_e0[slot], Ub + (2 * buf) * SU::USZ, tid);
-        stage_blocks<S, NT>(xr, s_e1[slot], Ub + (2 * buf + 1) * SU::USZ, tid);
-        cp_async_commit();
+        const int4* ids = s_ids[slot];
+        using SUT = Staged<S>;
+        constexpr int per_el = Q * NBF;
+        for (int i = tid; i < 2 * SUT::UE * per_el; i += NT) {
+            const int side = i / (SUT::UE * per_el), j = i % (SUT::UE * per_el);
+            const int te = j / per_el, w = j % per_el;
+            const int e = te < TE ? (side ? ids[te].z : ids[te].y) : -1;
+            if (e >= 0)
+                cp_async8(Ub + (2 * buf + side) * SUT::USZ + te * SUT::LDU + (w / NBF) * SUT::KS + (w % NBF),
+                          xr + static_cast<int64_t>(e) * BS + w);
+        }
     };
     int cur_a = -1, cur_b = -1;  // face tables held in TA / TB
-    if (tid < SU::UE) {
-        if (w0 < w1) write_ids(w0, 0);
-        if (w0 + 1 < w1) write_ids(w0 + 1, 1);
-    }
+    for (int k = 0; k < 2; ++k)
+        if (w0 + k < w1) ids_async(w0 + k, k);
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     if (w0 < w1) stage(w0, 0, 0);
+    cp_async_commit();
     int buf = 0, slot = 0;
     for (int64_t work = w0; work < w1; ++work, buf ^= 1, slot = (slot == 2 ? 0 : slot + 1)) {
         const int tile = static_cast<int>(work % ft.nftiles);
         double* yr = y + (work / ft.nftiles) * ld;
-        const int4 td = ft.ftiles[tile];
+        // own copies of this tile (and the next tiles' ids) landed; after the barrier everybody's
+        // have, and the previous tile is done with R, the tables, the other buffer and its ids
+        cp_async_wait<0>();
+        __syncthreads();
+        const int4 td = s_td[slot];
         const int key = td.z;
         const int l0 = key & 3, l1 = (key >> 2) & 3, mode = key >> 4;
         const bool two = (mode == 1);
-        // own copies of this tile landed; after the barrier everybody's have, and the previous
-        // tile is done with R, the tables, the other buffer and its ids
-        cp_async_wait<0>();
-        __syncthreads();
         const int slot1 = slot == 2 ? 0 : slot + 1, slot2 = slot1 == 2 ? 0 : slot1 + 1;
         if (work + 1 < w1) stage(work + 1, slot1, buf ^ 1);
-        if (work + 2 < w1 && tid < SU::UE) write_ids(work + 2, slot2);
+        if (work + 2 < w1) ids_async(work + 2, slot2);
+        cp_async_commit();
         if (l0 != cur_a || (two && l1 != cur_b)) {  // uniform: the key is the CTA's
             if (l0 != cur_a)
                 for (int i = tid; i < tab; i += NT) TA[i] = ft.tables[static_cast<int64_t>(l0) * tab + i];
@@ -559,9 +566,7 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         }
         const double* U0 = Ub + (2 * buf) * SU::USZ;
         const double* U1 = Ub + (2 * buf + 1) * SU::USZ;
-        const int* sf = s_f[slot];
-        const int* se0 = s_e0[slot];
-        const int* se1 = s_e1[slot];
+        const int4* sid = s_ids[slot];
         if (two)
             cta_gemm_store_staged<S, kFaceChains>(TA, U0, R0, TB, U1, R1, lay.MF, L::KP / 4, warp, lane);
         else
@@ -571,7 +576,7 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         const double* pens = tg.pen + static_cast<int64_t>(tile) * TE;
         for (int it = tid; it < TE * nq; it += NT) {
             const int te = it % TE, q = it / TE;
-            if (sf[te] < 0) continue;
+            if (sid[te].x < 0) continue;
             const double* gp = geo + it;  // field f at gp[f * nq * TE]
             const int64_t fs = static_cast<int64_t>(nq) * TE;
             double* ga0p = R0 + (q * D) * LDN + te * Q;
@@ -670,10 +675,11 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
                     const int c = yn * 8 + 2 * t + h;
                     if (k < NBF && c < L::NC) {
                         const int te = c / Q, r = c % Q;
-                        if (sf[te] >= 0) {
-                            atomicAdd(&yr[static_cast<int64_t>(se0[te]) * BS + k + NBF * r], y0[j][0][h] + y0[j][1][h]);
+                        const int4 id = sid[te];
+                        if (id.x >= 0) {
+                            atomicAdd(&yr[static_cast<int64_t>(id.y) * BS + k + NBF * r], y0[j][0][h] + y0[j][1][h]);
                             if (two)
-                                atomicAdd(&yr[static_cast<int64_t>(se1[te]) * BS + k + NBF * r],
+                                atomicAdd(&yr[static_cast<int64_t>(id.z) * BS + k + NBF * r],
                                           y1[j][0][h] + y1[j][1][h]);
                         }
                     }
