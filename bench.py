@@ -485,6 +485,120 @@ def _event_time(fn, steps: int, warmup: int, stream) -> float:
     return e0.elapsed_time(e1) / steps
 
 
+def _init_ranks():
+    """(world, rank) of a torchrun launch, with an nccl process group on this rank's GPU (world > 1)."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return world, rank
+
+
+def _timed_max(fn, world):
+    """Seconds of fn() on this rank (CUDA events on the current stream, barriers around), max over ranks."""
+    import torch
+    import torch.distributed as dist
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1) / 1e3], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), out
+
+
+def run_batch_sharded(args, world, rank):
+    """The uneven batch over the ranks: problems assigned longest-processing-time first by element
+    count (sharding.lpt_assign), each rank solving its share as one segmented solve; no data-path
+    collective.  value = DOF of the whole batch / the slowest rank's solve time."""
+    import torch
+    import torch.distributed as dist
+    from tandem_b200.operator import solve_segmented
+    from tandem_b200.sharding import lpt_assign
+    from tandem_b200.workloads import uneven_batch, uneven_batch_cells
+    cells = uneven_batch_cells(args.count)
+    sizes = 2 * cells.astype(np.int64) ** 2
+    mine = lpt_assign(sizes, world)[rank]
+    b = uneven_batch(args.count, 4, tandem_quadrature(2, 4), problems=mine)
+    op = b.op
+    rhs = torch.as_tensor(op.rhs(b.force, b.bc), device="cuda")
+    arms = select_arms(args, default=MG_ARMS)
+    res = {}
+    for name, prec, pcp, pc, method in arms:
+        setup_s = prepare_arm(op, pcp, pc)
+        xs = torch.zeros(op.ndof, dtype=torch.float64, device="cuda")
+        secs, (st, rel) = _timed_max(lambda: solve_segmented(op, rhs, xs, b.elem_offsets, precision=prec, rtol=1e-10,
+                                                             max_iterations=args.max_iterations, check=False,
+                                                             method=method), world)
+        worst = torch.tensor([float(np.max(rel))], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(worst, op=dist.ReduceOp.MAX)
+        res[name] = {"seconds": secs, "max_rel_residual": float(worst.item()), "pc_setup_seconds": setup_s}
+    total_dof = int(sizes.sum()) * 30
+    if rank == 0:
+        best = min(res, key=lambda k: res[k]["seconds"])
+        out = {"metric": "uneven batch solve DOF/s (every problem to 1e-10 rel. residual)",
+               "value": total_dof / res[best]["seconds"], "value_arm": best, "unit": "DOF/s", "n_gpus": world,
+               "higher_is_better": True, "scaling": "strong", "dtype": "f64", "data": "synthetic (seeded meshes)",
+               "config": {"workload": f"{args.count} uneven 2D elasticity problems p4", "dofs": total_dof,
+                          "parallelism": f"LPT problem assignment over {world} ranks"},
+               "solve": res}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_gf_sharded(args, world, rank):
+    """Green's-function columns over the ranks: contiguous column blocks per rank
+    (sharding.column_block), one gather of the column blocks to rank 0 at the end.  value = columns
+    / the slowest rank's time (solves and traction of its block)."""
+    import torch
+    import torch.distributed as dist
+    from tandem_b200 import mesh as M
+    from tandem_b200.operator import DGOperator, POISSON, Fault, greens_function
+    from tandem_b200.sharding import column_block, gather_columns
+    m = M.graded_fault_mesh()
+    M.topology(m, m.info["boundary_bc"], m.info["interior_bc"])
+    M.geometry_nodes(m, 4)
+    op = DGOperator(m, 4, POISSON, tandem_quadrature(2, 4))
+    op.set_material(np.ones((op.E, op.Nq)))
+    fl = Fault(op, M.fault_facets(m), np.array([1.0, 0.0]))
+    ncols = fl.ncoef if args.columns <= 0 else min(args.columns, fl.ncoef)
+    c0, c1 = column_block(ncols, world, rank)
+    res = {}
+    for name, prec, pcp, pc, method in select_arms(args, default=MG_ARMS):
+        prepare_arm(op, pcp, pc)
+        secs, (G, _) = _timed_max(lambda: greens_function(op, fl, precision=prec, rtol=1e-10,
+                                                          columns=np.arange(c0, c1), batch=args.batch,
+                                                          max_iterations=args.max_iterations, method=method), world)
+        full = gather_columns(G, ncols) if world > 1 else G
+        res[name] = {"seconds": secs, "rhs_per_s": ncols / secs}
+        if rank == 0:
+            res[name]["columns_gathered"] = int(full.shape[1])
+    if rank == 0:
+        best = max(res, key=lambda k: res[k]["rhs_per_s"])
+        print(json.dumps({"metric": "Green's function RHS/s (unit-slip columns solved to 1e-10 rel. residual)",
+                          "value": res[best]["rhs_per_s"], "value_arm": best, "unit": "RHS/s", "n_gpus": world,
+                          "higher_is_better": True, "scaling": "strong", "dtype": "f64",
+                          "data": "synthetic graded fault mesh",
+                          "config": {"workload": f"2D antiplane Poisson p4, {op.E:,} triangles", "columns": ncols,
+                                     "batch": args.batch, "parallelism": f"column blocks over {world} ranks"},
+                          "greens_function": res}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def run_batch(args):
     """Uneven batch: independent 2D elasticity problems in one block-diagonal operator; apply
     throughput after autotuning, then FP64 and mixed segmented solves to 1e-10 per problem."""
@@ -856,6 +970,9 @@ def main():
     MG_SMOOTH_ITS = args.mg_smooth_its
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload in ("batch", "gf") and int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        world, rank = _init_ranks()
+        (run_batch_sharded if args.workload == "batch" else run_gf_sharded)(args, world, rank)
     elif args.workload == "batch":
         run_batch(args)
     elif args.workload == "gf":

@@ -248,6 +248,25 @@ int tdg_solve_segmented(tdg_op* op, const double* b, double* x, int nseg, const 
                         const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel_residual,
                         void* stream);
 
+/* One rank's part of a solve over a distributed operator (tandem's MPI distribution of
+ * DGOperator, src/form/DGOperator.h:382-393, with PETSc's parallel KSPCG): `op` is the rank's local
+ * operator -- its owned elements first, then one layer of ghost elements -- and b, x are local device
+ * vectors of E * bs entries whose first owned_elements * bs rows are this rank's part of the global
+ * vectors.  CG with the block-Jacobi preconditioner of the local operator (tdg_bjacobi_setup) runs
+ * on the owned rows; before every apply the library calls exchange(ctx, v, stream), which must fill
+ * the ghost blocks of the device vector v with the owning ranks' values, and after every local
+ * reduction allreduce(ctx, values, count, stream), which must replace the `count` device doubles
+ * at `values` by their sums over the ranks.  Both are expected to enqueue their work on `stream`
+ * (e.g. NCCL point-to-point and all-reduce) and return 0; every rank calls them in the same order
+ * (two all-reduces per iteration, plus two per reliable update).  TDG_FP64 or TDG_MIXED, method
+ * TDG_KSP_CG; no CUDA graphs (the callbacks run on the host).  The stopping test uses the global
+ * FP64 residual. */
+typedef int (*tdg_exchange_fn)(void* ctx, double* v, void* stream);
+typedef int (*tdg_allreduce_fn)(void* ctx, double* values, int count, void* stream);
+int tdg_solve_distributed(tdg_op* op, const double* b, double* x, int64_t owned_elements,
+                          const tdg_solve_opts* opts, tdg_solve_stats* stats, tdg_exchange_fn exchange,
+                          tdg_allreduce_fn allreduce, void* ctx, void* stream);
+
 /* --- p-multigrid preconditioner (PetscLinearSolver::setup_mg, app/common/PetscLinearSolver.cpp:53-114,
  *     MGConfig, app/common/MGConfig.cpp:11-41, options examples/options/mg_cheby.cfg) ------------ */
 

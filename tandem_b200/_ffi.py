@@ -41,6 +41,7 @@ SYMBOLS = {
     "tdg_rhs": (C.c_int, [_p, _p, _p, _p]),
     "tdg_solve": (C.c_int, [_p, _p, _p, C.c_int, _i64, _p, _p, _p]),
     "tdg_solve_segmented": (C.c_int, [_p, _p, _p, C.c_int, _p, _p, _p, _p, _p]),
+    "tdg_solve_distributed": (C.c_int, [_p, _p, _p, _i64, _p, _p, _p, _p, _p, _p]),
     "tdg_adjoint_lame_gradient": (C.c_int, [_p, _p, _p, _p, _p, _p]),
     "tdg_adjoint_lame_gradient_noalloc": (C.c_int, [_p, _p, _p, _p, _p, _p]),
     "tdg_autotune": (C.c_int, [_p, C.c_int, C.c_int, _p, _p, C.c_int, _p]),
@@ -74,6 +75,11 @@ SYMBOLS = {
     "tdg_ref_basis": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _p, _p, _p]),
     "tdg_conical_rule": (C.c_int, [C.c_int, C.c_int, _p, _p]),
 }
+
+
+# callbacks of tdg_solve_distributed: exchange(ctx, v, stream), allreduce(ctx, values, count, stream)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p)
 
 
 class MeshDesc(C.Structure):

@@ -539,6 +539,16 @@ int ensure_uploaded(tdg_op* op, int precision) {
     return fail(TDG_E_INVALID, "precision must be TDG_FP64 or TDG_FP32");
 }
 
+// A solve over the owned rows of one rank of a distributed operator (tdg_solve_distributed):
+// before every apply the caller's exchange fills the ghost blocks of the apply's input, and every
+// dot product's per-rank sum is summed over the ranks by the caller's all-reduce, both enqueued on
+// the solve's stream.
+struct DistCtx {
+    tdg_exchange_fn exchange = nullptr;
+    tdg_allreduce_fn allreduce = nullptr;
+    void* ctx = nullptr;
+};
+
 // Chunk list of a segmented vector (see krylov.cuh), uploaded into solve workspace.
 struct SegPlan {
     int nseg = 0, nchunks = 0;
@@ -547,6 +557,7 @@ struct SegPlan {
     // operator view of the stacked vectors: apply / precondition with nrhs and leading dimension
     int op_nrhs = 1;
     int64_t op_ld = 0;
+    const DistCtx* dist = nullptr;  // distributed solve (one segment: the owned rows), else null
 };
 
 // Chunk length: about four chunks per SM over all segments (so short vectors still occupy the
@@ -578,7 +589,24 @@ int dots(SegPlan const& sp, const T* a, const T* b, const T* c, const T* d, doub
          int slot1, cudaStream_t s) {
     k_dot2<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, a, b, c, d, partial);
     k_dot_finalize<<<sp.nseg, 256, 0, s>>>(partial, sp.seg_chunk, scal, slot0, slot1);
-    return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "dot kernels");
+    if (cudaGetLastError() != cudaSuccess) return fail(TDG_E_CUDA, "dot kernels");
+    if (sp.dist) {  // one segment: sum the slots over the ranks (adjacent slots in one call)
+        const bool pair = slot0 >= 0 && slot1 == slot0 + 1;
+        for (int slot : {slot0, slot1}) {
+            if (slot < 0 || (pair && slot == slot1)) continue;
+            if (sp.dist->allreduce(sp.dist->ctx, scal + slot, pair ? 2 : 1, s) != 0)
+                return fail(TDG_E_STATE, "the all-reduce callback of the distributed solve failed");
+        }
+    }
+    return 0;
+}
+
+// The apply of the Krylov drivers: y = A x, with the ghost exchange of x in front for a
+// distributed solve.
+int krylov_apply(tdg_op* op, int prec, SegPlan const& sp, void* x, void* y, cudaStream_t s) {
+    if (sp.dist && sp.dist->exchange(sp.dist->ctx, static_cast<double*>(x), s) != 0)
+        return fail(TDG_E_STATE, "the exchange callback of the distributed solve failed");
+    return tdg_apply(op, prec, x, y, sp.op_nrhs, sp.op_ld, s);
 }
 
 // ---- block-Jacobi diagonal blocks ---------------------------------------------------------------
@@ -1542,7 +1570,7 @@ template <typename T>
 int cg_iteration(tdg_op* op, int prec, SegPlan const& sp, T* x, CgVectors<T> v, double* partial, double* scal,
                  cudaStream_t s) {
     const bool flexible = op->pc == TDG_PC_MG;
-    TDG_TRY(tdg_apply(op, prec, v.p, v.q, sp.op_nrhs, sp.op_ld, s));
+    TDG_TRY(krylov_apply(op, prec, sp, v.p, v.q, s));
     TDG_TRY(dots<T>(sp, v.p, v.q, nullptr, nullptr, partial, scal, kPQ, -1, s));
     k_cg_xr<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, x, v.r, v.p, v.q, scal);
     TDG_TRY(precondition<T>(op, prec, v.r, v.z, sp.op_nrhs, sp.op_ld, s));
@@ -1556,7 +1584,7 @@ int cg_iteration(tdg_op* op, int prec, SegPlan const& sp, T* x, CgVectors<T> v, 
 // r = b - A x (FP64); per-segment ||r|| and ||b|| on the host.
 int residual64(tdg_op* op, SegPlan const& sp, const double* b, const double* x, double* r, double* tmp,
                double* partial, double* scal, std::vector<double>& rn, std::vector<double>& bn, cudaStream_t s) {
-    TDG_TRY(tdg_apply(op, TDG_FP64, x, tmp, sp.op_nrhs, sp.op_ld, s));
+    TDG_TRY(krylov_apply(op, TDG_FP64, sp, const_cast<double*>(x), tmp, s));
     k_sub<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, b, tmp, r);
     TDG_TRY(dots<double>(sp, r, r, b, b, partial, scal, kRR, kBB, s));
     std::vector<double> hs(static_cast<size_t>(sp.nseg) * kScal);
@@ -1917,7 +1945,8 @@ int fgmres(tdg_op* op, int prec, SegPlan const& sp, const double* b, double* x, 
 // relative residual.
 int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> const& seg_begin,
                    std::vector<int64_t> const& seg_end, int op_nrhs, int64_t op_ld, size_t vec_entries,
-                   const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel, cudaStream_t s) {
+                   const tdg_solve_opts* opts, tdg_solve_stats* stats, double* seg_rel, cudaStream_t s,
+                   const DistCtx* dist = nullptr) {
     const int prec = opts->precision;
     if (prec != TDG_FP64 && prec != TDG_FP32 && prec != TDG_MIXED) return fail(TDG_E_INVALID, "bad precision");
     const bool gmres = opts->method == TDG_KSP_FGMRES;
@@ -1986,6 +2015,7 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     sp.seg_chunk = dseg;
     sp.op_nrhs = op_nrhs;
     sp.op_ld = op_ld;
+    sp.dist = dist;
 
     cudaEvent_t ev0, ev1;
     TDG_CUDA_TRY(cudaEventCreate(&ev0));
@@ -1994,7 +2024,7 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
 
     const int max_it = opts->max_iterations > 0 ? opts->max_iterations : 10000;
     const double rtol = opts->rtol > 0 ? opts->rtol : 1e-10;
-    const bool graphs = opts->use_graphs != 0;
+    const bool graphs = opts->use_graphs != 0 && !dist;  // the callbacks are host code: no capture
     std::vector<double> rn, bn;
     int total_it = 0, updates = 0;
     bool diverged = false;
@@ -2092,6 +2122,23 @@ extern "C" int tdg_solve(tdg_op* op, const double* b, double* x, int nrhs, int64
     }
     return solve_segments(op, b, x, sb, se, nrhs, ld, static_cast<size_t>(nrhs) * ld, opts, stats, nullptr,
                           static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int tdg_solve_distributed(tdg_op* op, const double* b, double* x, int64_t owned_elements,
+                                     const tdg_solve_opts* opts, tdg_solve_stats* stats, tdg_exchange_fn exchange,
+                                     tdg_allreduce_fn allreduce, void* ctx, void* stream) {
+    if (!op || !b || !x || !opts || !stats || !exchange || !allreduce) return fail(TDG_E_INVALID, "null argument");
+    auto const& h = op->h;
+    if (owned_elements < 0 || owned_elements > h.E) return fail(TDG_E_INVALID, "owned_elements outside [0, E]");
+    if (opts->precision != TDG_FP64 && opts->precision != TDG_MIXED)
+        return fail(TDG_E_INVALID, "a distributed solve runs with TDG_FP64 or TDG_MIXED");
+    if (opts->method != TDG_KSP_CG) return fail(TDG_E_INVALID, "a distributed solve runs CG");
+    if (op->pc != TDG_PC_BJACOBI)
+        return fail(TDG_E_INVALID, "a distributed solve is preconditioned by block Jacobi (element-local)");
+    const DistCtx dc{exchange, allreduce, ctx};
+    std::vector<int64_t> sb{0}, se{owned_elements * h.bs};
+    return solve_segments(op, b, x, sb, se, 1, h.E * h.bs, static_cast<size_t>(h.E) * h.bs, opts, stats, nullptr,
+                          static_cast<cudaStream_t>(stream), &dc);
 }
 
 extern "C" int tdg_solve_segmented(tdg_op* op, const double* b, double* x, int nseg, const int64_t* seg_elem_offset,

@@ -75,20 +75,28 @@ class Batch:
     op: DGOperator
 
 
-def uneven_batch(count: int, degree: int, quad: Quadrature, seed: int = 7, lo: int = 1000, hi: int = 40000,
-                 ell: float = 0.2) -> Batch:
+def uneven_batch_cells(count: int, seed: int = 7, lo: int = 1000, hi: int = 40000) -> np.ndarray:
+    """Cells per direction of each problem's n x n x 2 mesh (element counts log-uniform in [lo, hi])."""
     rng = np.random.Generator(np.random.PCG64(seed))
     target = np.exp(rng.uniform(np.log(lo), np.log(hi), size=count))
-    cells = np.maximum(2, np.rint(np.sqrt(target / 2.0))).astype(int)  # n x n x 2 triangles
-    meshes = [M.build(M.square_mesh(int(n)), degree, curve=M.box_boundary_surface(0.02)) for n in cells]
+    return np.maximum(2, np.rint(np.sqrt(target / 2.0))).astype(int)
+
+
+def uneven_batch(count: int, degree: int, quad: Quadrature, seed: int = 7, lo: int = 1000, hi: int = 40000,
+                 ell: float = 0.2, problems=None) -> Batch:
+    """The batch, or only the problems listed in `problems` (a rank's share of it; every problem's
+    mesh, material and force depend on its index alone)."""
+    cells = uneven_batch_cells(count, seed, lo, hi)
+    which = list(range(count)) if problems is None else [int(i) for i in problems]
+    meshes = [M.build(M.square_mesh(int(cells[i])), degree, curve=M.box_boundary_surface(0.02)) for i in which]
     um, eoff = M.union(meshes)
     op = DGOperator(um, degree, ELASTICITY, quad)
     X = op.volume_coords()
     lam = np.empty(X.shape[:2])
     mu = np.empty(X.shape[:2])
     force = np.empty((op.E, 2, op.Nq))
-    for i in range(count):
-        sl = slice(eoff[i], eoff[i + 1])
+    for j, i in enumerate(which):
+        sl = slice(eoff[j], eoff[j + 1])
         s = seed * 1000 + 10 * i
         lam[sl] = RandomField(2, s + 1, ell=ell)(X[sl])
         mu[sl] = RandomField(2, s + 2, ell=ell)(X[sl])
@@ -97,7 +105,7 @@ def uneven_batch(count: int, degree: int, quad: Quadrature, seed: int = 7, lo: i
     op.set_material(lam, mu)
     bc = np.zeros((op.F, 2, op.nq))
     sizes = np.diff(eoff)
-    name = (f"{count} independent 2D elasticity problems p{degree}, curved P2 unit squares, "
+    name = (f"{len(which)} independent 2D elasticity problems p{degree}, curved P2 unit squares, "
             f"{int(sizes.min()):,}-{int(sizes.max()):,} triangles each ({op.E:,} total), log-normal lambda/mu, "
             f"RFF body force, zero Dirichlet")
     return Batch(name, um, quad, degree, eoff, sizes, np.ascontiguousarray(force), bc, op)

@@ -94,3 +94,25 @@ def test_rank_failure_detected_by_timeout():
         if p.is_alive():
             p.kill()
     assert res != "no error"
+
+
+def test_uneven_batch_share_reproduces_its_problems():
+    """A rank's share of the uneven batch (workloads.uneven_batch(problems=...)) holds exactly the
+    listed problems of the full batch: same meshes, material and force, in the listed order."""
+    from cases import tandem_quadrature
+    from tandem_b200.sharding import lpt_assign
+    from tandem_b200.workloads import uneven_batch, uneven_batch_cells
+    q = tandem_quadrature(2, 2)
+    full = uneven_batch(6, 2, q, lo=20, hi=200)
+    cells = uneven_batch_cells(6, lo=20, hi=200)
+    shares = lpt_assign(2 * cells ** 2, 2)
+    assert sorted(shares[0] + shares[1]) == list(range(6))
+    for share in shares:
+        part = uneven_batch(6, 2, q, lo=20, hi=200, problems=share)
+        assert part.op.E == sum(int(full.sizes[i]) for i in share)
+        for j, i in enumerate(share):
+            a = slice(full.elem_offsets[i], full.elem_offsets[i + 1])
+            b = slice(part.elem_offsets[j], part.elem_offsets[j + 1])
+            np.testing.assert_array_equal(part.force[b], full.force[a])
+            np.testing.assert_array_equal(part.op.material_nodal(0)[b], full.op.material_nodal(0)[a])
+            np.testing.assert_array_equal(part.mesh.geo_nodes[b], full.mesh.geo_nodes[a])
