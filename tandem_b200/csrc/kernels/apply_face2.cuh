@@ -83,7 +83,16 @@ __device__ __forceinline__ void cp_async_wait() {
 // C[M x NP] = A[M x K] U for rows [0, mrows), U staged element-major (Staged<S>): as
 // cta_gemm_store with the B fragments read from the staged layout.  Two GEMMs of the same shape
 // at once when A1 != nullptr (C1 = A1 U1).
-template <class S, int CH = 8>
+// A load of a table entry: read-only global path (L1) for tables left in global memory, else shared.
+template <bool AG>
+__device__ __forceinline__ double table_ld(const double* p) {
+    if constexpr (AG)
+        return __ldg(p);
+    else
+        return *p;
+}
+
+template <class S, int CH = 8, bool AG = false>
 __device__ __forceinline__ void cta_gemm_store_staged(const double* A0, const double* U0, double* C0,
                                                       const double* A1, const double* U1, double* C1, int mrows,
                                                       int ksteps, int warp, int lane) {
@@ -114,7 +123,7 @@ __device__ __forceinline__ void cta_gemm_store_staged(const double* A0, const do
         for (int ks = 0; ks < ksteps; ++ks) {
 #pragma unroll
             for (int j = 0; j < CH; ++j)
-                if (j < cnt) dmma(acc[j], ap[j][ks * 4], bp[j][ks * 4]);
+                if (j < cnt) dmma(acc[j], table_ld<AG>(ap[j] + ks * 4), bp[j][ks * 4]);
         }
 #pragma unroll
         for (int j = 0; j < CH; ++j) {
@@ -129,6 +138,43 @@ __device__ __forceinline__ void cta_gemm_store_staged(const double* A0, const do
         }
     }
 }
+
+// Y += A^T B as cta_gemm_acc_t (apply_mma.cuh), the table A read through table_ld<AG>.
+template <class L, bool AG>
+__device__ __forceinline__ void cta_gemm_acc_t_tab(const double* A, const double* B, double (&y)[L::YPW][2][2],
+                                                   int krows, int warp, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const double* ac[L::YPW];
+    const double* bc[L::YPW];
+    bool on[L::YPW];
+#pragma unroll
+    for (int j = 0; j < L::YPW; ++j) {
+        const int tile = warp + j * L::GW;
+        on[j] = tile < L::YT;
+        const int tt = on[j] ? tile : 0;
+        const int ym = tt % L::MYT, yn = tt / L::MYT;
+        ac[j] = A + t * L::LDT + ym * 8 + g;
+        bc[j] = B + t * L::LDN + yn * 8 + g;
+    }
+    const int ks_n = krows / 4;
+    int ks = 0;
+    for (; ks + 1 < ks_n; ks += 2) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int j = 0; j < L::YPW; ++j)
+                if (on[j]) dmma(y[j][h], table_ld<AG>(ac[j] + (ks + h) * 4 * L::LDT), bc[j][(ks + h) * 4 * L::LDN]);
+    }
+    if (ks < ks_n) {
+#pragma unroll
+        for (int j = 0; j < L::YPW; ++j)
+            if (on[j]) dmma(y[j][0], table_ld<AG>(ac[j] + ks * 4 * L::LDT), bc[j][ks * 4 * L::LDN]);
+    }
+}
+
+// The facet kernel's face tables: read from global memory through the L1 (true) or copied into
+// shared memory per (l0, l1) pair (false).
+constexpr bool kFaceTablesGlobal = false;
 
 // Output tiles a warp advances together in the trace GEMMs (independent accumulators).  Measured on
 // the 32^3 p4 elasticity apply (B200, 2 CTAs per SM, 16 warps per SM): volume 1 / facets 2 ran
@@ -472,8 +518,8 @@ __host__ __device__ inline Face2Layout<S> face2_layout(int nq) {
     using L = MmaTile<S>;
     Face2Layout<S> l;
     l.MF = round8((S::D + 1) * nq);
-    l.off_TB = l.MF * L::LDT;
-    l.off_U = l.off_TB + l.MF * L::LDT;
+    l.off_TB = kFaceTablesGlobal ? 0 : l.MF * L::LDT;
+    l.off_U = kFaceTablesGlobal ? 0 : l.off_TB + l.MF * L::LDT;
     l.off_R0 = l.off_U + 4 * Staged<S>::USZ;  // [buffer][side]
     l.off_R1 = l.off_R0 + l.MF * L::LDN;
     l.total = l.off_R1 + l.MF * L::LDN;
@@ -555,7 +601,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         if (work + 1 < w1) stage(work + 1, slot1, buf ^ 1);
         if (work + 2 < w1) ids_async(work + 2, slot2);
         cp_async_commit();
-        if (l0 != cur_a || (two && l1 != cur_b)) {  // uniform: the key is the CTA's
+        const double* tA = kFaceTablesGlobal ? ft.tables + static_cast<int64_t>(l0) * tab : TA;
+        const double* tB = kFaceTablesGlobal ? ft.tables + static_cast<int64_t>(l1) * tab : TB;
+        if (!kFaceTablesGlobal && (l0 != cur_a || (two && l1 != cur_b))) {  // uniform: the key is the CTA's
             if (l0 != cur_a)
                 for (int i = tid; i < tab; i += NT) TA[i] = ft.tables[static_cast<int64_t>(l0) * tab + i];
             if (two && l1 != cur_b)
@@ -568,9 +616,11 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         const double* U1 = Ub + (2 * buf + 1) * SU::USZ;
         const int4* sid = s_ids[slot];
         if (two)
-            cta_gemm_store_staged<S, kFaceChains>(TA, U0, R0, TB, U1, R1, lay.MF, L::KP / 4, warp, lane);
+            cta_gemm_store_staged<S, kFaceChains, kFaceTablesGlobal>(tA, U0, R0, tB, U1, R1, lay.MF, L::KP / 4, warp,
+                                                                     lane);
         else
-            cta_gemm_store_staged<S, kFaceChains>(TA, U0, R0, nullptr, nullptr, nullptr, lay.MF, L::KP / 4, warp, lane);
+            cta_gemm_store_staged<S, kFaceChains, kFaceTablesGlobal>(tA, U0, R0, nullptr, nullptr, nullptr, lay.MF,
+                                                                     L::KP / 4, warp, lane);
         __syncthreads();
         const double* geo = tg.fct + static_cast<int64_t>(tile) * NFLD * nq * TE;
         const double* pens = tg.pen + static_cast<int64_t>(tile) * TE;
@@ -661,8 +711,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         for (int j = 0; j < L::YPW; ++j)
 #pragma unroll
             for (int a = 0; a < 2; ++a) y0[j][a][0] = y0[j][a][1] = y1[j][a][0] = y1[j][a][1] = 0.0;
-        cta_gemm_acc_t<L>(TA, R0, y0, lay.MF, warp, lane);
-        if (two) cta_gemm_acc_t<L>(TB, R1, y1, lay.MF, warp, lane);
+        cta_gemm_acc_t_tab<L, kFaceTablesGlobal>(tA, R0, y0, lay.MF, warp, lane);
+        if (two) cta_gemm_acc_t_tab<L, kFaceTablesGlobal>(tB, R1, y1, lay.MF, warp, lane);
         const int g = lane >> 2, t = lane & 3;
 #pragma unroll
         for (int j = 0; j < L::YPW; ++j) {
