@@ -341,6 +341,11 @@ int upload_tile_geometry(tdg_op* op, DevArena& arena, std::vector<int> const& fi
         }
     }
     if (nft) TDG_CUDA_TRY(arena.upload(&op->face.tids, tids));
+    {
+        const int* st = nullptr;
+        TDG_CUDA_TRY(arena.upload(&st, std::vector<int>(1, 0)));
+        op->tgeo.status = const_cast<int*>(st);
+    }
     TDG_CUDA_TRY(arena.upload(&op->tgeo.vol, vol));
     if (nft) {
         TDG_CUDA_TRY(arena.upload(&op->tgeo.fct, fct));
@@ -2103,6 +2108,11 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     stats->seconds = ms * 1e-3;
     stats->converged = (!diverged && worst <= rtol) ? 1 : 0;
     if (diverged) return fail(TDG_E_DIVERGED, "non-finite residual in the Krylov iteration");
+    if (op->tgeo.status) {  // a bounded wait of the facet kernel that ran out makes the solve invalid
+        int st = 0;
+        TDG_CUDA_TRY(cudaMemcpy(&st, op->tgeo.status, sizeof st, cudaMemcpyDeviceToHost));
+        if (st) return fail(TDG_E_TIMEOUT, "a bounded wait of the facet kernel ran out");
+    }
     if (!stats->converged) return fail(TDG_E_DIVERGED, "iteration limit reached before the residual target");
     return 0;
 }

@@ -26,7 +26,13 @@ int run_face2(DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, 
               double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas) {
     using L = MmaTile<S>;
     const Vol2Layout<S> vl = vol2_layout_auto<S>(op.Nq);
-    const Face2Layout<S> fl = face2_layout<S>(op.nq);
+    // the geometry prefetch where the policy allows it (two CTAs per SM: at most ~113 KB each)
+    const size_t two_cta = 112 * 1024;
+    int gpre = 0;
+    if (kFacetGeometryPrefetch == 2 ||
+        (kFacetGeometryPrefetch == 1 && sizeof(double) * face2_layout<S>(op.nq, 1).total <= two_cta))
+        gpre = tg.status ? 1 : 0;
+    const Face2Layout<S> fl = face2_layout<S>(op.nq, gpre);
     const size_t vsmem = sizeof(double) * static_cast<size_t>(vl.total);
     const size_t fsmem = sizeof(double) * static_cast<size_t>(fl.total);
     auto vk = vol2_kernel<S>;
@@ -37,7 +43,7 @@ int run_face2(DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, 
     auto fk2 = face2_kernel<S, 2>;
     auto fk1 = face2_kernel<S, kTwoVariants ? 1 : 2>;
     auto fk = one ? fk1 : fk2;
-    static size_t vconf = 0, fconf2 = 0, fconf1 = 0;
+    static size_t vconf = 0, fconf2 = 0, fconf1 = 0;  // configured dynamic shared memory (grows)
     static int vper = 1, fper2 = 1, fper1 = 1;
     if (vconf < vsmem) {
         if (int rc = configure2(vk, vsmem, L::NT, vper)) return rc;
@@ -61,7 +67,7 @@ int run_face2(DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, 
         int64_t fg = static_cast<int64_t>(sms) * ((ctas > 0 && ctas < fper) ? ctas : fper);
         if (fg > fwork) fg = fwork;
         if (fg < 1) fg = 1;
-        fk<<<static_cast<unsigned>(fg), L::NT, fsmem, s>>>(op, ft, tg, x, y, ld, nrhs);
+        fk<<<static_cast<unsigned>(fg), L::NT, fsmem, s>>>(op, ft, tg, x, y, ld, nrhs, gpre);
         if (cudaGetLastError() != cudaSuccess) return TDG_E_CUDA;
     }
     return 0;

@@ -74,6 +74,42 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
+// mbarrier-tracked bulk copies (the bulk-copy engine, untiled): one CTA-scope barrier whose
+// transaction count the copy completes; waits are bounded (a wait that runs out records a status
+// and gives up instead of spinning on).
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// dst[0, bytes) = src[0, bytes) (bytes a multiple of 16, both 16-byte aligned), completing on bar
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for phase `parity` of bar, at most kMaxWaitTries tries; false when it ran out.
+constexpr int kMaxWaitTries = 1 << 24;
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (int i = 0; i < kMaxWaitTries; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -175,6 +211,9 @@ __device__ __forceinline__ void cta_gemm_acc_t_tab(const double* A, const double
 // The facet kernel's face tables: read from global memory through the L1 (true) or copied into
 // shared memory per (l0, l1) pair (false).
 constexpr bool kFaceTablesGlobal = false;
+// Bulk-copy prefetch of each facet tile's geometry into shared memory: 0 never, 1 where it still
+// fits two CTAs per SM, 2 always (then one CTA per SM where it does not).
+constexpr int kFacetGeometryPrefetch = 1;
 
 // Output tiles a warp advances together in the trace GEMMs (independent accumulators).  Measured on
 // the 32^3 p4 elasticity apply (B200, 2 CTAs per SM, 16 warps per SM): volume 1 / facets 2 ran
@@ -207,6 +246,7 @@ struct TileGeo {
     const double* vol = nullptr;
     const double* fct = nullptr;
     const double* pen = nullptr;
+    int* status = nullptr;  // device word: non-zero once a bounded wait of the facet kernel ran out
 };
 
 template <class S>
@@ -511,10 +551,11 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
 
 template <class S>
 struct Face2Layout {
-    int MF, off_TB, off_U, off_R0, off_R1, total;
+    int MF, off_TB, off_U, off_R0, off_R1, off_G, total;
 };
+// gpre: room for the current facet tile's geometry, prefetched by the bulk-copy engine.
 template <class S>
-__host__ __device__ inline Face2Layout<S> face2_layout(int nq) {
+__host__ __device__ inline Face2Layout<S> face2_layout(int nq, int gpre = 0) {
     using L = MmaTile<S>;
     Face2Layout<S> l;
     l.MF = round8((S::D + 1) * nq);
@@ -522,14 +563,15 @@ __host__ __device__ inline Face2Layout<S> face2_layout(int nq) {
     l.off_U = kFaceTablesGlobal ? 0 : l.off_TB + l.MF * L::LDT;
     l.off_R0 = l.off_U + 4 * Staged<S>::USZ;  // [buffer][side]
     l.off_R1 = l.off_R0 + l.MF * L::LDN;
-    l.total = l.off_R1 + l.MF * L::LDN;
+    l.off_G = l.off_R1 + l.MF * L::LDN;
+    l.total = l.off_G + (gpre ? fct_fields<S>() * nq * L::TE : 0);
     return l;
 }
 
 template <class S, int MINB>
 __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     face2_kernel(DevOp<double> op, FaceTiles ft, TileGeo tg, const double* __restrict__ x, double* __restrict__ y,
-                 int64_t ld, int nrhs) {
+                 int64_t ld, int nrhs, int gpre) {
     using L = MmaTile<S>;
     using SU = Staged<S>;
     constexpr int D = S::D, NBF = S::NBF, Q = S::Q, BS = S::BS, DD = S::DD;
@@ -537,7 +579,7 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     constexpr int NFLD = fct_fields<S>();
     const int nq = op.nq;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const Face2Layout<S> lay = face2_layout<S>(nq);
+    const Face2Layout<S> lay = face2_layout<S>(nq, gpre);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sm = reinterpret_cast<double*>(smem_raw);
     double* TA = sm;
@@ -545,6 +587,10 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     double* Ub = sm + lay.off_U;
     double* R0 = sm + lay.off_R0;
     double* R1 = sm + lay.off_R1;
+    double* Gs = sm + lay.off_G;  // the current facet tile's geometry (gpre)
+    __shared__ __align__(8) unsigned long long s_gbar;
+    const unsigned gbytes = static_cast<unsigned>(NFLD * nq * TE * sizeof(double));
+    if (gpre && tid == 0) mbar_init(&s_gbar, 1);
     // tile descriptors and {facet, element 0, element 1} ids of three tiles in flight: the current
     // one, the one whose blocks are being copied in, and the one after it (copied asynchronously one
     // iteration ahead, so nothing waits for them)
@@ -601,6 +647,10 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         if (work + 1 < w1) stage(work + 1, slot1, buf ^ 1);
         if (work + 2 < w1) ids_async(work + 2, slot2);
         cp_async_commit();
+        // the geometry of this tile into shared memory, behind the trace GEMMs (the previous tile's
+        // pointwise phase, the last reader, ended before the barrier above)
+        if (gpre && tid == 0)
+            bulk_load(Gs, tg.fct + static_cast<int64_t>(tile) * NFLD * nq * TE, gbytes, &s_gbar);
         const double* tA = kFaceTablesGlobal ? ft.tables + static_cast<int64_t>(l0) * tab : TA;
         const double* tB = kFaceTablesGlobal ? ft.tables + static_cast<int64_t>(l1) * tab : TB;
         if (!kFaceTablesGlobal && (l0 != cur_a || (two && l1 != cur_b))) {  // uniform: the key is the CTA's
@@ -623,6 +673,11 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
                                                                      L::KP / 4, warp, lane);
         __syncthreads();
         const double* geo = tg.fct + static_cast<int64_t>(tile) * NFLD * nq * TE;
+        if (gpre) {
+            if (!mbar_wait_bounded(&s_gbar, static_cast<unsigned>((work - w0) & 1)) && tid == 0 && tg.status)
+                atomicExch(tg.status, 1);
+            geo = Gs;
+        }
         const double* pens = tg.pen + static_cast<int64_t>(tile) * TE;
         for (int it = tid; it < TE * nq; it += NT) {
             const int te = it % TE, q = it / TE;
