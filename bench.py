@@ -784,9 +784,10 @@ def run_adjoint(args):
     """Lame gradient of a point misfit on the 16^3 x 6 curved tet mesh (degree 4, per-element
     lambda, mu ~ U[0.5, 2]): time of one gradient (forward solve, adjoint solve, gradient kernel)
     and the check against central finite differences on `fd_elements` random elements (lambda_e
-    and mu_e separately, step 1e-4 relative).  Each FD side solves for the correction
-    A(theta') du = b(theta') - A(theta') u0 from the converged u0, so the difference of the two
-    misfits carries no solve-tolerance cancellation."""
+    and mu_e separately, relative step --fd-step).  Each FD side solves for the correction
+    A(theta') du = b(theta') - A(theta') u0 from the converged u0 and takes the misfit change
+    J(u0 + du) - J(u0) = r0 . P du + |P du|^2 / 2 (r0 = P u0 - d), so neither the solve tolerance
+    nor the size of J(u0) cancels in the difference."""
     import torch
     from tandem_b200 import mesh as M
     from tandem_b200.adjoint import LameProblem, PointObservation, lame_solve
@@ -836,7 +837,8 @@ def run_adjoint(args):
     from tandem_b200.operator import MIXED
     fd_prec = {"fp64": FP64, "mixed": MIXED}[args.fd_precision]
     sel = np.random.Generator(np.random.PCG64(args.seed + 3)).choice(op.E, size=args.fd_elements, replace=False)
-    h = 1e-4
+    h = args.fd_step
+    r0 = (P.apply(u0) - d).detach()  # misfit residual at the base point
     ones = np.ones((1, op.Nq))
     au = torch.empty_like(u0)
     fd_its = []
@@ -855,7 +857,9 @@ def run_adjoint(args):
                           check=False)
             fd_its.append(st["iterations"])
             du_prev = du
-            vals.append(0.5 * float(torch.sum((P.apply(u0 + du) - d) ** 2)))
+            # J(u0 + du) - J(u0) = r0 . P du + |P du|^2 / 2, without the cancellation of J(u0)
+            pdu = P.apply(du)  # P is linear
+            vals.append(float(torch.sum(r0 * pdu)) + 0.5 * float(torch.sum(pdu * pdu)))
         return vals
 
     errs = {"lambda": [], "mu": []}
@@ -962,6 +966,7 @@ def main():
     ap.add_argument("--adj-n", type=int, default=16, help="adjoint: cube cells per direction")
     ap.add_argument("--fd-elements", type=int, default=64, help="adjoint: elements checked by FD")
     ap.add_argument("--fd-rtol", type=float, default=1e-12, help="adjoint: FD correction solve tolerance")
+    ap.add_argument("--fd-step", type=float, default=1e-5, help="adjoint: relative FD step")
     ap.add_argument("--fd-precision", choices=["fp64", "mixed"], default="fp64", help="adjoint: FD solve precision")
     ap.add_argument("--grad-rtol", type=float, default=1e-12, help="adjoint: forward / adjoint solve tolerance")
     ap.add_argument("--adj-pc", choices=["bjacobi", "mg"], default="mg", help="adjoint: gradient solves' preconditioner")

@@ -157,7 +157,10 @@ typedef struct {
     int family;       /* 0 = element-centric tensor-core kernel, 1 = SIMT kernel, 2 = face-centric
                          tensor-core kernels (volume kernel + one pass over the facets), 3 = the
                          face-centric pair software-pipelined (FP64: asynchronous copies of the next
-                         tile's coefficient blocks, tile-ordered geometry; FP32 runs family 2) */
+                         tile's coefficient blocks, tile-ordered geometry; FP32 runs family 2),
+                         4 = FP32 only: family 2 with the volume term on the 5th-generation tensor
+                         cores (tcgen05.mma kind::tf32, accumulators in tensor memory; shapes with at
+                         most 64 volume points, else family 2) */
     int ctas_per_sm;  /* persistent CTAs per SM requested (0 = default) */
     double ms;        /* measured time of one apply */
 } tdg_tune_entry;
@@ -182,6 +185,15 @@ int tdg_set_apply_config(tdg_op* op, int precision, int family, int ctas_per_sm)
  * events on `stream` after a warm-up and returns the best rate in *tflops.  Allocates and frees
  * two small device buffers; synchronises `stream`. */
 int tdg_probe_fp64_peak(int kind, int ctas_per_sm, void* stream, double* tflops);
+
+/* Known-answer check of the 5th-generation tensor-core path of the FP32 operator (no counterpart in
+ * tandem): D[128 x n] = A[128 x k] B[n x k]^T on device row-major FP32 operands through tcgen05.mma
+ * kind::tf32 with the accumulator in tensor memory, in three TF32 products (hi hi + hi lo + lo hi)
+ * when split3 != 0, else one; A and B staged K-major (a_mn / b_mn = 0) or MN-major (!= 0) in shared
+ * memory.  n a multiple of 16 in [16, 256], k a multiple of 8 in [8, 64].  Synchronises `stream`;
+ * TDG_E_TIMEOUT when the MMA's completion was not seen within the bounded wait. */
+int tdg_probe_tc05_gemm(const float* A, const float* B, float* D, int n, int k, int split3, int a_mn, int b_mn,
+                        void* stream);
 
 /* --- right-hand side (DGOperator::rhs, src/form/DGOperator.h:189-237) ---------------------- */
 

@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-O
               "--expt-relaxed-constexpr", "-I", str(ROOT / "include")]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-march=x86-64-v3", "-I", str(ROOT / "include")]
 
-SOURCES_CU = ["capi.cu", "kernels/apply.cu", "kernels/bjacobi.cu", "kernels/fault.cu", "kernels/adjoint.cu", "kernels/apply_tc32.cu", "kernels/apply_face.cu", "kernels/apply_face_tc32.cu", "kernels/wave.cu", "kernels/mg.cu", "kernels/peak.cu", "kernels/gf_traction.cu", "kernels/apply_face2.cu"]
+SOURCES_CU = ["capi.cu", "kernels/apply.cu", "kernels/bjacobi.cu", "kernels/fault.cu", "kernels/adjoint.cu", "kernels/apply_tc32.cu", "kernels/apply_face.cu", "kernels/apply_face_tc32.cu", "kernels/wave.cu", "kernels/mg.cu", "kernels/peak.cu", "kernels/gf_traction.cu", "kernels/apply_face2.cu", "kernels/tc05_probe.cu", "kernels/apply_tc05.cu"]
 SOURCES_CXX = ["host/refelem.cpp", "host/setup.cpp"]
 
 

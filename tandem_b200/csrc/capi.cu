@@ -272,6 +272,53 @@ void facet_tiles(HostOperator const& h, int TE, std::vector<int4>& finfo, std::v
     }
 }
 
+// The facet tiles' geometry [tile][field][nq][TE] (n, n_unit, then Poisson K G0, K G1 or
+// elasticity G0, G1, lam0, mu0, lam1, mu1; unused slots zero), the penalty [tile][TE] and the facet
+// and element ids of every slot {facet, side-0 element, side-1 element (-1 unless mode 1), 0}.
+template <typename T>
+void tile_facet_geometry(HostOperator const& h, int TE, std::vector<int> const& fids, std::vector<int4> const& ftiles,
+                         std::vector<T>& fct, std::vector<double>& pen, std::vector<int4>& tids) {
+    const int D = h.D, DD = D * D, nq = h.nq;
+    const bool poisson = h.kind == 0;
+    const int ff = 2 * D + 2 * DD + (poisson ? 0 : 4);
+    const size_t nft = ftiles.size();
+    fct.assign(nft * ff * nq * TE, T(0));
+    pen.assign(nft * TE, 0.0);
+    tids.assign(nft * TE, make_int4(-1, -1, -1, 0));
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < static_cast<int64_t>(nft); ++t) {
+        const int4 td = ftiles[t];
+        const bool two = (td.z >> 4) == 1;
+        T* base = &fct[static_cast<size_t>(t) * ff * nq * TE];
+        for (int te = 0; te < td.y; ++te) {
+            const int64_t f = fids[td.x + te];
+            auto put = [&](int field, int q, double v) {
+                base[(static_cast<size_t>(field) * nq + q) * TE + te] = static_cast<T>(v);
+            };
+            for (int q = 0; q < nq; ++q) {
+                for (int i = 0; i < D; ++i) {
+                    put(i, q, h.fN[(static_cast<size_t>(f) * D + i) * nq + q]);
+                    put(D + i, q, h.fNunit[(static_cast<size_t>(f) * D + i) * nq + q]);
+                }
+                if (poisson) {
+                    for (int side = 0; side < 2; ++side)
+                        for (int c = 0; c < DD; ++c)
+                            put(2 * D + side * DD + c, q, h.fCoef[((static_cast<size_t>(f) * 2 + side) * DD + c) * nq + q]);
+                } else {
+                    for (int c = 0; c < DD; ++c) {
+                        put(2 * D + c, q, h.fG0[(static_cast<size_t>(f) * DD + c) * nq + q]);
+                        put(2 * D + DD + c, q, h.fG1[(static_cast<size_t>(f) * DD + c) * nq + q]);
+                    }
+                    for (int c = 0; c < 4; ++c) put(2 * D + 2 * DD + c, q, h.fCoef[(static_cast<size_t>(f) * 4 + c) * nq + q]);
+                }
+            }
+            pen[static_cast<size_t>(t) * TE + te] = h.penalty[f];
+            tids[static_cast<size_t>(t) * TE + te] = make_int4(static_cast<int>(f), static_cast<int>(h.up[2 * f]),
+                                                                two ? static_cast<int>(h.up[2 * f + 1]) : -1, 0);
+        }
+    }
+}
+
 // Geometry and coefficients of the software-pipelined face-centric apply (apply_face2.cuh) in tile
 // order: per element tile of TE consecutive elements [field][Nq][TE] (J^-1, then the volume
 // coefficients), per facet tile [field][nq][TE] (n, n_unit, then Poisson K G0, K G1 or elasticity
@@ -279,7 +326,7 @@ void facet_tiles(HostOperator const& h, int TE, std::vector<int4>& finfo, std::v
 // reference-layout arrays, read with the tile's elements or facets fastest.
 int upload_tile_geometry(tdg_op* op, DevArena& arena, std::vector<int> const& fids, std::vector<int4> const& ftiles) {
     auto const& h = op->h;
-    const int D = h.D, DD = D * D, Nq = h.Nq, nq = h.nq;
+    const int D = h.D, DD = D * D, Nq = h.Nq;
     const int TE = mma_tile_elements(D, h.N, h.Q);
     const bool poisson = h.kind == 0;
     const int ncoef = poisson ? 1 : 2;
@@ -299,47 +346,10 @@ int upload_tile_geometry(tdg_op* op, DevArena& arena, std::vector<int> const& fi
                 base[(static_cast<size_t>(DD + c) * Nq + q) * TE + te] =
                     h.vCoef[(static_cast<size_t>(e) * ncoef + c) * Nq + q];
     }
-    const int ff = 2 * D + 2 * DD + (poisson ? 0 : 4);
     const size_t nft = ftiles.size();
-    std::vector<double> fct(nft * ff * nq * TE, 0.0), pen(nft * TE, 0.0);
-#pragma omp parallel for schedule(static)
-    for (int64_t t = 0; t < static_cast<int64_t>(nft); ++t) {
-        const int4 td = ftiles[t];
-        double* base = &fct[static_cast<size_t>(t) * ff * nq * TE];
-        for (int te = 0; te < td.y; ++te) {
-            const int64_t f = fids[td.x + te];
-            auto put = [&](int field, int q, double v) { base[(static_cast<size_t>(field) * nq + q) * TE + te] = v; };
-            for (int q = 0; q < nq; ++q) {
-                for (int i = 0; i < D; ++i) {
-                    put(i, q, h.fN[(static_cast<size_t>(f) * D + i) * nq + q]);
-                    put(D + i, q, h.fNunit[(static_cast<size_t>(f) * D + i) * nq + q]);
-                }
-                if (poisson) {
-                    for (int side = 0; side < 2; ++side)
-                        for (int c = 0; c < DD; ++c)
-                            put(2 * D + side * DD + c, q, h.fCoef[((static_cast<size_t>(f) * 2 + side) * DD + c) * nq + q]);
-                } else {
-                    for (int c = 0; c < DD; ++c) {
-                        put(2 * D + c, q, h.fG0[(static_cast<size_t>(f) * DD + c) * nq + q]);
-                        put(2 * D + DD + c, q, h.fG1[(static_cast<size_t>(f) * DD + c) * nq + q]);
-                    }
-                    for (int c = 0; c < 4; ++c) put(2 * D + 2 * DD + c, q, h.fCoef[(static_cast<size_t>(f) * 4 + c) * nq + q]);
-                }
-            }
-            pen[static_cast<size_t>(t) * TE + te] = h.penalty[f];
-        }
-    }
-    // the facet and element ids of every tile slot, in one load per slot
-    std::vector<int4> tids(nft * TE, make_int4(-1, -1, -1, 0));
-    for (size_t t = 0; t < nft; ++t) {
-        const int4 td = ftiles[t];
-        const bool two = (td.z >> 4) == 1;
-        for (int te = 0; te < td.y; ++te) {
-            const int64_t f = fids[td.x + te];
-            tids[t * TE + te] = make_int4(static_cast<int>(f), static_cast<int>(h.up[2 * f]),
-                                          two ? static_cast<int>(h.up[2 * f + 1]) : -1, 0);
-        }
-    }
+    std::vector<double> fct, pen;
+    std::vector<int4> tids;
+    tile_facet_geometry(h, TE, fids, ftiles, fct, pen, tids);
     if (nft) TDG_CUDA_TRY(arena.upload(&op->face.tids, tids));
     {
         const int* st = nullptr;
@@ -450,6 +460,11 @@ int upload_tc32(tdg_op* op, DevArena& arena) {
     op->tc32.ntiles = static_cast<int>(tiles.size());
     op->tc32.table_floats = static_cast<int>(tab.size());
     {
+        const int* st = nullptr;
+        TDG_CUDA_TRY(arena.upload(&st, std::vector<int>(1, 0)));
+        op->tc32.status = const_cast<int*>(st);
+    }
+    {
         std::vector<int4> finfo, ftiles;
         std::vector<int> fids;
         facet_tiles(h, tc32_tile_elements(D, h.Q), finfo, fids, ftiles);
@@ -459,6 +474,15 @@ int upload_tc32(tdg_op* op, DevArena& arena) {
         }
         TDG_CUDA_TRY(arena.upload(&op->face32.finfo, finfo));
         op->face32.nftiles = static_cast<int>(ftiles.size());
+        std::vector<float> fct;
+        std::vector<double> pen;
+        std::vector<int4> tids;
+        tile_facet_geometry(h, tc32_tile_elements(D, h.Q), fids, ftiles, fct, pen, tids);
+        if (!ftiles.empty()) {
+            TDG_CUDA_TRY(arena.upload(&op->face32.tids, tids));
+            TDG_CUDA_TRY(arena.upload(&op->face32.geo, fct));
+            TDG_CUDA_TRY(arena.upload(&op->face32.pen, pen));
+        }
     }
     return 0;
 }
@@ -1316,10 +1340,11 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
         rc = launch_apply<double>(h.D, h.N, h.kind, op->op64, static_cast<const double*>(x),
                                   static_cast<double*>(y), nrhs, ld, s);
     const bool face32 = op->use_mma && op->family[1] >= 2;  // face-centric (the FP32 kernels have one form)
+    const bool vol05 = op->family[1] == 4;                    // its volume term on tcgen05
     if (precision == TDG_FP32 && face32)
         rc = launch_apply_face_tc32<float>(h.D, h.N, h.kind, op->op32, op->tc32, op->face32,
                                            static_cast<const float*>(x), static_cast<float*>(y), nrhs, ld, s,
-                                           op->ctas[1]);
+                                           op->ctas[1], vol05);
     else if (precision == TDG_FP32 && tensor)
         rc = launch_apply_tc32<float>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const float*>(x),
                                       static_cast<float*>(y), nrhs, ld, s, op->ctas[1]);
@@ -1330,7 +1355,7 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
         auto face = [&] {
             return launch_apply_face_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, op->face32,
                                                   static_cast<const double*>(x), static_cast<double*>(y), nrhs, ld, s,
-                                                  op->ctas[1]);
+                                                  op->ctas[1], vol05);
         };
         auto elem = [&] {
             return launch_apply_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const double*>(x),
@@ -1349,7 +1374,8 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
 }
 
 int tdg_set_apply_config(tdg_op* op, int precision, int family, int ctas_per_sm) {
-    if (!op || (precision != TDG_FP64 && precision != TDG_FP32) || family < 0 || family > 3 || ctas_per_sm < 0)
+    if (!op || (precision != TDG_FP64 && precision != TDG_FP32) || family < 0 || family > 4 || ctas_per_sm < 0 ||
+        (family == 4 && precision != TDG_FP32))
         return fail(TDG_E_INVALID, "bad argument");
     const int pi = precision == TDG_FP64 ? 0 : 1;
     op->family[pi] = family;
@@ -2108,11 +2134,12 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     stats->seconds = ms * 1e-3;
     stats->converged = (!diverged && worst <= rtol) ? 1 : 0;
     if (diverged) return fail(TDG_E_DIVERGED, "non-finite residual in the Krylov iteration");
-    if (op->tgeo.status) {  // a bounded wait of the facet kernel that ran out makes the solve invalid
-        int st = 0;
-        TDG_CUDA_TRY(cudaMemcpy(&st, op->tgeo.status, sizeof st, cudaMemcpyDeviceToHost));
-        if (st) return fail(TDG_E_TIMEOUT, "a bounded wait of the facet kernel ran out");
-    }
+    for (int* word : {op->tgeo.status, op->tc32.status})
+        if (word) {  // a bounded wait of a pipelined kernel that ran out makes the solve invalid
+            int st = 0;
+            TDG_CUDA_TRY(cudaMemcpy(&st, word, sizeof st, cudaMemcpyDeviceToHost));
+            if (st) return fail(TDG_E_TIMEOUT, "a bounded wait of an apply kernel ran out");
+        }
     if (!stats->converged) return fail(TDG_E_DIVERGED, "iteration limit reached before the residual target");
     return 0;
 }

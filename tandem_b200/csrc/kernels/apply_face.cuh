@@ -30,6 +30,8 @@ struct FaceTiles {
     const double* tables = nullptr;  // the face tables of the FP64 tensor kernel, [NF][MF][LDT]
     const int4* tids = nullptr;    // per tile slot [ntiles][TE]: {facet, side-0 element, side-1 element
                                    // (-1 unless mode 1), 0}, facet -1 for unused slots
+    const float* geo = nullptr;    // FP32 kernel: the tiles' facet geometry [tile][field][nq][TE]
+    const double* pen = nullptr;   // FP32 kernel: the tiles' penalties [tile][TE]
     int nftiles = 0;
 };
 
@@ -160,6 +162,123 @@ __device__ __forceinline__ void facet_lift(int mode, const T* n, const T* nu, do
 #pragma unroll
             for (int j = 0; j < D; ++j) bsum += n[j] * sg[uu][j];
             gb[uu] = -wq * bsum;
+        }
+    }
+}
+
+// Lift inputs of both sides of an interior facet point (mode 1; mode 3 passes the element's own
+// data as side 1): the same values facet_lift gives for side 0 (n, u0 own) and side 1 (-n, u1 own),
+// with the averaged stress / flux computed once.  T: the arithmetic (double, or float for the FP32
+// kernels); the penalty times the jump is formed in FP64 and rounded once, as in facet_lift.
+template <class S, typename T = double>
+__device__ __forceinline__ void facet_lift_pair(const T* n, const T* nu, double pen, T wq,
+                                                const T (&u0)[S::Q], const T (&g0)[S::D][S::Q],
+                                                const T (&u1)[S::Q], const T (&g1)[S::D][S::Q],
+                                                const T* G0, const T* G1, const T* c0,
+                                                const T* c1, T (&ga0)[S::D][S::Q], T (&gb0)[S::Q],
+                                                T (&ga1)[S::D][S::Q], T (&gb1)[S::Q]) {
+    constexpr int D = S::D;
+    if constexpr (S::KIND == kPoisson) {
+        const T uh = T(0.5) * (u1[0] - u0[0]);
+        const T pj = static_cast<T>(pen * (static_cast<double>(u0[0]) - static_cast<double>(u1[0])));
+        T bsum = T(0);
+#pragma unroll
+        for (int p = 0; p < D; ++p) {
+            T s = T(0);
+#pragma unroll
+            for (int a = 0; a < D; ++a) s += c0[a * D + p] * g0[a][0] + c1[a * D + p] * g1[a][0];
+            bsum += n[p] * (T(0.5) * s - pj * nu[p]);
+        }
+        gb0[0] = -wq * bsum;
+        gb1[0] = wq * bsum;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            T s0 = 0.0, s1 = T(0);
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                s0 += n[r] * c0[a * D + r];
+                s1 += n[r] * c1[a * D + r];
+            }
+            ga0[a][0] = wq * uh * s0;
+            ga1[a][0] = wq * uh * s1;
+        }
+    } else {
+        const T lam0 = c0[0], mu0 = c0[1], lam1 = c1[0], mu1 = c1[1];
+        T sg[D][D];
+        {
+            T J[D][D];
+#pragma unroll
+            for (int s = 0; s < D; ++s)
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    T acc = T(0);
+#pragma unroll
+                    for (int a = 0; a < D; ++a) acc += G0[a * D + s] * g0[a][r];
+                    J[s][r] = acc;
+                }
+            T d = T(0);
+#pragma unroll
+            for (int r = 0; r < D; ++r) d += J[r][r];
+#pragma unroll
+            for (int i = 0; i < D; ++i)
+#pragma unroll
+                for (int j = 0; j < D; ++j) sg[i][j] = mu0 * (J[i][j] + J[j][i]) + ((i == j) ? lam0 * d : T(0));
+        }
+        {
+            T J[D][D];
+#pragma unroll
+            for (int s = 0; s < D; ++s)
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    T acc = T(0);
+#pragma unroll
+                    for (int a = 0; a < D; ++a) acc += G1[a * D + s] * g1[a][r];
+                    J[s][r] = acc;
+                }
+            T d = T(0);
+#pragma unroll
+            for (int r = 0; r < D; ++r) d += J[r][r];
+#pragma unroll
+            for (int i = 0; i < D; ++i) {
+                const T pj = static_cast<T>(pen * (static_cast<double>(u0[i]) - static_cast<double>(u1[i])));
+#pragma unroll
+                for (int j = 0; j < D; ++j) {
+                    const T s1 = mu1 * (J[i][j] + J[j][i]) + ((i == j) ? lam1 * d : T(0));
+                    sg[i][j] = T(0.5) * (sg[i][j] + s1) - pj * nu[j];
+                }
+            }
+        }
+        T uhm[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) uhm[i] = T(0.5) * (u1[i] - u0[i]);
+        T un = T(0);
+#pragma unroll
+        for (int r = 0; r < D; ++r) un += uhm[r] * n[r];
+#pragma unroll
+        for (int uu = 0; uu < D; ++uu) {
+            T X0[D], X1[D];
+#pragma unroll
+            for (int j = 0; j < D; ++j) {
+                const T sym = uhm[uu] * n[j] + uhm[j] * n[uu];
+                X0[j] = mu0 * sym + ((uu == j) ? lam0 * un : T(0));
+                X1[j] = mu1 * sym + ((uu == j) ? lam1 * un : T(0));
+            }
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                T s0 = 0.0, s1 = T(0);
+#pragma unroll
+                for (int j = 0; j < D; ++j) {
+                    s0 += G0[a * D + j] * X0[j];
+                    s1 += G1[a * D + j] * X1[j];
+                }
+                ga0[a][uu] = wq * s0;
+                ga1[a][uu] = wq * s1;
+            }
+            T bsum = T(0);
+#pragma unroll
+            for (int j = 0; j < D; ++j) bsum += n[j] * sg[uu][j];
+            gb0[uu] = -wq * bsum;
+            gb1[uu] = wq * bsum;
         }
     }
 }

@@ -19,6 +19,7 @@
 #pragma once
 
 #include "apply_face.cuh"
+#include "async.cuh"
 
 namespace tdg {
 
@@ -65,56 +66,6 @@ struct Staged {
     static constexpr int UE = (L::NP + S::Q - 1) / S::Q;           // elements per staged tile
     static constexpr int USZ = UE * LDU;                           // doubles per staged tile
 };
-
-__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-}
-// mbarrier-tracked bulk copies (the bulk-copy engine, untiled): one CTA-scope barrier whose
-// transaction count the copy completes; waits are bounded (a wait that runs out records a status
-// and gives up instead of spinning on).
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-}
-// dst[0, bytes) = src[0, bytes) (bytes a multiple of 16, both 16-byte aligned), completing on bar
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok = 0;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Waits for phase `parity` of bar, at most kMaxWaitTries tries; false when it ran out.
-constexpr int kMaxWaitTries = 1 << 24;
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (int i = 0; i < kMaxWaitTries; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 // C[M x NP] = A[M x K] U for rows [0, mrows), U staged element-major (Staged<S>): as
 // cta_gemm_store with the B fragments read from the staged layout.  Two GEMMs of the same shape
@@ -256,122 +207,6 @@ __host__ __device__ constexpr int vol_fields() {
 template <class S>
 __host__ __device__ constexpr int fct_fields() {
     return 2 * S::D + 2 * S::DD + (S::KIND == kPoisson ? 0 : 4);
-}
-
-// Lift inputs of both sides of an interior facet point (mode 1; mode 3 passes the element's own
-// data as side 1): the same values facet_lift gives for side 0 (n, u0 own) and side 1 (-n, u1 own),
-// with the averaged stress / flux computed once.
-template <class S>
-__device__ __forceinline__ void facet_lift_pair(const double* n, const double* nu, double pen, double wq,
-                                                const double (&u0)[S::Q], const double (&g0)[S::D][S::Q],
-                                                const double (&u1)[S::Q], const double (&g1)[S::D][S::Q],
-                                                const double* G0, const double* G1, const double* c0,
-                                                const double* c1, double (&ga0)[S::D][S::Q], double (&gb0)[S::Q],
-                                                double (&ga1)[S::D][S::Q], double (&gb1)[S::Q]) {
-    constexpr int D = S::D;
-    if constexpr (S::KIND == kPoisson) {
-        const double uh = 0.5 * (u1[0] - u0[0]);
-        const double pj = pen * (u0[0] - u1[0]);
-        double bsum = 0.0;
-#pragma unroll
-        for (int p = 0; p < D; ++p) {
-            double s = 0.0;
-#pragma unroll
-            for (int a = 0; a < D; ++a) s += c0[a * D + p] * g0[a][0] + c1[a * D + p] * g1[a][0];
-            bsum += n[p] * (0.5 * s - pj * nu[p]);
-        }
-        gb0[0] = -wq * bsum;
-        gb1[0] = wq * bsum;
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-            double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-            for (int r = 0; r < D; ++r) {
-                s0 += n[r] * c0[a * D + r];
-                s1 += n[r] * c1[a * D + r];
-            }
-            ga0[a][0] = wq * uh * s0;
-            ga1[a][0] = wq * uh * s1;
-        }
-    } else {
-        const double lam0 = c0[0], mu0 = c0[1], lam1 = c1[0], mu1 = c1[1];
-        double sg[D][D];
-        {
-            double J[D][D];
-#pragma unroll
-            for (int s = 0; s < D; ++s)
-#pragma unroll
-                for (int r = 0; r < D; ++r) {
-                    double acc = 0.0;
-#pragma unroll
-                    for (int a = 0; a < D; ++a) acc += G0[a * D + s] * g0[a][r];
-                    J[s][r] = acc;
-                }
-            double d = 0.0;
-#pragma unroll
-            for (int r = 0; r < D; ++r) d += J[r][r];
-#pragma unroll
-            for (int i = 0; i < D; ++i)
-#pragma unroll
-                for (int j = 0; j < D; ++j) sg[i][j] = mu0 * (J[i][j] + J[j][i]) + ((i == j) ? lam0 * d : 0.0);
-        }
-        {
-            double J[D][D];
-#pragma unroll
-            for (int s = 0; s < D; ++s)
-#pragma unroll
-                for (int r = 0; r < D; ++r) {
-                    double acc = 0.0;
-#pragma unroll
-                    for (int a = 0; a < D; ++a) acc += G1[a * D + s] * g1[a][r];
-                    J[s][r] = acc;
-                }
-            double d = 0.0;
-#pragma unroll
-            for (int r = 0; r < D; ++r) d += J[r][r];
-#pragma unroll
-            for (int i = 0; i < D; ++i) {
-                const double pj = pen * (u0[i] - u1[i]);
-#pragma unroll
-                for (int j = 0; j < D; ++j) {
-                    const double s1 = mu1 * (J[i][j] + J[j][i]) + ((i == j) ? lam1 * d : 0.0);
-                    sg[i][j] = 0.5 * (sg[i][j] + s1) - pj * nu[j];
-                }
-            }
-        }
-        double uhm[D];
-#pragma unroll
-        for (int i = 0; i < D; ++i) uhm[i] = 0.5 * (u1[i] - u0[i]);
-        double un = 0.0;
-#pragma unroll
-        for (int r = 0; r < D; ++r) un += uhm[r] * n[r];
-#pragma unroll
-        for (int uu = 0; uu < D; ++uu) {
-            double X0[D], X1[D];
-#pragma unroll
-            for (int j = 0; j < D; ++j) {
-                const double sym = uhm[uu] * n[j] + uhm[j] * n[uu];
-                X0[j] = mu0 * sym + ((uu == j) ? lam0 * un : 0.0);
-                X1[j] = mu1 * sym + ((uu == j) ? lam1 * un : 0.0);
-            }
-#pragma unroll
-            for (int a = 0; a < D; ++a) {
-                double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-                for (int j = 0; j < D; ++j) {
-                    s0 += G0[a * D + j] * X0[j];
-                    s1 += G1[a * D + j] * X1[j];
-                }
-                ga0[a][uu] = wq * s0;
-                ga1[a][uu] = wq * s1;
-            }
-            double bsum = 0.0;
-#pragma unroll
-            for (int j = 0; j < D; ++j) bsum += n[j] * sg[uu][j];
-            gb0[uu] = -wq * bsum;
-            gb1[uu] = wq * bsum;
-        }
-    }
 }
 
 // ---- volume kernel ----------------------------------------------------------------------------------

@@ -23,7 +23,7 @@ int configure_tcf(K kern, size_t smem, int threads, int& per_sm) {
 
 template <class S, typename TX>
 int run_face_tc32(DevOp<float> const& op, Tc32Tiles const& mt, FaceTiles const& ft, const TX* x, TX* y, int nrhs,
-                  int64_t ld, cudaStream_t s, int ctas) {
+                  int64_t ld, cudaStream_t s, int ctas, bool vol) {
     using L = TcfTile<S>;
     const TcfLayoutV vl = tcf_vol_layout<S>(op.Nq);
     const TcfLayoutF fl = tcf_face_layout<S>(op.nq);
@@ -46,8 +46,10 @@ int run_face_tc32(DevOp<float> const& op, Tc32Tiles const& mt, FaceTiles const& 
     int64_t vg = static_cast<int64_t>(sms) * ((ctas > 0 && ctas < vper) ? ctas : vper);
     if (vg > vwork) vg = vwork;
     if (vg < 1) vg = 1;
-    vk<<<static_cast<unsigned>(vg), L::NT, vsmem, s>>>(op, mt.tables, x, y, ld, nrhs);
-    if (cudaGetLastError() != cudaSuccess) return TDG_E_CUDA;
+    if (vol) {
+        vk<<<static_cast<unsigned>(vg), L::NT, vsmem, s>>>(op, mt.tables, x, y, ld, nrhs);
+        if (cudaGetLastError() != cudaSuccess) return TDG_E_CUDA;
+    }
     if (ft.nftiles > 0) {
         const int64_t fwork = static_cast<int64_t>(ft.nftiles) * nrhs;
         int64_t fg = static_cast<int64_t>(sms) * ((ctas > 0 && ctas < fper) ? ctas : fper);
@@ -62,19 +64,19 @@ int run_face_tc32(DevOp<float> const& op, Tc32Tiles const& mt, FaceTiles const& 
 
 template <int D, int N, typename TX>
 int tcf_kind(int kind, DevOp<float> const& op, Tc32Tiles const& mt, FaceTiles const& ft, const TX* x, TX* y,
-             int nrhs, int64_t ld, cudaStream_t s, int ctas) {
-    if (kind == kPoisson) return run_face_tc32<Shape<D, N, kPoisson>, TX>(op, mt, ft, x, y, nrhs, ld, s, ctas);
-    return run_face_tc32<Shape<D, N, kElasticity>, TX>(op, mt, ft, x, y, nrhs, ld, s, ctas);
+             int nrhs, int64_t ld, cudaStream_t s, int ctas, bool vol) {
+    if (kind == kPoisson) return run_face_tc32<Shape<D, N, kPoisson>, TX>(op, mt, ft, x, y, nrhs, ld, s, ctas, vol);
+    return run_face_tc32<Shape<D, N, kElasticity>, TX>(op, mt, ft, x, y, nrhs, ld, s, ctas, vol);
 }
 
 template <int D, typename TX>
 int tcf_deg(int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, FaceTiles const& ft, const TX* x, TX* y,
-            int nrhs, int64_t ld, cudaStream_t s, int ctas) {
+            int nrhs, int64_t ld, cudaStream_t s, int ctas, bool vol) {
     switch (N) {
-        case 1: return tcf_kind<D, 1, TX>(kind, op, mt, ft, x, y, nrhs, ld, s, ctas);
-        case 2: return tcf_kind<D, 2, TX>(kind, op, mt, ft, x, y, nrhs, ld, s, ctas);
-        case 3: return tcf_kind<D, 3, TX>(kind, op, mt, ft, x, y, nrhs, ld, s, ctas);
-        case 4: return tcf_kind<D, 4, TX>(kind, op, mt, ft, x, y, nrhs, ld, s, ctas);
+        case 1: return tcf_kind<D, 1, TX>(kind, op, mt, ft, x, y, nrhs, ld, s, ctas, vol);
+        case 2: return tcf_kind<D, 2, TX>(kind, op, mt, ft, x, y, nrhs, ld, s, ctas, vol);
+        case 3: return tcf_kind<D, 3, TX>(kind, op, mt, ft, x, y, nrhs, ld, s, ctas, vol);
+        case 4: return tcf_kind<D, 4, TX>(kind, op, mt, ft, x, y, nrhs, ld, s, ctas, vol);
         default: return TDG_E_INVALID;
     }
 }
@@ -83,16 +85,22 @@ int tcf_deg(int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, FaceTi
 
 template <typename TX>
 int launch_apply_face_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, FaceTiles const& ft,
-                           const TX* x, TX* y, int nrhs, int64_t ld, cudaStream_t s, int ctas) {
-    if (nrhs < 1 || !mt.tables) return TDG_E_INVALID;
-    if (D == 2) return tcf_deg<2, TX>(N, kind, op, mt, ft, x, y, nrhs, ld, s, ctas);
-    if (D == 3) return tcf_deg<3, TX>(N, kind, op, mt, ft, x, y, nrhs, ld, s, ctas);
-    return TDG_E_INVALID;
+                           const TX* x, TX* y, int nrhs, int64_t ld, cudaStream_t s, int ctas, bool vol05) {
+    if (nrhs < 1 || !mt.tables || (ft.nftiles > 0 && (!ft.tids || !ft.geo || !ft.pen))) return TDG_E_INVALID;
+    if (D != 2 && D != 3) return TDG_E_INVALID;
+    bool vol = true;  // the mma.sync volume kernel, unless the tcgen05 one took the volume term
+    if (vol05) {
+        const int rc = launch_vol_tc05<TX>(D, N, kind, op, mt, x, y, nrhs, ld, s);
+        if (rc && rc != TDG_E_INVALID) return rc;
+        vol = rc != 0;
+    }
+    if (D == 2) return tcf_deg<2, TX>(N, kind, op, mt, ft, x, y, nrhs, ld, s, ctas, vol);
+    return tcf_deg<3, TX>(N, kind, op, mt, ft, x, y, nrhs, ld, s, ctas, vol);
 }
 
 template int launch_apply_face_tc32<float>(int, int, int, DevOp<float> const&, Tc32Tiles const&, FaceTiles const&,
-                                           const float*, float*, int, int64_t, cudaStream_t, int);
+                                           const float*, float*, int, int64_t, cudaStream_t, int, bool);
 template int launch_apply_face_tc32<double>(int, int, int, DevOp<float> const&, Tc32Tiles const&, FaceTiles const&,
-                                            const double*, double*, int, int64_t, cudaStream_t, int);
+                                            const double*, double*, int, int64_t, cudaStream_t, int, bool);
 
 }  // namespace tdg

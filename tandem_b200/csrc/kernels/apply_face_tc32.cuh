@@ -235,6 +235,7 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     using L = TcfTile<S>;
     constexpr int D = S::D, NBF = S::NBF, Q = S::Q, BS = S::BS, DD = S::DD;
     constexpr int TE = L::TE, NT = L::NT, LDR = L::LDR, LDT = L::LDT, LDU = L::LDU;
+    constexpr int FF = 2 * D + 2 * DD + (S::KIND == kPoisson ? 0 : 4);  // facet geometry fields
     const int nq = op.nq;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TcfLayoutF lay = tcf_face_layout<S>(nq);
@@ -272,17 +273,11 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
             for (int i = tid; i < tab; i += NT) TB[i] = tf[static_cast<int64_t>(l1) * tab + i];
             cur_b = l1;
         }
-        if (tid < TE) {
-            int f = -1, e0 = -1, e1 = -1;
-            if (tid < td.y) {
-                f = ft.fperm[td.x + tid];
-                const int4 fi = ft.finfo[f];
-                e0 = fi.x;
-                e1 = fi.y;
-            }
-            s_f[tid] = f;
-            s_e0[tid] = e0;
-            s_e1[tid] = e1;
+        if (tid < TE) {  // {facet, side-0 element, side-1 element}, facet -1 in unused slots
+            const int4 id = ft.tids[static_cast<int64_t>(tile) * TE + tid];
+            s_f[tid] = id.x;
+            s_e0[tid] = id.y;
+            s_e1[tid] = id.z;
         }
         __syncthreads();
         for (int i = tid; i < L::NP * L::KP; i += NT) {
@@ -326,60 +321,58 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
                     for (int a = 0; a < D; ++a) g1[a][r] = g0[a][r];
                 }
             }
-            float n[D], nu[D], mn[D], mnu[D];
+            const float* gp = ft.geo + static_cast<int64_t>(tile) * FF * nq * TE + it;  // field f at gp[f * fs]
+            const int fs = nq * TE;
+            float n[D], nu[D];
 #pragma unroll
             for (int i = 0; i < D; ++i) {
-                n[i] = op.fN[(static_cast<int64_t>(fct) * D + i) * nq + q];
-                nu[i] = op.fNunit[(static_cast<int64_t>(fct) * D + i) * nq + q];
-                mn[i] = -n[i];
-                mnu[i] = -nu[i];
+                n[i] = gp[i * fs];
+                nu[i] = gp[(D + i) * fs];
             }
-            const double pen = op.penalty[fct];
+            const double pen = ft.pen[static_cast<int64_t>(tile) * TE + te];
             const float wq = op.w[q];
             float Gs0[DD], Gs1[DD], cs0[DD], cs1[DD];
             if constexpr (S::KIND == kPoisson) {
-                const float* kg = op.fCoef + static_cast<int64_t>(fct) * 2 * DD * nq + q;
 #pragma unroll
                 for (int c = 0; c < DD; ++c) {
-                    cs0[c] = kg[(0 * DD + c) * nq];
-                    cs1[c] = kg[(1 * DD + c) * nq];
+                    cs0[c] = gp[(2 * D + c) * fs];
+                    cs1[c] = gp[(2 * D + DD + c) * fs];
                     Gs0[c] = Gs1[c] = 0.0f;
                 }
             } else {
-                const float* gg = op.fG + static_cast<int64_t>(fct) * 2 * DD * nq + q;
 #pragma unroll
                 for (int c = 0; c < DD; ++c) {
-                    Gs0[c] = gg[(0 * DD + c) * nq];
-                    Gs1[c] = gg[(1 * DD + c) * nq];
+                    Gs0[c] = gp[(2 * D + c) * fs];
+                    Gs1[c] = gp[(2 * D + DD + c) * fs];
                 }
-                const float* lm = op.fCoef + static_cast<int64_t>(fct) * 4 * nq + q;
-                cs0[0] = lm[0 * nq];
-                cs0[1] = lm[1 * nq];
-                cs1[0] = lm[2 * nq];
-                cs1[1] = lm[3 * nq];
+                cs0[0] = gp[(2 * D + 2 * DD + 0) * fs];
+                cs0[1] = gp[(2 * D + 2 * DD + 1) * fs];
+                cs1[0] = gp[(2 * D + 2 * DD + 2) * fs];
+                cs1[1] = gp[(2 * D + 2 * DD + 3) * fs];
             }
-            {
-                float ga[D][Q], gb[Q];
-                if (mode == 3)
-                    facet_lift<S, float>(1, n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs0, cs0, cs0, ga, gb);
-                else
-                    facet_lift<S, float>(mode, n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs1, cs0, cs1, ga, gb);
-#pragma unroll
-                for (int r = 0; r < Q; ++r) {
-                    gb0p[r] = gb[r];
-#pragma unroll
-                    for (int a = 0; a < D; ++a) ga0p[a * LDR + r] = ga[a][r];
-                }
-            }
-            if (two) {
+            float ga[D][Q], gb[Q];
+            if (mode == 2) {
+                facet_lift<S, float>(2, n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs1, cs0, cs1, ga, gb);
+            } else {  // both sides' lift inputs from one averaged stress / flux
                 float ha[D][Q], hb[Q];
-                facet_lift<S, float>(1, mn, mnu, pen, wq, u1, g1, u0, g0, Gs1, Gs0, cs1, cs0, ha, hb);
+                if (mode == 3)
+                    facet_lift_pair<S, float>(n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs0, cs0, cs0, ga, gb, ha, hb);
+                else
+                    facet_lift_pair<S, float>(n, nu, pen, wq, u0, g0, u1, g1, Gs0, Gs1, cs0, cs1, ga, gb, ha, hb);
+                if (two) {
 #pragma unroll
-                for (int r = 0; r < Q; ++r) {
-                    gb1p[r] = hb[r];
+                    for (int r = 0; r < Q; ++r) {
+                        gb1p[r] = hb[r];
 #pragma unroll
-                    for (int a = 0; a < D; ++a) ga1p[a * LDR + r] = ha[a][r];
+                        for (int a = 0; a < D; ++a) ga1p[a * LDR + r] = ha[a][r];
+                    }
                 }
+            }
+#pragma unroll
+            for (int r = 0; r < Q; ++r) {
+                gb0p[r] = gb[r];
+#pragma unroll
+                for (int a = 0; a < D; ++a) ga0p[a * LDR + r] = ga[a][r];
             }
         }
         __syncthreads();

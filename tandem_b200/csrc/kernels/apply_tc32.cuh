@@ -110,6 +110,7 @@ struct Tc32Tiles {
     const float* tables = nullptr; // TV then TF[0..NF-1], packed as in shared memory
     int ntiles = 0;
     int table_floats = 0;
+    int* status = nullptr;         // device word: non-zero once a bounded wait of the tcgen05 kernel ran out
 };
 
 // x = hi + lo with hi = x rounded to TF32 (nearest, ties away from zero: add half an ulp of the

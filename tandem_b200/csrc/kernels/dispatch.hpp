@@ -39,9 +39,16 @@ int launch_apply_face2(int D, int N, int kind, DevOp<double> const& op, MmaTiles
 
 // Face-centric FP32 apply (apply_face_tc32.cuh), TX = float or double vectors.
 struct Tc32Tiles;
+// vol05: the volume term on the 5th-generation tensor cores (apply_tc05.cuh) where the shape allows
+// it, else the mma.sync volume kernel.
 template <typename TX>
 int launch_apply_face_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, FaceTiles const& ft,
-                           const TX* x, TX* y, int nrhs, int64_t ld, cudaStream_t s, int ctas = 0);
+                           const TX* x, TX* y, int nrhs, int64_t ld, cudaStream_t s, int ctas = 0, bool vol05 = false);
+// The volume term alone on the 5th-generation tensor cores (stores y); TDG_E_INVALID when the
+// shape does not fit (more than 64 volume points).
+template <typename TX>
+int launch_vol_tc05(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y,
+                    int nrhs, int64_t ld, cudaStream_t s);
 
 // FP32 apply on the tensor cores in the 3xTF32 form (apply_tc32.cuh); TDG_E_INVALID when the
 // shape's shared-memory layout does not fit (the caller then uses the SIMT kernel).

@@ -19,7 +19,7 @@ from .mesh import SimplexMesh
 
 POISSON, ELASTICITY = _ffi.TDG_POISSON, _ffi.TDG_ELASTICITY
 FP64, FP32, MIXED = _ffi.TDG_FP64, _ffi.TDG_FP32, _ffi.TDG_MIXED
-FAMILIES = ("tensor", "simt", "face", "face2")
+FAMILIES = ("tensor", "simt", "face", "face2", "tc05")
 MG_STRATEGIES = ("twolevel", "logarithmic", "full")  # MGStrategy (app/common/MGConfig.h:8)
 PRECONDITIONERS = ("bjacobi", "mg")
 MG_COARSE_SPACES = ("dg", "p1")
@@ -184,7 +184,8 @@ class DGOperator:
 
     def set_apply_config(self, precision: int, family: str, ctas_per_sm: int = 0) -> None:
         """Selects the apply kernel explicitly: family "tensor" (element-centric tensor cores),
-        "face" (face-centric), "face2" (face-centric, software-pipelined; FP64) or "simt";
+        "face" (face-centric), "face2" (face-centric, software-pipelined; FP64), "tc05" (FP32:
+        face-centric with the volume term on tcgen05) or "simt";
         ctas_per_sm 0 = the default occupancy."""
         _ffi.check(_ffi.lib().tdg_set_apply_config(self._h, precision, FAMILIES.index(family), ctas_per_sm))
 

@@ -305,14 +305,16 @@ def test_face_centric_multi_rhs_and_solve(family):
         assert torch.all(Y[r, op.ndof:] == 7.0)
 
 
-@pytest.mark.parametrize("case", CASES[::2], ids=lambda c: "k{}d{}n{}p{}c{}v{}".format(*c))
-def test_apply_face_centric_fp32_and_mixed(case):
-    """Face-centric FP32 kernels (3xTF32) on FP32 and on FP64 vectors (mixed) against the oracle to
-    FP32 accuracy (2e-5, as the element-centric FP32 apply)."""
+@pytest.mark.parametrize("family", ["face", "tc05"])
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "k{}d{}n{}p{}c{}v{}".format(*c))
+def test_apply_face_centric_fp32_and_mixed(case, family):
+    """Face-centric FP32 kernels (3xTF32; family tc05 with the volume term on tcgen05.mma and
+    tensor memory) on FP32 and on FP64 vectors (mixed) against the oracle to FP32 accuracy (2e-5,
+    as the element-centric FP32 apply)."""
     from tandem_b200.operator import MIXED
     kind, dim, n, N, curved, var = case
     _, op, orc = product_and_oracle(kind, dim, n, N, curved, var)
-    op.set_apply_config(FP32, "face")
+    op.set_apply_config(FP32, family)
     x = np.random.default_rng(12).standard_normal(op.ndof)
     xr = x.astype(np.float32).astype(np.float64)
     ref = orc.apply(xr)

@@ -4,7 +4,8 @@ None (the element as its own neighbour), interior Fault (skeleton flux) and inte
 crack: no flux), see cases.mixed_bc_codes.
 
 Every kernel family is pinned separately (set_apply_config): the face-centric tensor-core pair
-(and its software-pipelined form, FP64), the element-centric tensor-core kernel and the SIMT kernel.  Tolerances: FP64 1e-12 relative
+(and its software-pipelined form, FP64; with the volume term on tcgen05, FP32), the element-centric
+tensor-core kernel and the SIMT kernel.  Tolerances: FP64 1e-12 relative
 (max-norm over the vector; summation order differs), FP32 and mixed (FP32 arithmetic on FP64
 vectors) 2e-5 relative in the 2-norm."""
 import numpy as np
@@ -57,7 +58,7 @@ def test_apply_fp64_mixed_bc(case, family):
     assert rel_max(y.cpu().numpy(), ref) < 1e-12
 
 
-@pytest.mark.parametrize("family", ["face", "tensor", "simt"])
+@pytest.mark.parametrize("family", ["face", "tc05", "tensor", "simt"])
 def test_apply_fp32_mixed_bc(case, family):
     op, orc, x, _ = case
     op.set_apply_config(FP32, family)
@@ -68,7 +69,7 @@ def test_apply_fp32_mixed_bc(case, family):
     assert rel_2(y.cpu().numpy().astype(np.float64), ref) < 2e-5
 
 
-@pytest.mark.parametrize("family", ["face", "tensor"])
+@pytest.mark.parametrize("family", ["face", "tc05", "tensor"])
 def test_apply_mixed_precision_mixed_bc(case, family):
     op, orc, x, ref = case
     op.set_apply_config(FP32, family)
