@@ -189,11 +189,12 @@ int tdg_probe_fp64_peak(int kind, int ctas_per_sm, void* stream, double* tflops)
 /* Known-answer check of the 5th-generation tensor-core path of the FP32 operator (no counterpart in
  * tandem): D[128 x n] = A[128 x k] B[n x k]^T on device row-major FP32 operands through tcgen05.mma
  * kind::tf32 with the accumulator in tensor memory, in three TF32 products (hi hi + hi lo + lo hi)
- * when split3 != 0, else one; A and B staged K-major (a_mn / b_mn = 0) or MN-major (!= 0) in shared
- * memory.  n a multiple of 16 in [16, 256], k a multiple of 8 in [8, 64].  Synchronises `stream`;
- * TDG_E_TIMEOUT when the MMA's completion was not seen within the bounded wait. */
-int tdg_probe_tc05_gemm(const float* A, const float* B, float* D, int n, int k, int split3, int a_mn, int b_mn,
-                        void* stream);
+ * when split3 = 1, one when 0; both operands K-major in shared memory (core matrices of 8 rows x
+ * 16 bytes).  n a multiple of 16 in [16, 256], k a multiple of 8 in [8, 64].  Synchronises `stream`;
+ * TDG_E_TIMEOUT when the MMA's completion was not seen within the bounded wait (about 2 s of wall
+ * clock); split3 = -1 issues no MMA and no commit, so that the wait runs out and the error path
+ * (status word, tensor memory freed, TDG_E_TIMEOUT) can be tested. */
+int tdg_probe_tc05_gemm(const float* A, const float* B, float* D, int n, int k, int split3, void* stream);
 
 /* --- right-hand side (DGOperator::rhs, src/form/DGOperator.h:189-237) ---------------------- */
 

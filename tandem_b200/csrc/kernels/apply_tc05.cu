@@ -9,12 +9,15 @@ namespace tdg {
 
 namespace {
 
+// The warp-specialised form (vol_tc05p_kernel) or one tile at a time (vol_tc05_kernel).
+constexpr bool kTc05Pipelined = false;
+
 template <class S, typename TX>
 int run_vol_tc05(DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y, int nrhs, int64_t ld,
                  cudaStream_t s) {
     using L = Tc05Vol<S>;
     if (op.Nq > L::NQ || op.Nq < 1 || !mt.tables) return TDG_E_INVALID;
-    auto k = vol_tc05_kernel<S, TX>;
+    auto k = kTc05Pipelined ? vol_tc05p_kernel<S, TX> : vol_tc05_kernel<S, TX>;
     static bool conf = false;
     if (!conf) {
         int dev = 0, optin = 0;
@@ -29,7 +32,8 @@ int run_vol_tc05(DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y
     int64_t grid = device_sm_count();  // one CTA per SM: the shared memory and half the tensor memory
     if (grid > nwork) grid = nwork;
     if (grid < 1) return 0;
-    k<<<static_cast<unsigned>(grid), L::NT, L::BYTES, s>>>(op, mt.tables, TcfTile<S>::LDT, x, y, ld, nrhs, mt.status);
+    k<<<static_cast<unsigned>(grid), kTc05Pipelined ? 288 : 256, L::BYTES, s>>>(op, mt.tables, TcfTile<S>::LDT, x, y, ld,
+                                                                                 nrhs, mt.status);
     return cudaGetLastError() == cudaSuccess ? 0 : TDG_E_CUDA;
 }
 

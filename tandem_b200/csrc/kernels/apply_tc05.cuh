@@ -12,17 +12,18 @@
 //  3. pointwise: the warps that own lanes 0..63 (warps 0, 1, 4, 5: lane q, half of the tile's
 //     elements each) read R_a[q][(r, te)] with 32x32b loads, form the stress / flux with the point's
 //     J^-1 and coefficients (read coalesced over q from [E][field][Nq]) and write S[(r, te)][(a, q)]
-//     (MN-major, one 16-byte store per 4 elements) split hi / lo;
+//     split hi / lo;
 //  4. backward: Y[k][n] = sum_(a, q) D_a[q][k] S[n][(a, q)] into TMEM (M = 128 lanes = basis k,
-//     K = D * 64; the table read MN-major through a second descriptor over the same copy);
+//     K = D * 64);
 //  5. y: lanes k < NBF store y[e BS + k + NBF r] (32 consecutive k per warp store).
 //
-// The table D_a[q][k] lives once per CTA in shared memory as core matrices [k/4][a][q/8][8 q][4 k]
-// (hi and lo copies), read K-major by the forward MMA (rows q: SBO 128 bytes, K chunks: LBO D KB)
-// and MN-major by the backward MMA (rows k in groups of 4: SBO D KB, K groups (a, q/8): LBO 128
-// bytes).  Rows of an M = 128 operand past the stored ones read other shared memory; they only
-// produce accumulator rows that are never read, and the buffer is sized so that every such read
-// stays inside it.
+// Every operand is K-major in core matrices (tc05.cuh).  The table D_a[q][k] is held twice per CTA
+// (hi and lo each): [k/4][a][q/8][8 q][4 k] for the forward MMA (rows q: SBO 128 bytes, K chunks:
+// LBO D KB) and [(a, q)/4][k/8][8 k][4 (a, q)] for the backward one.  S's K chunks are 16 bytes
+// further apart than its rows need, so that the pointwise phase's stores (32 consecutive q of one
+// column per warp) fall on 32 distinct banks.  Rows of an M = 128 operand past the stored ones read
+// the following shared memory; they only produce accumulator rows that are never read, and the
+// buffer extends past every such read.
 #pragma once
 
 #include "apply_face.cuh"
@@ -40,16 +41,18 @@ struct Tc05Vol {
     static constexpr int NQ = 64;                    // quadrature points per direction block
     static constexpr int KB = D * NQ;                // backward K: (a, q)
     static constexpr int NT = 256;
-    static constexpr int KCS = D * NQ * 16;          // bytes between K chunks of the table
-    static constexpr int TAB = KC * KCS;             // bytes of one table copy
+    static constexpr int KCS = D * NQ * 16;          // bytes between K chunks of the forward table
+    static constexpr int TAB = KC * KCS;             // bytes of one forward table copy
+    static constexpr int LBO_B = (KF / 8) * 128;     // bytes between K chunks of the backward table
+    static constexpr int TABB = (KB / 4) * LBO_B;    // bytes of one backward table copy
     static constexpr int UB = NCOL * KF * 4;         // bytes of one U copy
-    static constexpr int SB = NCOL * KB * 4;         // bytes of one S copy
-    static constexpr int OFF_TL = TAB, OFF_UH = 2 * TAB, OFF_UL = OFF_UH + UB, OFF_SH = OFF_UL + UB,
-                         OFF_SL = OFF_SH + SB, END = OFF_SL + SB;
-    // last byte the backward MMA's 32 m-groups can reach from the lo table, plus the forward's
-    // 16 q-groups past the last block
-    static constexpr int REACH = OFF_TL + 32 * KCS + 2048;
-    static constexpr int BYTES = (END > REACH ? END : REACH) + 1024;  // + alignment
+    static constexpr int SCS = (NCOL / 8) * 128 + 16;  // bytes between K chunks of S (padded)
+    static constexpr int SB = (KB / 4) * SCS;        // bytes of one S copy
+    static constexpr int OFF_AFL = TAB, OFF_ABH = 2 * TAB, OFF_ABL = OFF_ABH + TABB, OFF_UH = OFF_ABL + TABB,
+                         OFF_UL = OFF_UH + UB, OFF_SH = OFF_UL + UB, OFF_SL = OFF_SH + SB, END = OFF_SL + SB;
+    // + reads of M = 128 operands past their stored rows (at most 16 row groups past a chunk),
+    // + alignment of the base
+    static constexpr int BYTES = END + 2048 + 1024;
     static constexpr int COLS_USED = (D + 1) * NCOL;
     static constexpr int TCOLS = COLS_USED <= 32 ? 32 : COLS_USED <= 64 ? 64 : COLS_USED <= 128 ? 128 : 256;
     static_assert(NCOL % 16 == 0 && NCOL <= 256, "M = 128 MMAs need N a multiple of 16");
@@ -128,45 +131,208 @@ __device__ __forceinline__ void vol_point(const float (&G)[S::DD], float c0, flo
     }
 }
 
-// tv: the FP32 volume table of the tensor kernels, row (q D + a), ld = ldt, columns k < NBF.
-template <class S, typename TX>
-__global__ void __launch_bounds__(256, 1)
-    vol_tc05_kernel(DevOp<float> op, const float* __restrict__ tv, int ldt, const TX* __restrict__ x,
-                    TX* __restrict__ y, int64_t ld, int nrhs, int* status) {
+// Shared-memory buffers of one CTA (Tc05Vol offsets from a 1024-byte aligned base).
+struct Tc05Smem {
+    float *Th, *Tl, *Bh, *Bl, *Uh, *Ul, *Sh, *Sl;
+};
+template <class S>
+__device__ __forceinline__ Tc05Smem tc05_smem(unsigned char* raw_base) {
     using L = Tc05Vol<S>;
-    constexpr int D = S::D, Q = S::Q, NBF = S::NBF, BS = S::BS, DD = S::DD;
-    constexpr int TE = L::TE, NCOL = L::NCOL, KF = L::KF, KC = L::KC, NQ = L::NQ, NT = L::NT;
-    const int Nq = op.Nq;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ unsigned long long bar;
-    __shared__ uint32_t tbase;
-    const uint32_t raw = smem_u32(smem_raw);
-    unsigned char* base = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
-    float* Th = reinterpret_cast<float*>(base);
-    float* Tl = reinterpret_cast<float*>(base + L::OFF_TL);
-    float* Uh = reinterpret_cast<float*>(base + L::OFF_UH);
-    float* Ul = reinterpret_cast<float*>(base + L::OFF_UL);
-    float* Sh = reinterpret_cast<float*>(base + L::OFF_SH);
-    float* Sl = reinterpret_cast<float*>(base + L::OFF_SL);
-    if (warp == 0) {
-        tmem_alloc(&tbase, L::TCOLS);
-        tmem_relinquish();
-    }
-    if (tid == 0) mbar_init(&bar, 1);
-    // the table D_a[q][k] as core matrices [k/4][a][q/8][8][4], zero past Nq and NBF
-    for (int i = tid; i < KC * D * NQ * 4; i += NT) {
+    const uint32_t raw = smem_u32(raw_base);
+    unsigned char* b = raw_base + ((1024u - (raw & 1023u)) & 1023u);
+    return {reinterpret_cast<float*>(b), reinterpret_cast<float*>(b + L::OFF_AFL),
+            reinterpret_cast<float*>(b + L::OFF_ABH), reinterpret_cast<float*>(b + L::OFF_ABL),
+            reinterpret_cast<float*>(b + L::OFF_UH), reinterpret_cast<float*>(b + L::OFF_UL),
+            reinterpret_cast<float*>(b + L::OFF_SH), reinterpret_cast<float*>(b + L::OFF_SL)};
+}
+
+// Both table copies (hi / lo split) from the FP32 volume table tv (row q D + a, ld ldt), zero past
+// Nq and NBF, and S zeroed (rows past Nq stay zero); threads t0, t0 + nt, ...
+template <class S>
+__device__ void tc05_init(Tc05Smem const& b, const float* __restrict__ tv, int ldt, int Nq, int t0, int nt) {
+    using L = Tc05Vol<S>;
+    constexpr int D = S::D, NBF = S::NBF, KF = L::KF, KC = L::KC, NQ = L::NQ;
+    // forward: core matrices [k/4][a][q/8][8 q][4 k]
+    for (int i = t0; i < KC * D * NQ * 4; i += nt) {
         const int kk = i & 3, qq = (i >> 2) & 7, rest = i >> 5;  // rest = (kc * D + a) * 8 + qg
         const int qg = rest & 7, a = (rest >> 3) % D, kc = (rest >> 3) / D;
         const int q = qg * 8 + qq, k = kc * 4 + kk;
         const float v = (q < Nq && k < NBF) ? tv[static_cast<int64_t>(q * D + a) * ldt + k] : 0.0f;
         float h, l;
         split_tf32(v, h, l);
-        Th[i] = h;
-        Tl[i] = l;
+        b.Th[i] = h;
+        b.Tl[i] = l;
     }
-    // S starts (and stays, past Nq) zero
-    for (int i = tid; i < 2 * NCOL * L::KB; i += NT) Sh[i] = 0.0f;  // Sh and Sl are adjacent
+    // backward: element (k, (a, q)) of the K-major [k][(a, q)] operand
+    for (int i = t0; i < KF * L::KB; i += nt) {
+        const int k = i % KF, kk = i / KF, a = kk / NQ, q = kk % NQ;
+        const float v = (q < Nq && k < NBF) ? tv[static_cast<int64_t>(q * D + a) * ldt + k] : 0.0f;
+        float h, l;
+        split_tf32(v, h, l);
+        const int o = (kk >> 2) * (L::LBO_B / 4) + (k >> 3) * 32 + (k & 7) * 4 + (kk & 3);
+        b.Bh[o] = h;
+        b.Bl[o] = l;
+    }
+    for (int i = t0; i < 2 * L::SB / 4; i += nt) b.Sh[i] = 0.0f;  // Sh and Sl are adjacent
+}
+
+// U hi / lo of the tile at element e0: one 16-byte K chunk of one column per item, columns fastest;
+// items t0, t0 + nt, ...
+template <class S, typename TX>
+__device__ __forceinline__ void tc05_stage(Tc05Smem const& b, const TX* __restrict__ xr, int64_t e0, int64_t E,
+                                           int t0, int nt) {
+    using L = Tc05Vol<S>;
+    constexpr int NBF = S::NBF, BS = S::BS, TE = L::TE, NCOL = L::NCOL, KC = L::KC;
+    for (int i = t0; i < NCOL * KC; i += nt) {
+        const int n = i % NCOL, kc = i / NCOL;
+        const int r = n / TE, te = n % TE;
+        const int64_t e = e0 + te;
+        float h[4], l[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k = kc * 4 + j;
+            const float v = (e < E && k < NBF) ? static_cast<float>(xr[e * BS + k + NBF * r]) : 0.0f;
+            split_tf32(v, h[j], l[j]);
+        }
+        const int o = core_offset(NCOL, n, kc * 4);
+        *reinterpret_cast<float4*>(b.Uh + o) = make_float4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<float4*>(b.Ul + o) = make_float4(l[0], l[1], l[2], l[3]);
+    }
+}
+
+// Forward MMAs (one thread): R_a = D_a U^T into TMEM columns a * NCOL, 3xTF32.
+template <class S>
+__device__ __forceinline__ void tc05_issue_fwd(Tc05Smem const& b, uint32_t tmem) {
+    using L = Tc05Vol<S>;
+    constexpr int NCOL = L::NCOL;
+    const uint32_t idf = idesc_tf32(128, NCOL);
+    const uint32_t th = smem_u32(b.Th), tl = smem_u32(b.Tl), uh = smem_u32(b.Uh), ul = smem_u32(b.Ul);
+    constexpr uint32_t lboU = (NCOL / 8) * 128;
+#pragma unroll 1
+    for (int a = 0; a < S::D; ++a)
+#pragma unroll 1
+        for (int s = 0; s < L::KF / 8; ++s) {
+            const uint32_t ot = 2u * s * L::KCS + a * 1024u, ou = 2u * s * lboU;
+            const uint64_t ah = umma_desc(th + ot, L::KCS, 128), al = umma_desc(tl + ot, L::KCS, 128);
+            const uint64_t bh = umma_desc(uh + ou, lboU, 128), bl = umma_desc(ul + ou, lboU, 128);
+            const uint32_t d = tmem + static_cast<uint32_t>(a * NCOL);
+            umma_tf32(d, ah, bh, idf, s > 0 ? 1u : 0u);
+            umma_tf32(d, ah, bl, idf, 1u);
+            umma_tf32(d, al, bh, idf, 1u);
+        }
+}
+
+// Backward MMAs (one thread): Y = D^T S^T into TMEM columns D * NCOL, 3xTF32.
+template <class S>
+__device__ __forceinline__ void tc05_issue_bwd(Tc05Smem const& b, uint32_t tmem) {
+    using L = Tc05Vol<S>;
+    constexpr int NCOL = L::NCOL;
+    const uint32_t idb = idesc_tf32(128, NCOL);
+    const uint32_t bh0 = smem_u32(b.Bh), bl0 = smem_u32(b.Bl), sh = smem_u32(b.Sh), sl = smem_u32(b.Sl);
+    const uint32_t d = tmem + static_cast<uint32_t>(S::D * NCOL);
+#pragma unroll 1
+    for (int s = 0; s < S::D * L::NQ / 8; ++s) {
+        const uint32_t ob = 2u * s * L::LBO_B, os = 2u * s * L::SCS;
+        const uint64_t ah = umma_desc(bh0 + ob, L::LBO_B, 128), al = umma_desc(bl0 + ob, L::LBO_B, 128);
+        const uint64_t bh = umma_desc(sh + os, L::SCS, 128), bl = umma_desc(sl + os, L::SCS, 128);
+        umma_tf32(d, ah, bh, idb, s > 0 ? 1u : 0u);
+        umma_tf32(d, ah, bl, idb, 1u);
+        umma_tf32(d, al, bh, idb, 1u);
+    }
+}
+
+// Pointwise flux of the elements te0 .. te0 + NE - 1 at the thread's point q (a lane of 0..63) from
+// R[a][r][j], written to S split hi / lo; zero past Nq and past E.
+template <class S, int NE>
+__device__ __forceinline__ void tc05_pointwise(Tc05Smem const& b, DevOp<float> const& op, int q, int64_t e0, int te0,
+                                               const float (&R)[S::D][S::Q][NE]) {
+    using L = Tc05Vol<S>;
+    constexpr int D = S::D, Q = S::Q, DD = S::DD, TE = L::TE, NQ = L::NQ;
+    const int Nq = op.Nq;
+#pragma unroll
+    for (int j = 0; j < NE; ++j) {
+        const int64_t e = e0 + te0 + j;
+        float T[D][Q];
+        if (q < Nq && e < op.E) {
+            float G[DD], g[D][Q];
+            const float* vg = op.vG + e * DD * Nq + q;
+#pragma unroll
+            for (int c = 0; c < DD; ++c) G[c] = vg[c * Nq];
+            float c0, c1 = 0.0f;
+            if constexpr (S::KIND == kPoisson) {
+                c0 = op.vCoef[e * Nq + q];
+            } else {
+                c0 = op.vCoef[(e * 2 + 0) * Nq + q];
+                c1 = op.vCoef[(e * 2 + 1) * Nq + q];
+            }
+#pragma unroll
+            for (int a = 0; a < D; ++a)
+#pragma unroll
+                for (int r = 0; r < Q; ++r) g[a][r] = R[a][r][j];
+            vol_point<S>(G, c0, c1, g, T);
+        } else {
+#pragma unroll
+            for (int a = 0; a < D; ++a)
+#pragma unroll
+                for (int r = 0; r < Q; ++r) T[a][r] = 0.0f;
+        }
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            const int kk = a * NQ + q;
+            const int ob = (kk >> 2) * (L::SCS / 4) + (kk & 3);
+#pragma unroll
+            for (int r = 0; r < Q; ++r) {
+                const int n = r * TE + te0 + j;
+                float h, l;
+                split_tf32(T[a][r], h, l);
+                b.Sh[ob + (n >> 3) * 32 + (n & 7) * 4] = h;
+                b.Sl[ob + (n >> 3) * 32 + (n & 7) * 4] = l;
+            }
+        }
+    }
+}
+
+// y of the tile's elements half * 8 .. half * 8 + 7 from the backward accumulator (warp-collective;
+// lanes k < NBF store).
+template <class S, typename TX>
+__device__ __forceinline__ void tc05_store_y(uint32_t tmem, uint32_t lane_base, int k, int half, int64_t e0, int64_t E,
+                                             TX* __restrict__ yr) {
+    using L = Tc05Vol<S>;
+    constexpr int Q = S::Q, NBF = S::NBF, BS = S::BS, TE = L::TE, NCOL = L::NCOL;
+#pragma unroll
+    for (int r = 0; r < Q; ++r) {
+        float v[8];
+        tmem_ld8(tmem + lane_base + static_cast<uint32_t>(S::D * NCOL + r * TE + half * 8), v);
+        tmem_wait_ld();
+        if (k < NBF) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int64_t e = e0 + half * 8 + j;
+                if (e < E) yr[e * BS + k + NBF * r] = static_cast<TX>(v[j]);
+            }
+        }
+    }
+}
+
+// One tile at a time, every phase by the whole CTA (256 threads): stage, forward, pointwise
+// (warps owning lanes 0..63), backward, store.  tv: the FP32 volume table, row (q D + a), ld ldt.
+template <class S, typename TX>
+__global__ void __launch_bounds__(256, 1)
+    vol_tc05_kernel(DevOp<float> op, const float* __restrict__ tv, int ldt, const TX* __restrict__ x,
+                    TX* __restrict__ y, int64_t ld, int nrhs, int* status) {
+    using L = Tc05Vol<S>;
+    constexpr int D = S::D, Q = S::Q, TE = L::TE, NCOL = L::NCOL, NT = 256;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned long long bar;
+    __shared__ uint32_t tbase;
+    const Tc05Smem b = tc05_smem<S>(smem_raw);
+    if (warp == 0) {
+        tmem_alloc(&tbase, L::TCOLS);
+        tmem_relinquish();
+    }
+    if (tid == 0) mbar_init(&bar, 1);
+    tc05_init<S>(b, tv, ldt, op.Nq, tid, NT);
     fence_async_smem();
     tc05_fence_before();
     __syncthreads();
@@ -180,53 +346,21 @@ __global__ void __launch_bounds__(256, 1)
     unsigned phase = 0;
     bool ok = true;
     for (int64_t work = blockIdx.x; work < nwork && ok; work += gridDim.x) {
-        const int tile = static_cast<int>(work % ntiles);
+        const int64_t e0 = static_cast<int64_t>(work % ntiles) * TE;
         const TX* xr = x + (work / ntiles) * ld;
         TX* yr = y + (work / ntiles) * ld;
-        const int64_t e0 = static_cast<int64_t>(tile) * TE;
-        // 1. U hi / lo: one 16-byte K chunk of one column per item, columns fastest
-        for (int i = tid; i < NCOL * KC; i += NT) {
-            const int n = i % NCOL, kc = i / NCOL;
-            const int r = n / TE, te = n % TE;
-            const int64_t e = e0 + te;
-            float v[4], h[4], l[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int k = kc * 4 + j;
-                v[j] = (e < op.E && k < NBF) ? static_cast<float>(xr[e * BS + k + NBF * r]) : 0.0f;
-                split_tf32(v[j], h[j], l[j]);
-            }
-            const int o = core_offset(NCOL, n, kc * 4);
-            *reinterpret_cast<float4*>(Uh + o) = make_float4(h[0], h[1], h[2], h[3]);
-            *reinterpret_cast<float4*>(Ul + o) = make_float4(l[0], l[1], l[2], l[3]);
-        }
+        tc05_stage<S, TX>(b, xr, e0, op.E, tid, NT);
         fence_async_smem();
         tc05_fence_before();
         __syncthreads();
         tc05_fence_after();
-        // 2. forward MMAs
         if (tid == 0) {
-            const uint32_t idf = idesc_tf32(128, NCOL);
-            const uint32_t th = smem_u32(Th), tl = smem_u32(Tl), uh = smem_u32(Uh), ul = smem_u32(Ul);
-            constexpr uint32_t lboU = (NCOL / 8) * 128;
-#pragma unroll 1
-            for (int a = 0; a < D; ++a)
-#pragma unroll 1
-                for (int s = 0; s < KF / 8; ++s) {
-                    const uint32_t ot = 2u * s * L::KCS + a * 1024u, ou = 2u * s * lboU;
-                    const uint64_t ah = umma_desc(th + ot, L::KCS, 128), al = umma_desc(tl + ot, L::KCS, 128);
-                    const uint64_t bh = umma_desc(uh + ou, lboU, 128), bl = umma_desc(ul + ou, lboU, 128);
-                    const uint32_t d = tmem + static_cast<uint32_t>(a * NCOL);
-                    umma_tf32(d, ah, bh, idf, s > 0 ? 1u : 0u);
-                    umma_tf32(d, ah, bl, idf, 1u);
-                    umma_tf32(d, al, bh, idf, 1u);
-                }
+            tc05_issue_fwd<S>(b, tmem);
             umma_commit(&bar);
         }
         ok = __syncthreads_and(mbar_wait_bounded(&bar, phase) ? 1 : 0) != 0;  // block-uniform
         phase ^= 1u;
         tc05_fence_after();
-        // 3. pointwise (warps owning lanes 0..63); lanes past Nq and elements past E give zero S
         if (ok && pw) {
             const int q = 32 * (warp & 3) + lane;
 #pragma unroll 1
@@ -239,70 +373,15 @@ __global__ void __launch_bounds__(256, 1)
                     for (int r = 0; r < Q; ++r)
                         tmem_ld4(tmem + lane_base + static_cast<uint32_t>(a * NCOL + r * TE + te0), R[a][r]);
                 tmem_wait_ld();
-                float T[D][Q][4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int64_t e = e0 + te0 + j;
-                    float Tj[D][Q];
-                    if (q < Nq && e < op.E) {
-                        float G[DD], g[D][Q];
-                        const float* vg = op.vG + e * DD * Nq + q;
-#pragma unroll
-                        for (int c = 0; c < DD; ++c) G[c] = vg[c * Nq];
-                        float c0, c1 = 0.0f;
-                        if constexpr (S::KIND == kPoisson) {
-                            c0 = op.vCoef[e * Nq + q];
-                        } else {
-                            c0 = op.vCoef[(e * 2 + 0) * Nq + q];
-                            c1 = op.vCoef[(e * 2 + 1) * Nq + q];
-                        }
-#pragma unroll
-                        for (int a = 0; a < D; ++a)
-#pragma unroll
-                            for (int r = 0; r < Q; ++r) g[a][r] = R[a][r][j];
-                        vol_point<S>(G, c0, c1, g, Tj);
-                    } else {
-#pragma unroll
-                        for (int a = 0; a < D; ++a)
-#pragma unroll
-                            for (int r = 0; r < Q; ++r) Tj[a][r] = 0.0f;
-                    }
-#pragma unroll
-                    for (int a = 0; a < D; ++a)
-#pragma unroll
-                        for (int r = 0; r < Q; ++r) T[a][r][j] = Tj[a][r];
-                }
-#pragma unroll
-                for (int a = 0; a < D; ++a)
-#pragma unroll
-                    for (int r = 0; r < Q; ++r) {
-                        const int o = core_offset_mn(NCOL, r * TE + te0, a * NQ + q);
-                        float h[4], l[4];
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) split_tf32(T[a][r][j], h[j], l[j]);
-                        *reinterpret_cast<float4*>(Sh + o) = make_float4(h[0], h[1], h[2], h[3]);
-                        *reinterpret_cast<float4*>(Sl + o) = make_float4(l[0], l[1], l[2], l[3]);
-                    }
+                tc05_pointwise<S, 4>(b, op, q, e0, te0, R);
             }
         }
         fence_async_smem();
         tc05_fence_before();
         __syncthreads();
         tc05_fence_after();
-        // 4. backward MMAs: the table read MN-major (rows k), S MN-major
         if (ok && tid == 0) {
-            const uint32_t idb = idesc_tf32(128, NCOL, true, true);
-            const uint32_t th = smem_u32(Th), tl = smem_u32(Tl), sh = smem_u32(Sh), sl = smem_u32(Sl);
-            constexpr uint32_t lboS = (NCOL / 4) * 128;
-            const uint32_t d = tmem + static_cast<uint32_t>(D * NCOL);
-#pragma unroll 1
-            for (int s = 0; s < D * NQ / 8; ++s) {
-                const uint64_t ah = umma_desc(th + 128u * s, 128, L::KCS), al = umma_desc(tl + 128u * s, 128, L::KCS);
-                const uint64_t bh = umma_desc(sh + lboS * s, lboS, 128), bl = umma_desc(sl + lboS * s, lboS, 128);
-                umma_tf32(d, ah, bh, idb, s > 0 ? 1u : 0u);
-                umma_tf32(d, ah, bl, idb, 1u);
-                umma_tf32(d, al, bh, idb, 1u);
-            }
+            tc05_issue_bwd<S>(b, tmem);
             umma_commit(&bar);
         }
         if (ok) {
@@ -310,27 +389,124 @@ __global__ void __launch_bounds__(256, 1)
             phase ^= 1u;
         }
         tc05_fence_after();
-        // 5. y = Y (lanes k < NBF; each half of the warps stores half of the tile's elements)
-        if (ok && pw) {
-            const int k = 32 * (warp & 3) + lane;
-#pragma unroll
-            for (int r = 0; r < Q; ++r) {
-                float v[8];
-                tmem_ld8(tmem + lane_base + static_cast<uint32_t>(D * NCOL + r * TE + half * 8), v);
-                tmem_wait_ld();
-                if (k < NBF) {
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const int64_t e = e0 + half * 8 + j;
-                        if (e < op.E) yr[e * BS + k + NBF * r] = static_cast<TX>(v[j]);
-                    }
-                }
-            }
-        }
+        if (ok && pw) tc05_store_y<S, TX>(tmem, lane_base, 32 * (warp & 3) + lane, half, e0, op.E, yr);
         tc05_fence_before();
         __syncthreads();
     }
     if (!ok && tid == 0 && status) atomicExch(status, 1);
+    tc05_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, L::TCOLS);
+}
+
+// Warp-specialised form (288 threads): warps 0, 1, 4, 5 own TMEM lanes 0..63 and run the pointwise
+// flux and the stores of y; warps 2, 3, 6, 7 stage the next tile's U as soon as the forward MMAs of
+// the current one have read theirs; warp 8 (one thread) issues the MMAs.  Five mbarriers, one phase
+// per tile each: U staged (128 arrivals), forward done (commit), R read (128), S written (128),
+// backward done (commit).  So the staging of tile i + 1 and its forward MMAs overlap the pointwise
+// phase and the backward MMAs of tile i, and the stores of tile i overlap the forward MMAs of
+// tile i + 1.  Every wait is bounded; a thread whose wait runs out records the status word and
+// leaves its loop, so the threads that wait on it run out in turn and the CTA ends.
+template <class S, typename TX>
+__global__ void __launch_bounds__(288, 1)
+    vol_tc05p_kernel(DevOp<float> op, const float* __restrict__ tv, int ldt, const TX* __restrict__ x,
+                     TX* __restrict__ y, int64_t ld, int nrhs, int* status) {
+    using L = Tc05Vol<S>;
+    constexpr int D = S::D, Q = S::Q, TE = L::TE, NCOL = L::NCOL, NT = 288;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned long long barU, barF, barR, barS, barB;
+    __shared__ uint32_t tbase;
+    const Tc05Smem b = tc05_smem<S>(smem_raw);
+    if (warp == 0) {
+        tmem_alloc(&tbase, L::TCOLS);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(&barU, 128);
+        mbar_init(&barF, 1);
+        mbar_init(&barR, 128);
+        mbar_init(&barS, 128);
+        mbar_init(&barB, 1);
+    }
+    tc05_init<S>(b, tv, ldt, op.Nq, tid, NT);
+    fence_async_smem();
+    tc05_fence_before();
+    __syncthreads();
+    tc05_fence_after();
+    const uint32_t tmem = tbase;
+    const int ntiles = static_cast<int>((op.E + TE - 1) / TE);
+    const int64_t nwork = static_cast<int64_t>(ntiles) * nrhs;
+    const int64_t nmine = nwork > blockIdx.x ? (nwork - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    auto work_of = [&](int64_t i) { return blockIdx.x + i * gridDim.x; };
+    bool ok = true;
+    if (warp == 8) {  // MMA issue
+        if (lane == 0) {
+            for (int64_t i = 0; i < nmine && ok; ++i) {
+                const unsigned p = static_cast<unsigned>(i & 1);
+                ok = mbar_wait_bounded(&barU, p) && (i == 0 || mbar_wait_bounded(&barR, p ^ 1u));
+                if (!ok) break;
+                tc05_fence_after();
+                tc05_issue_fwd<S>(b, tmem);
+                umma_commit(&barF);
+                ok = mbar_wait_bounded(&barS, p);
+                if (!ok) break;
+                tc05_fence_after();
+                tc05_issue_bwd<S>(b, tmem);
+                umma_commit(&barB);
+            }
+        }
+    } else if ((warp & 3) >= 2) {  // staging: U of tile i once the forward MMAs of tile i - 1 are done
+        const int t0 = ((warp >> 2) * 2 + (warp & 1)) * 32 + lane;
+        for (int64_t i = 0; i < nmine && ok; ++i) {
+            if (i > 0) ok = __all_sync(0xffffffffu, mbar_wait_bounded(&barF, static_cast<unsigned>((i - 1) & 1)));
+            if (!ok) break;
+            const int64_t w = work_of(i);
+            tc05_stage<S, TX>(b, x + (w / ntiles) * ld, (w % ntiles) * TE, op.E, t0, 128);
+            fence_async_smem();
+            mbar_arrive(&barU);
+        }
+    } else {  // pointwise and stores: lane q / k of 0..63, half of the tile's elements
+        const uint32_t lane_base = static_cast<uint32_t>(32 * (warp & 3)) << 16;
+        const int q = 32 * (warp & 3) + lane, half = warp >> 2, te0 = half * (TE / 2);
+        for (int64_t i = 0; i < nmine && ok; ++i) {
+            const unsigned p = static_cast<unsigned>(i & 1);
+            ok = __all_sync(0xffffffffu, mbar_wait_bounded(&barF, p));
+            if (!ok) break;
+            tc05_fence_after();
+            float R[D][Q][8];
+#pragma unroll
+            for (int a = 0; a < D; ++a)
+#pragma unroll
+                for (int r = 0; r < Q; ++r)
+                    tmem_ld8(tmem + lane_base + static_cast<uint32_t>(a * NCOL + r * TE + te0), R[a][r]);
+            tmem_wait_ld();
+            tc05_fence_before();
+            mbar_arrive(&barR);
+            if (i > 0) {  // the previous tile's y (its backward MMAs also released S)
+                ok = __all_sync(0xffffffffu, mbar_wait_bounded(&barB, p ^ 1u));
+                if (!ok) break;
+                tc05_fence_after();
+                const int64_t wp = work_of(i - 1);
+                tc05_store_y<S, TX>(tmem, lane_base, q, half, (wp % ntiles) * TE, op.E, y + (wp / ntiles) * ld);
+                tc05_fence_before();
+            }
+            const int64_t w = work_of(i);
+            tc05_pointwise<S, 8>(b, op, q, (w % ntiles) * TE, te0, R);
+            fence_async_smem();
+            mbar_arrive(&barS);
+        }
+        if (ok && nmine > 0) {
+            ok = __all_sync(0xffffffffu, mbar_wait_bounded(&barB, static_cast<unsigned>((nmine - 1) & 1)));
+            if (ok) {
+                tc05_fence_after();
+                const int64_t wp = work_of(nmine - 1);
+                tc05_store_y<S, TX>(tmem, lane_base, q, half, (wp % ntiles) * TE, op.E, y + (wp / ntiles) * ld);
+            }
+        }
+    }
+    if (!ok && status) atomicExch(status, 1);
+    tc05_fence_before();
+    __syncthreads();
     tc05_fence_after();
     if (warp == 0) tmem_dealloc(tmem, L::TCOLS);
 }

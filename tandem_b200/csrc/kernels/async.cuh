@@ -35,6 +35,11 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+// one arrival of this thread on bar (release: this thread's earlier shared-memory writes are
+// visible to the threads that see the phase complete)
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
     unsigned ok = 0;
     asm volatile(

@@ -23,14 +23,6 @@ __host__ __device__ constexpr int core_offset(int R, int row, int k) {
     return ((k >> 2) * (R >> 3) + (row >> 3)) * 32 + (row & 7) * 4 + (k & 3);
 }
 
-// The MN-major form of an operand (tf32 allows it): [K/8 groups][R/4 groups][8 k][4 rows]; core
-// matrix = 8 K values x 16 bytes of 4 rows.  Per K step the descriptor starts at group s with
-// stride byte offset (between 4-row groups) 128 and leading byte offset (between K groups)
-// R/4 * 128; the instruction descriptor's major bit of that operand is 1.
-__host__ __device__ constexpr int core_offset_mn(int R, int row, int k) {
-    return ((k >> 3) * (R >> 2) + (row >> 2)) * 32 + (k & 7) * 4 + (row & 3);
-}
-
 // Shared memory matrix descriptor: start address, leading / stride byte offsets (16-byte units,
 // 14 bits each), version 1 (sm_100) at bit 46, base offset 0, no swizzle.
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -39,10 +31,12 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 }
 
 // Instruction descriptor of kind::tf32: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2),
-// no negation, A / B K-major (bit 15 / 16 = 0) or MN-major (1), N >> 3 at bit 17, M >> 4 at bit 24.
-__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, bool a_mn = false, bool b_mn = false) {
-    return (1u << 4) | (2u << 7) | (2u << 10) | (a_mn ? 1u << 15 : 0u) | (b_mn ? 1u << 16 : 0u) |
-           (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
+// no negation, A and B K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24.  (MN-major
+// TF32 operands in the no-swizzle canonical layout gave all-zero products on B200; the kernels use
+// K-major operands only.)
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+           (static_cast<uint32_t>(M >> 4) << 24);
 }
 
 // D (+)= A B^T, issued by one thread; accumulate = 0 overwrites D

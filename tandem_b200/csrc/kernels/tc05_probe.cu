@@ -12,7 +12,7 @@ namespace tdg {
 namespace {
 
 __global__ void __launch_bounds__(128) k_tc05_gemm(const float* __restrict__ A, const float* __restrict__ B,
-                                                   float* __restrict__ D, int N, int K, int split3, int amn, int bmn, uint32_t cols,
+                                                   float* __restrict__ D, int N, int K, int split3, uint32_t cols,
                                                    int* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long bar;
@@ -33,30 +33,26 @@ __global__ void __launch_bounds__(128) k_tc05_gemm(const float* __restrict__ A, 
         const int r = i / K, k = i % K;
         float h, l;
         split_tf32(A[i], h, l);
-        const int o = amn ? core_offset_mn(128, r, k) : core_offset(128, r, k);
-        Ah[o] = h;
-        Al[o] = l;
+        Ah[core_offset(128, r, k)] = h;
+        Al[core_offset(128, r, k)] = l;
     }
     for (int i = tid; i < N * K; i += 128) {
         const int r = i / K, k = i % K;
         float h, l;
         split_tf32(B[i], h, l);
-        const int o = bmn ? core_offset_mn(N, r, k) : core_offset(N, r, k);
-        Bh[o] = h;
-        Bl[o] = l;
+        Bh[core_offset(N, r, k)] = h;
+        Bl[core_offset(N, r, k)] = l;
     }
     fence_async_smem();
     tc05_fence_before();
     __syncthreads();
     tc05_fence_after();
     const uint32_t tmem = tbase;
-    if (tid == 0) {
-        const uint32_t idesc = idesc_tf32(128, N, amn != 0, bmn != 0);
-        const uint32_t lboA = (amn ? 128 / 4 : 128 / 8) * 128;
-        // K-major B: two K chunks of N/8 row groups per step; MN-major B: one K group of N/4 groups
-        const uint32_t lboB = static_cast<uint32_t>(bmn ? N / 4 : N / 8) * 128;
+    if (tid == 0 && split3 >= 0) {  // split3 < 0: nothing issued, nothing arrives (the bounded wait runs out)
+        const uint32_t idesc = idesc_tf32(128, N);
+        const uint32_t lboA = (128 / 8) * 128, lboB = static_cast<uint32_t>(N / 8) * 128;
         for (int s = 0; s < K / 8; ++s) {
-            const uint32_t offA = (amn ? 1u : 2u) * s * lboA, offB = (bmn ? 1u : 2u) * s * lboB;
+            const uint32_t offA = 2u * s * lboA, offB = 2u * s * lboB;
             const uint64_t ah = umma_desc(smem_u32(Ah) + offA, lboA, 128), al = umma_desc(smem_u32(Al) + offA, lboA, 128);
             const uint64_t bh = umma_desc(smem_u32(Bh) + offB, lboB, 128), bl = umma_desc(smem_u32(Bl) + offB, lboB, 128);
             umma_tf32(tmem, ah, bh, idesc, s > 0 ? 1u : 0u);
@@ -88,22 +84,22 @@ __global__ void __launch_bounds__(128) k_tc05_gemm(const float* __restrict__ A, 
 }  // namespace
 }  // namespace tdg
 
-extern "C" int tdg_probe_tc05_gemm(const float* A, const float* B, float* D, int n, int k, int split3, int a_mn,
-                                   int b_mn, void* stream) {
+extern "C" int tdg_probe_tc05_gemm(const float* A, const float* B, float* D, int n, int k, int split3, void* stream) {
     using namespace tdg;
-    if (!A || !B || !D || n < 16 || n > 256 || n % 16 || k < 8 || k > 64 || k % 8) return TDG_E_INVALID;
+    if (!A || !B || !D || n < 16 || n > 256 || n % 16 || k < 8 || k > 64 || k % 8 || split3 < -1 || split3 > 1)
+        return TDG_E_INVALID;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     uint32_t cols = 32;
     while (cols < static_cast<uint32_t>(n)) cols *= 2;
-    // operands, 1 KB for the alignment and one K group of slack behind the last operand
-    const size_t smem = static_cast<size_t>(128 + n) * k * 2 * sizeof(float) + 1024 + static_cast<size_t>(n) * 32 + 4096;
+    // operands, 1 KB for the alignment, 4 KB of slack behind the last operand
+    const size_t smem = static_cast<size_t>(128 + n) * k * 2 * sizeof(float) + 1024 + 4096;
     if (cudaFuncSetAttribute(k_tc05_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
         cudaSuccess)
         return TDG_E_CUDA;
     int* status = nullptr;
     if (cudaMallocAsync(&status, sizeof(int), s) != cudaSuccess) return TDG_E_NOMEM;
     cudaMemsetAsync(status, 0, sizeof(int), s);
-    k_tc05_gemm<<<1, 128, smem, s>>>(A, B, D, n, k, split3, a_mn, b_mn, cols, status);
+    k_tc05_gemm<<<1, 128, smem, s>>>(A, B, D, n, k, split3, cols, status);
     int rc = cudaGetLastError() == cudaSuccess ? 0 : TDG_E_CUDA;
     int h = 0;
     if (!rc && cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) rc = TDG_E_CUDA;
