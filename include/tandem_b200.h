@@ -303,7 +303,8 @@ typedef struct {
     double coarse_rtol;      /* coarsest-level CG relative tolerance (-mg_coarse_ksp_rtol; 0.1) */
     int32_t coarse_max_it;   /* coarsest-level CG iteration cap (default 1000) */
     int32_t smooth_precision; /* TDG_FP64, or TDG_MIXED: FP32 arithmetic for the finest level's
-                                 smoother applies (the level operators stay FP64) */
+                                 smoother applies, FP32 copies of the blocks for the smoothed levels
+                                 below it (vectors, accumulation and the coarse solve stay FP64) */
     int32_t coarse_space;    /* TDG_MG_COARSE_DG: the coarse CG works on the coarsest DG level (as
                                 tandem's -mg_coarse_ksp_type cg).  TDG_MG_COARSE_P1 (default): the
                                 coarsest DG level is smoothed too and corrected from the continuous

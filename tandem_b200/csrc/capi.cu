@@ -127,6 +127,7 @@ struct MgLevel {
     int degree = 0, bs = 0;
     int64_t n = 0, ld = 0;
     double* A = nullptr;
+    float* A32 = nullptr;  // FP32 copy of A for the smoother under mixed precision (levels below the finest)
     double* dinv = nullptr;
     MgInterp ip{};
     double *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *y = nullptr, *w = nullptr;
@@ -669,6 +670,7 @@ int mg_level_apply(tdg_op* op, int l, const double* x, double* y, const double* 
         if (b) TDG_TRY(mgk(launch_vec_rsub_cols(L.n, nrhs, L.ld, b, y, s), "residual"));
         return 0;
     }
+    if (L.A32) return mgk(launch_mg_bsr_apply(op->h.E, mg.NB, L.bs, mg.nbr, L.A32, x, b, y, nrhs, L.ld, s), "level apply");
     return mgk(launch_mg_bsr_apply(op->h.E, mg.NB, L.bs, mg.nbr, L.A, x, b, y, nrhs, L.ld, s), "level apply");
 }
 
@@ -1162,6 +1164,15 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
     mg.cap = 0;
     mg.fine_ld = 0;
     TDG_TRY(mg_ensure_ws(op, 1, mg.lv.back().n, s));
+    // mixed precision: the smoothed levels below the finest apply FP32 copies of their blocks
+    // (half the bytes of the HBM-bound block-sparse apply; vectors and accumulation stay FP64)
+    if (mg.fine_prec == TDG_MIXED)
+        for (int l = mg.aux ? 0 : 1; l + 1 < nl; ++l) {
+            auto& L = mg.lv[static_cast<size_t>(l)];
+            const int64_t nb = E * mg.NB * L.bs * L.bs;
+            TDG_CUDA_TRY(mg.arena.alloc(&L.A32, static_cast<size_t>(nb)));
+            TDG_TRY(mgk(launch_round_to_float(nb, L.A, L.A32, s), "FP32 level blocks"));
+        }
     // Chebyshev bounds of the smoothed levels
     for (int l = mg.aux ? 0 : 1; l < nl; ++l) TDG_TRY(mg_estimate_lmax(op, l, s));
     mg.ready = true;

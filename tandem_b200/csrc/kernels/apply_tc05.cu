@@ -10,7 +10,7 @@ namespace tdg {
 namespace {
 
 // The warp-specialised form (vol_tc05p_kernel) or one tile at a time (vol_tc05_kernel).
-constexpr bool kTc05Pipelined = false;
+constexpr bool kTc05Pipelined = true;
 
 template <class S, typename TX>
 int run_vol_tc05(DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y, int nrhs, int64_t ld,
@@ -32,7 +32,7 @@ int run_vol_tc05(DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y
     int64_t grid = device_sm_count();  // one CTA per SM: the shared memory and half the tensor memory
     if (grid > nwork) grid = nwork;
     if (grid < 1) return 0;
-    k<<<static_cast<unsigned>(grid), kTc05Pipelined ? 288 : 256, L::BYTES, s>>>(op, mt.tables, TcfTile<S>::LDT, x, y, ld,
+    k<<<static_cast<unsigned>(grid), kTc05Pipelined ? 512 : 256, L::BYTES, s>>>(op, mt.tables, TcfTile<S>::LDT, x, y, ld,
                                                                                  nrhs, mt.status);
     return cudaGetLastError() == cudaSuccess ? 0 : TDG_E_CUDA;
 }

@@ -241,6 +241,62 @@ __device__ __forceinline__ void tc05_issue_bwd(Tc05Smem const& b, uint32_t tmem)
     }
 }
 
+// J^-1 and the coefficients of the elements te0 .. te0 + NE - 1 at the thread's point q (coalesced
+// over q); zero past Nq and past E.
+template <class S, int NE>
+__device__ __forceinline__ void tc05_load_geo(DevOp<float> const& op, int q, int64_t e0, int te0,
+                                              float (&G)[NE][S::DD], float (&c0)[NE], float (&c1)[NE]) {
+    constexpr int DD = S::DD;
+    const int Nq = op.Nq;
+#pragma unroll
+    for (int j = 0; j < NE; ++j) {
+        const int64_t e = e0 + te0 + j;
+        const bool in = q < Nq && e < op.E;
+        const float* vg = op.vG + (in ? e * DD * Nq + q : 0);
+#pragma unroll
+        for (int c = 0; c < DD; ++c) G[j][c] = in ? vg[c * Nq] : 0.0f;
+        if constexpr (S::KIND == kPoisson) {
+            c0[j] = in ? op.vCoef[e * Nq + q] : 0.0f;
+            c1[j] = 0.0f;
+        } else {
+            c0[j] = in ? op.vCoef[(e * 2 + 0) * Nq + q] : 0.0f;
+            c1[j] = in ? op.vCoef[(e * 2 + 1) * Nq + q] : 0.0f;
+        }
+    }
+}
+
+// The pointwise flux from geometry already in registers (zero geometry gives zero flux), written to
+// S split hi / lo.
+template <class S, int NE>
+__device__ __forceinline__ void tc05_pointwise_regs(Tc05Smem const& b, int q, int te0, const float (&R)[S::D][S::Q][NE],
+                                                    const float (&G)[NE][S::DD], const float (&c0)[NE],
+                                                    const float (&c1)[NE]) {
+    using L = Tc05Vol<S>;
+    constexpr int D = S::D, Q = S::Q, TE = L::TE, NQ = L::NQ;
+#pragma unroll
+    for (int j = 0; j < NE; ++j) {
+        float T[D][Q], g[D][Q];
+#pragma unroll
+        for (int a = 0; a < D; ++a)
+#pragma unroll
+            for (int r = 0; r < Q; ++r) g[a][r] = R[a][r][j];
+        vol_point<S>(G[j], c0[j], c1[j], g, T);
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            const int kk = a * NQ + q;
+            const int ob = (kk >> 2) * (L::SCS / 4) + (kk & 3);
+#pragma unroll
+            for (int r = 0; r < Q; ++r) {
+                const int n = r * TE + te0 + j;
+                float h, l;
+                split_tf32(T[a][r], h, l);
+                b.Sh[ob + (n >> 3) * 32 + (n & 7) * 4] = h;
+                b.Sl[ob + (n >> 3) * 32 + (n & 7) * 4] = l;
+            }
+        }
+    }
+}
+
 // Pointwise flux of the elements te0 .. te0 + NE - 1 at the thread's point q (a lane of 0..63) from
 // R[a][r][j], written to S split hi / lo; zero past Nq and past E.
 template <class S, int NE>
@@ -294,6 +350,26 @@ __device__ __forceinline__ void tc05_pointwise(Tc05Smem const& b, DevOp<float> c
 
 // y of the tile's elements half * 8 .. half * 8 + 7 from the backward accumulator (warp-collective;
 // lanes k < NBF store).
+template <class S, typename TX>
+__device__ __forceinline__ void tc05_store_y4(uint32_t tmem, uint32_t lane_base, int k, int te0, int64_t e0, int64_t E,
+                                              TX* __restrict__ yr) {
+    using L = Tc05Vol<S>;
+    constexpr int Q = S::Q, NBF = S::NBF, BS = S::BS, TE = L::TE, NCOL = L::NCOL;
+    float v[Q][4];
+#pragma unroll
+    for (int r = 0; r < Q; ++r) tmem_ld4(tmem + lane_base + static_cast<uint32_t>(S::D * NCOL + r * TE + te0), v[r]);
+    tmem_wait_ld();
+    if (k < NBF) {
+#pragma unroll
+        for (int r = 0; r < Q; ++r)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t e = e0 + te0 + j;
+                if (e < E) yr[e * BS + k + NBF * r] = static_cast<TX>(v[r][j]);
+            }
+    }
+}
+
 template <class S, typename TX>
 __device__ __forceinline__ void tc05_store_y(uint32_t tmem, uint32_t lane_base, int k, int half, int64_t e0, int64_t E,
                                              TX* __restrict__ yr) {
@@ -398,20 +474,21 @@ __global__ void __launch_bounds__(256, 1)
     if (warp == 0) tmem_dealloc(tmem, L::TCOLS);
 }
 
-// Warp-specialised form (288 threads): warps 0, 1, 4, 5 own TMEM lanes 0..63 and run the pointwise
-// flux and the stores of y; warps 2, 3, 6, 7 stage the next tile's U as soon as the forward MMAs of
-// the current one have read theirs; warp 8 (one thread) issues the MMAs.  Five mbarriers, one phase
-// per tile each: U staged (128 arrivals), forward done (commit), R read (128), S written (128),
-// backward done (commit).  So the staging of tile i + 1 and its forward MMAs overlap the pointwise
-// phase and the backward MMAs of tile i, and the stores of tile i overlap the forward MMAs of
-// tile i + 1.  Every wait is bounded; a thread whose wait runs out records the status word and
-// leaves its loop, so the threads that wait on it run out in turn and the CTA ends.
+// Warp-specialised form (512 threads, 16 warps): in each of the four groups of warps 4g .. 4g + 3,
+// the two warps that own TMEM lanes 0..63 run the pointwise flux and the stores of y for elements
+// 4g .. 4g + 3 of the tile (lane = point q / basis function k), the other two stage U, except lane 0
+// of warp 2, which issues the MMAs.  Five mbarriers, one phase per tile each: U staged (255
+// arrivals), forward done (commit), R read (256), S written (256), backward done (commit).  The
+// staging of tile i + 1 and its forward MMAs overlap the pointwise phase and the backward MMAs of
+// tile i; the pointwise threads load the next tile's geometry before they wait for its forward
+// MMAs.  Every wait is bounded; a thread whose wait runs out records the status word and leaves its
+// loop, so the threads that wait on it run out in turn and the CTA ends.
 template <class S, typename TX>
-__global__ void __launch_bounds__(288, 1)
+__global__ void __launch_bounds__(512, 1)
     vol_tc05p_kernel(DevOp<float> op, const float* __restrict__ tv, int ldt, const TX* __restrict__ x,
                      TX* __restrict__ y, int64_t ld, int nrhs, int* status) {
     using L = Tc05Vol<S>;
-    constexpr int D = S::D, Q = S::Q, TE = L::TE, NCOL = L::NCOL, NT = 288;
+    constexpr int D = S::D, Q = S::Q, DD = S::DD, TE = L::TE, NCOL = L::NCOL, NT = 512;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long barU, barF, barR, barS, barB;
@@ -422,10 +499,10 @@ __global__ void __launch_bounds__(288, 1)
         tmem_relinquish();
     }
     if (tid == 0) {
-        mbar_init(&barU, 128);
+        mbar_init(&barU, 255);
         mbar_init(&barF, 1);
-        mbar_init(&barR, 128);
-        mbar_init(&barS, 128);
+        mbar_init(&barR, 256);
+        mbar_init(&barS, 256);
         mbar_init(&barB, 1);
     }
     tc05_init<S>(b, tv, ldt, op.Nq, tid, NT);
@@ -438,9 +515,10 @@ __global__ void __launch_bounds__(288, 1)
     const int64_t nwork = static_cast<int64_t>(ntiles) * nrhs;
     const int64_t nmine = nwork > blockIdx.x ? (nwork - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
     auto work_of = [&](int64_t i) { return blockIdx.x + i * gridDim.x; };
+    const int grp = warp >> 2, sub = warp & 3;
     bool ok = true;
-    if (warp == 8) {  // MMA issue
-        if (lane == 0) {
+    if (warp == 2 && lane == 0) {  // MMA issue
+        {
             for (int64_t i = 0; i < nmine && ok; ++i) {
                 const unsigned p = static_cast<unsigned>(i & 1);
                 ok = mbar_wait_bounded(&barU, p) && (i == 0 || mbar_wait_bounded(&barR, p ^ 1u));
@@ -455,30 +533,35 @@ __global__ void __launch_bounds__(288, 1)
                 umma_commit(&barB);
             }
         }
-    } else if ((warp & 3) >= 2) {  // staging: U of tile i once the forward MMAs of tile i - 1 are done
-        const int t0 = ((warp >> 2) * 2 + (warp & 1)) * 32 + lane;
+    } else if (sub >= 2) {  // staging (255 threads): U of tile i once the forward MMAs of tile i - 1 are done
+        const int t0 = (grp * 2 + (sub - 2)) * 32 + lane - 1;
+        const unsigned mask = warp == 2 ? 0xfffffffeu : 0xffffffffu;
         for (int64_t i = 0; i < nmine && ok; ++i) {
-            if (i > 0) ok = __all_sync(0xffffffffu, mbar_wait_bounded(&barF, static_cast<unsigned>((i - 1) & 1)));
+            if (i > 0) ok = __all_sync(mask, mbar_wait_bounded(&barF, static_cast<unsigned>((i - 1) & 1)));
             if (!ok) break;
             const int64_t w = work_of(i);
-            tc05_stage<S, TX>(b, x + (w / ntiles) * ld, (w % ntiles) * TE, op.E, t0, 128);
+            tc05_stage<S, TX>(b, x + (w / ntiles) * ld, (w % ntiles) * TE, op.E, t0, 255);
             fence_async_smem();
             mbar_arrive(&barU);
         }
-    } else {  // pointwise and stores: lane q / k of 0..63, half of the tile's elements
-        const uint32_t lane_base = static_cast<uint32_t>(32 * (warp & 3)) << 16;
-        const int q = 32 * (warp & 3) + lane, half = warp >> 2, te0 = half * (TE / 2);
+    } else {  // pointwise and stores: lane q / k of 0..63, elements 4 grp .. 4 grp + 3
+        const uint32_t lane_base = static_cast<uint32_t>(32 * sub) << 16;
+        const int q = 32 * sub + lane, te0 = 4 * grp;
         for (int64_t i = 0; i < nmine && ok; ++i) {
             const unsigned p = static_cast<unsigned>(i & 1);
+            const int64_t w = work_of(i);
+            const int64_t e0 = (w % ntiles) * TE;
+            float G[4][DD], c0[4], c1[4];
+            tc05_load_geo<S, 4>(op, q, e0, te0, G, c0, c1);  // in flight during the wait
             ok = __all_sync(0xffffffffu, mbar_wait_bounded(&barF, p));
             if (!ok) break;
             tc05_fence_after();
-            float R[D][Q][8];
+            float R[D][Q][4];
 #pragma unroll
             for (int a = 0; a < D; ++a)
 #pragma unroll
                 for (int r = 0; r < Q; ++r)
-                    tmem_ld8(tmem + lane_base + static_cast<uint32_t>(a * NCOL + r * TE + te0), R[a][r]);
+                    tmem_ld4(tmem + lane_base + static_cast<uint32_t>(a * NCOL + r * TE + te0), R[a][r]);
             tmem_wait_ld();
             tc05_fence_before();
             mbar_arrive(&barR);
@@ -487,11 +570,10 @@ __global__ void __launch_bounds__(288, 1)
                 if (!ok) break;
                 tc05_fence_after();
                 const int64_t wp = work_of(i - 1);
-                tc05_store_y<S, TX>(tmem, lane_base, q, half, (wp % ntiles) * TE, op.E, y + (wp / ntiles) * ld);
+                tc05_store_y4<S, TX>(tmem, lane_base, q, te0, (wp % ntiles) * TE, op.E, y + (wp / ntiles) * ld);
                 tc05_fence_before();
             }
-            const int64_t w = work_of(i);
-            tc05_pointwise<S, 8>(b, op, q, (w % ntiles) * TE, te0, R);
+            tc05_pointwise_regs<S, 4>(b, q, te0, R, G, c0, c1);
             fence_async_smem();
             mbar_arrive(&barS);
         }
@@ -500,7 +582,7 @@ __global__ void __launch_bounds__(288, 1)
             if (ok) {
                 tc05_fence_after();
                 const int64_t wp = work_of(nmine - 1);
-                tc05_store_y<S, TX>(tmem, lane_base, q, half, (wp % ntiles) * TE, op.E, y + (wp / ntiles) * ld);
+                tc05_store_y4<S, TX>(tmem, lane_base, q, te0, (wp % ntiles) * TE, op.E, y + (wp / ntiles) * ld);
             }
         }
     }

@@ -94,9 +94,11 @@ __global__ void __launch_bounds__(128)
     }
 }
 
-// Column c of x, b, y starts at c * ld (nrhs columns).
+// Column c of x, b, y starts at c * ld (nrhs columns); TA: the blocks' type (FP64, or FP32 copies
+// for the mixed-precision smoother), accumulation in FP64.
+template <typename TA>
 __global__ void __launch_bounds__(kT)
-    k_bsr_apply(int64_t E, int NB, int bs, const int32_t* __restrict__ nbr, const double* __restrict__ A,
+    k_bsr_apply(int64_t E, int NB, int bs, const int32_t* __restrict__ nbr, const TA* __restrict__ A,
                 const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y, int nrhs,
                 int64_t ld) {
     const int64_t n = E * bs;
@@ -109,9 +111,9 @@ __global__ void __launch_bounds__(kT)
         for (int s = 0; s < NB; ++s) {
             const int32_t t = nbr[e * NB + s];
             if (t < 0) continue;
-            const double* blk = A + (e * NB + s) * bs * bs;
+            const TA* blk = A + (e * NB + s) * bs * bs;
             const double* xt = xc + static_cast<int64_t>(t) * bs;
-            for (int col = 0; col < bs; ++col) acc += blk[col * bs + row] * xt[col];
+            for (int col = 0; col < bs; ++col) acc += static_cast<double>(blk[col * bs + row]) * xt[col];
         }
         y[c * ld + gi] = b ? b[c * ld + gi] - acc : acc;
     }
@@ -119,9 +121,9 @@ __global__ void __launch_bounds__(kT)
 
 // The same with the block size known at compile time: the column loop unrolls, so every thread
 // issues its block row's loads back to back.
-template <int BS>
+template <int BS, typename TA>
 __global__ void __launch_bounds__(kT)
-    k_bsr_apply_t(int64_t E, int NB, const int32_t* __restrict__ nbr, const double* __restrict__ A,
+    k_bsr_apply_t(int64_t E, int NB, const int32_t* __restrict__ nbr, const TA* __restrict__ A,
                   const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y, int nrhs,
                   int64_t ld) {
     const int64_t n = E * BS;
@@ -134,10 +136,10 @@ __global__ void __launch_bounds__(kT)
         for (int s = 0; s < NB; ++s) {
             const int32_t t = nbr[e * NB + s];
             if (t < 0) continue;
-            const double* blk = A + (e * NB + s) * (BS * BS) + row;
+            const TA* blk = A + (e * NB + s) * (BS * BS) + row;
             const double* xt = xc + static_cast<int64_t>(t) * BS;
 #pragma unroll
-            for (int col = 0; col < BS; ++col) acc += blk[col * BS] * xt[col];
+            for (int col = 0; col < BS; ++col) acc += static_cast<double>(blk[col * BS]) * xt[col];
         }
         y[c * ld + gi] = b ? b[c * ld + gi] - acc : acc;
     }
@@ -354,6 +356,10 @@ __global__ void __launch_bounds__(kT) k_random(int64_t n, uint64_t seed, double*
     }
 }
 
+__global__ void __launch_bounds__(kT) k_round_to_float(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+    TDG_GRID_LOOP(i, n) b[i] = static_cast<float>(a[i]);
+}
+
 #undef TDG_GRID_LOOP
 
 }  // namespace
@@ -380,17 +386,27 @@ int launch_mg_triple(int64_t E, int NB, const int32_t* nbr, MgInterp ip, const d
     return launched();
 }
 
-int launch_mg_bsr_apply(int64_t E, int NB, int bs, const int32_t* nbr, const double* A, const double* x,
+template <typename TA>
+int launch_mg_bsr_apply(int64_t E, int NB, int bs, const int32_t* nbr, const TA* A, const double* x,
                         const double* b, double* y, int nrhs, int64_t ld, cudaStream_t s) {
     const unsigned g = grid_for(E * bs * nrhs);
     switch (bs) {
 #define TDG_BSR_CASE(B) \
-    case B: k_bsr_apply_t<B><<<g, kT, 0, s>>>(E, NB, nbr, A, x, b, y, nrhs, ld); break;
+    case B: k_bsr_apply_t<B, TA><<<g, kT, 0, s>>>(E, NB, nbr, A, x, b, y, nrhs, ld); break;
         TDG_BSR_CASE(1) TDG_BSR_CASE(2) TDG_BSR_CASE(3) TDG_BSR_CASE(4) TDG_BSR_CASE(6) TDG_BSR_CASE(10)
         TDG_BSR_CASE(12) TDG_BSR_CASE(20) TDG_BSR_CASE(30) TDG_BSR_CASE(60)
 #undef TDG_BSR_CASE
-        default: k_bsr_apply<<<g, kT, 0, s>>>(E, NB, bs, nbr, A, x, b, y, nrhs, ld);
+        default: k_bsr_apply<TA><<<g, kT, 0, s>>>(E, NB, bs, nbr, A, x, b, y, nrhs, ld);
     }
+    return launched();
+}
+template int launch_mg_bsr_apply<double>(int64_t, int, int, const int32_t*, const double*, const double*,
+                                         const double*, double*, int, int64_t, cudaStream_t);
+template int launch_mg_bsr_apply<float>(int64_t, int, int, const int32_t*, const float*, const double*,
+                                        const double*, double*, int, int64_t, cudaStream_t);
+
+int launch_round_to_float(int64_t n, const double* a, float* b, cudaStream_t s) {
+    k_round_to_float<<<grid_for(n), kT, 0, s>>>(n, a, b);
     return launched();
 }
 

@@ -31,8 +31,11 @@ int launch_mg_probe_extract(int64_t E, int NB, const int32_t* nbr, const int32_t
 int launch_mg_triple(int64_t E, int NB, const int32_t* nbr, MgInterp ip, const double* Af, double* Ac,
                      cudaStream_t s);
 // y = A x (b == nullptr) or y = b - A x, for nrhs columns starting at multiples of ld.
-int launch_mg_bsr_apply(int64_t E, int NB, int bs, const int32_t* nbr, const double* A, const double* x,
+template <typename TA>
+int launch_mg_bsr_apply(int64_t E, int NB, int bs, const int32_t* nbr, const TA* A, const double* x,
                         const double* b, double* y, int nrhs, int64_t ld, cudaStream_t s);
+// b[i] = a[i] rounded to FP32 (the mixed-precision smoother's copies of the level blocks).
+int launch_round_to_float(int64_t n, const double* a, float* b, cudaStream_t s);
 // dinv[e][i] = 1 / blocks[e * stride + i * bs + i] (point Jacobi); status set on a non-positive
 // diagonal entry.
 int launch_mg_diag_inv(int64_t E, int bs, int64_t stride, const double* blocks, double* dinv, int* status,

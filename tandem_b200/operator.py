@@ -220,7 +220,8 @@ class DGOperator:
         coarse operators, Chebyshev smoothers on esteig x lambda_max(D^-1 A) with point Jacobi, and
         a block-Jacobi CG coarse solve -- on the coarsest DG level (coarse_space "dg") or on the
         continuous P1 space below it ("p1").  smooth_precision MIXED runs the finest level's
-        smoother applies in FP32 arithmetic."""
+        smoother applies in FP32 arithmetic and the smoothed levels below it on FP32 copies of
+        their blocks (FP64 vectors and accumulation)."""
         o = _ffi.MgOpts(MG_STRATEGIES.index(strategy), coarse_degree, smooth_its, esteig[0], esteig[1],
                         esteig_steps, coarse_rtol, coarse_max_it, smooth_precision,
                         MG_COARSE_SPACES.index(coarse_space))
