@@ -375,7 +375,11 @@ def run_ours(args):
            "d2h_bytes_per_step": n * 8, "ms_per_step": ms_e2e}
 
     # ---- FP32 apply (inner operator of the mixed-precision solve), fastest configuration ----
-    tune32 = op.autotune(FP32, stream=stream)
+    if args.family32:
+        op.set_apply_config(FP32, args.family32, args.ctas)
+        tune32 = [{"family": args.family32, "ctas_per_sm": args.ctas, "ms": 0.0}]
+    else:
+        tune32 = op.autotune(FP32, stream=stream)
     best32 = min(tune32, key=lambda e: e["ms"])
     x32, y32 = x.float(), torch.empty(n, dtype=torch.float32, device="cuda")
     for _ in range(args.warmup):
@@ -959,7 +963,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--family", choices=["tensor", "face", "face2", "simt"], default="",
                     help="cube: FP64 apply kernel family to use instead of the autotuner's pick")
-    ap.add_argument("--ctas", type=int, default=2, help="cube: persistent CTAs per SM with --family")
+    ap.add_argument("--family32", choices=["tensor", "face", "tc05", "simt"], default="",
+                    help="cube: FP32 apply kernel family to use instead of the autotuner's pick")
+    ap.add_argument("--ctas", type=int, default=2, help="cube: persistent CTAs per SM with --family / --family32")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", choices=["cube", "batch", "gf", "poisson", "adjoint", "vcycle"], default="cube",
                     help="cube: the apply benchmark (default); batch: uneven batch of 2D elasticity "

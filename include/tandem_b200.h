@@ -167,7 +167,8 @@ typedef struct {
 
 /* Times the apply of this operator (its own mesh, `nrhs` right-hand sides, `precision`) for each
  * candidate launch configuration -- the tensor-core kernels (element-centric, and the
- * face-centric pair) at 1 to 4 persistent CTAs per SM (clipped to the occupancy limit of the
+ * face-centric pair; FP64 also its software-pipelined form, FP32 also the pair with the tcgen05
+ * volume kernel) at 1 to 4 persistent CTAs per SM (clipped to the occupancy limit of the
  * shape's tile) and the SIMT kernel -- with CUDA events on
  * `stream`, and keeps the fastest for later tdg_apply / tdg_solve calls of that precision.
  * entries (optional, up to max_entries) receives every measurement; n_entries their count. */

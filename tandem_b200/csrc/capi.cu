@@ -1423,6 +1423,8 @@ int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_ent
         for (int c = 1; c <= 4; ++c) cands.push_back({2, c});
     if (op->use_mma && precision == TDG_FP64)
         for (int c = 1; c <= 2; ++c) cands.push_back({3, c});
+    if (op->use_mma && precision == TDG_FP32)  // the facet kernel's CTAs; the tcgen05 volume kernel runs one per SM
+        for (int c = 1; c <= 4; ++c) cands.push_back({4, c});
     cands.push_back({1, 0});
     const int fam0 = op->family[pi], ct0 = op->ctas[pi];
     cudaEvent_t e0, e1;
