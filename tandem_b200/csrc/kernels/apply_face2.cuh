@@ -126,6 +126,95 @@ __device__ __forceinline__ void cta_gemm_store_staged(const double* A0, const do
     }
 }
 
+// The same product with register blocking over whole rows of output tiles: a warp's work item is
+// one m-tile and all NTN n-tiles of it, so each k step loads one A fragment and NTN B fragments
+// for NTN mma (1 + 1/NTN shared-memory loads per mma instead of 2).
+template <class S, bool AG = false>
+__device__ __forceinline__ void cta_gemm_store_rows(const double* A0, const double* U0, double* C0, const double* A1,
+                                                    const double* U1, double* C1, int mrows, int ksteps, int warp,
+                                                    int lane) {
+    using L = MmaTile<S>;
+    using SU = Staged<S>;
+    constexpr int Q = S::Q, NTN = L::NTN;
+    const int g = lane >> 2, t = lane & 3;
+    const int per = mrows / 8;
+    const int nitems = A1 ? 2 * per : per;
+    for (int it = warp; it < nitems; it += L::GW) {
+        const int which = it / per, mt = it % per;
+        const double* ap = (which ? A1 : A0) + (mt * 8 + g) * L::LDT + t;
+        const double* ub = which ? U1 : U0;
+        const double* bp[NTN];
+#pragma unroll
+        for (int j = 0; j < NTN; ++j) {
+            const int n = j * 8 + g;
+            bp[j] = ub + (n / Q) * SU::LDU + (n % Q) * SU::KS + t;
+        }
+        double acc[NTN][2];
+#pragma unroll
+        for (int j = 0; j < NTN; ++j) acc[j][0] = acc[j][1] = 0.0;
+        for (int ks = 0; ks < ksteps; ++ks) {
+            const double a = table_ld<AG>(ap + ks * 4);
+#pragma unroll
+            for (int j = 0; j < NTN; ++j) dmma(acc[j], a, bp[j][ks * 4]);
+        }
+        double* c = (which ? C1 : C0) + (mt * 8 + g) * L::LDN + 2 * t;
+#pragma unroll
+        for (int j = 0; j < NTN; ++j) {
+            c[j * 8] = acc[j][0];
+            c[j * 8 + 1] = acc[j][1];
+        }
+    }
+}
+
+// D (16 x 8) += A (16 x 4) B (4 x 8) in FP64: a0 / a1 = A[g][t] / A[g + 8][t], b = B[t][g],
+// d0, d1 = D[g][2t, 2t + 1], d2, d3 = D[g + 8][2t, 2t + 1] (g = lane / 4, t = lane % 4).
+__device__ __forceinline__ void dmma16(double (&c)[4], double a0, double a1, double b) {
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a0), "d"(a1), "d"(b));
+}
+
+// cta_gemm_store_rows on 16-row m-tiles (m16n8k4: two A fragments and NTN B fragments per k step
+// for NTN mma of twice the work); mrows a multiple of 16.
+template <class S, bool AG = false>
+__device__ __forceinline__ void cta_gemm_store_rows16(const double* A0, const double* U0, double* C0, const double* A1,
+                                                      const double* U1, double* C1, int mrows, int ksteps, int warp,
+                                                      int lane) {
+    using L = MmaTile<S>;
+    using SU = Staged<S>;
+    constexpr int Q = S::Q, NTN = L::NTN;
+    const int g = lane >> 2, t = lane & 3;
+    const int per = mrows / 16;
+    const int nitems = A1 ? 2 * per : per;
+    for (int it = warp; it < nitems; it += L::GW) {
+        const int which = it / per, mt = it % per;
+        const double* ap = (which ? A1 : A0) + (mt * 16 + g) * L::LDT + t;
+        const double* ub = which ? U1 : U0;
+        const double* bp[NTN];
+#pragma unroll
+        for (int j = 0; j < NTN; ++j) {
+            const int n = j * 8 + g;
+            bp[j] = ub + (n / Q) * SU::LDU + (n % Q) * SU::KS + t;
+        }
+        double acc[NTN][4];
+#pragma unroll
+        for (int j = 0; j < NTN; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+        for (int ks = 0; ks < ksteps; ++ks) {
+            const double a0 = table_ld<AG>(ap + ks * 4), a1 = table_ld<AG>(ap + 8 * L::LDT + ks * 4);
+#pragma unroll
+            for (int j = 0; j < NTN; ++j) dmma16(acc[j], a0, a1, bp[j][ks * 4]);
+        }
+        double* c = (which ? C1 : C0) + (mt * 16 + g) * L::LDN + 2 * t;
+#pragma unroll
+        for (int j = 0; j < NTN; ++j) {
+            c[j * 8] = acc[j][0];
+            c[j * 8 + 1] = acc[j][1];
+            c[8 * L::LDN + j * 8] = acc[j][2];
+            c[8 * L::LDN + j * 8 + 1] = acc[j][3];
+        }
+    }
+}
+
 // Y += A^T B as cta_gemm_acc_t (apply_mma.cuh), the table A read through table_ld<AG>.
 template <class L, bool AG>
 __device__ __forceinline__ void cta_gemm_acc_t_tab(const double* A, const double* B, double (&y)[L::YPW][2][2],
@@ -172,6 +261,11 @@ constexpr int kFacetGeometryPrefetch = 1;
 // latency, and more chains per warp only add live registers and shared-memory traffic in flight.
 constexpr int kVolChains = 1;
 constexpr int kFaceChains = 2;
+// Forward products register-blocked over whole rows of output tiles (cta_gemm_store_rows): measured
+// on the same 32^3 apply 3.044 -> 2.844 ms (2 CTAs per SM), the same results bit for bit.
+constexpr bool kGemmRows = true;
+// The row-blocked forward products on 16-row m-tiles (m16n8k4) where the rows allow it.
+constexpr bool kGemmRows16 = false;
 
 // Issues the cp.async copies of the coefficient blocks of up to UE elements (el[te] < 0: skipped)
 // from xr into the staged buffer U.
@@ -292,8 +386,14 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
         for (int q0 = 0; q0 < Nq; q0 += qc) {
             const int nqc = (Nq - q0 < qc) ? (Nq - q0) : qc;
             const int rows = round8(nqc * D);
-            cta_gemm_store_staged<S, kVolChains>(TV + q0 * D * LDT, U, R0, nullptr, nullptr, nullptr, rows, L::KP / 4,
-                                                 warp, lane);
+            if (kGemmRows16 && rows % 16 == 0)
+                cta_gemm_store_rows16<S>(TV + q0 * D * LDT, U, R0, nullptr, nullptr, nullptr, rows, L::KP / 4, warp,
+                                         lane);
+            else if constexpr (kGemmRows)
+                cta_gemm_store_rows<S>(TV + q0 * D * LDT, U, R0, nullptr, nullptr, nullptr, rows, L::KP / 4, warp, lane);
+            else
+                cta_gemm_store_staged<S, kVolChains>(TV + q0 * D * LDT, U, R0, nullptr, nullptr, nullptr, rows,
+                                                     L::KP / 4, warp, lane);
             __syncthreads();
             for (int it = tid; it < TE * nqc; it += NT) {
                 const int te = it % TE, qq = it / TE;
@@ -500,12 +600,25 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         const double* U0 = Ub + (2 * buf) * SU::USZ;
         const double* U1 = Ub + (2 * buf + 1) * SU::USZ;
         const int4* sid = s_ids[slot];
-        if (two)
+        if (kGemmRows16 && lay.MF % 16 == 0) {
+            if (two)
+                cta_gemm_store_rows16<S, kFaceTablesGlobal>(tA, U0, R0, tB, U1, R1, lay.MF, L::KP / 4, warp, lane);
+            else
+                cta_gemm_store_rows16<S, kFaceTablesGlobal>(tA, U0, R0, nullptr, nullptr, nullptr, lay.MF, L::KP / 4,
+                                                            warp, lane);
+        } else if constexpr (kGemmRows) {
+            if (two)
+                cta_gemm_store_rows<S, kFaceTablesGlobal>(tA, U0, R0, tB, U1, R1, lay.MF, L::KP / 4, warp, lane);
+            else
+                cta_gemm_store_rows<S, kFaceTablesGlobal>(tA, U0, R0, nullptr, nullptr, nullptr, lay.MF, L::KP / 4, warp,
+                                                          lane);
+        } else if (two) {
             cta_gemm_store_staged<S, kFaceChains, kFaceTablesGlobal>(tA, U0, R0, tB, U1, R1, lay.MF, L::KP / 4, warp,
                                                                      lane);
-        else
+        } else {
             cta_gemm_store_staged<S, kFaceChains, kFaceTablesGlobal>(tA, U0, R0, nullptr, nullptr, nullptr, lay.MF,
                                                                      L::KP / 4, warp, lane);
+        }
         __syncthreads();
         const double* geo = tg.fct + static_cast<int64_t>(tile) * NFLD * nq * TE;
         if (gpre) {
