@@ -267,12 +267,28 @@ constexpr bool kGemmRows = true;
 // The row-blocked forward products on 16-row m-tiles (m16n8k4) where the rows allow it.
 constexpr bool kGemmRows16 = false;
 
+// cp.async issue of the coefficient blocks: one (side, element) block per warp with the lanes along
+// the block (true), or one flat index per thread over all blocks (false).  Measured on the 32^3
+// apply: 2.860 -> 2.789 ms (less index arithmetic per copy).
+constexpr bool kStageByWarp = true;
+
 // Issues the cp.async copies of the coefficient blocks of up to UE elements (el[te] < 0: skipped)
 // from xr into the staged buffer U.
 template <class S, int NT>
 __device__ __forceinline__ void stage_blocks(const double* __restrict__ xr, const int* el, double* U, int tid) {
     using SU = Staged<S>;
     constexpr int per_el = S::Q * S::NBF;
+    if constexpr (kStageByWarp) {  // one element block per warp, lanes along the block
+        const int warp = tid >> 5, lane = tid & 31;
+        for (int te = warp; te < SU::UE; te += NT / 32) {
+            const int e = el[te];
+            if (e < 0) continue;
+            double* dst = U + te * SU::LDU;
+            const double* src = xr + static_cast<int64_t>(e) * S::BS;
+            for (int w = lane; w < per_el; w += 32) cp_async8(dst + (w / S::NBF) * SU::KS + (w % S::NBF), src + w);
+        }
+        return;
+    }
     for (int i = tid; i < SU::UE * per_el; i += NT) {
         const int te = i / per_el, w = i % per_el;
         const int r = w / S::NBF, k = w % S::NBF;
@@ -549,13 +565,24 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         const int4* ids = s_ids[slot];
         using SUT = Staged<S>;
         constexpr int per_el = Q * NBF;
-        for (int i = tid; i < 2 * SUT::UE * per_el; i += NT) {
-            const int side = i / (SUT::UE * per_el), j = i % (SUT::UE * per_el);
-            const int te = j / per_el, w = j % per_el;
-            const int e = te < TE ? (side ? ids[te].z : ids[te].y) : -1;
-            if (e >= 0)
-                cp_async8(Ub + (2 * buf + side) * SUT::USZ + te * SUT::LDU + (w / NBF) * SUT::KS + (w % NBF),
-                          xr + static_cast<int64_t>(e) * BS + w);
+        if constexpr (kStageByWarp) {  // one (side, element) block per warp, lanes along the block
+            for (int pb = warp; pb < 2 * SUT::UE; pb += NT / 32) {
+                const int side = pb / SUT::UE, te = pb % SUT::UE;
+                const int e = te < TE ? (side ? ids[te].z : ids[te].y) : -1;  // warp-uniform
+                if (e < 0) continue;
+                double* dst = Ub + (2 * buf + side) * SUT::USZ + te * SUT::LDU;
+                const double* src = xr + static_cast<int64_t>(e) * BS;
+                for (int w = lane; w < per_el; w += 32) cp_async8(dst + (w / NBF) * SUT::KS + (w % NBF), src + w);
+            }
+        } else {
+            for (int i = tid; i < 2 * SUT::UE * per_el; i += NT) {
+                const int side = i / (SUT::UE * per_el), j = i % (SUT::UE * per_el);
+                const int te = j / per_el, w = j % per_el;
+                const int e = te < TE ? (side ? ids[te].z : ids[te].y) : -1;
+                if (e >= 0)
+                    cp_async8(Ub + (2 * buf + side) * SUT::USZ + te * SUT::LDU + (w / NBF) * SUT::KS + (w % NBF),
+                              xr + static_cast<int64_t>(e) * BS + w);
+            }
         }
     };
     int cur_a = -1, cur_b = -1;  // face tables held in TA / TB

@@ -228,6 +228,10 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     }
 }
 
+// Coefficient blocks of the facet kernel staged one (side, element) block per warp (true) or by
+// one flat index per thread with the padding rewritten every tile (false).
+constexpr bool kTc32StageByWarp = true;
+
 template <class S, typename TX>
 __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     face_tc32_kernel(DevOp<float> op, const float* __restrict__ tf, FaceTiles ft, const TX* __restrict__ x,
@@ -255,6 +259,8 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     const int64_t w0 = static_cast<int64_t>(blockIdx.x) * per;
     const int64_t w1 = (w0 + per < nwork) ? w0 + per : nwork;
     int cur_a = -1, cur_b = -1;
+    if constexpr (kTc32StageByWarp)
+        for (int i = tid; i < L::NP * LDU; i += NT) U0[i] = U1[i] = 0.0f;  // padding stays zero
     for (int64_t work = w0; work < w1; ++work) {
         const int tile = static_cast<int>(work % ft.nftiles);
         const int rhs = static_cast<int>(work / ft.nftiles);
@@ -280,16 +286,43 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
             s_e1[tid] = id.z;
         }
         __syncthreads();
-        for (int i = tid; i < L::NP * L::KP; i += NT) {
-            const int c = i / L::KP, k = i % L::KP;
-            const int te = c / Q, r = c % Q;
-            float v0 = 0.0f, v1 = 0.0f;
-            if (k < NBF && c < L::NC && s_f[te] >= 0) {
-                v0 = static_cast<float>(xr[static_cast<int64_t>(s_e0[te]) * BS + k + NBF * r]);
-                if (two) v1 = static_cast<float>(xr[static_cast<int64_t>(s_e1[te]) * BS + k + NBF * r]);
+        if constexpr (kTc32StageByWarp) {
+            // one (side, element) block per warp, the lanes along the block's BS values (all loads
+            // of a lane in flight together); the padding (k >= NBF, columns >= NC) stays zero from
+            // the start, the columns of empty slots keep stale values that only feed their own
+            // (discarded) outputs
+            for (int pb = warp; pb < 2 * TE; pb += NT / 32) {
+                const int side = pb / TE, te = pb % TE;
+                if (side && !two) continue;
+                const int e = side ? s_e1[te] : s_e0[te];
+                if (s_f[te] < 0 || e < 0) continue;
+                const TX* src = xr + static_cast<int64_t>(e) * BS;
+                float* dst = (side ? U1 : U0) + te * Q * LDU;
+                constexpr int IT = (BS + 31) / 32;
+                float v[IT];
+#pragma unroll
+                for (int j = 0; j < IT; ++j) {
+                    const int w = lane + 32 * j;
+                    v[j] = w < BS ? static_cast<float>(src[w]) : 0.0f;
+                }
+#pragma unroll
+                for (int j = 0; j < IT; ++j) {
+                    const int w = lane + 32 * j;
+                    if (w < BS) dst[(w / NBF) * LDU + w % NBF] = v[j];
+                }
             }
-            U0[c * LDU + k] = v0;
-            if (two) U1[c * LDU + k] = v1;
+        } else {
+            for (int i = tid; i < L::NP * L::KP; i += NT) {
+                const int c = i / L::KP, k = i % L::KP;
+                const int te = c / Q, r = c % Q;
+                float v0 = 0.0f, v1 = 0.0f;
+                if (k < NBF && c < L::NC && s_f[te] >= 0) {
+                    v0 = static_cast<float>(xr[static_cast<int64_t>(s_e0[te]) * BS + k + NBF * r]);
+                    if (two) v1 = static_cast<float>(xr[static_cast<int64_t>(s_e1[te]) * BS + k + NBF * r]);
+                }
+                U0[c * LDU + k] = v0;
+                if (two) U1[c * LDU + k] = v1;
+            }
         }
         __syncthreads();
         tc_forward<L>(TA, U0, R0, TB, U1, R1, two ? 2 : 1, lay.MF / 16, warp, lane);
