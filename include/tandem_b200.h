@@ -133,6 +133,17 @@ int tdg_penalty(const tdg_op* op, double* out);
 int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64_t ld,
               void* stream);
 
+/* y_i = A x_i for `count` independent vectors in HOST memory (x_host + i * host_stride,
+ * y_host + i * host_stride; host_stride 0 = the same vector every time; double* for TDG_FP64 and
+ * TDG_MIXED, float* for TDG_FP32) -- a MatMult on host-resident vectors (PetscDGShell::apply,
+ * app/common/PetscDGShell.cpp:48-55, with PETSc Vecs in host memory).  Each vector is copied to
+ * the device, applied and copied back; with pinned host memory the copy in of vector i + 1 and the
+ * copy out of vector i - 1 overlap the apply of vector i (two device buffer pairs, three internal
+ * streams, events).  Ordered after the work already on `stream`; `stream` waits for all of it.
+ * Allocates the device buffers on first use and when the vectors grow. */
+int tdg_apply_host(tdg_op* op, int precision, const void* x_host, void* y_host, int count, int64_t host_stride,
+                   void* stream);
+
 /* Algorithmic FLOPs and compulsory HBM bytes of one single-RHS apply (face-centric counting;
  * tandem's own count is DGOperator::flops_apply, src/form/DGOperator.h:272-280). */
 int64_t tdg_flops_apply(const tdg_op* op);

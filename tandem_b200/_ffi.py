@@ -33,6 +33,7 @@ SYMBOLS = {
     "tdg_material_nodal": (C.c_int, [_p, C.c_int, _p]),
     "tdg_penalty": (C.c_int, [_p, _p]),
     "tdg_apply": (C.c_int, [_p, C.c_int, _p, _p, C.c_int, _i64, _p]),
+    "tdg_apply_host": (C.c_int, [_p, C.c_int, _p, _p, C.c_int, C.c_int64, _p]),
     "tdg_flops_apply": (_i64, [_p]),
     "tdg_bytes_apply": (_i64, [_p, C.c_int]),
     "tdg_bjacobi_setup": (C.c_int, [_p, C.c_int, _p]),

@@ -212,6 +212,34 @@ struct tdg_op {
     // p-multigrid hierarchy and the preconditioner the solves use
     MgHierarchy mg;
     int pc = TDG_PC_BJACOBI;
+    // tdg_apply_host: two device buffer pairs, copy-in / apply / copy-out streams and their events
+    struct HostStream {
+        cudaStream_t s[3] = {nullptr, nullptr, nullptr};
+        cudaEvent_t in[2] = {}, out[2] = {}, freed[2] = {}, entry = nullptr, done[2] = {};
+        void* xd[2] = {nullptr, nullptr};
+        void* yd[2] = {nullptr, nullptr};
+        size_t bytes = 0;
+        bool ready = false;
+        void release() {
+            for (int b = 0; b < 2; ++b) {
+                if (xd[b]) cudaFree(xd[b]);
+                if (yd[b]) cudaFree(yd[b]);
+                xd[b] = yd[b] = nullptr;
+            }
+            bytes = 0;
+            if (!ready) return;
+            for (int k = 0; k < 3; ++k) cudaStreamDestroy(s[k]);
+            for (int b = 0; b < 2; ++b) {
+                cudaEventDestroy(in[b]);
+                cudaEventDestroy(out[b]);
+                cudaEventDestroy(freed[b]);
+                cudaEventDestroy(done[b]);
+            }
+            cudaEventDestroy(entry);
+            ready = false;
+        }
+    } hs;
+    ~tdg_op() { hs.release(); }
 };
 
 namespace {
@@ -1381,6 +1409,71 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
         rc = launch_apply<float>(h.D, h.N, h.kind, op->op32, static_cast<const float*>(x),
                                  static_cast<float*>(y), nrhs, ld, s);
     if (rc) return fail(rc, std::string("apply launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
+int tdg_apply_host(tdg_op* op, int precision, const void* x_host, void* y_host, int count, int64_t host_stride,
+                   void* stream) {
+    if (!op || !x_host || !y_host) return fail(TDG_E_INVALID, "null argument");
+    if (precision != TDG_FP64 && precision != TDG_FP32 && precision != TDG_MIXED)
+        return fail(TDG_E_INVALID, "unknown precision");
+    auto const& h = op->h;
+    const int64_t n = h.E * h.bs;
+    if (count < 1 || (host_stride != 0 && host_stride < n)) return fail(TDG_E_INVALID, "count < 1 or 0 < host_stride < E * bs");
+    if (x_host == y_host) return fail(TDG_E_INVALID, "x and y must not alias");
+    const size_t esz = precision == TDG_FP32 ? sizeof(float) : sizeof(double);
+    const size_t bytes = static_cast<size_t>(n) * esz;
+    auto& hs = op->hs;
+    if (!hs.ready) {
+        for (int k = 0; k < 3; ++k) TDG_CUDA_TRY(cudaStreamCreateWithFlags(&hs.s[k], cudaStreamNonBlocking));
+        for (int b = 0; b < 2; ++b) {
+            TDG_CUDA_TRY(cudaEventCreateWithFlags(&hs.in[b], cudaEventDisableTiming));
+            TDG_CUDA_TRY(cudaEventCreateWithFlags(&hs.out[b], cudaEventDisableTiming));
+            TDG_CUDA_TRY(cudaEventCreateWithFlags(&hs.freed[b], cudaEventDisableTiming));
+            TDG_CUDA_TRY(cudaEventCreateWithFlags(&hs.done[b], cudaEventDisableTiming));
+        }
+        TDG_CUDA_TRY(cudaEventCreateWithFlags(&hs.entry, cudaEventDisableTiming));
+        hs.ready = true;
+    }
+    if (hs.bytes < bytes) {
+        for (int b = 0; b < 2; ++b) {
+            if (hs.xd[b]) cudaFree(hs.xd[b]);
+            if (hs.yd[b]) cudaFree(hs.yd[b]);
+            hs.xd[b] = hs.yd[b] = nullptr;
+        }
+        hs.bytes = 0;
+        for (int b = 0; b < 2; ++b) {
+            if (cudaMalloc(&hs.xd[b], bytes) != cudaSuccess || cudaMalloc(&hs.yd[b], bytes) != cudaSuccess)
+                return fail(TDG_E_NOMEM, "tdg_apply_host: device buffers");
+        }
+        hs.bytes = bytes;
+    }
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    cudaStream_t cin = hs.s[0], cmp = hs.s[1], cout = hs.s[2];
+    // everything already on the caller's stream comes first
+    TDG_CUDA_TRY(cudaEventRecord(hs.entry, user));
+    for (int k = 0; k < 3; ++k) TDG_CUDA_TRY(cudaStreamWaitEvent(hs.s[k], hs.entry, 0));
+    const char* xb = static_cast<const char*>(x_host);
+    char* yb = static_cast<char*>(y_host);
+    const size_t hstep = static_cast<size_t>(host_stride) * esz;
+    for (int i = 0; i < count; ++i) {
+        const int b = i & 1;
+        // buffer pair b is free once the vector two steps back has been copied out
+        if (i >= 2) TDG_CUDA_TRY(cudaStreamWaitEvent(cin, hs.freed[b], 0));
+        TDG_CUDA_TRY(cudaMemcpyAsync(hs.xd[b], xb + i * hstep, bytes, cudaMemcpyHostToDevice, cin));
+        TDG_CUDA_TRY(cudaEventRecord(hs.in[b], cin));
+        TDG_CUDA_TRY(cudaStreamWaitEvent(cmp, hs.in[b], 0));
+        TDG_TRY(tdg_apply(op, precision, hs.xd[b], hs.yd[b], 1, n, cmp));
+        TDG_CUDA_TRY(cudaEventRecord(hs.out[b], cmp));
+        TDG_CUDA_TRY(cudaStreamWaitEvent(cout, hs.out[b], 0));
+        TDG_CUDA_TRY(cudaMemcpyAsync(yb + i * hstep, hs.yd[b], bytes, cudaMemcpyDeviceToHost, cout));
+        TDG_CUDA_TRY(cudaEventRecord(hs.freed[b], cout));
+    }
+    // the caller's stream continues after the last copy out (and after every apply)
+    TDG_CUDA_TRY(cudaEventRecord(hs.done[0], cout));
+    TDG_CUDA_TRY(cudaEventRecord(hs.done[1], cmp));
+    TDG_CUDA_TRY(cudaStreamWaitEvent(user, hs.done[0], 0));
+    TDG_CUDA_TRY(cudaStreamWaitEvent(user, hs.done[1], 0));
     return 0;
 }
 

@@ -146,6 +146,22 @@ class DGOperator:
         _ffi.check(_ffi.lib().tdg_apply(self._h, precision, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
                                         nrhs, ld, _stream(stream)))
 
+    def apply_host(self, x, y, precision: int = FP64, count: int = 1, stride: int | None = None,
+                   stream=None) -> None:
+        """y_i = A x_i for `count` vectors in host memory (CPU tensors, pinned for overlap) at
+        `stride` entries apart (default ndof; 0 = the same vector every time): copy in, apply and
+        copy out, the copies of neighbouring vectors overlapping the apply (tdg_apply_host).
+        Ordered on `stream` like a device apply."""
+        import torch
+        stride = self.ndof if stride is None else stride
+        want = torch.float32 if precision == FP32 else torch.float64
+        need = self.ndof + (count - 1) * stride
+        for t in (x, y):
+            if t.is_cuda or t.dtype != want or not t.is_contiguous() or t.numel() < need:
+                raise ValueError(f"expected a contiguous host {want} tensor with >= {need} entries")
+        _ffi.check(_ffi.lib().tdg_apply_host(self._h, precision, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                             count, stride, _stream(stream)))
+
     # -- explicit wave operator (Elasticity::wave_rhs) ------------------------------------------
     def set_density(self, rho_Q: np.ndarray) -> None:
         """Density at the volume points [E, Nq] (elasticity; default 1)."""
