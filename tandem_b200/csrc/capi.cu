@@ -301,13 +301,20 @@ void facet_tiles(HostOperator const& h, int TE, std::vector<int4>& finfo, std::v
     }
 }
 
+// The face2 facet kernel's geometry rows (see face2_point_swizzle): quads of points with the middle
+// two swapped, rows per field rounded up to the quad, for 8-facet tiles.
+inline bool face2_swizzle_host(int D, int N, int Q) { return mma_tile_elements(D, N, Q) == 8; }
+inline int face2_geo_rows_host(int D, int N, int Q, int nq) { return face2_swizzle_host(D, N, Q) ? (nq + 3) / 4 * 4 : nq; }
+
 // The facet tiles' geometry [tile][field][nq][TE] (n, n_unit, then Poisson K G0, K G1 or
 // elasticity G0, G1, lam0, mu0, lam1, mu1; unused slots zero), the penalty [tile][TE] and the facet
 // and element ids of every slot {facet, side-0 element, side-1 element (-1 unless mode 1), 0}.
 template <typename T>
 void tile_facet_geometry(HostOperator const& h, int TE, std::vector<int> const& fids, std::vector<int4> const& ftiles,
-                         std::vector<T>& fct, std::vector<double>& pen, std::vector<int4>& tids) {
-    const int D = h.D, DD = D * D, nq = h.nq;
+                         std::vector<T>& fct, std::vector<double>& pen, std::vector<int4>& tids, int rows = 0,
+                         bool swizzle = false) {
+    // rows per field (>= nq, zero past nq); point q at row q, or at row face2_point(q) (an involution)
+    const int D = h.D, DD = D * D, nq = rows > 0 ? rows : h.nq, nqh = h.nq;
     const bool poisson = h.kind == 0;
     const int ff = 2 * D + 2 * DD + (poisson ? 0 : 4);
     const size_t nft = ftiles.size();
@@ -322,23 +329,24 @@ void tile_facet_geometry(HostOperator const& h, int TE, std::vector<int> const& 
         for (int te = 0; te < td.y; ++te) {
             const int64_t f = fids[td.x + te];
             auto put = [&](int field, int q, double v) {
-                base[(static_cast<size_t>(field) * nq + q) * TE + te] = static_cast<T>(v);
+                const int row = swizzle ? face2_point(q) : q;
+                base[(static_cast<size_t>(field) * nq + row) * TE + te] = static_cast<T>(v);
             };
-            for (int q = 0; q < nq; ++q) {
+            for (int q = 0; q < nqh; ++q) {
                 for (int i = 0; i < D; ++i) {
-                    put(i, q, h.fN[(static_cast<size_t>(f) * D + i) * nq + q]);
-                    put(D + i, q, h.fNunit[(static_cast<size_t>(f) * D + i) * nq + q]);
+                    put(i, q, h.fN[(static_cast<size_t>(f) * D + i) * nqh + q]);
+                    put(D + i, q, h.fNunit[(static_cast<size_t>(f) * D + i) * nqh + q]);
                 }
                 if (poisson) {
                     for (int side = 0; side < 2; ++side)
                         for (int c = 0; c < DD; ++c)
-                            put(2 * D + side * DD + c, q, h.fCoef[((static_cast<size_t>(f) * 2 + side) * DD + c) * nq + q]);
+                            put(2 * D + side * DD + c, q, h.fCoef[((static_cast<size_t>(f) * 2 + side) * DD + c) * nqh + q]);
                 } else {
                     for (int c = 0; c < DD; ++c) {
-                        put(2 * D + c, q, h.fG0[(static_cast<size_t>(f) * DD + c) * nq + q]);
-                        put(2 * D + DD + c, q, h.fG1[(static_cast<size_t>(f) * DD + c) * nq + q]);
+                        put(2 * D + c, q, h.fG0[(static_cast<size_t>(f) * DD + c) * nqh + q]);
+                        put(2 * D + DD + c, q, h.fG1[(static_cast<size_t>(f) * DD + c) * nqh + q]);
                     }
-                    for (int c = 0; c < 4; ++c) put(2 * D + 2 * DD + c, q, h.fCoef[(static_cast<size_t>(f) * 4 + c) * nq + q]);
+                    for (int c = 0; c < 4; ++c) put(2 * D + 2 * DD + c, q, h.fCoef[(static_cast<size_t>(f) * 4 + c) * nqh + q]);
                 }
             }
             pen[static_cast<size_t>(t) * TE + te] = h.penalty[f];
@@ -378,7 +386,8 @@ int upload_tile_geometry(tdg_op* op, DevArena& arena, std::vector<int> const& fi
     const size_t nft = ftiles.size();
     std::vector<double> fct, pen;
     std::vector<int4> tids;
-    tile_facet_geometry(h, TE, fids, ftiles, fct, pen, tids);
+    tile_facet_geometry(h, TE, fids, ftiles, fct, pen, tids, face2_geo_rows_host(h.D, h.N, h.Q, h.nq),
+                        face2_swizzle_host(h.D, h.N, h.Q));
     if (nft) TDG_CUDA_TRY(arena.upload(&op->face.tids, tids));
     {
         const int* st = nullptr;

@@ -157,12 +157,9 @@ __device__ __forceinline__ void cta_gemm_store_rows(const double* A0, const doub
 #pragma unroll
             for (int j = 0; j < NTN; ++j) dmma(acc[j], a, bp[j][ks * 4]);
         }
-        double* c = (which ? C1 : C0) + (mt * 8 + g) * L::LDN + 2 * t;
+        double* c = (which ? C1 : C0) + (mt * 8 + g) * L::LDN + 2 * t;  // 16-byte aligned (LDN, 2t even)
 #pragma unroll
-        for (int j = 0; j < NTN; ++j) {
-            c[j * 8] = acc[j][0];
-            c[j * 8 + 1] = acc[j][1];
-        }
+        for (int j = 0; j < NTN; ++j) *reinterpret_cast<double2*>(c + j * 8) = make_double2(acc[j][0], acc[j][1]);
     }
 }
 
@@ -500,6 +497,21 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
 
 // ---- facet kernel -----------------------------------------------------------------------------------
 
+// Facet points of a tile's geometry rows: with 8 facets per tile (3D elasticity) the points are
+// stored in quads with the middle two swapped (row r holds point face2_point(r)), so that the
+// pointwise phase's half warps (rows 4c, 4c + 1 or 4c + 2, 4c + 3: points two apart) read and
+// write the trace rows on disjoint banks while still reading the geometry rows contiguously;
+// rows per field: nq rounded up to the quad.  Other tiles keep the points in order.
+template <class S>
+__host__ __device__ constexpr bool face2_point_swizzle() {
+    return MmaTile<S>::TE == 8;
+}
+template <class S>
+__host__ __device__ inline int face2_geo_rows(int nq) {
+    return face2_point_swizzle<S>() ? (nq + 3) / 4 * 4 : nq;
+}
+__host__ __device__ inline int face2_point(int r) { return (r & ~3) | ((r & 1) << 1) | ((r >> 1) & 1); }
+
 template <class S>
 struct Face2Layout {
     int MF, off_TB, off_U, off_R0, off_R1, off_G, total;
@@ -515,7 +527,7 @@ __host__ __device__ inline Face2Layout<S> face2_layout(int nq, int gpre = 0) {
     l.off_R0 = l.off_U + 4 * Staged<S>::USZ;  // [buffer][side]
     l.off_R1 = l.off_R0 + l.MF * L::LDN;
     l.off_G = l.off_R1 + l.MF * L::LDN;
-    l.total = l.off_G + (gpre ? fct_fields<S>() * nq * L::TE : 0);
+    l.total = l.off_G + (gpre ? fct_fields<S>() * face2_geo_rows<S>(nq) * L::TE : 0);
     return l;
 }
 
@@ -540,7 +552,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     double* R1 = sm + lay.off_R1;
     double* Gs = sm + lay.off_G;  // the current facet tile's geometry (gpre)
     __shared__ __align__(8) unsigned long long s_gbar;
-    const unsigned gbytes = static_cast<unsigned>(NFLD * nq * TE * sizeof(double));
+    const int nqg = face2_geo_rows<S>(nq);  // geometry rows per field
+    const unsigned gbytes = static_cast<unsigned>(NFLD * nqg * TE * sizeof(double));
     if (gpre && tid == 0) mbar_init(&s_gbar, 1);
     // tile descriptors and {facet, element 0, element 1} ids of three tiles in flight: the current
     // one, the one whose blocks are being copied in, and the one after it (copied asynchronously one
@@ -612,7 +625,7 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
         // the geometry of this tile into shared memory, behind the trace GEMMs (the previous tile's
         // pointwise phase, the last reader, ended before the barrier above)
         if (gpre && tid == 0)
-            bulk_load(Gs, tg.fct + static_cast<int64_t>(tile) * NFLD * nq * TE, gbytes, &s_gbar);
+            bulk_load(Gs, tg.fct + static_cast<int64_t>(tile) * NFLD * nqg * TE, gbytes, &s_gbar);
         const double* tA = kFaceTablesGlobal ? ft.tables + static_cast<int64_t>(l0) * tab : TA;
         const double* tB = kFaceTablesGlobal ? ft.tables + static_cast<int64_t>(l1) * tab : TB;
         if (!kFaceTablesGlobal && (l0 != cur_a || (two && l1 != cur_b))) {  // uniform: the key is the CTA's
@@ -647,18 +660,18 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
                                                                      L::KP / 4, warp, lane);
         }
         __syncthreads();
-        const double* geo = tg.fct + static_cast<int64_t>(tile) * NFLD * nq * TE;
+        const double* geo = tg.fct + static_cast<int64_t>(tile) * NFLD * nqg * TE;
         if (gpre) {
             if (!mbar_wait_bounded(&s_gbar, static_cast<unsigned>((work - w0) & 1)) && tid == 0 && tg.status)
                 atomicExch(tg.status, 1);
             geo = Gs;
         }
         const double* pens = tg.pen + static_cast<int64_t>(tile) * TE;
-        for (int it = tid; it < TE * nq; it += NT) {
-            const int te = it % TE, q = it / TE;
-            if (sid[te].x < 0) continue;
-            const double* gp = geo + it;  // field f at gp[f * nq * TE]
-            const int64_t fs = static_cast<int64_t>(nq) * TE;
+        for (int it = tid; it < TE * nqg; it += NT) {
+            const int te = it % TE, q = face2_point_swizzle<S>() ? face2_point(it / TE) : it / TE;
+            if (q >= nq || sid[te].x < 0) continue;
+            const double* gp = geo + it;  // field f at gp[f * nqg * TE]
+            const int64_t fs = static_cast<int64_t>(nqg) * TE;
             double* ga0p = R0 + (q * D) * LDN + te * Q;
             double* gb0p = R0 + (D * nq + q) * LDN + te * Q;
             double* ga1p = R1 + (q * D) * LDN + te * Q;
