@@ -357,10 +357,11 @@ void tile_facet_geometry(HostOperator const& h, int TE, std::vector<int> const& 
 }
 
 // Geometry and coefficients of the software-pipelined face-centric apply (apply_face2.cuh) in tile
-// order: per element tile of TE consecutive elements [field][Nq][TE] (J^-1, then the volume
-// coefficients), per facet tile [field][nq][TE] (n, n_unit, then Poisson K G0, K G1 or elasticity
-// G0, G1, lam0, mu0, lam1, mu1) and the penalty [TE]; unused slots zero.  The same values as the
-// reference-layout arrays, read with the tile's elements or facets fastest.
+// order: per element tile of TE consecutive elements [field][Nq rows][TE] (J^-1, then the volume
+// coefficients), per facet tile [field][nq rows][TE] (n, n_unit, then Poisson K G0, K G1 or
+// elasticity G0, G1, lam0, mu0, lam1, mu1) and the penalty [TE]; unused slots and padding rows
+// zero; 8-wide tiles hold point q in row face2_point(q) of nq rounded up to 4 rows.  The same values
+// as the reference-layout arrays, read with the tile's elements or facets fastest.
 int upload_tile_geometry(tdg_op* op, DevArena& arena, std::vector<int> const& fids, std::vector<int4> const& ftiles) {
     auto const& h = op->h;
     const int D = h.D, DD = D * D, Nq = h.Nq;
@@ -369,18 +370,22 @@ int upload_tile_geometry(tdg_op* op, DevArena& arena, std::vector<int> const& fi
     const int ncoef = poisson ? 1 : 2;
     const int vf = DD + ncoef;
     const int64_t vtiles = (h.E + TE - 1) / TE;
-    std::vector<double> vol(static_cast<size_t>(vtiles) * vf * Nq * TE, 0.0);
+    // rows per field and the row of point q (the volume kernel's point swizzle)
+    const bool swz = face2_swizzle_host(D, h.N, h.Q);
+    const int Nqg = face2_geo_rows_host(D, h.N, h.Q, Nq);
+    std::vector<double> vol(static_cast<size_t>(vtiles) * vf * Nqg * TE, 0.0);
 #pragma omp parallel for schedule(static)
     for (int64_t e = 0; e < h.E; ++e) {
         const int64_t t = e / TE;
         const int te = static_cast<int>(e % TE);
-        double* base = &vol[static_cast<size_t>(t) * vf * Nq * TE];
+        double* base = &vol[static_cast<size_t>(t) * vf * Nqg * TE];
         for (int c = 0; c < DD; ++c)
             for (int q = 0; q < Nq; ++q)
-                base[(static_cast<size_t>(c) * Nq + q) * TE + te] = h.vG[(static_cast<size_t>(e) * DD + c) * Nq + q];
+                base[(static_cast<size_t>(c) * Nqg + (swz ? face2_point(q) : q)) * TE + te] =
+                    h.vG[(static_cast<size_t>(e) * DD + c) * Nq + q];
         for (int c = 0; c < ncoef; ++c)
             for (int q = 0; q < Nq; ++q)
-                base[(static_cast<size_t>(DD + c) * Nq + q) * TE + te] =
+                base[(static_cast<size_t>(DD + c) * Nqg + (swz ? face2_point(q) : q)) * TE + te] =
                     h.vCoef[(static_cast<size_t>(e) * ncoef + c) * Nq + q];
     }
     const size_t nft = ftiles.size();

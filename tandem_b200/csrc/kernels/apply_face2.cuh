@@ -316,6 +316,22 @@ __host__ __device__ constexpr int fct_fields() {
     return 2 * S::D + 2 * S::DD + (S::KIND == kPoisson ? 0 : 4);
 }
 
+// Points of a tile's geometry rows (volume and facet kernels): with 8 elements / facets per tile
+// (3D elasticity) the points are stored in quads with the middle two swapped (row r holds point
+// face2_point(r)), so that the pointwise phases' half warps (rows 4c, 4c + 1 or 4c + 2, 4c + 3:
+// points two apart) read and write the product rows on disjoint banks while still reading the
+// geometry rows contiguously; rows per field: the point count rounded up to the quad.  Other tiles
+// keep the points in order.
+template <class S>
+__host__ __device__ constexpr bool face2_point_swizzle() {
+    return MmaTile<S>::TE == 8;
+}
+template <class S>
+__host__ __device__ inline int face2_geo_rows(int nq) {
+    return face2_point_swizzle<S>() ? (nq + 3) / 4 * 4 : nq;
+}
+__host__ __device__ inline int face2_point(int r) { return (r & ~3) | ((r & 1) << 1) | ((r >> 1) & 1); }
+
 // ---- volume kernel ----------------------------------------------------------------------------------
 
 // qc: volume points per pass (all Nq where the buffer fits two CTAs per SM, else MmaTile::QC);
@@ -351,6 +367,7 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
     constexpr int TE = L::TE, NT = L::NT, LDN = L::LDN, LDT = L::LDT;
     constexpr int NFLD = vol_fields<S>();
     const int Nq = op.Nq;
+    const int Nqg = face2_geo_rows<S>(Nq);  // geometry rows per field
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const Vol2Layout<S> lay = vol2_layout<S>(Nq, qc);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -392,7 +409,7 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
         __syncthreads();
         const double* U = Ub + buf * SU::USZ;
         const int* el = s_el[buf];
-        const double* geo = tg.vol + tile * static_cast<int64_t>(NFLD) * Nq * TE;
+        const double* geo = tg.vol + tile * static_cast<int64_t>(NFLD) * Nqg * TE;
         double yacc[L::YPW][2][2];
 #pragma unroll
         for (int j = 0; j < L::YPW; ++j) yacc[j][0][0] = yacc[j][0][1] = yacc[j][1][0] = yacc[j][1][1] = 0.0;
@@ -408,16 +425,19 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
                 cta_gemm_store_staged<S, kVolChains>(TV + q0 * D * LDT, U, R0, nullptr, nullptr, nullptr, rows,
                                                      L::KP / 4, warp, lane);
             __syncthreads();
-            for (int it = tid; it < TE * nqc; it += NT) {
-                const int te = it % TE, qq = it / TE;
-                if (el[te] < 0) continue;
-                const double* gp = geo + static_cast<int64_t>(q0 + qq) * TE + te;  // field f at gp[f * Nq * TE]
+            // chunk starts are multiples of 4, so a chunk's rows hold exactly its points
+            const int nrow = face2_point_swizzle<S>() ? (nqc + 3) / 4 * 4 : nqc;
+            for (int it = tid; it < TE * nrow; it += NT) {
+                const int te = it % TE, row = q0 + it / TE;
+                const int q = face2_point_swizzle<S>() ? face2_point(row) : row, qq = q - q0;
+                if (q >= Nq || el[te] < 0) continue;
+                const double* gp = geo + static_cast<int64_t>(row) * TE + te;  // field f at gp[f * Nqg * TE]
                 double G[DD];
 #pragma unroll
-                for (int c = 0; c < DD; ++c) G[c] = gp[static_cast<int64_t>(c) * Nq * TE];
+                for (int c = 0; c < DD; ++c) G[c] = gp[static_cast<int64_t>(c) * Nqg * TE];
                 double* rr = R0 + (qq * D) * LDN + te * Q;
                 if constexpr (S::KIND == kPoisson) {
-                    const double jwk = gp[static_cast<int64_t>(DD) * Nq * TE];
+                    const double jwk = gp[static_cast<int64_t>(DD) * Nqg * TE];
                     double gx[D];
 #pragma unroll
                     for (int i = 0; i < D; ++i) {
@@ -434,8 +454,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
                         rr[a * LDN] = s;
                     }
                 } else {
-                    const double lam = gp[static_cast<int64_t>(DD) * Nq * TE];
-                    const double mu = gp[static_cast<int64_t>(DD + 1) * Nq * TE];
+                    const double lam = gp[static_cast<int64_t>(DD) * Nqg * TE];
+                    const double mu = gp[static_cast<int64_t>(DD + 1) * Nqg * TE];
                     double Ju[D][D];
 #pragma unroll
                     for (int s = 0; s < D; ++s)
@@ -496,21 +516,6 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
 }
 
 // ---- facet kernel -----------------------------------------------------------------------------------
-
-// Facet points of a tile's geometry rows: with 8 facets per tile (3D elasticity) the points are
-// stored in quads with the middle two swapped (row r holds point face2_point(r)), so that the
-// pointwise phase's half warps (rows 4c, 4c + 1 or 4c + 2, 4c + 3: points two apart) read and
-// write the trace rows on disjoint banks while still reading the geometry rows contiguously;
-// rows per field: nq rounded up to the quad.  Other tiles keep the points in order.
-template <class S>
-__host__ __device__ constexpr bool face2_point_swizzle() {
-    return MmaTile<S>::TE == 8;
-}
-template <class S>
-__host__ __device__ inline int face2_geo_rows(int nq) {
-    return face2_point_swizzle<S>() ? (nq + 3) / 4 * 4 : nq;
-}
-__host__ __device__ inline int face2_point(int r) { return (r & ~3) | ((r & 1) << 1) | ((r >> 1) & 1); }
 
 template <class S>
 struct Face2Layout {
