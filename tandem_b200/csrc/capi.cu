@@ -520,7 +520,10 @@ int upload_tc32(tdg_op* op, DevArena& arena) {
         std::vector<float> fct;
         std::vector<double> pen;
         std::vector<int4> tids;
-        tile_facet_geometry(h, tc32_tile_elements(D, h.Q), fids, ftiles, fct, pen, tids);
+        // the FP32 facet kernel's point swizzle (kTc32PointSwizzle): 3D elasticity, 16-facet tiles
+        const bool swz = D == 3 && h.kind == 1 && tc32_tile_elements(D, h.Q) == 16;
+        tile_facet_geometry(h, tc32_tile_elements(D, h.Q), fids, ftiles, fct, pen, tids, swz ? (nq + 3) / 4 * 4 : nq,
+                            swz);
         if (!ftiles.empty()) {
             TDG_CUDA_TRY(arena.upload(&op->face32.tids, tids));
             TDG_CUDA_TRY(arena.upload(&op->face32.geo, fct));

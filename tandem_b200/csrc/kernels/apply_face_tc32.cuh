@@ -7,6 +7,7 @@
 
 #include "apply_face.cuh"
 #include "apply_tc32.cuh"
+#include "apply_face2.cuh"  // face2_point
 
 namespace tdg {
 
@@ -228,6 +229,19 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     }
 }
 
+// Facet points of the FP32 facet kernel's geometry rows: for 3D elasticity (16 facets per tile, trace
+// rows 3 x 56 words apart) the points are stored in quads with the middle two swapped
+// (face2_point), so that the two points of a warp's pointwise access are two apart and their trace
+// rows fall on disjoint banks; rows per field: nq rounded up to the quad.
+template <class S>
+__host__ __device__ constexpr bool kTc32PointSwizzle() {
+    return S::D == 3 && S::KIND == kElasticity && TcfTile<S>::TE == 16 && TcfTile<S>::LDR % 32 == 24;
+}
+template <class S>
+__host__ __device__ inline int tc32_geo_rows(int nq) {
+    return kTc32PointSwizzle<S>() ? (nq + 3) / 4 * 4 : nq;
+}
+
 // Coefficient blocks of the facet kernel staged one (side, element) block per warp (true) or by
 // one flat index per thread with the padding rewritten every tile (false).
 constexpr bool kTc32StageByWarp = true;
@@ -241,6 +255,7 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     constexpr int TE = L::TE, NT = L::NT, LDR = L::LDR, LDT = L::LDT, LDU = L::LDU;
     constexpr int FF = 2 * D + 2 * DD + (S::KIND == kPoisson ? 0 : 4);  // facet geometry fields
     const int nq = op.nq;
+    const int nqg = tc32_geo_rows<S>(nq);  // geometry rows per field
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TcfLayoutF lay = tcf_face_layout<S>(nq);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -327,10 +342,10 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
         __syncthreads();
         tc_forward<L>(TA, U0, R0, TB, U1, R1, two ? 2 : 1, lay.MF / 16, warp, lane);
         __syncthreads();
-        for (int it = tid; it < TE * nq; it += NT) {
-            const int te = it % TE, q = it / TE;
+        for (int it = tid; it < TE * nqg; it += NT) {
+            const int te = it % TE, q = kTc32PointSwizzle<S>() ? face2_point(it / TE) : it / TE;
             const int fct = s_f[te];
-            if (fct < 0) continue;
+            if (q >= nq || fct < 0) continue;
             float* ga0p = R0 + (q * D) * LDR + te * Q;
             float* gb0p = R0 + (D * nq + q) * LDR + te * Q;
             float* ga1p = R1 + (q * D) * LDR + te * Q;
@@ -354,8 +369,8 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
                     for (int a = 0; a < D; ++a) g1[a][r] = g0[a][r];
                 }
             }
-            const float* gp = ft.geo + static_cast<int64_t>(tile) * FF * nq * TE + it;  // field f at gp[f * fs]
-            const int fs = nq * TE;
+            const float* gp = ft.geo + static_cast<int64_t>(tile) * FF * nqg * TE + it;  // field f at gp[f * fs]
+            const int fs = nqg * TE;
             float n[D], nu[D];
 #pragma unroll
             for (int i = 0; i < D; ++i) {
