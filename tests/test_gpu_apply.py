@@ -325,3 +325,26 @@ def test_apply_face_centric_fp32_and_mixed(case, family):
     torch.cuda.synchronize()
     for got in (y32.double().cpu().numpy(), ym.cpu().numpy()):
         assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-5
+
+
+@pytest.mark.parametrize("family", ["face", "tc05"])
+@pytest.mark.parametrize("kind,dim,N", [(ELASTICITY, 3, 4), (POISSON, 3, 3), (ELASTICITY, 2, 4)])
+def test_fp32_face_families_multi_rhs_padded(family, kind, dim, N):
+    """The FP32 face-centric families (tc05: the tcgen05 volume kernel) on three right-hand sides at
+    a padded leading dimension, FP32 and mixed vectors: every column matches its own single-vector
+    apply to FP32 rounding (1e-6 relative; the facet atomics may add in another order) and the
+    padding is left untouched."""
+    from tandem_b200.operator import MIXED
+    _, op, orc = product_and_oracle(kind, dim, 2, N, True, True)
+    op.set_apply_config(FP32, family)
+    nrhs, ld = 3, op.ndof + 37
+    for prec, dt in ((FP32, torch.float32), (MIXED, torch.float64)):
+        X = torch.randn(nrhs, ld, dtype=dt, device=DEV)
+        Y = torch.full((nrhs, ld), 7.0, dtype=dt, device=DEV)
+        op.apply(X, Y, precision=prec, nrhs=nrhs, ld=ld)
+        for r in range(nrhs):
+            y = torch.zeros(op.ndof, dtype=dt, device=DEV)
+            op.apply(X[r, :op.ndof].contiguous(), y, precision=prec)
+            scale = torch.max(torch.abs(y)).item()
+            assert torch.max(torch.abs(y - Y[r, :op.ndof])).item() <= 1e-6 * scale
+            assert torch.all(Y[r, op.ndof:] == 7.0)
