@@ -242,6 +242,9 @@ __host__ __device__ inline int tc32_geo_rows(int nq) {
     return kTc32PointSwizzle<S>() ? (nq + 3) / 4 * 4 : nq;
 }
 
+// L2 prefetch of each facet tile's geometry block at the start of the tile.
+constexpr bool kTc32L2Prefetch = false;
+
 // Coefficient blocks of the facet kernel staged one (side, element) block per warp (true) or by
 // one flat index per thread with the padding rewritten every tile (false).
 constexpr bool kTc32StageByWarp = true;
@@ -266,7 +269,8 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     float* U1 = sm + lay.off_U1;
     float* R0 = sm + lay.off_R0;
     float* R1 = sm + lay.off_R1;
-    __shared__ int s_f[TE], s_e0[TE], s_e1[TE];
+    // the tile's facet and element ids, double-buffered: the next tile's are loaded during this one
+    __shared__ int s_fb[2][TE], s_e0b[2][TE], s_e1b[2][TE];
     const int tab = lay.MF * LDT;
 
     const int64_t nwork = static_cast<int64_t>(ft.nftiles) * nrhs;
@@ -276,16 +280,48 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     int cur_a = -1, cur_b = -1;
     if constexpr (kTc32StageByWarp)
         for (int i = tid; i < L::NP * LDU; i += NT) U0[i] = U1[i] = 0.0f;  // padding stays zero
-    for (int64_t work = w0; work < w1; ++work) {
+    // {facet, side-0 element, side-1 element} per slot (facet -1 in unused slots) and the tile
+    // descriptor: the first tile's now, each next tile's one iteration ahead
+    int4 td_next = make_int4(0, 0, 0, 0);
+    if (w0 < w1) {
+        const int tile0 = static_cast<int>(w0 % ft.nftiles);
+        td_next = ft.ftiles[tile0];
+        if (tid < TE) {
+            const int4 id = ft.tids[static_cast<int64_t>(tile0) * TE + tid];
+            s_fb[0][tid] = id.x;
+            s_e0b[0][tid] = id.y;
+            s_e1b[0][tid] = id.z;
+        }
+    }
+    int sb = 0;
+    for (int64_t work = w0; work < w1; ++work, sb ^= 1) {
         const int tile = static_cast<int>(work % ft.nftiles);
         const int rhs = static_cast<int>(work / ft.nftiles);
         const TX* xr = x + rhs * ld;
         TX* yr = y + rhs * ld;
-        const int4 td = ft.ftiles[tile];
+        const int4 td = td_next;
         const int key = td.z;
         const int l0 = key & 3, l1 = (key >> 2) & 3, mode = key >> 4;
         const bool two = (mode == 1);
-        __syncthreads();
+        const int* s_f = s_fb[sb];
+        const int* s_e0 = s_e0b[sb];
+        const int* s_e1 = s_e1b[sb];
+        // the next tile's ids and descriptor, in flight during this tile (written to the other
+        // buffer at its end, after every read of that buffer in the previous tile)
+        int4 id_next = make_int4(-1, -1, -1, 0);
+        if (work + 1 < w1) {
+            const int tile1 = static_cast<int>((work + 1) % ft.nftiles);
+            td_next = ft.ftiles[tile1];
+            if (tid < TE) id_next = ft.tids[static_cast<int64_t>(tile1) * TE + tid];
+        }
+        __syncthreads();  // the previous tile is done; this tile's ids are visible
+        if constexpr (kTc32L2Prefetch) {
+            // this tile's geometry block into L2 ahead of its pointwise phase, and the next tile's
+            // coefficient blocks (their ids arrive with this tile) ahead of its staging
+            const char* gb = reinterpret_cast<const char*>(ft.geo + static_cast<int64_t>(tile) * FF * tc32_geo_rows<S>(nq) * TE);
+            const int glines = (FF * tc32_geo_rows<S>(nq) * TE * 4 + 127) / 128;
+            for (int i = tid; i < glines; i += NT) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(gb + 128 * i));
+        }
         if (l0 != cur_a) {
             for (int i = tid; i < tab; i += NT) TA[i] = tf[static_cast<int64_t>(l0) * tab + i];
             cur_a = l0;
@@ -294,13 +330,6 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
             for (int i = tid; i < tab; i += NT) TB[i] = tf[static_cast<int64_t>(l1) * tab + i];
             cur_b = l1;
         }
-        if (tid < TE) {  // {facet, side-0 element, side-1 element}, facet -1 in unused slots
-            const int4 id = ft.tids[static_cast<int64_t>(tile) * TE + tid];
-            s_f[tid] = id.x;
-            s_e0[tid] = id.y;
-            s_e1[tid] = id.z;
-        }
-        __syncthreads();
         if constexpr (kTc32StageByWarp) {
             // one (side, element) block per warp, the lanes along the block's BS values (all loads
             // of a lane in flight together); the padding (k >= NBF, columns >= NC) stays zero from
@@ -449,6 +478,11 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
             }
             atomicAdd(&yr[static_cast<int64_t>(s_e0[te]) * BS + k + NBF * r], static_cast<TX>(v0));
             if (two) atomicAdd(&yr[static_cast<int64_t>(s_e1[te]) * BS + k + NBF * r], static_cast<TX>(v1));
+        }
+        if (tid < TE && work + 1 < w1) {
+            s_fb[sb ^ 1][tid] = id_next.x;
+            s_e0b[sb ^ 1][tid] = id_next.y;
+            s_e1b[sb ^ 1][tid] = id_next.z;
         }
     }
 }
