@@ -242,9 +242,6 @@ __host__ __device__ inline int tc32_geo_rows(int nq) {
     return kTc32PointSwizzle<S>() ? (nq + 3) / 4 * 4 : nq;
 }
 
-// L2 prefetch of each facet tile's geometry block at the start of the tile.
-constexpr bool kTc32L2Prefetch = false;
-
 // Coefficient blocks of the facet kernel staged one (side, element) block per warp (true) or by
 // one flat index per thread with the padding rewritten every tile (false).
 constexpr bool kTc32StageByWarp = true;
@@ -315,13 +312,6 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
             if (tid < TE) id_next = ft.tids[static_cast<int64_t>(tile1) * TE + tid];
         }
         __syncthreads();  // the previous tile is done; this tile's ids are visible
-        if constexpr (kTc32L2Prefetch) {
-            // this tile's geometry block into L2 ahead of its pointwise phase, and the next tile's
-            // coefficient blocks (their ids arrive with this tile) ahead of its staging
-            const char* gb = reinterpret_cast<const char*>(ft.geo + static_cast<int64_t>(tile) * FF * tc32_geo_rows<S>(nq) * TE);
-            const int glines = (FF * tc32_geo_rows<S>(nq) * TE * 4 + 127) / 128;
-            for (int i = tid; i < glines; i += NT) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(gb + 128 * i));
-        }
         if (l0 != cur_a) {
             for (int i = tid; i < tab; i += NT) TA[i] = tf[static_cast<int64_t>(l0) * tab + i];
             cur_a = l0;
