@@ -207,6 +207,11 @@ int tdg_probe_fp64_peak(int kind, int ctas_per_sm, void* stream, double* tflops)
  * clock); split3 = -1 issues no MMA and no commit, so that the wait runs out and the error path
  * (status word, tensor memory freed, TDG_E_TIMEOUT) can be tested. */
 int tdg_probe_tc05_gemm(const float* A, const float* B, float* D, int n, int k, int split3, void* stream);
+/* The accumulator layout of a tcgen05 kind::tf32 MMA (no counterpart in tandem): D = A[m x k]
+ * B[n x k]^T in three TF32 products for m = 64 or 128, then every tensor-memory lane 0..127 and
+ * columns 0..2n-1 (pre-filled with -12345) copied to dump[128][2n].  n a multiple of 16 in [16, 128],
+ * k a multiple of 8 in [8, 64].  Synchronises `stream`. */
+int tdg_probe_tc05_layout(const float* A, const float* B, float* dump, int m, int n, int k, void* stream);
 
 /* --- right-hand side (DGOperator::rhs, src/form/DGOperator.h:189-237) ---------------------- */
 

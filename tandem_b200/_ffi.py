@@ -49,6 +49,7 @@ SYMBOLS = {
     "tdg_set_apply_config": (C.c_int, [_p, C.c_int, C.c_int, C.c_int]),
     "tdg_probe_fp64_peak": (C.c_int, [C.c_int, C.c_int, _p, C.POINTER(C.c_double)]),
     "tdg_probe_tc05_gemm": (C.c_int, [_p, _p, _p, C.c_int, C.c_int, C.c_int, _p]),
+    "tdg_probe_tc05_layout": (C.c_int, [_p, _p, _p, C.c_int, C.c_int, C.c_int, _p]),
     "tdg_set_density": (C.c_int, [_p, _p]),
     "tdg_apply_inverse_mass": (C.c_int, [_p, _p, _p, C.c_int, _i64, _p]),
     "tdg_wave_rhs": (C.c_int, [_p, _p, _p, _p, C.c_int, _i64, _p]),
