@@ -265,6 +265,43 @@ __device__ __forceinline__ void tc05_load_geo(DevOp<float> const& op, int q, int
     }
 }
 
+// The pointwise flux from geometry already in registers (zero geometry gives zero flux).
+template <class S, int NE>
+__device__ __forceinline__ void tc05_flux(const float (&R)[S::D][S::Q][NE], const float (&G)[NE][S::DD],
+                                          const float (&c0)[NE], const float (&c1)[NE],
+                                          float (&T)[NE][S::D][S::Q]) {
+#pragma unroll
+    for (int j = 0; j < NE; ++j) {
+        float g[S::D][S::Q];
+#pragma unroll
+        for (int a = 0; a < S::D; ++a)
+#pragma unroll
+            for (int r = 0; r < S::Q; ++r) g[a][r] = R[a][r][j];
+        vol_point<S>(G[j], c0[j], c1[j], g, T[j]);
+    }
+}
+// ... written to S split hi / lo.
+template <class S, int NE>
+__device__ __forceinline__ void tc05_write_s(Tc05Smem const& b, int q, int te0, const float (&T)[NE][S::D][S::Q]) {
+    using L = Tc05Vol<S>;
+    constexpr int D = S::D, Q = S::Q, TE = L::TE, NQ = L::NQ;
+#pragma unroll
+    for (int j = 0; j < NE; ++j)
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            const int kk = a * NQ + q;
+            const int ob = (kk >> 2) * (L::SCS / 4) + (kk & 3);
+#pragma unroll
+            for (int r = 0; r < Q; ++r) {
+                const int n = r * TE + te0 + j;
+                float h, l;
+                split_tf32(T[j][a][r], h, l);
+                b.Sh[ob + (n >> 3) * 32 + (n & 7) * 4] = h;
+                b.Sl[ob + (n >> 3) * 32 + (n & 7) * 4] = l;
+            }
+        }
+}
+
 // The pointwise flux from geometry already in registers (zero geometry gives zero flux), written to
 // S split hi / lo.
 template <class S, int NE>
@@ -479,9 +516,10 @@ __global__ void __launch_bounds__(256, 1)
 // 4g .. 4g + 3 of the tile (lane = point q / basis function k), the other two stage U, except lane 0
 // of warp 2, which issues the MMAs.  Five mbarriers, one phase per tile each: U staged (255
 // arrivals), forward done (commit), R read (256), S written (256), backward done (commit).  The
-// staging of tile i + 1 and its forward MMAs overlap the pointwise phase and the backward MMAs of
-// tile i; the pointwise threads load the next tile's geometry before they wait for its forward
-// MMAs.  Every wait is bounded; a thread whose wait runs out records the status word and leaves its
+// forward MMAs of tile i + 1 are issued as soon as its U is staged and tile i's R has been read, so
+// they run under the pointwise phase of tile i; the pointwise threads compute tile i's flux in
+// registers while the backward MMAs of tile i - 1 run, and load each tile's geometry before they
+// wait for its forward MMAs.  Every wait is bounded; a thread whose wait runs out records the status word and leaves its
 // loop, so the threads that wait on it run out in turn and the CTA ends.
 template <class S, typename TX>
 __global__ void __launch_bounds__(512, 1)
@@ -517,21 +555,29 @@ __global__ void __launch_bounds__(512, 1)
     auto work_of = [&](int64_t i) { return blockIdx.x + i * gridDim.x; };
     const int grp = warp >> 2, sub = warp & 3;
     bool ok = true;
-    if (warp == 2 && lane == 0) {  // MMA issue
-        {
-            for (int64_t i = 0; i < nmine && ok; ++i) {
-                const unsigned p = static_cast<unsigned>(i & 1);
-                ok = mbar_wait_bounded(&barU, p) && (i == 0 || mbar_wait_bounded(&barR, p ^ 1u));
+    if (warp == 2 && lane == 0) {  // MMA issue: the forward MMAs of tile i + 1 ahead of the backward of tile i
+        if (nmine > 0) {
+            ok = mbar_wait_bounded(&barU, 0u);
+            if (ok) {
+                tc05_fence_after();
+                tc05_issue_fwd<S>(b, tmem);
+                umma_commit(&barF);
+            }
+        }
+        for (int64_t i = 0; i < nmine && ok; ++i) {
+            const unsigned p = static_cast<unsigned>(i & 1);
+            if (i + 1 < nmine) {  // U of tile i + 1 staged, R of tile i read
+                ok = mbar_wait_bounded(&barU, p ^ 1u) && mbar_wait_bounded(&barR, p);
                 if (!ok) break;
                 tc05_fence_after();
                 tc05_issue_fwd<S>(b, tmem);
                 umma_commit(&barF);
-                ok = mbar_wait_bounded(&barS, p);
-                if (!ok) break;
-                tc05_fence_after();
-                tc05_issue_bwd<S>(b, tmem);
-                umma_commit(&barB);
             }
+            ok = mbar_wait_bounded(&barS, p);
+            if (!ok) break;
+            tc05_fence_after();
+            tc05_issue_bwd<S>(b, tmem);
+            umma_commit(&barB);
         }
     } else if (sub >= 2) {  // staging (255 threads): U of tile i once the forward MMAs of tile i - 1 are done
         const int t0 = (grp * 2 + (sub - 2)) * 32 + lane - 1;
@@ -565,6 +611,8 @@ __global__ void __launch_bounds__(512, 1)
             tmem_wait_ld();
             tc05_fence_before();
             mbar_arrive(&barR);
+            float T[4][D][Q];  // the flux, computed while the previous tile's backward MMAs run
+            tc05_flux<S, 4>(R, G, c0, c1, T);
             if (i > 0) {  // the previous tile's y (its backward MMAs also released S)
                 ok = __all_sync(0xffffffffu, mbar_wait_bounded(&barB, p ^ 1u));
                 if (!ok) break;
@@ -573,7 +621,7 @@ __global__ void __launch_bounds__(512, 1)
                 tc05_store_y4<S, TX>(tmem, lane_base, q, te0, (wp % ntiles) * TE, op.E, y + (wp / ntiles) * ld);
                 tc05_fence_before();
             }
-            tc05_pointwise_regs<S, 4>(b, q, te0, R, G, c0, c1);
+            tc05_write_s<S, 4>(b, q, te0, T);
             fence_async_smem();
             mbar_arrive(&barS);
         }
