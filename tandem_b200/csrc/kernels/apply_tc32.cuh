@@ -145,6 +145,23 @@ __device__ __forceinline__ void mma3(float (&c)[4], const uint32_t (&ah)[4], con
     mma_tf32(c, ah, bh0, bh1);
 }
 
+// The same for NPW accumulators sharing one A fragment, the three products of each accumulator in
+// the same order but interleaved across the accumulators, so that consecutive mma are independent
+// (three dependent mma per accumulator would otherwise stall on each other's latency).
+template <int NPW>
+__device__ __forceinline__ void mma3_rows(float (&c)[NPW][4], const uint32_t (&ah)[4], const uint32_t (&al)[4],
+                                          const uint32_t (&bh0)[NPW], const uint32_t (&bh1)[NPW],
+                                          const uint32_t (&bl0)[NPW], const uint32_t (&bl1)[NPW]) {
+#pragma unroll
+    for (int j = 0; j < NPW; ++j) mma_tf32(c[j], al, bh0[j], bh1[j]);
+#pragma unroll
+    for (int j = 0; j < NPW; ++j) mma_tf32(c[j], ah, bl0[j], bl1[j]);
+#pragma unroll
+    for (int j = 0; j < NPW; ++j) mma_tf32(c[j], ah, bh0[j], bh1[j]);
+}
+// 3xTF32 products interleaved across a row's accumulators (mma3_rows) or one accumulator at a time.
+constexpr bool kMma3Interleave = true;
+
 // Forward GEMMs: for each of `nops` (1 or 2) operand pairs (A_i: table rows [mtiles*16][LDT], B_i: U
 // [NP][LDU] column-major), R_i[m][c] = sum_k A_i[m][k] B_i[c][k], stored with ld LDR.  Units
 // (operand, m-tile, n-group) are dealt round-robin to the warps of the pipeline; each table
@@ -170,12 +187,22 @@ __device__ __forceinline__ void tc_forward(const float* A0, const float* B0, flo
             tf32_split(ap[ks * 8 + 8 * L::LDT], ah[1], al[1]);
             tf32_split(ap[ks * 8 + 4], ah[2], al[2]);
             tf32_split(ap[ks * 8 + 4 + 8 * L::LDT], ah[3], al[3]);
+            if constexpr (kMma3Interleave) {
+                uint32_t bh0[L::NPW], bl0[L::NPW], bh1[L::NPW], bl1[L::NPW];
 #pragma unroll
-            for (int j = 0; j < L::NPW; ++j) {
-                uint32_t bh0, bl0, bh1, bl1;
-                tf32_split(bp[j * 8 * L::LDU + ks * 8], bh0, bl0);
-                tf32_split(bp[j * 8 * L::LDU + ks * 8 + 4], bh1, bl1);
-                mma3(acc[j], ah, al, bh0, bh1, bl0, bl1);
+                for (int j = 0; j < L::NPW; ++j) {
+                    tf32_split(bp[j * 8 * L::LDU + ks * 8], bh0[j], bl0[j]);
+                    tf32_split(bp[j * 8 * L::LDU + ks * 8 + 4], bh1[j], bl1[j]);
+                }
+                mma3_rows<L::NPW>(acc, ah, al, bh0, bh1, bl0, bl1);
+            } else {
+#pragma unroll
+                for (int j = 0; j < L::NPW; ++j) {
+                    uint32_t bh0, bl0, bh1, bl1;
+                    tf32_split(bp[j * 8 * L::LDU + ks * 8], bh0, bl0);
+                    tf32_split(bp[j * 8 * L::LDU + ks * 8 + 4], bh1, bl1);
+                    mma3(acc[j], ah, al, bh0, bh1, bl0, bl1);
+                }
             }
         }
         float* rp = (op ? R1 : R0) + (mt * 16 + g) * L::LDR + ng * L::NPW * 8 + 2 * t;
@@ -212,12 +239,22 @@ __device__ __forceinline__ void tc_backproject(const float* A, const float* R, f
             tf32_split(a[4 * L::LDT], ah[2], al[2]);
             tf32_split(a[4 * L::LDT + 8], ah[3], al[3]);
             const float* r = rp + ks * 8 * L::LDR;
+            if constexpr (kMma3Interleave) {
+                uint32_t bh0[L::NPW], bl0[L::NPW], bh1[L::NPW], bl1[L::NPW];
 #pragma unroll
-            for (int j = 0; j < L::NPW; ++j) {
-                uint32_t bh0, bl0, bh1, bl1;
-                tf32_split(r[j * 8], bh0, bl0);
-                tf32_split(r[j * 8 + 4 * L::LDR], bh1, bl1);
-                mma3(y[uu][j], ah, al, bh0, bh1, bl0, bl1);
+                for (int j = 0; j < L::NPW; ++j) {
+                    tf32_split(r[j * 8], bh0[j], bl0[j]);
+                    tf32_split(r[j * 8 + 4 * L::LDR], bh1[j], bl1[j]);
+                }
+                mma3_rows<L::NPW>(y[uu], ah, al, bh0, bh1, bl0, bl1);
+            } else {
+#pragma unroll
+                for (int j = 0; j < L::NPW; ++j) {
+                    uint32_t bh0, bl0, bh1, bl1;
+                    tf32_split(r[j * 8], bh0, bl0);
+                    tf32_split(r[j * 8 + 4 * L::LDR], bh1, bl1);
+                    mma3(y[uu][j], ah, al, bh0, bh1, bl0, bl1);
+                }
             }
         }
     }
