@@ -1473,7 +1473,7 @@ int tdg_apply_host(tdg_op* op, int precision, const void* x_host, void* y_host, 
     const char* xb = static_cast<const char*>(x_host);
     char* yb = static_cast<char*>(y_host);
     const size_t hstep = static_cast<size_t>(host_stride) * esz;
-    for (int i = 0; i < count; ++i) {
+    auto step = [&](int i) -> int {
         const int b = i & 1;
         // buffer pair b is free once the vector two steps back has been copied out
         if (i >= 2) TDG_CUDA_TRY(cudaStreamWaitEvent(cin, hs.freed[b], 0));
@@ -1485,6 +1485,14 @@ int tdg_apply_host(tdg_op* op, int precision, const void* x_host, void* y_host, 
         TDG_CUDA_TRY(cudaStreamWaitEvent(cout, hs.out[b], 0));
         TDG_CUDA_TRY(cudaMemcpyAsync(yb + i * hstep, hs.yd[b], bytes, cudaMemcpyDeviceToHost, cout));
         TDG_CUDA_TRY(cudaEventRecord(hs.freed[b], cout));
+        return 0;
+    };
+    for (int i = 0; i < count; ++i) {
+        if (int rc = step(i)) {
+            // nothing of the caller's host buffers stays in flight after an error
+            for (int k = 0; k < 3; ++k) cudaStreamSynchronize(hs.s[k]);
+            return rc;
+        }
     }
     // the caller's stream continues after the last copy out (and after every apply)
     TDG_CUDA_TRY(cudaEventRecord(hs.done[0], cout));
