@@ -289,6 +289,42 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def host_link_bandwidth(hx, hy, stream, reps=3):
+    """Host link bandwidth with pinned buffers: one direction alone and both directions at once
+    (the copy-in and copy-out streams of the host-buffer apply run together).  Best of `reps`."""
+    dx = torch.empty_like(hx, device="cuda")
+    dy = torch.zeros_like(hy, device="cuda")
+    other = torch.cuda.Stream()
+    nbytes = hx.numel() * hx.element_size()
+
+    def timed(fn):
+        best = float("inf")
+        for _ in range(reps + 1):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b))
+        return best
+
+    def h2d():
+        with torch.cuda.stream(stream):
+            dx.copy_(hx, non_blocking=True)
+
+    def both():
+        other.wait_stream(stream)
+        with torch.cuda.stream(stream):
+            dx.copy_(hx, non_blocking=True)
+        with torch.cuda.stream(other):
+            hy.copy_(dy, non_blocking=True)
+        stream.wait_stream(other)
+
+    ms1, ms2 = timed(h2d), timed(both)
+    return {"h2d_gbs": nbytes / (ms1 * 1e6), "both_gbs": 2 * nbytes / (ms2 * 1e6)}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -367,10 +403,12 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+    link = host_link_bandwidth(hx, hy, stream)
     e2e = {"value": world * n / (ms_e2e * 1e-3), "unit": "DOF/s", "h2d_bytes_per_step": n * 8,
            "d2h_bytes_per_step": n * 8, "ms_per_step": ms_e2e,
            "api": "tdg_apply_host: per step H2D of x from pinned host memory, apply, D2H of y; the copies "
-                  "of neighbouring steps overlap the apply (two device buffer pairs, three streams)"}
+                  "of neighbouring steps overlap the apply (two device buffer pairs, three streams)",
+           "link": link, "link_bound_ms": 2 * n * 8 / (link["both_gbs"] * 1e6)}
 
     # ---- FP32 apply (inner operator of the mixed-precision solve), fastest configuration ----
     if args.family32:

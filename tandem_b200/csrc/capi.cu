@@ -1475,11 +1475,14 @@ int tdg_apply_host(tdg_op* op, int precision, const void* x_host, void* y_host, 
     const size_t hstep = static_cast<size_t>(host_stride) * esz;
     auto step = [&](int i) -> int {
         const int b = i & 1;
-        // buffer pair b is free once the vector two steps back has been copied out
-        if (i >= 2) TDG_CUDA_TRY(cudaStreamWaitEvent(cin, hs.freed[b], 0));
+        // x buffer b is free once the apply two steps back has read it; y buffer b once that apply's
+        // result has been copied out.  Freeing them separately keeps the copy-in stream busy while
+        // the copy-out of two steps back still runs.
+        if (i >= 2) TDG_CUDA_TRY(cudaStreamWaitEvent(cin, hs.out[b], 0));
         TDG_CUDA_TRY(cudaMemcpyAsync(hs.xd[b], xb + i * hstep, bytes, cudaMemcpyHostToDevice, cin));
         TDG_CUDA_TRY(cudaEventRecord(hs.in[b], cin));
         TDG_CUDA_TRY(cudaStreamWaitEvent(cmp, hs.in[b], 0));
+        if (i >= 2) TDG_CUDA_TRY(cudaStreamWaitEvent(cmp, hs.freed[b], 0));
         TDG_TRY(tdg_apply(op, precision, hs.xd[b], hs.yd[b], 1, n, cmp));
         TDG_CUDA_TRY(cudaEventRecord(hs.out[b], cmp));
         TDG_CUDA_TRY(cudaStreamWaitEvent(cout, hs.out[b], 0));
