@@ -292,6 +292,7 @@ def run_reference(args):
 def host_link_bandwidth(hx, hy, stream, reps=3):
     """Host link bandwidth with pinned buffers: one direction alone and both directions at once
     (the copy-in and copy-out streams of the host-buffer apply run together).  Best of `reps`."""
+    import torch
     dx = torch.empty_like(hx, device="cuda")
     dy = torch.zeros_like(hy, device="cuda")
     other = torch.cuda.Stream()
@@ -363,8 +364,8 @@ def run_ours(args):
     probes = fp64_peaks(stream)
     if args.family:
         # a fixed launch configuration (profiling runs): no autotuner candidates before the apply
-        op.set_apply_config(FP64, args.family, args.ctas)
-        tune64 = [{"family": args.family, "ctas_per_sm": args.ctas, "ms": None}]
+        op.set_apply_config(FP64, args.family, args.ctas, args.tile)
+        tune64 = [{"family": args.family, "ctas_per_sm": args.ctas, "tile": args.tile, "ms": None}]
     else:
         tune64 = op.autotune(FP64, stream=stream)
     best64 = min(tune64, key=lambda e: e["ms"] or 0.0)
@@ -1002,6 +1003,8 @@ def main():
     ap.add_argument("--family32", choices=["tensor", "face", "tc05", "simt"], default="",
                     help="cube: FP32 apply kernel family to use instead of the autotuner's pick")
     ap.add_argument("--ctas", type=int, default=2, help="cube: persistent CTAs per SM with --family / --family32")
+    ap.add_argument("--tile", type=int, default=0,
+                    help="cube: volume points per pass with --family face2 (0 = automatic)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", choices=["cube", "batch", "gf", "poisson", "adjoint", "vcycle"], default="cube",
                     help="cube: the apply benchmark (default); batch: uneven batch of 2D elasticity "

@@ -173,6 +173,9 @@ typedef struct {
                          cores (tcgen05.mma kind::tf32, accumulators in tensor memory; shapes with at
                          most 64 volume points, else family 2) */
     int ctas_per_sm;  /* persistent CTAs per SM requested (0 = default) */
+    int tile;         /* family 3, FP64: volume quadrature points per pass of the volume kernel (its
+                         GEMM tiles are D x tile rows of the volume table); 0 = every point in one
+                         pass where the buffers fit two CTAs per SM, else 24; other families 0 */
     double ms;        /* measured time of one apply */
 } tdg_tune_entry;
 
@@ -180,7 +183,8 @@ typedef struct {
  * candidate launch configuration -- the tensor-core kernels (element-centric, and the
  * face-centric pair; FP64 also its software-pipelined form, FP32 also the pair with the tcgen05
  * volume kernel) at 1 to 4 persistent CTAs per SM (clipped to the occupancy limit of the
- * shape's tile) and the SIMT kernel -- with CUDA events on
+ * shape's tile), the software-pipelined FP64 form also at the tile heights that cover the volume
+ * points in 1, 2, 3 and 4 passes, and the SIMT kernel -- with CUDA events on
  * `stream`, and keeps the fastest for later tdg_apply / tdg_solve calls of that precision.
  * entries (optional, up to max_entries) receives every measurement; n_entries their count. */
 int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_entry* entries, int max_entries,
@@ -188,6 +192,10 @@ int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_ent
 /* Sets the apply configuration of `precision` (TDG_FP64 / TDG_FP32; TDG_MIXED follows TDG_FP32)
  * explicitly: kernel family as in tdg_tune_entry and persistent CTAs per SM. */
 int tdg_set_apply_config(tdg_op* op, int precision, int family, int ctas_per_sm);
+/* Sets the tile height of family 3 (TDG_FP64 only): volume points per pass of its volume kernel, as
+ * tdg_tune_entry.tile; a multiple of 8 (3D) or 4 (2D), or 0 for the automatic layout.  A height whose
+ * buffers do not fit the shape makes tdg_apply return TDG_E_INVALID. */
+int tdg_set_apply_tile(tdg_op* op, int precision, int points_per_pass);
 
 /* Measured FP64 throughput of the current device (no counterpart in tandem; the denominator of the
  * FP64 apply's roofline): kind 0 = FP64 FMA on the CUDA cores, 1..4 = the FP64 tensor pipe through

@@ -47,6 +47,7 @@ SYMBOLS = {
     "tdg_adjoint_lame_gradient_noalloc": (C.c_int, [_p, _p, _p, _p, _p, _p]),
     "tdg_autotune": (C.c_int, [_p, C.c_int, C.c_int, _p, _p, C.c_int, _p]),
     "tdg_set_apply_config": (C.c_int, [_p, C.c_int, C.c_int, C.c_int]),
+    "tdg_set_apply_tile": (C.c_int, [_p, C.c_int, C.c_int]),
     "tdg_probe_fp64_peak": (C.c_int, [C.c_int, C.c_int, _p, C.POINTER(C.c_double)]),
     "tdg_probe_tc05_gemm": (C.c_int, [_p, _p, _p, C.c_int, C.c_int, C.c_int, _p]),
     "tdg_probe_tc05_layout": (C.c_int, [_p, _p, _p, C.c_int, C.c_int, C.c_int, _p]),
@@ -97,7 +98,7 @@ class Quadrature(C.Structure):
 
 
 class TuneEntry(C.Structure):
-    _fields_ = [("family", C.c_int), ("ctas_per_sm", C.c_int), ("ms", C.c_double)]
+    _fields_ = [("family", C.c_int), ("ctas_per_sm", C.c_int), ("tile", C.c_int), ("ms", C.c_double)]
 
 
 class SolveOpts(C.Structure):

@@ -199,6 +199,8 @@ struct tdg_op {
     // per SM (0 = default); set by tdg_autotune
     int family[2] = {0, 0};
     int ctas[2] = {0, 0};
+    // volume points per pass of the FP64 face-centric pipelined volume kernel (0 = automatic)
+    int tile[2] = {0, 0};
     const double* penalty = nullptr;
     const int4* sides = nullptr;
     // block-Jacobi
@@ -1385,7 +1387,12 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
     const bool tensor = op->use_mma && op->family[pi] == 0;
     if (precision == TDG_FP64 && op->use_mma && op->family[0] == 3)
         rc = launch_apply_face2(h.D, h.N, h.kind, op->op64, op->mma, op->face, op->tgeo,
-                                static_cast<const double*>(x), static_cast<double*>(y), nrhs, ld, s, op->ctas[0]);
+                                static_cast<const double*>(x), static_cast<double*>(y), nrhs, ld, s, op->ctas[0],
+                                op->tile[0]);
+    // family 3 falls back to family 2 only where its automatic layout does not fit; an explicit
+    // points-per-pass that does not fit is the caller's error
+    if (precision == TDG_FP64 && op->family[0] == 3 && op->tile[0] != 0 && rc == TDG_E_INVALID)
+        return fail(rc, "points per pass do not fit this shape");
     if (precision == TDG_FP64 && op->use_mma && (op->family[0] == 2 || (op->family[0] == 3 && rc == TDG_E_INVALID)))
         rc = launch_apply_face(h.D, h.N, h.kind, op->op64, op->mma, op->face, static_cast<const double*>(x),
                                static_cast<double*>(y), nrhs, ld, s, op->ctas[0]);
@@ -1515,6 +1522,27 @@ int tdg_set_apply_config(tdg_op* op, int precision, int family, int ctas_per_sm)
     return 0;
 }
 
+int tdg_set_apply_tile(tdg_op* op, int precision, int points_per_pass) {
+    if (!op || (precision != TDG_FP64 && precision != TDG_FP32) || points_per_pass < 0)
+        return fail(TDG_E_INVALID, "bad argument");
+    if (points_per_pass != 0 && (precision != TDG_FP64 || points_per_pass % face2_pass_step(op->h.D) != 0))
+        return fail(TDG_E_INVALID, "points per pass: FP64 only, a multiple of 8 (3D) or 4 (2D)");
+    op->tile[precision == TDG_FP64 ? 0 : 1] = points_per_pass;
+    return 0;
+}
+
+// Points-per-pass candidates of the FP64 pipelined volume kernel: one pass (0, the automatic
+// layout), then the smallest multiple of the step that covers the points in 2, 3 and 4 passes.
+static std::vector<int> face2_tile_candidates(int D, int Nq) {
+    std::vector<int> t{0};
+    const int step = face2_pass_step(D);
+    for (int p = 2; p <= 4; ++p) {
+        const int qc = ((Nq + p - 1) / p + step - 1) / step * step;
+        if (qc < Nq && qc >= step && (t.size() == 1 || t.back() != qc)) t.push_back(qc);
+    }
+    return t;
+}
+
 int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_entry* entries, int max_entries,
                  int* n_entries) {
     if (!op || nrhs < 1 || (precision != TDG_FP64 && precision != TDG_FP32))
@@ -1535,19 +1563,20 @@ int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_ent
     // candidates: tensor-core kernel at 1..4 persistent CTAs per SM (clipped to the occupancy
     // limit), then the SIMT kernel
     struct Cand {
-        int family, ctas;
+        int family, ctas, tile;
     };
     std::vector<Cand> cands;
     if (op->use_mma)
-        for (int c = 1; c <= 4; ++c) cands.push_back({0, c});
+        for (int c = 1; c <= 4; ++c) cands.push_back({0, c, 0});
     if (op->use_mma)
-        for (int c = 1; c <= 4; ++c) cands.push_back({2, c});
+        for (int c = 1; c <= 4; ++c) cands.push_back({2, c, 0});
     if (op->use_mma && precision == TDG_FP64)
-        for (int c = 1; c <= 2; ++c) cands.push_back({3, c});
+        for (int c = 1; c <= 2; ++c)
+            for (int t : face2_tile_candidates(h.D, h.Nq)) cands.push_back({3, c, t});
     if (op->use_mma && precision == TDG_FP32)  // the facet kernel's CTAs; the tcgen05 volume kernel runs one per SM
-        for (int c = 1; c <= 4; ++c) cands.push_back({4, c});
-    cands.push_back({1, 0});
-    const int fam0 = op->family[pi], ct0 = op->ctas[pi];
+        for (int c = 1; c <= 4; ++c) cands.push_back({4, c, 0});
+    cands.push_back({1, 0, 0});
+    const int fam0 = op->family[pi], ct0 = op->ctas[pi], tl0 = op->tile[pi];
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1556,7 +1585,12 @@ int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_ent
     for (size_t i = 0; i < cands.size() && rc == 0; ++i) {
         op->family[pi] = cands[i].family;
         op->ctas[pi] = cands[i].ctas;
+        op->tile[pi] = cands[i].tile;
         for (int w = 0; w < 2 && rc == 0; ++w) rc = tdg_apply(op, precision, x, y, nrhs, ld, stream);
+        if (rc == TDG_E_INVALID && cands[i].tile != 0) {  // a points-per-pass that does not fit: skip it
+            rc = 0;
+            continue;
+        }
         if (rc) break;
         constexpr int reps = 5;
         cudaEventRecord(e0, s);
@@ -1566,7 +1600,7 @@ int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_ent
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, e0, e1);
         const double per = ms / reps;
-        if (entries && n < max_entries) entries[n] = tdg_tune_entry{cands[i].family, cands[i].ctas, per};
+        if (entries && n < max_entries) entries[n] = tdg_tune_entry{cands[i].family, cands[i].ctas, cands[i].tile, per};
         ++n;
         if (per < best) {
             best = per;
@@ -1580,10 +1614,12 @@ int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_ent
     if (rc || bi < 0) {
         op->family[pi] = fam0;
         op->ctas[pi] = ct0;
+        op->tile[pi] = tl0;
         return rc ? rc : fail(TDG_E_CUDA, "autotune found no candidate");
     }
     op->family[pi] = cands[bi].family;
     op->ctas[pi] = cands[bi].ctas;
+    op->tile[pi] = cands[bi].tile;
     if (n_entries) *n_entries = n;
     return 0;
 }

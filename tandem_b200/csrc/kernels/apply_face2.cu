@@ -23,9 +23,10 @@ int configure2(K kern, size_t smem, int threads, int& per_sm) {
 
 template <class S>
 int run_face2(DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, TileGeo const& tg, const double* x,
-              double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas) {
+              double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas, int qc) {
     using L = MmaTile<S>;
-    const Vol2Layout<S> vl = vol2_layout_auto<S>(op.Nq);
+    if (qc < 0 || (qc > 0 && qc % face2_pass_step(S::D) != 0)) return TDG_E_INVALID;
+    const Vol2Layout<S> vl = qc == 0 ? vol2_layout_auto<S>(op.Nq) : vol2_layout<S>(op.Nq, qc < op.Nq ? qc : op.Nq);
     // the geometry prefetch where the policy allows it (two CTAs per SM: at most ~113 KB each)
     const size_t two_cta = 112 * 1024;
     int gpre = 0;
@@ -75,19 +76,19 @@ int run_face2(DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, 
 
 template <int D, int N>
 int face2_kind(int kind, DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, TileGeo const& tg,
-               const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas) {
-    if (kind == kPoisson) return run_face2<Shape<D, N, kPoisson>>(op, mt, ft, tg, x, y, nrhs, ld, s, ctas);
-    return run_face2<Shape<D, N, kElasticity>>(op, mt, ft, tg, x, y, nrhs, ld, s, ctas);
+               const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas, int qc) {
+    if (kind == kPoisson) return run_face2<Shape<D, N, kPoisson>>(op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
+    return run_face2<Shape<D, N, kElasticity>>(op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
 }
 
 template <int D>
 int face2_deg(int N, int kind, DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, TileGeo const& tg,
-              const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas) {
+              const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas, int qc) {
     switch (N) {
-        case 1: return face2_kind<D, 1>(kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas);
-        case 2: return face2_kind<D, 2>(kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas);
-        case 3: return face2_kind<D, 3>(kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas);
-        case 4: return face2_kind<D, 4>(kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas);
+        case 1: return face2_kind<D, 1>(kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
+        case 2: return face2_kind<D, 2>(kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
+        case 3: return face2_kind<D, 3>(kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
+        case 4: return face2_kind<D, 4>(kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
         default: return TDG_E_INVALID;
     }
 }
@@ -95,10 +96,11 @@ int face2_deg(int N, int kind, DevOp<double> const& op, MmaTiles const& mt, Face
 }  // namespace
 
 int launch_apply_face2(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft,
-                       TileGeo const& tg, const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas) {
+                       TileGeo const& tg, const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas,
+                       int qc) {
     if (nrhs < 1 || !mt.tables || !tg.vol || (ft.nftiles > 0 && (!tg.fct || !ft.tids))) return TDG_E_INVALID;
-    if (D == 2) return face2_deg<2>(N, kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas);
-    if (D == 3) return face2_deg<3>(N, kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas);
+    if (D == 2) return face2_deg<2>(N, kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
+    if (D == 3) return face2_deg<3>(N, kind, op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
     return TDG_E_INVALID;
 }
 

@@ -334,8 +334,10 @@ __host__ __device__ inline int face2_point(int r) { return (r & ~3) | ((r & 1) <
 
 // ---- volume kernel ----------------------------------------------------------------------------------
 
-// qc: volume points per pass (all Nq where the buffer fits two CTAs per SM, else MmaTile::QC);
-// fewer passes mean fewer barriers per tile and more pointwise items per pass.
+// qc: volume points per pass (all Nq where the buffer fits two CTAs per SM, else MmaTile::QC, or the
+// autotuner's pick); fewer passes mean fewer barriers per tile and more pointwise items per pass.
+// Every pass but the last starts its table rows on an 8-row mma tile (qc * D rows) and its points on
+// a quad of swizzled points, so qc is a multiple of face2_pass_step(D) (dispatch.hpp).
 template <class S>
 struct Vol2Layout {
     int MV, qc, off_U, off_R, total;

@@ -33,9 +33,14 @@ int launch_apply_face(int D, int N, int kind, DevOp<double> const& op, MmaTiles 
 // Software-pipelined face-centric FP64 apply (apply_face2.cuh): cp.async double-buffered
 // coefficient blocks, tile-ordered geometry (TileGeo), both sides' fluxes from one stress.
 struct TileGeo;
+// qc: volume points per pass of the volume kernel (the M extent of its GEMM tiles is D x qc rows);
+// 0 = every point in one pass where the buffers fit two CTAs per SM, else 24; otherwise a multiple
+// of face2_pass_step(D) (TDG_E_INVALID else).
 int launch_apply_face2(int D, int N, int kind, DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft,
                        TileGeo const& tg, const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s,
-                       int ctas = 0);
+                       int ctas = 0, int qc = 0);
+// Granularity of qc: passes start on whole 8-row GEMM tiles and on whole point quads.
+constexpr int face2_pass_step(int D) { return D == 3 ? 8 : 4; }
 
 // Face-centric FP32 apply (apply_face_tc32.cuh), TX = float or double vectors.
 struct Tc32Tiles;

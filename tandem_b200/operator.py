@@ -193,17 +193,20 @@ class DGOperator:
     def autotune(self, precision: int = FP64, nrhs: int = 1, stream=None) -> list[dict]:
         """Times the candidate apply launch configurations on this operator and keeps the fastest
         for later applies and solves in `precision` (tdg_autotune).  Returns every measurement."""
-        entries = (_ffi.TuneEntry * 16)()
+        entries = (_ffi.TuneEntry * 64)()
         n = C.c_int(0)
-        _ffi.check(_ffi.lib().tdg_autotune(self._h, precision, nrhs, _stream(stream), entries, 16, C.byref(n)))
-        return [dict(family=FAMILIES[e.family], ctas_per_sm=e.ctas_per_sm, ms=e.ms) for e in entries[:n.value]]
+        _ffi.check(_ffi.lib().tdg_autotune(self._h, precision, nrhs, _stream(stream), entries, 64, C.byref(n)))
+        return [dict(family=FAMILIES[e.family], ctas_per_sm=e.ctas_per_sm, tile=e.tile, ms=e.ms)
+                for e in entries[:n.value]]
 
-    def set_apply_config(self, precision: int, family: str, ctas_per_sm: int = 0) -> None:
+    def set_apply_config(self, precision: int, family: str, ctas_per_sm: int = 0, tile: int = 0) -> None:
         """Selects the apply kernel explicitly: family "tensor" (element-centric tensor cores),
         "face" (face-centric), "face2" (face-centric, software-pipelined; FP64), "tc05" (FP32:
         face-centric with the volume term on tcgen05) or "simt";
-        ctas_per_sm 0 = the default occupancy."""
+        ctas_per_sm 0 = the default occupancy; tile (FP64 "face2" only) = volume points per pass of
+        its volume kernel, a multiple of 8 (3D) or 4 (2D), 0 = automatic (tdg_set_apply_tile)."""
         _ffi.check(_ffi.lib().tdg_set_apply_config(self._h, precision, FAMILIES.index(family), ctas_per_sm))
+        _ffi.check(_ffi.lib().tdg_set_apply_tile(self._h, precision, tile))
 
     def flops_apply(self) -> int:
         return int(_ffi.lib().tdg_flops_apply(self._h))

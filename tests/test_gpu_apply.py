@@ -3,6 +3,8 @@
 Tolerances: FP64 results agree with the oracle to 1e-12 relative (max-norm over the vector,
 summation order differs); FP32 applies to 2e-5 relative; solutions to the relative residual
 target 1e-10 of the metric."""
+import math
+
 import numpy as np
 import pytest
 import torch
@@ -303,6 +305,49 @@ def test_face_centric_multi_rhs_and_solve(family):
         scale = torch.max(torch.abs(y)).item()
         assert torch.max(torch.abs(y - Y[r, :op.ndof])).item() <= 1e-14 * scale
         assert torch.all(Y[r, op.ndof:] == 7.0)
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "k{}d{}n{}p{}c{}v{}".format(*c))
+def test_face2_points_per_pass_matches_oracle(case):
+    """The pipelined FP64 pair with its volume term in several passes over the quadrature points
+    (tdg_set_apply_tile: every pass height from one step up to the first at or above the point count)
+    against the oracle, 1e-12 like the one-pass layout."""
+    kind, dim, n, N, curved, var = case
+    _, op, orc = product_and_oracle(kind, dim, n, N, curved, var)
+    x = np.random.default_rng(7).standard_normal(op.ndof)
+    ref = orc.apply(x)
+    step = 8 if dim == 3 else 4
+    heights = list(range(step, op.Nq + step, step))
+    assert len(heights) >= 1 and heights[-1] >= op.Nq
+    for tile in heights:
+        op.set_apply_config(FP64, "face2", 2, tile)
+        y = torch.full((op.ndof,), 3.0, dtype=torch.float64, device=DEV)
+        op.apply(dev(x), y)
+        torch.cuda.synchronize()
+        assert rel(y.cpu().numpy(), ref) < 1e-12, tile
+
+
+def test_face2_points_per_pass_arguments_and_autotune():
+    """Pass heights off the step, negative or for FP32 are refused; the autotuner times the
+    pipelined pair at the heights that cover the points in 1 to 4 passes and keeps a working pick."""
+    _, op, orc = product_and_oracle(ELASTICITY, 3, 2, 4, True, True)
+    for bad in (-8, 4, 12, 57):
+        with pytest.raises(RuntimeError):
+            op.set_apply_config(FP64, "face2", 2, bad)
+    with pytest.raises(RuntimeError):
+        op.set_apply_config(FP32, "tc05", 2, 8)
+    tune = op.autotune(FP64)
+    tiles = sorted({e["tile"] for e in tune if e["family"] == "face2"})
+    step = 8
+    heights = {math.ceil(math.ceil(op.Nq / p) / step) * step for p in (2, 3, 4)}
+    want = [0] + sorted(h for h in heights if h < op.Nq)
+    assert tiles == want, (tiles, op.Nq)
+    assert all(e["tile"] == 0 for e in tune if e["family"] != "face2")
+    x = np.random.default_rng(3).standard_normal(op.ndof)
+    y = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+    op.apply(dev(x), y)
+    torch.cuda.synchronize()
+    assert rel(y.cpu().numpy(), orc.apply(x)) < 1e-12
 
 
 @pytest.mark.parametrize("family", ["face", "tc05"])
