@@ -50,6 +50,84 @@ __global__ void k_cg_shift(double* __restrict__ scal, int nseg, int only_replace
         scal[r * kScal + kRZ] = scal[r * kScal + kRZnew];
 }
 
+// ---- device-side loop control (CUDA graph conditional `while` nodes) -------------------------------
+//
+// A loop whose trip count depends on device data (a Krylov block that ends when a segment asks for a
+// reliable update, the coarse CG of the multigrid preconditioner that ends at its tolerance) runs as
+// a conditional while node of a CUDA graph: its body ends with one of the control kernels below,
+// which sets the loop condition from the Krylov scalars.  Every loop is bounded by an iteration
+// limit that the control kernel itself counts, so it ends even when no segment converges.
+//
+// Loop counters, per operator (long long each): kLoopIts iterations of the current outer block,
+// kLoopLimit its limit (written by the host before each launch), kCoarseIts iterations of the
+// current coarse solve, kCoarseDiverged set when a coarse column's residual is not finite,
+// kCoarseTotal coarse iterations since the multigrid set-up.
+enum LoopSlot { kLoopIts = 0, kLoopLimit = 1, kCoarseIts = 2, kCoarseDiverged = 3, kCoarseTotal = 4, kLoopSlots = 8 };
+// Krylov scalar slot of the outer block's stopping threshold: max(delta rmax, tol)^2 per segment.
+constexpr int kThr = 9;
+static_assert(kThr < kScal, "threshold slot inside the scalar row");
+
+// After each iteration of a device-looped Krylov block: counts it and ends the loop when an active
+// segment's recurrence residual r.r met its threshold scal[kThr] or is not finite, or when the
+// block's limit is reached.  One CTA.
+__global__ void k_block_ctl(const double* __restrict__ scal, int nseg, long long* __restrict__ ctl,
+                            cudaGraphConditionalHandle h) {
+    __shared__ int stop;
+    if (threadIdx.x == 0) stop = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nseg; i += blockDim.x) {
+        const double* sc = scal + static_cast<int64_t>(i) * kScal;
+        const double rr = sc[kRR];
+        if (sc[kActive] != 0.0 && !(rr > sc[kThr] && rr < INFINITY)) stop = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const long long n = ++ctl[kLoopIts];
+        cudaGraphSetConditional(h, (stop || n >= ctl[kLoopLimit]) ? 0u : 1u);
+    }
+}
+
+// Coarse CG control of the multigrid preconditioner, one CTA.  mode 0, before the loop: tolerance
+// scal[kThr] = rtol2 r0.r0 per column, columns with r0 = 0 inactive, counter reset.  mode 1, after
+// each block of `block` iterations: columns whose r.r met their tolerance stop, a non-finite r.r
+// stops its column and raises the divergence flag.  Both set the loop condition: a column is
+// active and fewer than max_it iterations ran.  mode 2, after the loop: the solve's iterations
+// are added to the running total.
+__global__ void k_coarse_ctl(double* __restrict__ scal, int ncol, double rtol2, long long* __restrict__ ctl,
+                             int max_it, int block, int mode, cudaGraphConditionalHandle h) {
+    if (mode == 2) {
+        if (threadIdx.x == 0) ctl[kCoarseTotal] += ctl[kCoarseIts];
+        return;
+    }
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    int mine = 0;
+    for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+        double* sc = scal + static_cast<int64_t>(c) * kScal;
+        const double rr = sc[kRR];
+        if (mode == 0) {
+            sc[kThr] = rtol2 * rr;
+            sc[kActive] = rr > 0.0 ? 1.0 : 0.0;
+        } else if (sc[kActive] != 0.0) {
+            if (!(rr < INFINITY) || rr != rr) {
+                sc[kActive] = 0.0;
+                ctl[kCoarseDiverged] = 1;
+            } else if (rr <= sc[kThr]) {
+                sc[kActive] = 0.0;
+            }
+        }
+        mine |= sc[kActive] != 0.0;
+    }
+    if (mine) any = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const long long n = mode == 0 ? 0 : ctl[kCoarseIts] + block;
+        ctl[kCoarseIts] = n;
+        cudaGraphSetConditional(h, (any && n < max_it) ? 1u : 0u);
+    }
+}
+
 }  // namespace tdg
 
 using namespace tdg;
@@ -147,7 +225,6 @@ struct MgHierarchy {
     int32_t* nbr = nullptr;
     int32_t* colour = nullptr;
     int* status = nullptr;
-    int64_t coarse_its = 0;
     // the coarse system the CG solves: the coarsest DG level, or (aux) the continuous P1 level
     // below it; cn unknowns per right-hand side, block-Jacobi blocks of cbs x cbs, cnb of them
     bool aux = false;
@@ -164,13 +241,17 @@ struct MgHierarchy {
     Chunk* chunks = nullptr;
     int* seg_chunk = nullptr;
     std::vector<int> seg_chunk_h;
-    // coarse CG: a block of kCoarseBlock iterations captured for graph_nrhs columns
+    // the whole coarse CG (start, device loop of kCoarseBlock-iteration blocks) as one graph for
+    // graph_nrhs columns of the right-hand side graph_b and the solution graph_x
     cudaGraphExec_t coarse_exec = nullptr;
     int graph_nrhs = 0;
+    const double* graph_b = nullptr;
+    const double* graph_x = nullptr;
     void reset_graph() {
         if (coarse_exec) cudaGraphExecDestroy(coarse_exec);
         coarse_exec = nullptr;
         graph_nrhs = 0;
+        graph_b = graph_x = nullptr;
     }
     ~MgHierarchy() { reset_graph(); }
 };
@@ -214,6 +295,11 @@ struct tdg_op {
     // p-multigrid hierarchy and the preconditioner the solves use
     MgHierarchy mg;
     int pc = TDG_PC_BJACOBI;
+    // device-looped graphs: loop counters (LoopSlot) and two non-blocking streams on which loop
+    // bodies (and the stand-alone coarse-solve graph) are captured
+    DevArena arena_loop;
+    long long* loop = nullptr;
+    cudaStream_t side[2] = {nullptr, nullptr};
     // tdg_apply_host: two device buffer pairs, copy-in / apply / copy-out streams and their events
     struct HostStream {
         cudaStream_t s[3] = {nullptr, nullptr, nullptr};
@@ -241,10 +327,72 @@ struct tdg_op {
             ready = false;
         }
     } hs;
-    ~tdg_op() { hs.release(); }
+    ~tdg_op() {
+        hs.release();
+        for (cudaStream_t& q : side)
+            if (q) cudaStreamDestroy(q);
+    }
 };
 
 namespace {
+
+// Loop counters and side streams of the device-looped graphs (once per operator; outside any
+// capture).
+int ensure_loop(tdg_op* op) {
+    if (op->loop) return 0;
+    for (cudaStream_t& q : op->side)
+        if (!q) TDG_CUDA_TRY(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+    long long* c = nullptr;
+    TDG_CUDA_TRY(op->arena_loop.alloc(&c, kLoopSlots));
+    TDG_CUDA_TRY(cudaMemset(c, 0, kLoopSlots * sizeof(long long)));
+    op->loop = c;
+    return 0;
+}
+
+// The side stream on which the body of a loop emitted from stream s is captured.
+cudaStream_t side_for(tdg_op* op, cudaStream_t s) { return s == op->side[0] ? op->side[1] : op->side[0]; }
+
+// Emits a device loop into the graph being captured on s: start(h) launches on s what sets the
+// first condition through the handle h (the loop runs while it is non-zero; it starts at `first`
+// when start sets nothing), a while node follows, and body(b, h) launches one pass of the loop
+// body on the side stream b, ending with a kernel that sets the next condition.  Later work on s
+// follows the loop.
+template <class Start, class Body>
+int emit_while(tdg_op* op, cudaStream_t s, unsigned first, Start&& start, Body&& body) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    TDG_CUDA_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+    if (st != cudaStreamCaptureStatusActive) return fail(TDG_E_CUDA, "device loop outside a stream capture");
+    cudaGraphConditionalHandle h{};
+    TDG_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, first, cudaGraphCondAssignDefault));
+    TDG_TRY(start(h));
+    TDG_CUDA_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    TDG_CUDA_TRY(cudaGraphAddNode(&node, g, deps, nd, &p));
+    TDG_CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaStream_t b = side_for(op, s);
+    TDG_CUDA_TRY(cudaStreamBeginCaptureToGraph(b, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal));
+    const int rc = body(b, h);
+    cudaGraph_t done = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(b, &done);
+    if (rc) return rc;
+    if (ce != cudaSuccess) return fail(TDG_E_CUDA, std::string("device loop body: ") + cudaGetErrorString(ce));
+    return 0;
+}
+
+// True when s is capturing a graph.
+bool capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    return s != nullptr && cudaStreamIsCapturing(s, &st) == cudaSuccess && st == cudaStreamCaptureStatusActive;
+}
 
 int upload_common(tdg_op* op) {
     if (op->penalty) return 0;
@@ -744,13 +892,6 @@ int mg_smooth(tdg_op* op, int l, const double* b, double* x, bool x_zero, int nr
     return 0;
 }
 
-int mg_read_scalars(tdg_op* op, std::vector<double>& hs, int nrhs, cudaStream_t s) {
-    hs.resize(static_cast<size_t>(nrhs) * kScal);
-    TDG_CUDA_TRY(cudaMemcpyAsync(hs.data(), op->mg.scal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-    TDG_CUDA_TRY(cudaStreamSynchronize(s));
-    return 0;
-}
-
 // kCoarseBlock CG iterations of the coarse system with device-resident scalars, nrhs columns.
 int mg_coarse_block(tdg_op* op, SegPlan const& sp, double* x, int nrhs, cudaStream_t s) {
     auto& mg = op->mg;
@@ -774,10 +915,13 @@ int mg_coarse_block(tdg_op* op, SegPlan const& sp, double* x, int nrhs, cudaStre
 
 // Coarse solve of nrhs columns (contiguous, cn entries each): CG with the block-Jacobi inverses
 // from x = 0, one segment per column, until every column has ||r|| <= coarse_rtol ||b|| (checked
-// every kCoarseBlock iterations, the blocks replayed from a CUDA graph on a non-default stream) or
-// coarse_max_it iterations.  x is always the coarse system's own vector (the coarsest DG level's,
-// or the continuous P1 level's).
-int mg_coarse_solve(tdg_op* op, const double* b, double* x, int nrhs, cudaStream_t s) {
+// on the device every kCoarseBlock iterations) or coarse_max_it iterations.  The whole solve is a
+// device loop (emit_while) with no host synchronisation: emitted into the caller's capture when s
+// is capturing (a V-cycle inside a graph-captured Krylov block), else captured once per (nrhs, b,
+// x) as a graph of its own and launched on s.  A column whose residual is not finite stops and
+// raises the loop counter kCoarseDiverged, which the solve drivers and tdg_mg_apply read.  x is
+// always the coarse system's own vector (the coarsest DG level's, or the continuous P1 level's).
+int mg_coarse_emit(tdg_op* op, const double* b, double* x, int nrhs, cudaStream_t s) {
     auto& mg = op->mg;
     SegPlan sp;
     sp.nseg = nrhs;
@@ -787,70 +931,66 @@ int mg_coarse_solve(tdg_op* op, const double* b, double* x, int nrhs, cudaStream
     sp.op_nrhs = nrhs;
     sp.op_ld = mg.cn;
     const size_t nc = static_cast<size_t>(mg.cn) * nrhs;
-    std::vector<double> hs(static_cast<size_t>(nrhs) * kScal, 0.0);
-    for (int c = 0; c < nrhs; ++c) hs[static_cast<size_t>(c) * kScal + kActive] = 1.0;
+    long long* ctl = op->loop;
+    const double rtol2 = mg.opts.coarse_rtol * mg.opts.coarse_rtol;
+    const int max_it = mg.opts.coarse_max_it;
     TDG_CUDA_TRY(cudaMemsetAsync(x, 0, nc * sizeof(double), s));
     TDG_CUDA_TRY(cudaMemcpyAsync(mg.cr, b, nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    TDG_CUDA_TRY(cudaMemcpyAsync(mg.scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    TDG_CUDA_TRY(cudaMemsetAsync(mg.scal, 0, static_cast<size_t>(nrhs) * kScal * sizeof(double), s));
     TDG_TRY(mgk(launch_bjac_apply<double, double>(mg.cbs, mg.cnb, mg.cinv, mg.cr, mg.cz, nrhs, mg.cn, s), "coarse PC"));
     k_copy<double><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, mg.cz, mg.cp);
     TDG_TRY(dots<double>(sp, mg.cr, mg.cz, mg.cr, mg.cr, mg.partial, mg.scal, kRZ, kRR, s));
-    TDG_TRY(mg_read_scalars(op, hs, nrhs, s));
-    std::vector<double> tol2(static_cast<size_t>(nrhs));
-    bool any = false, changed = false;
-    for (int c = 0; c < nrhs; ++c) {
-        double* sc = &hs[static_cast<size_t>(c) * kScal];
-        tol2[static_cast<size_t>(c)] = mg.opts.coarse_rtol * mg.opts.coarse_rtol * sc[kRR];
-        if (!(sc[kRR] > 0.0)) {
-            sc[kActive] = 0.0;
-            changed = true;
-        } else {
-            any = true;
+    auto start = [&](cudaGraphConditionalHandle h) {
+        k_coarse_ctl<<<1, 256, 0, s>>>(mg.scal, nrhs, rtol2, ctl, max_it, kCoarseBlock, 0, h);
+        return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "multigrid: coarse CG control");
+    };
+    auto body = [&](cudaStream_t bs, cudaGraphConditionalHandle h) {
+        TDG_TRY(mg_coarse_block(op, sp, x, nrhs, bs));
+        k_coarse_ctl<<<1, 256, 0, bs>>>(mg.scal, nrhs, rtol2, ctl, max_it, kCoarseBlock, 1, h);
+        return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "multigrid: coarse CG control");
+    };
+    TDG_TRY(emit_while(op, s, 0u, start, body));
+    k_coarse_ctl<<<1, 32, 0, s>>>(mg.scal, nrhs, rtol2, ctl, max_it, kCoarseBlock, 2, cudaGraphConditionalHandle{});
+    return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "multigrid: coarse CG control");
+}
+
+int mg_coarse_solve(tdg_op* op, const double* b, double* x, int nrhs, cudaStream_t s) {
+    auto& mg = op->mg;
+    if (capturing(s)) return mg_coarse_emit(op, b, x, nrhs, s);
+    TDG_TRY(ensure_loop(op));
+    if (!mg.coarse_exec || mg.graph_nrhs != nrhs || mg.graph_b != b || mg.graph_x != x) {
+        mg.reset_graph();
+        cudaStream_t cs = op->side[0];
+        cudaGraph_t graph = nullptr;
+        TDG_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        const int rc = mg_coarse_emit(op, b, x, nrhs, cs);
+        const cudaError_t ce = cudaStreamEndCapture(cs, &graph);
+        cudaError_t ci = cudaSuccess;
+        if (rc == 0 && ce == cudaSuccess) ci = cudaGraphInstantiate(&mg.coarse_exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (rc) return rc;
+        if (ce != cudaSuccess || ci != cudaSuccess) {
+            mg.coarse_exec = nullptr;
+            return fail(TDG_E_CUDA, std::string("multigrid: coarse CG graph: ") +
+                                        cudaGetErrorString(ce != cudaSuccess ? ce : ci));
         }
+        mg.graph_nrhs = nrhs;
+        mg.graph_b = b;
+        mg.graph_x = x;
     }
-    if (!any) return 0;
-    if (changed) TDG_CUDA_TRY(cudaMemcpyAsync(mg.scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-    int it = 0;
-    while (it < mg.opts.coarse_max_it) {
-        if (s != nullptr && (!mg.coarse_exec || mg.graph_nrhs != nrhs)) {
-            mg.reset_graph();
-            cudaGraph_t graph = nullptr;
-            TDG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            int rc = mg_coarse_block(op, sp, x, nrhs, s);
-            cudaError_t ce = cudaStreamEndCapture(s, &graph);
-            if (rc == 0 && ce == cudaSuccess) ce = cudaGraphInstantiate(&mg.coarse_exec, graph, 0);
-            if (graph) cudaGraphDestroy(graph);
-            if (rc) return rc;
-            if (ce != cudaSuccess) {
-                mg.coarse_exec = nullptr;
-                return fail(TDG_E_CUDA, std::string("multigrid: coarse CG graph: ") + cudaGetErrorString(ce));
-            }
-            mg.graph_nrhs = nrhs;
-        }
-        if (mg.coarse_exec)
-            TDG_CUDA_TRY(cudaGraphLaunch(mg.coarse_exec, s));
-        else
-            TDG_TRY(mg_coarse_block(op, sp, x, nrhs, s));
-        it += kCoarseBlock;
-        TDG_TRY(mg_read_scalars(op, hs, nrhs, s));
-        any = false;
-        changed = false;
-        for (int c = 0; c < nrhs; ++c) {
-            double* sc = &hs[static_cast<size_t>(c) * kScal];
-            if (sc[kActive] == 0.0) continue;
-            if (!std::isfinite(sc[kRR])) return fail(TDG_E_DIVERGED, "multigrid: coarse CG diverged");
-            if (sc[kRR] <= tol2[static_cast<size_t>(c)]) {
-                sc[kActive] = 0.0;
-                changed = true;
-            } else {
-                any = true;
-            }
-        }
-        if (!any) break;
-        if (changed) TDG_CUDA_TRY(cudaMemcpyAsync(mg.scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-    }
-    mg.coarse_its += it;
+    TDG_CUDA_TRY(cudaGraphLaunch(mg.coarse_exec, s));
     return 0;
+}
+
+// Reads and clears the coarse CG's divergence flag (synchronises s).
+int mg_check_coarse(tdg_op* op, cudaStream_t s) {
+    if (!op->loop) return 0;
+    long long flag = 0;
+    TDG_CUDA_TRY(cudaMemcpyAsync(&flag, op->loop + kCoarseDiverged, sizeof flag, cudaMemcpyDeviceToHost, s));
+    TDG_CUDA_TRY(cudaStreamSynchronize(s));
+    if (!flag) return 0;
+    TDG_CUDA_TRY(cudaMemsetAsync(op->loop + kCoarseDiverged, 0, sizeof flag, s));
+    return fail(TDG_E_DIVERGED, "multigrid: coarse CG diverged");
 }
 
 // One V-cycle on level l for nrhs columns: x = M_l b.  Below the coarsest DG level sits either the
@@ -1130,7 +1270,8 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
     mg.arena.release();
     mg.lv.clear();
     mg.ready = false;
-    mg.coarse_its = 0;
+    TDG_TRY(ensure_loop(op));
+    TDG_CUDA_TRY(cudaMemset(op->loop + kCoarseIts, 0, 3 * sizeof(long long)));  // its, diverged, total
     mg.opts = o;
     mg.fine_prec = o.smooth_precision;
     // the continuous P1 level embeds in the coarsest DG level only from degree 1 on
@@ -1803,9 +1944,12 @@ int residual64(tdg_op* op, SegPlan const& sp, const double* b, const double* x, 
 // z = M r, p = z, rz = r.z, rr = r.r, active flags from `active`.
 template <typename T>
 int cg_start(tdg_op* op, int prec, SegPlan const& sp, CgVectors<T> v, double* partial, double* scal,
-             std::vector<double> const& active, cudaStream_t s) {
+             std::vector<double> const& active, std::vector<double> const& thr, cudaStream_t s) {
     std::vector<double> hs(static_cast<size_t>(sp.nseg) * kScal, 0.0);
-    for (int i = 0; i < sp.nseg; ++i) hs[static_cast<size_t>(i) * kScal + kActive] = active[i];
+    for (int i = 0; i < sp.nseg; ++i) {
+        hs[static_cast<size_t>(i) * kScal + kActive] = active[i];
+        hs[static_cast<size_t>(i) * kScal + kThr] = thr[i];
+    }
     TDG_CUDA_TRY(cudaMemcpyAsync(scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     TDG_TRY(precondition<T>(op, prec, v.r, v.z, sp.op_nrhs, sp.op_ld, s));
     k_copy<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, v.z, v.p);
@@ -1871,14 +2015,26 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
                  int max_updates, bool graphs, cudaStream_t s, std::vector<double>& rn, std::vector<double>& bn,
                  int* iters, int* updates, bool* diverged) {
     constexpr bool kLow = !std::is_same_v<T, double>;
-    // the multigrid preconditioner synchronises with the host (coarse CG), so its iterations are
-    // neither captured in graphs nor batched between checks
+    // Iterations run in blocks.  The first block (kCheck iterations) is launched from the host; the
+    // later ones replay a captured graph whose device loop (k_block_ctl) ends the block after the
+    // iteration at which a segment asks for a reliable update (its recurrence residual met
+    // max(delta rmax, tol) or is not finite) or after kBlock iterations; the host then reads the
+    // scalars, so the updates happen at the same iterations as with a check after every iteration.
+    // Without graphs (no stream, the distributed solve's host callbacks) the host checks after
+    // every kCheck iterations.  The multigrid preconditioner is captured with its coarse solve's
+    // own device loop inside the block.
     const bool mg = op->pc == TDG_PC_MG;
     const int kCheck = mg ? 1 : 8;
-    graphs = graphs && !mg;
+    constexpr int kBlock = 32;
+    graphs = graphs && s != nullptr;
+    if (graphs) TDG_TRY(ensure_loop(op));
     const int nseg = sp.nseg;
     if (max_updates <= 0) max_updates = 1 << 20;
-    std::vector<double> tol(nseg), act(nseg), rmax(nseg), best(nseg);
+    std::vector<double> tol(nseg), act(nseg), rmax(nseg), best(nseg), thr(nseg);
+    auto threshold = [&](int i) {  // squared recurrence-residual norm that triggers an update
+        const double t = std::max(delta * rmax[i], tol[i]);
+        return t * t;
+    };
     std::vector<int> stall(nseg, 0), poor(nseg, 0);
     std::vector<double> hs(static_cast<size_t>(nseg) * kScal);
     *iters = 0;
@@ -1892,6 +2048,7 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
         act[i] = rn[i] > tol[i] ? 1.0 : 0.0;
         rmax[i] = rn[i];
         best[i] = rn[i];
+        thr[i] = threshold(i);
         any = any || act[i] != 0.0;
     }
     if (!any) return 0;
@@ -1899,24 +2056,39 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
         k_scale_convert<double, T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, r64, rh, scal, -1);
         k_fill<T><<<sp.nchunks, kVecThreads, 0, s>>>(sp.chunks, xh, T(0));
     }
-    TDG_TRY(cg_start<T>(op, prec, sp, v, partial, scal, act, s));
+    TDG_TRY(cg_start<T>(op, prec, sp, v, partial, scal, act, thr, s));
     cudaGraphExec_t exec = nullptr;
+    long long lc[2] = {0, 0};  // kLoopIts, kLoopLimit of the next graph block
     int rc = 0;
     for (;;) {
         // one block of iterations
-        const bool use_graph = graphs && s != nullptr && *iters >= kCheck;
+        const bool use_graph = graphs && *iters >= kCheck;
         if (use_graph && !exec) {
             cudaGraph_t graph = nullptr;
             rc = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess ? 0 : TDG_E_CUDA;
-            for (int i = 0; i < kCheck && rc == 0; ++i) rc = cg_iteration<T>(op, prec, sp, xh, v, partial, scal, s);
+            if (rc == 0)
+                rc = emit_while(op, s, 1u, [](cudaGraphConditionalHandle) { return 0; },
+                                [&](cudaStream_t bs, cudaGraphConditionalHandle h) {
+                                    TDG_TRY(cg_iteration<T>(op, prec, sp, xh, v, partial, scal, bs));
+                                    k_block_ctl<<<1, 256, 0, bs>>>(scal, nseg, op->loop, h);
+                                    return cudaGetLastError() == cudaSuccess ? 0 : fail(TDG_E_CUDA, "block control");
+                                });
             cudaError_t ce = cudaStreamEndCapture(s, &graph);
             if (rc == 0 && ce == cudaSuccess) rc = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess ? 0 : TDG_E_CUDA;
             else if (rc == 0) rc = TDG_E_CUDA;
             if (graph) cudaGraphDestroy(graph);
-            if (rc) break;
+            if (rc) {
+                if (g_last_error.empty()) fail(rc, "capturing the device-looped CG block");
+                break;
+            }
         }
+        int done = kCheck;
         if (exec) {
-            if (cudaGraphLaunch(exec, s) != cudaSuccess) {
+            lc[kLoopIts] = 0;
+            lc[kLoopLimit] = std::min(kBlock, max_it - *iters);
+            if (cudaMemcpyAsync(op->loop, lc, sizeof lc, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+                cudaGraphLaunch(exec, s) != cudaSuccess ||
+                cudaMemcpyAsync(lc, op->loop, sizeof lc, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
                 rc = fail(TDG_E_CUDA, "graph launch");
                 break;
             }
@@ -1924,13 +2096,14 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
             for (int i = 0; i < kCheck && rc == 0; ++i) rc = cg_iteration<T>(op, prec, sp, xh, v, partial, scal, s);
             if (rc) break;
         }
-        *iters += kCheck;
         // decide on reliable updates from the recurrence residuals
         if (cudaMemcpyAsync(hs.data(), scal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess) {
             rc = fail(TDG_E_CUDA, "reading the Krylov scalars");
             break;
         }
+        if (exec) done = static_cast<int>(lc[kLoopIts]);
+        *iters += done;
         const bool last = *iters >= max_it;
         bool update = last;
         for (int i = 0; i < nseg; ++i) {
@@ -2001,6 +2174,7 @@ int pcg_reliable(tdg_op* op, int prec, SegPlan const& sp, const double* b, doubl
                 // direction recurrence the rebuild does not follow)
                 if (mg || !(rn[i] <= 2.0 * rrec)) sr[kTmp] = 1.0;
                 rmax[i] = rn[i];
+                sr[kThr] = threshold(i);
             }
             any = true;
         }
@@ -2165,6 +2339,8 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     TDG_TRY(ensure_uploaded(op, TDG_FP64));
     if (prec != TDG_FP64) TDG_TRY(ensure_uploaded(op, TDG_FP32));
     std::memset(stats, 0, sizeof(*stats));
+    if (op->pc == TDG_PC_MG && op->loop)  // a divergence flag left by an earlier failed call
+        TDG_CUDA_TRY(cudaMemsetAsync(op->loop + kCoarseDiverged, 0, sizeof(long long), s));
 
     std::vector<Chunk> hchunks;
     std::vector<int> hseg;
@@ -2303,6 +2479,7 @@ int solve_segments(tdg_op* op, const double* b, double* x, std::vector<int64_t> 
     stats->rel_residual = diverged ? NAN : worst;
     stats->seconds = ms * 1e-3;
     stats->converged = (!diverged && worst <= rtol) ? 1 : 0;
+    if (op->pc == TDG_PC_MG) TDG_TRY(mg_check_coarse(op, s));
     if (diverged) return fail(TDG_E_DIVERGED, "non-finite residual in the Krylov iteration");
     for (int* word : {op->tgeo.status, op->tc32.status})
         if (word) {  // a bounded wait of a pipelined kernel that ran out makes the solve invalid
@@ -2387,7 +2564,9 @@ extern "C" int tdg_mg_setup(tdg_op* op, const tdg_mg_opts* opts, void* stream) {
 
 extern "C" int tdg_mg_apply(tdg_op* op, const double* r, double* z, int nrhs, int64_t ld, void* stream) {
     if (!op || !r || !z) return fail(TDG_E_INVALID, "null argument");
-    return mg_apply(op, r, z, nrhs, ld, static_cast<cudaStream_t>(stream));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    TDG_TRY(mg_apply(op, r, z, nrhs, ld, s));
+    return mg_check_coarse(op, s);
 }
 
 extern "C" int tdg_set_preconditioner(tdg_op* op, int pc) {
@@ -2409,7 +2588,11 @@ extern "C" int tdg_mg_info(tdg_op* op, int* nlevels, int max_levels, int* degree
         if (block_sizes) block_sizes[l] = mg.lv[static_cast<size_t>(l)].bs;
         if (lambda_max) lambda_max[l] = mg.lv[static_cast<size_t>(l)].lmax;
     }
-    if (coarse_its) *coarse_its = mg.coarse_its;
+    if (coarse_its) {
+        long long total = 0;
+        if (op->loop) TDG_CUDA_TRY(cudaMemcpy(&total, op->loop + kCoarseTotal, sizeof total, cudaMemcpyDeviceToHost));
+        *coarse_its = total;
+    }
     return 0;
 }
 
