@@ -244,7 +244,12 @@ typedef struct {
                                residual whenever the latter has dropped by this factor
                                (0 = default: 0.1) */
     int32_t max_outer;      /* cap on reliable updates (0 = none) */
-    int32_t use_graphs;     /* capture iteration blocks in CUDA graphs */
+    int32_t use_graphs;     /* capture iteration blocks in CUDA graphs (needs a non-NULL stream):
+                               each block is a device loop (a conditional while node) that ends
+                               at the iteration where a problem's recurrence residual asks for a
+                               reliable update, or after 32 iterations; the host reads the
+                               scalars between blocks.  0: the host launches every iteration and
+                               checks every 8 (every one under multigrid) */
     int32_t method;         /* TDG_KSP_CG (default) or TDG_KSP_FGMRES */
     int32_t restart;        /* FGMRES restart length m (0 = 30; at most 64) */
 } tdg_solve_opts;
@@ -350,7 +355,10 @@ typedef struct {
 int tdg_mg_setup(tdg_op* op, const tdg_mg_opts* opts, void* stream);
 /* z = M r, one V-cycle per right-hand side (PCMG's apply): Chebyshev pre-smoothing from zero,
  * restriction of the residual, the coarser levels, prolongation, Chebyshev post-smoothing; CG with
- * block Jacobi on the coarsest level.  FP64 device vectors. */
+ * block Jacobi on the coarsest level.  FP64 device vectors.  The coarse CG runs as a device loop
+ * (a CUDA graph with a conditional while node, its stopping test on the device every 8
+ * iterations), so the V-cycle itself never waits for the host; the call then synchronises `stream`
+ * to report a coarse CG whose residual became non-finite (TDG_E_DIVERGED). */
 int tdg_mg_apply(tdg_op* op, const double* r, double* z, int nrhs, int64_t ld, void* stream);
 /* Preconditioner of tdg_solve / tdg_solve_segmented (and the Green's-function and adjoint solves
  * built on them): TDG_PC_BJACOBI (default) or TDG_PC_MG (needs tdg_mg_setup; TDG_FP64 and
