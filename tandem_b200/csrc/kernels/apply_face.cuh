@@ -337,8 +337,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
     const int64_t ntiles = (op.E + TE - 1) / TE;
     const int64_t nwork = ntiles * nrhs;
     for (int64_t work = blockIdx.x; work < nwork; work += gridDim.x) {
-        const int64_t tile = work % ntiles;
-        const int rhs = static_cast<int>(work / ntiles);
+        int64_t tile, rhs;
+        work_tile_rhs(work, ntiles, nrhs, tile, rhs);
         const double* xr = x + rhs * ld;
         double* yr = y + rhs * ld;
         __syncthreads();
@@ -481,8 +481,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     const int64_t w1 = (w0 + per < nwork) ? w0 + per : nwork;
     int cur_a = -1, cur_b = -1;  // face tables held in TA / TB
     for (int64_t work = w0; work < w1; ++work) {
-        const int tile = static_cast<int>(work % ft.nftiles);
-        const int rhs = static_cast<int>(work / ft.nftiles);
+        int64_t t64, rhs;
+        work_tile_rhs(work, ft.nftiles, nrhs, t64, rhs);
+        const int tile = static_cast<int>(t64);
         const double* xr = x + rhs * ld;
         double* yr = y + rhs * ld;
         const int4 td = ft.ftiles[tile];

@@ -118,8 +118,8 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     const int64_t ntiles = (op.E + TE - 1) / TE;
     const int64_t nwork = ntiles * nrhs;
     for (int64_t work = blockIdx.x; work < nwork; work += gridDim.x) {
-        const int64_t tile = work % ntiles;
-        const int rhs = static_cast<int>(work / ntiles);
+        int64_t tile, rhs;
+        work_tile_rhs(work, ntiles, nrhs, tile, rhs);
         const TX* xr = x + rhs * ld;
         TX* yr = y + rhs * ld;
         __syncthreads();
@@ -281,7 +281,9 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     // descriptor: the first tile's now, each next tile's one iteration ahead
     int4 td_next = make_int4(0, 0, 0, 0);
     if (w0 < w1) {
-        const int tile0 = static_cast<int>(w0 % ft.nftiles);
+        int64_t t64, r64;
+        work_tile_rhs(w0, ft.nftiles, nrhs, t64, r64);
+        const int tile0 = static_cast<int>(t64);
         td_next = ft.ftiles[tile0];
         if (tid < TE) {
             const int4 id = ft.tids[static_cast<int64_t>(tile0) * TE + tid];
@@ -292,8 +294,9 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     }
     int sb = 0;
     for (int64_t work = w0; work < w1; ++work, sb ^= 1) {
-        const int tile = static_cast<int>(work % ft.nftiles);
-        const int rhs = static_cast<int>(work / ft.nftiles);
+        int64_t t64, rhs;
+        work_tile_rhs(work, ft.nftiles, nrhs, t64, rhs);
+        const int tile = static_cast<int>(t64);
         const TX* xr = x + rhs * ld;
         TX* yr = y + rhs * ld;
         const int4 td = td_next;
@@ -307,7 +310,9 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
         // buffer at its end, after every read of that buffer in the previous tile)
         int4 id_next = make_int4(-1, -1, -1, 0);
         if (work + 1 < w1) {
-            const int tile1 = static_cast<int>((work + 1) % ft.nftiles);
+            int64_t t1, r1;
+            work_tile_rhs(work + 1, ft.nftiles, nrhs, t1, r1);
+            const int tile1 = static_cast<int>(t1);
             td_next = ft.ftiles[tile1];
             if (tid < TE) id_next = ft.tids[static_cast<int64_t>(tile1) * TE + tid];
         }

@@ -268,8 +268,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, (S::D == 2) ? 2 : 1)
     const int64_t nwork = static_cast<int64_t>(mt.ntiles) * nrhs;
     for (int64_t work = static_cast<int64_t>(blockIdx.x) * L::NGRP + grp; work < nwork;
          work += static_cast<int64_t>(gridDim.x) * L::NGRP) {
-        const int tile = static_cast<int>(work % mt.ntiles);
-        const int rhs = static_cast<int>(work / mt.ntiles);
+        int64_t t64, rhs;
+        work_tile_rhs(work, mt.ntiles, nrhs, t64, rhs);
+        const int tile = static_cast<int>(t64);
         const double* xr = x + rhs * ld;
         double* yr = y + rhs * ld;
         const int4 td = mt.tiles[tile];

@@ -294,8 +294,9 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
     const int64_t nwork = static_cast<int64_t>(mt.ntiles) * nrhs;
     for (int64_t work = static_cast<int64_t>(blockIdx.x) * L::NGRP + grp; work < nwork;
          work += static_cast<int64_t>(gridDim.x) * L::NGRP) {
-        const int tile = static_cast<int>(work % mt.ntiles);
-        const int rhs = static_cast<int>(work / mt.ntiles);
+        int64_t t64, rhs;
+        work_tile_rhs(work, mt.ntiles, nrhs, t64, rhs);
+        const int tile = static_cast<int>(t64);
         const TX* xr = x + rhs * ld;
         TX* yr = y + rhs * ld;
         const int4 td = mt.tiles[tile];

@@ -15,6 +15,30 @@ __host__ __device__ constexpr int cbinom(int n, int k) {
     return r;
 }
 
+// ---- work items --------------------------------------------------------------------------------------
+
+// Work item -> (tile, right-hand side) of a multi-RHS apply.  Items run over groups of kRhsGroup
+// right-hand sides; inside a group the tile is the slower index and the right-hand side the faster
+// one, so consecutive items (a CTA's own, and those the CTAs run at one time) read the same tile's
+// geometry: it comes from memory once per group and then from L2, while a group's vectors
+// (kRhsGroup x the vector) stay small enough to be reused from L2 as well.  One right-hand side:
+// item = tile.
+constexpr int kRhsGroup = 8;
+__device__ __forceinline__ void work_tile_rhs(int64_t work, int64_t ntiles, int nrhs, int64_t& tile, int64_t& rhs) {
+    const int64_t full = nrhs / kRhsGroup;  // complete groups
+    const int64_t per = ntiles * kRhsGroup;
+    if (work < full * per) {
+        const int64_t grp = work / per, w = work - grp * per;
+        tile = w / kRhsGroup;
+        rhs = grp * kRhsGroup + (w - tile * kRhsGroup);
+    } else {  // the last, partial group of `rest` right-hand sides
+        const int64_t w = work - full * per;
+        const int64_t rest = nrhs - full * kRhsGroup;
+        tile = w / rest;
+        rhs = full * kRhsGroup + (w - tile * rest);
+    }
+}
+
 // Compile-time shape of one (dimension, degree, operator) instance.
 template <int D_, int N_, int KIND_>
 struct Shape {

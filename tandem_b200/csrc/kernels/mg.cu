@@ -360,6 +360,47 @@ __global__ void __launch_bounds__(kT) k_round_to_float(int64_t n, const double* 
     TDG_GRID_LOOP(i, n) b[i] = static_cast<float>(a[i]);
 }
 
+// Several right-hand sides: each thread takes one row for a group of up to RB right-hand sides
+// (one accumulator each), so a block row is read from memory once per group instead of once per
+// right-hand side (the level operators of a multi-RHS V-cycle, e.g. the Green's-function columns).
+template <int BS, int RB, typename TA>
+__global__ void __launch_bounds__(kT)
+    k_bsr_apply_mr(int64_t E, int NB, const int32_t* __restrict__ nbr, const TA* __restrict__ A,
+                   const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ y, int nrhs,
+                   int64_t ld) {
+    const int64_t n = E * BS;
+    const int64_t groups = (nrhs + RB - 1) / RB;
+    TDG_GRID_LOOP(g, n * groups) {
+        const int64_t cg = g / n, gi = g % n;
+        const int64_t c0 = cg * RB;
+        const int rb = static_cast<int>(nrhs - c0 < RB ? nrhs - c0 : RB);
+        const int row = static_cast<int>(gi % BS);
+        const int64_t e = gi / BS;
+        double acc[RB];
+#pragma unroll
+        for (int j = 0; j < RB; ++j) acc[j] = 0.0;
+        for (int s = 0; s < NB; ++s) {
+            const int32_t t = nbr[e * NB + s];
+            if (t < 0) continue;
+            const TA* blk = A + (e * NB + s) * (BS * BS) + row;
+            const double* xt = x + c0 * ld + static_cast<int64_t>(t) * BS;
+#pragma unroll
+            for (int col = 0; col < BS; ++col) {
+                const double a = static_cast<double>(blk[col * BS]);
+#pragma unroll
+                for (int j = 0; j < RB; ++j)
+                    if (j < rb) acc[j] += a * xt[j * ld + col];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < RB; ++j)
+            if (j < rb) {
+                const int64_t i = (c0 + j) * ld + gi;
+                y[i] = b ? b[i] - acc[j] : acc[j];
+            }
+    }
+}
+
 #undef TDG_GRID_LOOP
 
 }  // namespace
@@ -389,6 +430,17 @@ int launch_mg_triple(int64_t E, int NB, const int32_t* nbr, MgInterp ip, const d
 template <typename TA>
 int launch_mg_bsr_apply(int64_t E, int NB, int bs, const int32_t* nbr, const TA* A, const double* x,
                         const double* b, double* y, int nrhs, int64_t ld, cudaStream_t s) {
+    constexpr int RB = 8;
+    if (nrhs > 1 && (bs == 3 || bs == 4 || bs == 6 || bs == 10 || bs == 12 || bs == 30)) {
+        const unsigned gm = grid_for(E * bs * ((nrhs + RB - 1) / RB));
+        switch (bs) {
+#define TDG_BSR_MR_CASE(B) \
+    case B: k_bsr_apply_mr<B, RB, TA><<<gm, kT, 0, s>>>(E, NB, nbr, A, x, b, y, nrhs, ld); break;
+            TDG_BSR_MR_CASE(3) TDG_BSR_MR_CASE(4) TDG_BSR_MR_CASE(6) TDG_BSR_MR_CASE(10) TDG_BSR_MR_CASE(12) TDG_BSR_MR_CASE(30)
+#undef TDG_BSR_MR_CASE
+        }
+        return launched();
+    }
     const unsigned g = grid_for(E * bs * nrhs);
     switch (bs) {
 #define TDG_BSR_CASE(B) \
