@@ -45,8 +45,11 @@ FP64_PROBES = ("dfma", "dmma_m8n8k4", "dmma_m16n8k4", "dmma_m16n8k8", "dmma_m16n
 # configuration runs it (examples/options/mg_cheby.cfg: -ksp_type fgmres).
 BJ_ARMS = (("fp64", 0, 0, "bjacobi", "cg"), ("mixed", 2, 1, "bjacobi", "cg"), ("mixed_fp64_pc", 2, 0, "bjacobi", "cg"),
            ("fp32_recurrence", 1, 1, "bjacobi", "cg"))
-MG_ARMS = (("mg_fp64", 0, 0, "mg", "cg"), ("mg_mixed", 2, 2, "mg", "cg"))
-GMRES_ARMS = (("mg_fgmres_fp64", 0, 0, "mg", "fgmres"), ("mg_fgmres_mixed", 2, 2, "mg", "fgmres"))
+# mg_tf32: the mixed solve (3xTF32 operator in the FP64 refinement) whose smoother runs the
+# finest level's applies in one TF32 pass (precision 3, TDG_TF32)
+MG_ARMS = (("mg_fp64", 0, 0, "mg", "cg"), ("mg_mixed", 2, 2, "mg", "cg"), ("mg_tf32", 2, 3, "mg", "cg"))
+GMRES_ARMS = (("mg_fgmres_fp64", 0, 0, "mg", "fgmres"), ("mg_fgmres_mixed", 2, 2, "mg", "fgmres"),
+              ("mg_fgmres_tf32", 2, 3, "mg", "fgmres"))
 SOLVE_ARMS = BJ_ARMS + MG_ARMS + GMRES_ARMS
 # the default cube leg: tandem's FP64 configuration (block-Jacobi CG), the two multigrid CG arms
 # and multigrid FGMRES in FP64 (tandem's multigrid configuration)
@@ -86,12 +89,13 @@ def prepare_arm(op, pcp: int, pc: str) -> float:
 
 def add_speedups(res: dict, key: str = "seconds") -> None:
     """speedup_vs_fp64 (block-Jacobi FP64 CG, tandem's default solver configuration) for every other
-    arm, and speedup_vs_mg_fp64 for the mixed multigrid arm."""
+    arm, and speedup_vs_mg_fp64 for the mixed multigrid arms."""
     for name, r in res.items():
         if name != "fp64" and "fp64" in res:
             r["speedup_vs_fp64"] = res["fp64"][key] / r[key]
-    if "mg_fp64" in res and "mg_mixed" in res:
-        res["mg_mixed"]["speedup_vs_mg_fp64"] = res["mg_fp64"][key] / res["mg_mixed"][key]
+    for name in ("mg_mixed", "mg_tf32"):
+        if "mg_fp64" in res and name in res:
+            res[name]["speedup_vs_mg_fp64"] = res["mg_fp64"][key] / res[name][key]
 KERNEL_NAMES = {"tensor": "apply_mma_kernel<Shape<3,4,Elasticity>> (FP64 mma.sync m8n8k4, element-centric)",
                 "face": "vol_mma_kernel + face_mma_kernel<Shape<3,4,Elasticity>> (FP64 mma.sync m8n8k4, "
                         "face-centric; roofline over both launches of one apply)",
@@ -345,7 +349,7 @@ def host_link_bandwidth(hx, hy, stream, reps=3):
 def run_ours(args):
     import torch
     import torch.distributed as dist
-    from tandem_b200.operator import FP32, FP64
+    from tandem_b200.operator import FP32, FP64, MIXED, TF32
     from tandem_b200.workloads import elasticity_cube
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -444,6 +448,26 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     ms32 = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+    # the same operator on FP64 vectors: 3xTF32 (TDG_MIXED, the mixed solve's operator) and one TF32
+    # pass (TDG_TF32, the mixed multigrid smoother's), with their deviation from the FP64 apply
+    y64 = torch.empty_like(x)
+    op.apply(x, y64, FP64, stream=stream)
+    tf = {}
+    for name, prec in (("mixed", MIXED), ("tf32", TF32)):
+        yt = torch.empty_like(x)
+        for _ in range(args.warmup):
+            op.apply(x, yt, prec, stream=stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            op.apply(x, yt, prec, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        mst = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+        tf[name] = {"ms_per_step": mst, "value": world * n / (mst * 1e-3), "unit": "DOF/s",
+                    "rel_diff_vs_fp64": float(torch.norm(yt - y64) / torch.norm(y64))}
+        del yt
+    del y64
 
     solve = None
     arms = select_arms(args) if args.solve or args.arms else (() if args.no_solve else DEFAULT_CUBE_ARMS)
@@ -522,6 +546,7 @@ def run_ours(args):
            "roofline": roofline, "cpu_baseline": cpu,
            "fp32_apply": {"value": world * n / (ms32 * 1e-3), "unit": "DOF/s", "ms_per_step": ms32,
                           "config": best32},
+           "fp64_vector_applies": tf,
            "solve": solve}
     print(json.dumps(out), flush=True)
     if world > 1:

@@ -43,10 +43,15 @@ extern "C" {
 #define TDG_BC_DIRICHLET 5
 
 /* Arithmetic of an apply / preconditioner / solve.  TDG_MIXED: FP32 operator arithmetic (and FP32
- * block inverses) on FP64 vectors; as a solve precision, an FP64 CG recurrence around them. */
+ * block inverses) on FP64 vectors; as a solve precision, an FP64 CG recurrence around them.
+ * TDG_TF32: FP64 vectors, the operator's products in one TF32 tensor-core pass (about 1e-3 of
+ * |A| |x|; TDG_MIXED runs three, 3xTF32, for about 2e-7) -- for preconditioner applies only: an
+ * apply precision (tdg_apply) and the multigrid smoother's (tdg_mg_opts.smooth_precision), never a
+ * solve precision. */
 #define TDG_FP64 0
 #define TDG_FP32 1
 #define TDG_MIXED 2
+#define TDG_TF32 3
 
 typedef struct tdg_op tdg_op;
 
@@ -129,7 +134,8 @@ int tdg_penalty(const tdg_op* op, double* out);
 /* y = A x for nrhs stacked vectors (AbstractDGOperator::apply, src/form/AbstractDGOperator.h:34;
  * PetscDGShell::apply, app/common/PetscDGShell.cpp:48-55).  precision selects the element
  * arithmetic: TDG_FP64 takes double*, TDG_FP32 takes float*, TDG_MIXED takes double* and computes
- * in FP32 on the tensor cores (x rounded to FP32 on load, y widened on store). */
+ * in FP32 on the tensor cores (x rounded to FP32 on load, y widened on store); TDG_TF32 as
+ * TDG_MIXED with one TF32 pass per product. */
 int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64_t ld,
               void* stream);
 
@@ -334,7 +340,9 @@ typedef struct {
     int32_t coarse_max_it;   /* coarsest-level CG iteration cap (default 1000) */
     int32_t smooth_precision; /* TDG_FP64, or TDG_MIXED: FP32 arithmetic for the finest level's
                                  smoother applies, FP32 copies of the blocks for the smoothed levels
-                                 below it (vectors, accumulation and the coarse solve stay FP64) */
+                                 below it (vectors, accumulation and the coarse solve stay FP64);
+                                 TDG_TF32: the same with the finest level's smoother applies in one
+                                 TF32 pass (the solve's own operator keeps its precision) */
     int32_t coarse_space;    /* TDG_MG_COARSE_DG: the coarse CG works on the coarsest DG level (as
                                 tandem's -mg_coarse_ksp_type cg).  TDG_MG_COARSE_P1 (default): the
                                 coarsest DG level is smoothed too and corrected from the continuous

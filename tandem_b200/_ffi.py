@@ -12,7 +12,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libtandem_b200.so"
 
 TDG_POISSON, TDG_ELASTICITY = 0, 1
 TDG_BC_NONE, TDG_BC_NATURAL, TDG_BC_FAULT, TDG_BC_DIRICHLET = 0, 1, 3, 5
-TDG_FP64, TDG_FP32, TDG_MIXED = 0, 1, 2
+TDG_FP64, TDG_FP32, TDG_MIXED, TDG_TF32 = 0, 1, 2, 3
 ERRORS = {-1: "TDG_E_INVALID", -2: "TDG_E_CUDA", -3: "TDG_E_NOT_SPD", -4: "TDG_E_DIVERGED",
           -5: "TDG_E_STATE", -6: "TDG_E_TIMEOUT", -7: "TDG_E_NOMEM"}
 ERRORS_BY_NAME = {v: k for k, v in ERRORS.items()}

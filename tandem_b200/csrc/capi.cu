@@ -754,7 +754,7 @@ int ensure_uploaded(tdg_op* op, int precision) {
         }
         return 0;
     }
-    if (precision == TDG_FP32 || precision == TDG_MIXED) {
+    if (precision == TDG_FP32 || precision == TDG_MIXED || precision == TDG_TF32) {
         if (!op->uploaded32) {
             TDG_TRY(upload_precision<float>(op, op->arena32, op->op32));
             op->uploaded32 = true;
@@ -1253,7 +1253,7 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
     if (!(o.coarse_rtol > 0.0)) o.coarse_rtol = 0.1;
     if (o.coarse_max_it <= 0) o.coarse_max_it = 1000;
     if (o.coarse_degree < 0) o.coarse_degree = 1;
-    if (o.smooth_precision != TDG_MIXED) o.smooth_precision = TDG_FP64;
+    if (o.smooth_precision != TDG_MIXED && o.smooth_precision != TDG_TF32) o.smooth_precision = TDG_FP64;
     if (o.strategy < 0 || o.strategy > 2) return fail(TDG_E_INVALID, "multigrid: unknown strategy");
     if (!(o.esteig_lo < o.esteig_hi)) return fail(TDG_E_INVALID, "multigrid: esteig_lo must be below esteig_hi");
     if (!h.has_material) return fail(TDG_E_STATE, "multigrid: tdg_set_material first");
@@ -1277,7 +1277,7 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
     // the continuous P1 level embeds in the coarsest DG level only from degree 1 on
     mg.aux = o.coarse_space == TDG_MG_COARSE_P1 && deg[0] >= 1;
     TDG_TRY(ensure_uploaded(op, TDG_FP64));
-    if (mg.fine_prec == TDG_MIXED) TDG_TRY(ensure_uploaded(op, TDG_FP32));
+    if (mg.fine_prec != TDG_FP64) TDG_TRY(ensure_uploaded(op, TDG_FP32));
     TDG_TRY(ensure_blocks(op, s));
     const int64_t E = h.E;
     mg.NB = 1 + h.nfaces;
@@ -1354,7 +1354,7 @@ int mg_setup(tdg_op* op, tdg_mg_opts o, cudaStream_t s) {
     TDG_TRY(mg_ensure_ws(op, 1, mg.lv.back().n, s));
     // mixed precision: the smoothed levels below the finest apply FP32 copies of their blocks
     // (half the bytes of the HBM-bound block-sparse apply; vectors and accumulation stay FP64)
-    if (mg.fine_prec == TDG_MIXED)
+    if (mg.fine_prec != TDG_FP64)
         for (int l = mg.aux ? 0 : 1; l + 1 < nl; ++l) {
             auto& L = mg.lv[static_cast<size_t>(l)];
             const int64_t nb = E * mg.NB * L.bs * L.bs;
@@ -1552,18 +1552,19 @@ int tdg_apply(tdg_op* op, int precision, const void* x, void* y, int nrhs, int64
     else if (precision == TDG_FP32 && tensor)
         rc = launch_apply_tc32<float>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const float*>(x),
                                       static_cast<float*>(y), nrhs, ld, s, op->ctas[1]);
-    if (precision == TDG_MIXED) {
-        if (!op->use_mma) return fail(TDG_E_INVALID, "TDG_MIXED needs the tensor-core kernels");
+    if (precision == TDG_MIXED || precision == TDG_TF32) {
+        if (!op->use_mma) return fail(TDG_E_INVALID, "TDG_MIXED / TDG_TF32 need the tensor-core kernels");
+        const int passes = precision == TDG_TF32 ? 1 : 3;  // one TF32 pass, or 3xTF32
         // the selected tensor-core family, else the other one (a shape whose element-centric tile
         // does not fit shared memory runs face-centric, and the reverse)
         auto face = [&] {
             return launch_apply_face_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, op->face32,
                                                   static_cast<const double*>(x), static_cast<double*>(y), nrhs, ld, s,
-                                                  op->ctas[1], vol05);
+                                                  op->ctas[1], vol05, passes);
         };
         auto elem = [&] {
             return launch_apply_tc32<double>(h.D, h.N, h.kind, op->op32, op->tc32, static_cast<const double*>(x),
-                                             static_cast<double*>(y), nrhs, ld, s, op->ctas[1]);
+                                             static_cast<double*>(y), nrhs, ld, s, op->ctas[1], passes);
         };
         rc = face32 ? face() : elem();
         if (rc == TDG_E_INVALID) rc = face32 ? elem() : face();

@@ -97,7 +97,7 @@ __device__ __forceinline__ void tcf_stage(float* st, const float (&y)[L::UPW][L:
     }
 }
 
-template <class S, typename TX>
+template <class S, typename TX, int NP = 3>
 __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     vol_tc32_kernel(DevOp<float> op, const float* __restrict__ tv, const TX* __restrict__ x, TX* __restrict__ y,
                     int64_t ld, int nrhs) {
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
             const int nqc = (Nq - q0 < L::QCP) ? (Nq - q0) : L::QCP;
             const int rows = tc_round(nqc * D, 16);
             if (q0 > 0) __syncthreads();
-            tc_forward<L>(TV + q0 * D * LDT, sU, R0, TV, sU, R0, 1, rows / 16, warp, lane);
+            tc_forward<L, NP>(TV + q0 * D * LDT, sU, R0, TV, sU, R0, 1, rows / 16, warp, lane);
             __syncthreads();
             for (int it = tid; it < TE * nqc; it += NT) {
                 const int te = it % TE, qq = it / TE, q = q0 + qq;
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
                 }
             }
             __syncthreads();
-            tc_backproject<L>(TV + q0 * D * LDT, R0, yacc, rows, warp, lane);
+            tc_backproject<L, NP>(TV + q0 * D * LDT, R0, yacc, rows, warp, lane);
         }
         __syncthreads();
         tcf_stage<L>(R0, yacc, warp, lane);
@@ -246,7 +246,7 @@ __host__ __device__ inline int tc32_geo_rows(int nq) {
 // one flat index per thread with the padding rewritten every tile (false).
 constexpr bool kTc32StageByWarp = true;
 
-template <class S, typename TX>
+template <class S, typename TX, int NP = 3>
 __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
     face_tc32_kernel(DevOp<float> op, const float* __restrict__ tf, FaceTiles ft, const TX* __restrict__ x,
                      TX* __restrict__ y, int64_t ld, int nrhs) {
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
             }
         }
         __syncthreads();
-        tc_forward<L>(TA, U0, R0, TB, U1, R1, two ? 2 : 1, lay.MF / 16, warp, lane);
+        tc_forward<L, NP>(TA, U0, R0, TB, U1, R1, two ? 2 : 1, lay.MF / 16, warp, lane);
         __syncthreads();
         for (int it = tid; it < TE * nqg; it += NT) {
             const int te = it % TE, q = kTc32PointSwizzle<S>() ? face2_point(it / TE) : it / TE;
@@ -455,8 +455,8 @@ __global__ void __launch_bounds__(TcfTile<S>::NT, TcfTile<S>::MINB)
             for (int j = 0; j < L::NPW; ++j)
 #pragma unroll
                 for (int c = 0; c < 4; ++c) y0[a][j][c] = y1[a][j][c] = 0.0f;
-        tc_backproject<L>(TA, R0, y0, lay.MF, warp, lane);
-        if (two) tc_backproject<L>(TB, R1, y1, lay.MF, warp, lane);
+        tc_backproject<L, NP>(TA, R0, y0, lay.MF, warp, lane);
+        if (two) tc_backproject<L, NP>(TB, R1, y1, lay.MF, warp, lane);
         __syncthreads();
         tcf_stage<L>(R0, y0, warp, lane);
         if (two) tcf_stage<L>(R1, y1, warp, lane);

@@ -201,7 +201,7 @@ __device__ __forceinline__ void tc05_stage(Tc05Smem const& b, const TX* __restri
 }
 
 // Forward MMAs (one thread): R_a = D_a U^T into TMEM columns a * NCOL, 3xTF32.
-template <class S>
+template <class S, int NP = 3>
 __device__ __forceinline__ void tc05_issue_fwd(Tc05Smem const& b, uint32_t tmem) {
     using L = Tc05Vol<S>;
     constexpr int NCOL = L::NCOL;
@@ -217,13 +217,15 @@ __device__ __forceinline__ void tc05_issue_fwd(Tc05Smem const& b, uint32_t tmem)
             const uint64_t bh = umma_desc(uh + ou, lboU, 128), bl = umma_desc(ul + ou, lboU, 128);
             const uint32_t d = tmem + static_cast<uint32_t>(a * NCOL);
             umma_tf32(d, ah, bh, idf, s > 0 ? 1u : 0u);
-            umma_tf32(d, ah, bl, idf, 1u);
-            umma_tf32(d, al, bh, idf, 1u);
+            if constexpr (NP == 3) {
+                umma_tf32(d, ah, bl, idf, 1u);
+                umma_tf32(d, al, bh, idf, 1u);
+            }
         }
 }
 
 // Backward MMAs (one thread): Y = D^T S^T into TMEM columns D * NCOL, 3xTF32.
-template <class S>
+template <class S, int NP = 3>
 __device__ __forceinline__ void tc05_issue_bwd(Tc05Smem const& b, uint32_t tmem) {
     using L = Tc05Vol<S>;
     constexpr int NCOL = L::NCOL;
@@ -236,8 +238,10 @@ __device__ __forceinline__ void tc05_issue_bwd(Tc05Smem const& b, uint32_t tmem)
         const uint64_t ah = umma_desc(bh0 + ob, L::LBO_B, 128), al = umma_desc(bl0 + ob, L::LBO_B, 128);
         const uint64_t bh = umma_desc(sh + os, L::SCS, 128), bl = umma_desc(sl + os, L::SCS, 128);
         umma_tf32(d, ah, bh, idb, s > 0 ? 1u : 0u);
-        umma_tf32(d, ah, bl, idb, 1u);
-        umma_tf32(d, al, bh, idb, 1u);
+        if constexpr (NP == 3) {
+            umma_tf32(d, ah, bl, idb, 1u);
+            umma_tf32(d, al, bh, idb, 1u);
+        }
     }
 }
 
@@ -429,7 +433,7 @@ __device__ __forceinline__ void tc05_store_y(uint32_t tmem, uint32_t lane_base, 
 
 // One tile at a time, every phase by the whole CTA (256 threads): stage, forward, pointwise
 // (warps owning lanes 0..63), backward, store.  tv: the FP32 volume table, row (q D + a), ld ldt.
-template <class S, typename TX>
+template <class S, typename TX, int NP = 3>
 __global__ void __launch_bounds__(256, 1)
     vol_tc05_kernel(DevOp<float> op, const float* __restrict__ tv, int ldt, const TX* __restrict__ x,
                     TX* __restrict__ y, int64_t ld, int nrhs, int* status) {
@@ -468,7 +472,7 @@ __global__ void __launch_bounds__(256, 1)
         __syncthreads();
         tc05_fence_after();
         if (tid == 0) {
-            tc05_issue_fwd<S>(b, tmem);
+            tc05_issue_fwd<S, NP>(b, tmem);
             umma_commit(&bar);
         }
         ok = __syncthreads_and(mbar_wait_bounded(&bar, phase) ? 1 : 0) != 0;  // block-uniform
@@ -494,7 +498,7 @@ __global__ void __launch_bounds__(256, 1)
         __syncthreads();
         tc05_fence_after();
         if (ok && tid == 0) {
-            tc05_issue_bwd<S>(b, tmem);
+            tc05_issue_bwd<S, NP>(b, tmem);
             umma_commit(&bar);
         }
         if (ok) {
@@ -521,7 +525,7 @@ __global__ void __launch_bounds__(256, 1)
 // registers while the backward MMAs of tile i - 1 run, and load each tile's geometry before they
 // wait for its forward MMAs.  Every wait is bounded; a thread whose wait runs out records the status word and leaves its
 // loop, so the threads that wait on it run out in turn and the CTA ends.
-template <class S, typename TX>
+template <class S, typename TX, int NP = 3>
 __global__ void __launch_bounds__(512, 1)
     vol_tc05p_kernel(DevOp<float> op, const float* __restrict__ tv, int ldt, const TX* __restrict__ x,
                      TX* __restrict__ y, int64_t ld, int nrhs, int* status) {
@@ -560,7 +564,7 @@ __global__ void __launch_bounds__(512, 1)
             ok = mbar_wait_bounded(&barU, 0u);
             if (ok) {
                 tc05_fence_after();
-                tc05_issue_fwd<S>(b, tmem);
+                tc05_issue_fwd<S, NP>(b, tmem);
                 umma_commit(&barF);
             }
         }
@@ -570,13 +574,13 @@ __global__ void __launch_bounds__(512, 1)
                 ok = mbar_wait_bounded(&barU, p ^ 1u) && mbar_wait_bounded(&barR, p);
                 if (!ok) break;
                 tc05_fence_after();
-                tc05_issue_fwd<S>(b, tmem);
+                tc05_issue_fwd<S, NP>(b, tmem);
                 umma_commit(&barF);
             }
             ok = mbar_wait_bounded(&barS, p);
             if (!ok) break;
             tc05_fence_after();
-            tc05_issue_bwd<S>(b, tmem);
+            tc05_issue_bwd<S, NP>(b, tmem);
             umma_commit(&barB);
         }
     } else if (sub >= 2) {  // staging (255 threads): U of tile i once the forward MMAs of tile i - 1 are done

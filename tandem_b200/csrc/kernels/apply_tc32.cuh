@@ -137,25 +137,31 @@ __device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// a += x*y in the 3xTF32 form (small terms first).
+// a += x*y in the 3xTF32 form (small terms first); NP = 1: one TF32 pass (hi hi, about 2^-11 per
+// product), for preconditioner applies.
+template <int NP = 3>
 __device__ __forceinline__ void mma3(float (&c)[4], const uint32_t (&ah)[4], const uint32_t (&al)[4], uint32_t bh0,
                                      uint32_t bh1, uint32_t bl0, uint32_t bl1) {
-    mma_tf32(c, al, bh0, bh1);
-    mma_tf32(c, ah, bl0, bl1);
+    if constexpr (NP == 3) {
+        mma_tf32(c, al, bh0, bh1);
+        mma_tf32(c, ah, bl0, bl1);
+    }
     mma_tf32(c, ah, bh0, bh1);
 }
 
 // The same for NPW accumulators sharing one A fragment, the three products of each accumulator in
 // the same order but interleaved across the accumulators, so that consecutive mma are independent
 // (three dependent mma per accumulator would otherwise stall on each other's latency).
-template <int NPW>
+template <int NPW, int NP = 3>
 __device__ __forceinline__ void mma3_rows(float (&c)[NPW][4], const uint32_t (&ah)[4], const uint32_t (&al)[4],
                                           const uint32_t (&bh0)[NPW], const uint32_t (&bh1)[NPW],
                                           const uint32_t (&bl0)[NPW], const uint32_t (&bl1)[NPW]) {
+    if constexpr (NP == 3) {
 #pragma unroll
-    for (int j = 0; j < NPW; ++j) mma_tf32(c[j], al, bh0[j], bh1[j]);
+        for (int j = 0; j < NPW; ++j) mma_tf32(c[j], al, bh0[j], bh1[j]);
 #pragma unroll
-    for (int j = 0; j < NPW; ++j) mma_tf32(c[j], ah, bl0[j], bl1[j]);
+        for (int j = 0; j < NPW; ++j) mma_tf32(c[j], ah, bl0[j], bl1[j]);
+    }
 #pragma unroll
     for (int j = 0; j < NPW; ++j) mma_tf32(c[j], ah, bh0[j], bh1[j]);
 }
@@ -166,7 +172,7 @@ constexpr bool kMma3Interleave = true;
 // [NP][LDU] column-major), R_i[m][c] = sum_k A_i[m][k] B_i[c][k], stored with ld LDR.  Units
 // (operand, m-tile, n-group) are dealt round-robin to the warps of the pipeline; each table
 // fragment a warp loads (and splits) feeds the NPW n-tiles of its unit.
-template <class L>
+template <class L, int NP = 3>
 __device__ __forceinline__ void tc_forward(const float* A0, const float* B0, float* R0, const float* A1, const float* B1,
                                            float* R1, int nops, int mtiles, int warp, int lane) {
     const int g = lane >> 2, t = lane & 3;
@@ -194,14 +200,14 @@ __device__ __forceinline__ void tc_forward(const float* A0, const float* B0, flo
                     tf32_split(bp[j * 8 * L::LDU + ks * 8], bh0[j], bl0[j]);
                     tf32_split(bp[j * 8 * L::LDU + ks * 8 + 4], bh1[j], bl1[j]);
                 }
-                mma3_rows<L::NPW>(acc, ah, al, bh0, bh1, bl0, bl1);
+                mma3_rows<L::NPW, NP>(acc, ah, al, bh0, bh1, bl0, bl1);
             } else {
 #pragma unroll
                 for (int j = 0; j < L::NPW; ++j) {
                     uint32_t bh0, bl0, bh1, bl1;
                     tf32_split(bp[j * 8 * L::LDU + ks * 8], bh0, bl0);
                     tf32_split(bp[j * 8 * L::LDU + ks * 8 + 4], bh1, bl1);
-                    mma3(acc[j], ah, al, bh0, bh1, bl0, bl1);
+                    mma3<NP>(acc[j], ah, al, bh0, bh1, bl0, bl1);
                 }
             }
         }
@@ -217,7 +223,7 @@ __device__ __forceinline__ void tc_forward(const float* A0, const float* B0, flo
 // Back-projection Y += A^T R over `mrows` reduction rows (a multiple of 8): A is a table
 // [mrows][LDT] (Y row index = table column), R is [mrows][LDR].  Warp w owns Y units
 // w % YU (+ NW, ...) for reduction part w / YU (k-steps kp, kp + KSP, ...).
-template <class L>
+template <class L, int NP = 3>
 __device__ __forceinline__ void tc_backproject(const float* A, const float* R, float (&y)[L::UPW][L::NPW][4], int mrows,
                                                int warp, int lane) {
     const int g = lane >> 2, t = lane & 3;
@@ -246,14 +252,14 @@ __device__ __forceinline__ void tc_backproject(const float* A, const float* R, f
                     tf32_split(r[j * 8], bh0[j], bl0[j]);
                     tf32_split(r[j * 8 + 4 * L::LDR], bh1[j], bl1[j]);
                 }
-                mma3_rows<L::NPW>(y[uu], ah, al, bh0, bh1, bl0, bl1);
+                mma3_rows<L::NPW, NP>(y[uu], ah, al, bh0, bh1, bl0, bl1);
             } else {
 #pragma unroll
                 for (int j = 0; j < L::NPW; ++j) {
                     uint32_t bh0, bl0, bh1, bl1;
                     tf32_split(r[j * 8], bh0, bl0);
                     tf32_split(r[j * 8 + 4 * L::LDR], bh1, bl1);
-                    mma3(y[uu][j], ah, al, bh0, bh1, bl0, bl1);
+                    mma3<NP>(y[uu][j], ah, al, bh0, bh1, bl0, bl1);
                 }
             }
         }
@@ -262,7 +268,7 @@ __device__ __forceinline__ void tc_backproject(const float* A, const float* R, f
 
 // TX: the vectors' type -- float, or double for the mixed solve (FP32 operator arithmetic on FP64
 // vectors: x is rounded to FP32 when it is gathered, y widened when it is stored).
-template <class S, typename TX>
+template <class S, typename TX, int NP = 3>
 __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
     apply_tc32_kernel(DevOp<float> op, Tc32Tiles mt, const TX* __restrict__ x, TX* __restrict__ y, int64_t ld,
                       int nrhs) {
@@ -326,7 +332,7 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
             const int nqc = (Nq - q0 < L::QCP) ? (Nq - q0) : L::QCP;
             const int rows = tc_round(nqc * D, 16);
             if (q0 > 0) group_sync<GT>(grp);  // previous chunk's back-projection done with R0
-            tc_forward<L>(TV + q0 * D * LDT, sU, R0, TV, sU, R0, 1, rows / 16, gw, lane);
+            tc_forward<L, NP>(TV + q0 * D * LDT, sU, R0, TV, sU, R0, 1, rows / 16, gw, lane);
             group_sync<GT>(grp);
             for (int it = gtid; it < TE * nqc; it += GT) {
                 const int te = it % TE, qq = it / TE, q = q0 + qq;
@@ -391,7 +397,7 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
                 }
             }
             group_sync<GT>(grp);
-            tc_backproject<L>(TV + q0 * D * LDT, R0, yacc, rows, gw, lane);
+            tc_backproject<L, NP>(TV + q0 * D * LDT, R0, yacc, rows, gw, lane);
         }
 
         // ---------------- facets ----------------
@@ -410,7 +416,7 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
                 sUN[c * LDU + k] = v;
             }
             group_sync<GT>(grp);
-            tc_forward<L>(TF + f * lay.MF * LDT, sU, R0, TF + lp * lay.MF * LDT, sUN, R1, 2, lay.MF / 16, gw, lane);
+            tc_forward<L, NP>(TF + f * lay.MF * LDT, sU, R0, TF + lp * lay.MF * LDT, sUN, R1, 2, lay.MF / 16, gw, lane);
             group_sync<GT>(grp);
             for (int it = gtid; it < TE * nq; it += GT) {
                 const int te = it % TE, q = it / TE;
@@ -587,7 +593,7 @@ __global__ void __launch_bounds__(Tc32Tile<S>::NT, Tc32Tile<S>::MINB)
                 }
             }
             group_sync<GT>(grp);
-            tc_backproject<L>(TF + f * lay.MF * LDT, R0, yacc, lay.MF, gw, lane);
+            tc_backproject<L, NP>(TF + f * lay.MF * LDT, R0, yacc, lay.MF, gw, lane);
         }
 
         // ---------------- reduce the k-split partials and write the tile ----------------

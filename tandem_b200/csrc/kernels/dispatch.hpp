@@ -48,12 +48,13 @@ struct Tc32Tiles;
 // it, else the mma.sync volume kernel.
 template <typename TX>
 int launch_apply_face_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, FaceTiles const& ft,
-                           const TX* x, TX* y, int nrhs, int64_t ld, cudaStream_t s, int ctas = 0, bool vol05 = false);
+                           const TX* x, TX* y, int nrhs, int64_t ld, cudaStream_t s, int ctas = 0, bool vol05 = false,
+                           int passes = 3);
 // The volume term alone on the 5th-generation tensor cores (stores y); TDG_E_INVALID when the
 // shape does not fit (more than 64 volume points).
 template <typename TX>
 int launch_vol_tc05(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y,
-                    int nrhs, int64_t ld, cudaStream_t s);
+                    int nrhs, int64_t ld, cudaStream_t s, int passes = 3);
 
 // FP32 apply on the tensor cores in the 3xTF32 form (apply_tc32.cuh); TDG_E_INVALID when the
 // shape's shared-memory layout does not fit (the caller then uses the SIMT kernel).
@@ -61,7 +62,7 @@ struct Tc32Tiles;
 // TX = float (FP32 vectors) or double (FP64 vectors, FP32 operator arithmetic).
 template <typename TX>
 int launch_apply_tc32(int D, int N, int kind, DevOp<float> const& op, Tc32Tiles const& mt, const TX* x, TX* y,
-                      int nrhs, int64_t ld, cudaStream_t s, int ctas = 0);
+                      int nrhs, int64_t ld, cudaStream_t s, int ctas = 0, int passes = 3);
 int launch_bjac_assemble(int D, int N, int kind, DevOp<double> const& op, double* blk,
                          cudaStream_t s);
 template <typename T>

@@ -18,7 +18,7 @@ from . import _ffi
 from .mesh import SimplexMesh
 
 POISSON, ELASTICITY = _ffi.TDG_POISSON, _ffi.TDG_ELASTICITY
-FP64, FP32, MIXED = _ffi.TDG_FP64, _ffi.TDG_FP32, _ffi.TDG_MIXED
+FP64, FP32, MIXED, TF32 = _ffi.TDG_FP64, _ffi.TDG_FP32, _ffi.TDG_MIXED, _ffi.TDG_TF32
 FAMILIES = ("tensor", "simt", "face", "face2", "tc05")
 MG_STRATEGIES = ("twolevel", "logarithmic", "full")  # MGStrategy (app/common/MGConfig.h:8)
 PRECONDITIONERS = ("bjacobi", "mg")
@@ -240,7 +240,8 @@ class DGOperator:
         a block-Jacobi CG coarse solve -- on the coarsest DG level (coarse_space "dg") or on the
         continuous P1 space below it ("p1").  smooth_precision MIXED runs the finest level's
         smoother applies in FP32 arithmetic and the smoothed levels below it on FP32 copies of
-        their blocks (FP64 vectors and accumulation)."""
+        their blocks (FP64 vectors and accumulation); TF32 runs those smoother applies in one TF32
+        tensor-core pass instead of three."""
         o = _ffi.MgOpts(MG_STRATEGIES.index(strategy), coarse_degree, smooth_its, esteig[0], esteig[1],
                         esteig_steps, coarse_rtol, coarse_max_it, smooth_precision,
                         MG_COARSE_SPACES.index(coarse_space))
