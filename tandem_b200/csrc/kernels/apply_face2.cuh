@@ -384,9 +384,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
     const int64_t ntiles = (op.E + TE - 1) / TE;
     const int64_t nwork = ntiles * nrhs;
     auto stage = [&](int64_t work, int buf) {
-        int64_t tile, rhs;
-        work_tile_rhs(work, ntiles, nrhs, tile, rhs);
-        const double* xr = x + rhs * ld;
+        const int64_t tile = work % ntiles;
+        const double* xr = x + (work / ntiles) * ld;
         if (tid < SU::UE) {
             const int64_t e = tile * TE + tid;
             s_el[buf][tid] = (tid < TE && e < op.E) ? static_cast<int>(e) : -1;
@@ -399,9 +398,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
     int buf = 0;
     if (static_cast<int64_t>(blockIdx.x) < nwork) stage(blockIdx.x, 0);
     for (int64_t work = blockIdx.x; work < nwork; work += gridDim.x, buf ^= 1) {
-        int64_t tile, rhs;
-        work_tile_rhs(work, ntiles, nrhs, tile, rhs);
-        double* yr = y + rhs * ld;
+        const int64_t tile = work % ntiles;
+        double* yr = y + (work / ntiles) * ld;
         const int64_t next = work + gridDim.x;
         __syncthreads();  // the previous tile is done with the other buffer
         if (next < nwork) {
@@ -577,17 +575,13 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     const int64_t per = (nwork + gridDim.x - 1) / gridDim.x;
     const int64_t w0 = static_cast<int64_t>(blockIdx.x) * per;
     const int64_t w1 = (w0 + per < nwork) ? w0 + per : nwork;
-    auto ids_async = [&](int64_t work, int slot) {  // the descriptor and ids of work item `work`'s tile
-        int64_t t64, rhs;
-        work_tile_rhs(work, ft.nftiles, nrhs, t64, rhs);
-        const int tile = static_cast<int>(t64);
+    auto ids_async = [&](int64_t work, int slot) {  // the descriptor and ids of tile `work`
+        const int tile = static_cast<int>(work % ft.nftiles);
         if (tid < TE) cp_async16(&s_ids[slot][tid], &ft.tids[static_cast<int64_t>(tile) * TE + tid]);
         if (tid == TE) cp_async16(&s_td[slot], &ft.ftiles[tile]);
     };
     auto stage = [&](int64_t work, int slot, int buf) {  // every thread; ids of `slot` visible
-        int64_t t64, rhs;
-        work_tile_rhs(work, ft.nftiles, nrhs, t64, rhs);
-        const double* xr = x + rhs * ld;
+        const double* xr = x + (work / ft.nftiles) * ld;
         const int4* ids = s_ids[slot];
         using SUT = Staged<S>;
         constexpr int per_el = Q * NBF;
@@ -621,10 +615,8 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     cp_async_commit();
     int buf = 0, slot = 0;
     for (int64_t work = w0; work < w1; ++work, buf ^= 1, slot = (slot == 2 ? 0 : slot + 1)) {
-        int64_t t64, rhs;
-        work_tile_rhs(work, ft.nftiles, nrhs, t64, rhs);
-        const int tile = static_cast<int>(t64);
-        double* yr = y + rhs * ld;
+        const int tile = static_cast<int>(work % ft.nftiles);
+        double* yr = y + (work / ft.nftiles) * ld;
         // own copies of this tile (and the next tiles' ids) landed; after the barrier everybody's
         // have, and the previous tile is done with R, the tables, the other buffer and its ids
         cp_async_wait<0>();

@@ -25,8 +25,30 @@ __host__ __device__ constexpr int cbinom(int n, int k) {
 // item = tile.
 constexpr int kRhsGroup = 8;
 __device__ __forceinline__ void work_tile_rhs(int64_t work, int64_t ntiles, int nrhs, int64_t& tile, int64_t& rhs) {
+    // the kernels that call this per tile are issue-bound: one right-hand side needs no division,
+    // and 32-bit division serves every item count below 2^32
+    if (nrhs == 1) {
+        tile = work;
+        rhs = 0;
+        return;
+    }
     const int64_t full = nrhs / kRhsGroup;  // complete groups
     const int64_t per = ntiles * kRhsGroup;
+    if (static_cast<uint64_t>(ntiles) * static_cast<uint64_t>(nrhs) <= 0xffffffffull) {
+        const uint32_t w32 = static_cast<uint32_t>(work), per32 = static_cast<uint32_t>(per);
+        const uint32_t full32 = static_cast<uint32_t>(full);
+        if (w32 < full32 * per32) {
+            const uint32_t grp = w32 / per32, w = w32 - grp * per32;
+            tile = w / kRhsGroup;
+            rhs = static_cast<int64_t>(grp) * kRhsGroup + (w % kRhsGroup);
+        } else {
+            const uint32_t w = w32 - full32 * per32, rest = static_cast<uint32_t>(nrhs) - full32 * kRhsGroup;
+            const uint32_t t = w / rest;
+            tile = t;
+            rhs = static_cast<int64_t>(full32) * kRhsGroup + (w - t * rest);
+        }
+        return;
+    }
     if (work < full * per) {
         const int64_t grp = work / per, w = work - grp * per;
         tile = w / kRhsGroup;
