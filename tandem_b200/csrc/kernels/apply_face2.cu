@@ -21,7 +21,7 @@ int configure2(K kern, size_t smem, int threads, int& per_sm) {
     return 0;
 }
 
-template <class S>
+template <class S, bool ONE>
 int run_face2(DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, TileGeo const& tg, const double* x,
               double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas, int qc) {
     using L = MmaTile<S>;
@@ -36,13 +36,13 @@ int run_face2(DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, 
     const Face2Layout<S> fl = face2_layout<S>(op.nq, gpre);
     const size_t vsmem = sizeof(double) * static_cast<size_t>(vl.total);
     const size_t fsmem = sizeof(double) * static_cast<size_t>(fl.total);
-    auto vk = vol2_kernel<S>;
+    auto vk = vol2_kernel<S, ONE>;
     // 3D elasticity: a register-rich facet kernel for one CTA per SM (ctas == 1) besides the
     // two-CTA one
     constexpr bool kTwoVariants = (S::D == 3 && S::Q == 3);
     const bool one = kTwoVariants && ctas == 1;
-    auto fk2 = face2_kernel<S, 2>;
-    auto fk1 = face2_kernel<S, kTwoVariants ? 1 : 2>;
+    auto fk2 = face2_kernel<S, 2, ONE>;
+    auto fk1 = face2_kernel<S, kTwoVariants ? 1 : 2, ONE>;
     auto fk = one ? fk1 : fk2;
     static size_t vconf = 0, fconf2 = 0, fconf1 = 0;  // configured dynamic shared memory (grows)
     static int vper = 1, fper2 = 1, fper1 = 1;
@@ -77,8 +77,12 @@ int run_face2(DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, 
 template <int D, int N>
 int face2_kind(int kind, DevOp<double> const& op, MmaTiles const& mt, FaceTiles const& ft, TileGeo const& tg,
                const double* x, double* y, int nrhs, int64_t ld, cudaStream_t s, int ctas, int qc) {
-    if (kind == kPoisson) return run_face2<Shape<D, N, kPoisson>>(op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
-    return run_face2<Shape<D, N, kElasticity>>(op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
+    // one right-hand side: the instances whose work index is the tile itself
+    if (kind == kPoisson)
+        return nrhs == 1 ? run_face2<Shape<D, N, kPoisson>, true>(op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc)
+                         : run_face2<Shape<D, N, kPoisson>, false>(op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
+    return nrhs == 1 ? run_face2<Shape<D, N, kElasticity>, true>(op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc)
+                     : run_face2<Shape<D, N, kElasticity>, false>(op, mt, ft, tg, x, y, nrhs, ld, s, ctas, qc);
 }
 
 template <int D>

@@ -294,6 +294,25 @@ __device__ __forceinline__ void stage_blocks(const double* __restrict__ xr, cons
     }
 }
 
+// (tile, right-hand side) of work item `work` in the per-RHS sweep order (the tile fastest).  The
+// kernels call this several times per tile and are issue-bound, so one right-hand side needs no
+// division (the kernels' ONE instances, launched for nrhs = 1, fold it away) and 32-bit division
+// serves every item count below 2^32.
+__device__ __forceinline__ void sweep_tile_rhs(int64_t work, int64_t ntiles, int nrhs, int64_t& tile, int64_t& rhs) {
+    if (nrhs == 1) {
+        tile = work;
+        rhs = 0;
+    } else if (static_cast<uint64_t>(ntiles) * static_cast<uint64_t>(nrhs) <= 0xffffffffull) {
+        const uint32_t w = static_cast<uint32_t>(work), n = static_cast<uint32_t>(ntiles);
+        const uint32_t r = w / n;
+        rhs = r;
+        tile = w - r * n;
+    } else {
+        rhs = work / ntiles;
+        tile = work - rhs * ntiles;
+    }
+}
+
 // ---- tile-ordered geometry ------------------------------------------------------------------------
 
 // Volume data per element tile, [tile][field][q][te] with fields J^-1 (DD) then the coefficients
@@ -359,7 +378,7 @@ __host__ inline Vol2Layout<S> vol2_layout_auto(int Nq) {
     return full.total * sizeof(double) <= 112 * 1024 ? full : vol2_layout<S>(Nq, MmaTile<S>::QC);
 }
 
-template <class S>
+template <class S, bool ONE = false>
 __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
     vol2_kernel(DevOp<double> op, TileGeo tg, const double* __restrict__ tv, const double* __restrict__ x,
                 double* __restrict__ y, int64_t ld, int nrhs, int qc) {
@@ -384,8 +403,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
     const int64_t ntiles = (op.E + TE - 1) / TE;
     const int64_t nwork = ntiles * nrhs;
     auto stage = [&](int64_t work, int buf) {
-        const int64_t tile = work % ntiles;
-        const double* xr = x + (work / ntiles) * ld;
+        int64_t tile, rhs;
+        sweep_tile_rhs(work, ntiles, ONE ? 1 : nrhs, tile, rhs);
+        const double* xr = x + rhs * ld;
         if (tid < SU::UE) {
             const int64_t e = tile * TE + tid;
             s_el[buf][tid] = (tid < TE && e < op.E) ? static_cast<int>(e) : -1;
@@ -398,8 +418,9 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, 2)
     int buf = 0;
     if (static_cast<int64_t>(blockIdx.x) < nwork) stage(blockIdx.x, 0);
     for (int64_t work = blockIdx.x; work < nwork; work += gridDim.x, buf ^= 1) {
-        const int64_t tile = work % ntiles;
-        double* yr = y + (work / ntiles) * ld;
+        int64_t tile, rhs;
+        sweep_tile_rhs(work, ntiles, ONE ? 1 : nrhs, tile, rhs);
+        double* yr = y + rhs * ld;
         const int64_t next = work + gridDim.x;
         __syncthreads();  // the previous tile is done with the other buffer
         if (next < nwork) {
@@ -538,7 +559,7 @@ __host__ __device__ inline Face2Layout<S> face2_layout(int nq, int gpre = 0) {
     return l;
 }
 
-template <class S, int MINB>
+template <class S, int MINB, bool ONE = false>
 __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     face2_kernel(DevOp<double> op, FaceTiles ft, TileGeo tg, const double* __restrict__ x, double* __restrict__ y,
                  int64_t ld, int nrhs, int gpre) {
@@ -576,12 +597,16 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     const int64_t w0 = static_cast<int64_t>(blockIdx.x) * per;
     const int64_t w1 = (w0 + per < nwork) ? w0 + per : nwork;
     auto ids_async = [&](int64_t work, int slot) {  // the descriptor and ids of tile `work`
-        const int tile = static_cast<int>(work % ft.nftiles);
+        int64_t t64, rhs;
+        sweep_tile_rhs(work, ft.nftiles, ONE ? 1 : nrhs, t64, rhs);
+        const int tile = static_cast<int>(t64);
         if (tid < TE) cp_async16(&s_ids[slot][tid], &ft.tids[static_cast<int64_t>(tile) * TE + tid]);
         if (tid == TE) cp_async16(&s_td[slot], &ft.ftiles[tile]);
     };
     auto stage = [&](int64_t work, int slot, int buf) {  // every thread; ids of `slot` visible
-        const double* xr = x + (work / ft.nftiles) * ld;
+        int64_t t64, rhs;
+        sweep_tile_rhs(work, ft.nftiles, ONE ? 1 : nrhs, t64, rhs);
+        const double* xr = x + rhs * ld;
         const int4* ids = s_ids[slot];
         using SUT = Staged<S>;
         constexpr int per_el = Q * NBF;
@@ -615,8 +640,10 @@ __global__ void __launch_bounds__(MmaTile<S>::NT, MINB)
     cp_async_commit();
     int buf = 0, slot = 0;
     for (int64_t work = w0; work < w1; ++work, buf ^= 1, slot = (slot == 2 ? 0 : slot + 1)) {
-        const int tile = static_cast<int>(work % ft.nftiles);
-        double* yr = y + (work / ft.nftiles) * ld;
+        int64_t t64, rhs;
+        sweep_tile_rhs(work, ft.nftiles, ONE ? 1 : nrhs, t64, rhs);
+        const int tile = static_cast<int>(t64);
+        double* yr = y + rhs * ld;
         // own copies of this tile (and the next tiles' ids) landed; after the barrier everybody's
         // have, and the previous tile is done with R, the tables, the other buffer and its ids
         cp_async_wait<0>();
