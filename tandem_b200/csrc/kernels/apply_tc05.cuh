@@ -433,6 +433,11 @@ __device__ __forceinline__ void tc05_store_y(uint32_t tmem, uint32_t lane_base, 
 
 // One tile at a time, every phase by the whole CTA (256 threads): stage, forward, pointwise
 // (warps owning lanes 0..63), backward, store.  tv: the FP32 volume table, row (q D + a), ld ldt.
+// Element tile and right-hand side of work item w (the tile fastest); one right-hand side needs no
+// division.
+__device__ __forceinline__ int64_t t5_tile(int64_t w, int64_t ntiles, int nrhs) { return nrhs == 1 ? w : w % ntiles; }
+__device__ __forceinline__ int64_t t5_rhs(int64_t w, int64_t ntiles, int nrhs) { return nrhs == 1 ? 0 : w / ntiles; }
+
 template <class S, typename TX, int NP = 3>
 __global__ void __launch_bounds__(256, 1)
     vol_tc05_kernel(DevOp<float> op, const float* __restrict__ tv, int ldt, const TX* __restrict__ x,
@@ -463,9 +468,9 @@ __global__ void __launch_bounds__(256, 1)
     unsigned phase = 0;
     bool ok = true;
     for (int64_t work = blockIdx.x; work < nwork && ok; work += gridDim.x) {
-        const int64_t e0 = static_cast<int64_t>(work % ntiles) * TE;
-        const TX* xr = x + (work / ntiles) * ld;
-        TX* yr = y + (work / ntiles) * ld;
+        const int64_t e0 = t5_tile(work, ntiles, nrhs) * TE;
+        const TX* xr = x + t5_rhs(work, ntiles, nrhs) * ld;
+        TX* yr = y + t5_rhs(work, ntiles, nrhs) * ld;
         tc05_stage<S, TX>(b, xr, e0, op.E, tid, NT);
         fence_async_smem();
         tc05_fence_before();
@@ -590,7 +595,7 @@ __global__ void __launch_bounds__(512, 1)
             if (i > 0) ok = __all_sync(mask, mbar_wait_bounded(&barF, static_cast<unsigned>((i - 1) & 1)));
             if (!ok) break;
             const int64_t w = work_of(i);
-            tc05_stage<S, TX>(b, x + (w / ntiles) * ld, (w % ntiles) * TE, op.E, t0, 255);
+            tc05_stage<S, TX>(b, x + t5_rhs(w, ntiles, nrhs) * ld, t5_tile(w, ntiles, nrhs) * TE, op.E, t0, 255);
             fence_async_smem();
             mbar_arrive(&barU);
         }
@@ -600,7 +605,7 @@ __global__ void __launch_bounds__(512, 1)
         for (int64_t i = 0; i < nmine && ok; ++i) {
             const unsigned p = static_cast<unsigned>(i & 1);
             const int64_t w = work_of(i);
-            const int64_t e0 = (w % ntiles) * TE;
+            const int64_t e0 = t5_tile(w, ntiles, nrhs) * TE;
             float G[4][DD], c0[4], c1[4];
             tc05_load_geo<S, 4>(op, q, e0, te0, G, c0, c1);  // in flight during the wait
             ok = __all_sync(0xffffffffu, mbar_wait_bounded(&barF, p));
@@ -622,7 +627,8 @@ __global__ void __launch_bounds__(512, 1)
                 if (!ok) break;
                 tc05_fence_after();
                 const int64_t wp = work_of(i - 1);
-                tc05_store_y4<S, TX>(tmem, lane_base, q, te0, (wp % ntiles) * TE, op.E, y + (wp / ntiles) * ld);
+                tc05_store_y4<S, TX>(tmem, lane_base, q, te0, t5_tile(wp, ntiles, nrhs) * TE, op.E,
+                                     y + t5_rhs(wp, ntiles, nrhs) * ld);
                 tc05_fence_before();
             }
             tc05_write_s<S, 4>(b, q, te0, T);
@@ -634,7 +640,8 @@ __global__ void __launch_bounds__(512, 1)
             if (ok) {
                 tc05_fence_after();
                 const int64_t wp = work_of(nmine - 1);
-                tc05_store_y4<S, TX>(tmem, lane_base, q, te0, (wp % ntiles) * TE, op.E, y + (wp / ntiles) * ld);
+                tc05_store_y4<S, TX>(tmem, lane_base, q, te0, t5_tile(wp, ntiles, nrhs) * TE, op.E,
+                                     y + t5_rhs(wp, ntiles, nrhs) * ld);
             }
         }
     }
