@@ -92,3 +92,19 @@ def test_coarse_solve_device_loop():
     assert c2 - c1 == c1 - c0, (c0, c1, c2)
     assert torch.equal(z0, z1)
     assert torch.isfinite(z0).all() and z0.abs().max() > 0
+
+
+@pytest.mark.parametrize("limit", [50, 77])
+def test_device_loop_stops_at_the_iteration_limit(limit):
+    """A device-looped block never runs past max_iterations: the graph block's limit is the
+    remaining count, so a solve that cannot converge in time stops at exactly the limit."""
+    _, op, _ = product_and_oracle(ELASTICITY, 2, 5, 3, True, True)
+    _, _, _, f, g = mms_inputs(op, ELASTICITY, 2, True)
+    b = op.rhs(f, g)
+    op.bjacobi_setup(FP64)
+    x = torch.zeros(op.ndof, dtype=torch.float64, device=DEV)
+    st = op.solve(dev(b), x, precision=FP64, rtol=1e-14, max_iterations=limit, use_graphs=True,
+                  stream=torch.cuda.Stream(), check=False)
+    torch.cuda.synchronize()
+    assert st["iterations"] == limit and not st["converged"], st
+    assert np.isfinite(st["rel_residual"]) and st["rel_residual"] < 1.0, st
