@@ -195,7 +195,7 @@ typedef struct {
  * entries (optional, up to max_entries) receives every measurement; n_entries their count. */
 int tdg_autotune(tdg_op* op, int precision, int nrhs, void* stream, tdg_tune_entry* entries, int max_entries,
                  int* n_entries);
-/* Sets the apply configuration of `precision` (TDG_FP64 / TDG_FP32; TDG_MIXED follows TDG_FP32)
+/* Sets the apply configuration of `precision` (TDG_FP64 / TDG_FP32; TDG_MIXED and TDG_TF32 follow TDG_FP32)
  * explicitly: kernel family as in tdg_tune_entry and persistent CTAs per SM. */
 int tdg_set_apply_config(tdg_op* op, int precision, int family, int ctas_per_sm);
 /* Sets the tile height of family 3 (TDG_FP64 only): volume points per pass of its volume kernel, as
